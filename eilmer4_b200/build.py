@@ -1,0 +1,78 @@
+"""Build libe4cuda.so in-tree with nvcc for sm_100a (no GPU needed to compile).
+
+Usage: python -m eilmer4_b200.build [--force] [--verbose]
+
+Each translation unit is compiled with its own floating-point contract:
+the FP64 parity kernels with -fmad=false (every multiply and add rounded on
+its own, as in the reference), the FP32 flux kernels with contraction allowed.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libe4cuda.so")
+ROOT = os.path.dirname(HERE)
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+# (source, extra flags)
+UNITS = [
+    ("e4c_general.cu", ["-fmad=false"]),
+    ("e4c_fused.cu", ["-fmad=false"]),
+    ("e4c_fused32.cu", ["-fmad=true"]),
+    ("e4c_blocks.cu", ["-fmad=false"]),
+    ("e4c_api.cu", ["-fmad=false"]),
+]
+
+HEADERS = ["e4c_physics.cuh", "e4c_types.h", "e4c_kernels.h", "e4c_internal.h"]
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.isabs(c) and os.path.exists(c) or not os.path.isabs(c)):
+            return c
+    return "nvcc"
+
+
+def _mtime(p):
+    return os.path.getmtime(p) if os.path.exists(p) else -1.0
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    hdr_time = max(_mtime(os.path.join(CSRC, h)) for h in HEADERS)
+    hdr_time = max(hdr_time, _mtime(os.path.join(ROOT, "include", "e4cuda.h")))
+    objs = []
+    rebuilt = False
+    for src, flags in UNITS:
+        sp = os.path.join(CSRC, src)
+        if not os.path.exists(sp):
+            continue
+        op = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(op)
+        if force or _mtime(op) < max(_mtime(sp), hdr_time):
+            cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", sp, "-o", op]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            rebuilt = True
+    if force or rebuilt or _mtime(LIB) < max(_mtime(o) for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl",
+               "-lpthread"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    print(LIB)

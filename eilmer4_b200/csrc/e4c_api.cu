@@ -1,0 +1,460 @@
+// e4c_api.cu -- the extern "C" ABI of libe4cuda (declared in include/e4cuda.h).
+//
+// Host side of the library: one context, block storage, the device-side time
+// loop of integrate_in_time (src/eilmer/simcore.d:791-1110) recorded as CUDA
+// graphs, and the error conventions of src/gas/gas_cwrap.d (int handles,
+// 0 / negative return codes, never throwing across the ABI).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/e4cuda.h"
+#include "e4c_internal.h"
+#include "e4c_kernels.h"
+
+namespace e4c {
+
+Ctx g_ctx;
+
+int fail(int code, const std::string& msg) {
+    g_ctx.last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return fail(E4C_ERR_CUDA, m);
+}
+
+#define E4C_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+void* Ctx::dalloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    allocations.push_back(p);
+    return p;
+}
+
+void Ctx::reset_graphs() {
+    for (auto& gx : graphs) {
+        if (gx.exec) cudaGraphExecDestroy(gx.exec);
+        gx.exec = nullptr;
+    }
+}
+
+void Ctx::release() {
+    reset_graphs();
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* p : allocations) cudaFree(p);
+    allocations.clear();
+    if (host_pinned) cudaFreeHost(host_pinned);
+    host_pinned = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    blocks.clear();
+    initialised = false;
+}
+
+void Profiler::begin(cudaStream_t s, int c) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+    ev.push_back(a);
+    ev.push_back(b);
+    cls.push_back(c);
+}
+
+void Profiler::end(cudaStream_t s) { cudaEventRecord(ev.back(), s); }
+
+// Every kernel launch goes through this bracket: it counts the launch and,
+// while profiling, times it by class with events on the library stream.
+template <typename F>
+static inline void launch_as(Ctx& c, int cls, int nkernels, F&& f) {
+    c.launches += nkernels;
+    if (c.prof.on) c.prof.begin(c.stream, cls);
+    f();
+    if (c.prof.on) c.prof.end(c.stream);
+}
+
+// One stage over the given blocks (simcore.d:2325-2493 / 2529-2730).
+void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) {
+    launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_reset_bad(d_sim, stream); });
+    for (int h : hs) {
+        const BlockHost& b = blocks[h];
+        if (b.fused) launch_as(*this, E4C_KCLASS_STAGE, 1, [&] { fused_stage(b, stage, final_stage); });
+        else launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc(b.v, d_sim, stream); });
+    }
+    for (int h : hs) {
+        const BlockHost& b = blocks[h];
+        if (b.fused) continue;
+        for (int d = 0; d < b.v.dim; ++d)
+            launch_as(*this, E4C_KCLASS_FLUX, 1, [&] { launch_flux(b.v, d_sim, fopts, d, stream); });
+    }
+    for (int h : hs) {
+        const BlockHost& b = blocks[h];
+        if (b.fused) continue;
+        launch_as(*this, E4C_KCLASS_UPDATE, 1,
+                  [&] { launch_update(b.v, d_sim, gas, stage, final_stage, stream); });
+    }
+    launch_as(*this, E4C_KCLASS_OTHER, 1,
+              [&] { launch_stage_check(d_sim, cfg.max_invalid_cells, stream); });
+}
+
+void Ctx::enqueue_gasdynamic(const std::vector<int>& hs) {
+    const int nstages = (cfg.gasdynamic_update_scheme == E4C_UPDATE_PC) ? 2 : 1;
+    for (int s = 1; s <= nstages; ++s) enqueue_stage(hs, s, s == nstages);
+    launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_end_step(d_sim, stream); });
+}
+
+void Ctx::enqueue_dt(const std::vector<int>& hs, const double* dt_current, int check_cfl,
+                     int step0, SimDev* sim, double* out) {
+    launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_dt_reset(d_dtacc, int(hs.size()), stream); });
+    for (size_t q = 0; q < hs.size(); ++q) {
+        const BlockHost& b = blocks[hs[q]];
+        if (b.fused)
+            launch_as(*this, E4C_KCLASS_DT, 1, [&] { fused_dt(b, sim, dt_current, d_dtacc + 3 * q); });
+        else
+            launch_as(*this, E4C_KCLASS_DT, 1, [&] {
+                launch_dt(b.v, sim, cfg.cfl_value, dt_current, d_dtacc + 3 * q, stream);
+            });
+    }
+    const double cfl_allow = (cfg.gasdynamic_update_scheme == E4C_UPDATE_PC) ? 1.2 : 0.9;
+    launch_as(*this, E4C_KCLASS_OTHER, 1, [&] {
+        launch_dt_finalize(sim, d_dtacc, int(hs.size()), cfl_allow, cfg.dt_init, cfg.dt_max,
+                           check_cfl, step0, out, out ? out + 1 : nullptr, stream);
+    });
+}
+
+std::vector<int> Ctx::all_blocks() const {
+    std::vector<int> hs(blocks.size());
+    for (size_t q = 0; q < blocks.size(); ++q) hs[q] = int(q);
+    return hs;
+}
+
+}  // namespace e4c
+
+using namespace e4c;
+
+extern "C" {
+
+int e4c_config_default(e4c_config* c) {
+    if (!c) return fail(E4C_ERR_ARG, "e4c_config_default: null config");
+    std::memset(c, 0, sizeof(*c));
+    c->dimensions = 2;
+    c->flux_calculator = E4C_FLUX_AUSMDV;
+    c->interpolation_order = 2;
+    c->apply_limiter = 1;
+    c->extrema_clipping = 1;
+    c->interpolate_in_local_frame = 1;
+    c->gasdynamic_update_scheme = E4C_UPDATE_PC;
+    c->cfl_value = 0.5;
+    c->dt_init = 1.0e-3;
+    c->dt_max = 1.0e-3;
+    c->cfl_count = 10;
+    c->max_invalid_cells = 0;
+    c->gas_model = E4C_GAS_IDEAL;
+    c->ideal_mol_mass = 0.02896;
+    c->ideal_gamma = 1.4;
+    c->reacting = 0;
+    c->T_frozen = 300.0;
+    c->precision = E4C_PREC_FP64;
+    c->device = 0;
+    c->use_graphs = 1;
+    return E4C_OK;
+}
+
+int e4c_init(const e4c_config* cfg) {
+    if (!cfg) return fail(E4C_ERR_ARG, "e4c_init: null config");
+    if (g_ctx.initialised) g_ctx.release();
+    if (cfg->dimensions != 2 && cfg->dimensions != 3)
+        return fail(E4C_ERR_UNSUPPORTED, "dimensions must be 2 or 3");
+    if (cfg->flux_calculator != E4C_FLUX_AUSMDV && cfg->flux_calculator != E4C_FLUX_HLLC)
+        return fail(E4C_ERR_UNSUPPORTED, "flux_calculator must be ausmdv or hllc");
+    if (cfg->interpolation_order != 1 && cfg->interpolation_order != 2)
+        return fail(E4C_ERR_UNSUPPORTED, "interpolation_order must be 1 or 2");
+    if (cfg->gasdynamic_update_scheme != E4C_UPDATE_EULER &&
+        cfg->gasdynamic_update_scheme != E4C_UPDATE_PC)
+        return fail(E4C_ERR_UNSUPPORTED, "gasdynamic_update_scheme must be euler or predictor-corrector");
+    if (cfg->gas_model != E4C_GAS_IDEAL)
+        return fail(E4C_ERR_UNSUPPORTED, "gas model not available in this build");
+    if (cfg->precision != E4C_PREC_FP64)
+        return fail(E4C_ERR_UNSUPPORTED, "precision not available in this build");
+    if (cfg->reacting) return fail(E4C_ERR_UNSUPPORTED, "reacting flow not available in this build");
+    if (cfg->cfl_count < 1) return fail(E4C_ERR_ARG, "cfl_count must be >= 1");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(E4C_ERR_CUDA, "no CUDA device available");
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(E4C_ERR_ARG, "bad device ordinal");
+    E4C_CUDA(cudaSetDevice(cfg->device));
+    Ctx& c = g_ctx;
+    c.cfg = *cfg;
+    c.gas.Rgas = 8.31451 / cfg->ideal_mol_mass;  // ideal_gas.d:66-69
+    c.gas.gamma = cfg->ideal_gamma;
+    c.gas.Cv = c.gas.Rgas / (c.gas.gamma - 1.0);
+    c.gas.Cvinv = 1.0 / c.gas.Cv;
+    c.gas.Cp = c.gas.Rgas * c.gas.gamma / (c.gas.gamma - 1.0);
+    c.fopts.flux = cfg->flux_calculator;
+    c.fopts.order2 = cfg->interpolation_order > 1;
+    c.fopts.limiter = cfg->apply_limiter != 0;
+    c.fopts.clip = cfg->extrema_clipping != 0;
+    c.fopts.local_frame = cfg->interpolate_in_local_frame != 0;
+    c.fopts.gas = c.gas;
+    E4C_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.d_sim = static_cast<SimDev*>(c.dalloc(sizeof(SimDev) + 64));
+    c.d_dtacc = nullptr;
+    c.dtacc_cap = 0;
+    c.d_scalars = static_cast<double*>(c.dalloc(8 * sizeof(double)));
+    if (!c.d_sim || !c.d_scalars) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    E4C_CUDA(cudaMallocHost(&c.host_pinned, 4096));
+    SimDev s0{};
+    s0.dt_global = cfg->dt_init;  // simcore.d:562
+    s0.max_time = 1.0e300;
+    E4C_CUDA(cudaMemcpyAsync(c.d_sim, &s0, sizeof(SimDev), cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    c.host_step = 0;
+    c.initialised = true;
+    return E4C_OK;
+}
+
+int e4c_finalize(void) {
+    if (g_ctx.initialised) g_ctx.release();
+    return E4C_OK;
+}
+
+int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* bc_type,
+                     const double* inflow_prim) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "e4c_block_create before e4c_init");
+    if (!vtx_xyz || !bc_type || !inflow_prim) return fail(E4C_ERR_ARG, "null pointer");
+    const int dim = c.cfg.dimensions;
+    if (dim == 2) nk = 1;
+    if (ni < 2 || nj < 2 || (dim == 3 && nk < 2))
+        return fail(E4C_ERR_ARG, "a block needs at least 2 cells in each active direction");
+    for (int q = 0; q < 6; ++q)
+        if (bc_type[q] < 0 || bc_type[q] > 2) return fail(E4C_ERR_UNSUPPORTED, "unknown boundary type");
+    BlockHost b;
+    int rc = c.build_block(ni, nj, nk, vtx_xyz, bc_type, inflow_prim, b);
+    if (rc != E4C_OK) return rc;
+    c.blocks.push_back(b);
+    c.blocks.back().v.block_id = int(c.blocks.size()) - 1;
+    c.reset_graphs();
+    return int(c.blocks.size()) - 1;
+}
+
+int e4c_block_upload(int h, const double* prim) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size()) || !prim) return fail(E4C_ERR_ARG, "bad handle or pointer");
+    BlockHost& b = c.blocks[h];
+    size_t bytes = b.nprim_vars * b.ncell * sizeof(double);
+    E4C_CUDA(cudaMemcpyAsync(c.d_staging, prim, bytes, cudaMemcpyHostToDevice, c.stream));
+    if (b.fused) c.fused_upload(b, c.d_staging);
+    else launch_upload(b.v, c.d_staging, c.stream);
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    return E4C_OK;
+}
+
+int e4c_block_download(int h, double* prim, double* cons) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad handle");
+    BlockHost& b = c.blocks[h];
+    double* dp = c.d_staging;
+    double* dc = c.d_staging + b.nprim_vars * b.ncell;
+    if (b.fused) c.fused_download(b, prim ? dp : nullptr, cons ? dc : nullptr);
+    else launch_download(b.v, prim ? dp : nullptr, cons ? dc : nullptr, c.stream);
+    E4C_CUDA(cudaGetLastError());
+    if (prim)
+        E4C_CUDA(cudaMemcpyAsync(prim, dp, b.nprim_vars * b.ncell * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c.stream));
+    if (cons)
+        E4C_CUDA(cudaMemcpyAsync(cons, dc, b.v.nv * b.ncell * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    return E4C_OK;
+}
+
+static int check_handles(const int* h, int nb, std::vector<int>& hs) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!h || nb <= 0) return fail(E4C_ERR_ARG, "no blocks given");
+    hs.assign(h, h + nb);
+    for (int x : hs)
+        if (x < 0 || x >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad block handle");
+    return c.ensure_dtacc(nb);
+}
+
+int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double* dt_allow,
+                 double* cfl_max) {
+    std::vector<int> hs;
+    int rc = check_handles(h, nb, hs);
+    if (rc != E4C_OK) return rc;
+    if (!dt_allow || !cfl_max) return fail(E4C_ERR_ARG, "null output");
+    Ctx& c = g_ctx;
+    double* hp = static_cast<double*>(c.host_pinned);
+    hp[0] = dt_current;
+    E4C_CUDA(cudaMemcpyAsync(c.d_scalars, hp, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    c.enqueue_dt(hs, c.d_scalars, check_cfl ? 1 : 0, 0, nullptr, c.d_scalars + 2);
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaMemcpyAsync(hp + 2, c.d_scalars + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                             c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    *dt_allow = hp[2];
+    *cfl_max = hp[3];
+    return E4C_OK;
+}
+
+static int read_sim(SimDev& s) {
+    Ctx& c = g_ctx;
+    E4C_CUDA(cudaMemcpyAsync(c.host_pinned, c.d_sim, sizeof(SimDev), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    std::memcpy(&s, c.host_pinned, sizeof(SimDev));
+    return E4C_OK;
+}
+
+static int status_error(const SimDev& s) {
+    char msg[160];
+    const char* what = "device error";
+    switch (s.status) {
+        case E4C_ERR_BAD_CELLS: what = "Too many bad cells"; break;
+        case E4C_ERR_BAD_MASS: what = "Bad cell with negative mass"; break;
+        case E4C_ERR_THERMO: what = "Bad cell with failed thermodynamic update"; break;
+        case E4C_ERR_CHEM: what = "chemistry update failed"; break;
+        case E4C_ERR_TIMEOUT: what = "device wait timed out"; break;
+    }
+    std::snprintf(msg, sizeof(msg), "%s at step %d (%d invalid cells)", what, s.status_step,
+                  s.bad_cells);
+    return fail(s.status, msg);
+}
+
+int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
+    std::vector<int> hs;
+    int rc = check_handles(h, nb, hs);
+    if (rc != E4C_OK) return rc;
+    Ctx& c = g_ctx;
+    // The host owns dt: write it as SimState.dt_global, clear a stale finish flag.
+    launch_begin_run(c.d_sim, 1.0e300, c.stream);
+    double* hp = static_cast<double*>(c.host_pinned);
+    hp[8] = dt;
+    E4C_CUDA(cudaMemcpyAsync(&c.d_sim->dt_global, hp + 8, sizeof(double), cudaMemcpyHostToDevice,
+                             c.stream));
+    c.enqueue_gasdynamic(hs);
+    E4C_CUDA(cudaGetLastError());
+    SimDev s;
+    rc = read_sim(s);
+    if (rc != E4C_OK) return rc;
+    if (bad_cells) *bad_cells = s.bad_cells;
+    if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
+int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
+    if (nsteps < 0) return fail(E4C_ERR_ARG, "negative step count");
+    std::vector<int> hs = c.all_blocks();
+    int rc = c.ensure_dtacc(int(hs.size()));
+    if (rc != E4C_OK) return rc;
+    SimDev s0;
+    rc = read_sim(s0);
+    if (rc != E4C_OK) return rc;
+    launch_begin_run(c.d_sim, max_time, c.stream);
+    const int step_start = s0.step;
+    for (int q = 0; q < nsteps; ++q) {
+        const int step = step_start + q;
+        const bool dt_check = (step % c.cfg.cfl_count) == 0;  // simcore.d:1350-1352
+        rc = c.run_step(hs, dt_check);
+        if (rc != E4C_OK) return rc;
+    }
+    E4C_CUDA(cudaGetLastError());
+    SimDev s;
+    rc = read_sim(s);
+    if (rc != E4C_OK) return rc;
+    if (info) {
+        info->steps_taken = s.step - step_start;
+        info->time = s.time;
+        info->dt_global = s.dt_global;
+        info->status = s.status;
+        info->status_step = s.status_step;
+        info->bad_cells = s.bad_cells;
+    }
+    if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
+int e4c_sim_state(double* time, double* dt_global, int* step) {
+    if (!g_ctx.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    SimDev s;
+    int rc = read_sim(s);
+    if (rc != E4C_OK) return rc;
+    if (time) *time = s.time;
+    if (dt_global) *dt_global = s.dt_global;
+    if (step) *step = s.step;
+    return E4C_OK;
+}
+
+int e4c_synchronize(void) {
+    if (!g_ctx.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    E4C_CUDA(cudaStreamSynchronize(g_ctx.stream));
+    return E4C_OK;
+}
+
+void* e4c_stream(void) { return g_ctx.initialised ? static_cast<void*>(g_ctx.stream) : nullptr; }
+
+long long e4c_kernel_launches(void) { return g_ctx.launches; }
+
+int e4c_profile_steps(int nsteps, double* ms, int* launches) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
+    if (!ms || !launches || nsteps < 0) return fail(E4C_ERR_ARG, "bad arguments");
+    std::vector<int> hs = c.all_blocks();
+    int rc = c.ensure_dtacc(int(hs.size()));
+    if (rc != E4C_OK) return rc;
+    SimDev s0;
+    rc = read_sim(s0);
+    if (rc != E4C_OK) return rc;
+    launch_begin_run(c.d_sim, 1.0e300, c.stream);
+    c.prof.on = true;
+    for (int q = 0; q < nsteps; ++q) {
+        const bool dt_check = ((s0.step + q) % c.cfg.cfl_count) == 0;
+        if (dt_check) c.enqueue_dt(hs, &c.d_sim->dt_global, -1, -1, c.d_sim, nullptr);
+        c.enqueue_gasdynamic(hs);
+    }
+    c.prof.on = false;
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    for (int k = 0; k < E4C_NKCLASS; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    for (size_t q = 0; q < c.prof.cls.size(); ++q) {
+        float t = 0.0f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&t, c.prof.ev[2 * q], c.prof.ev[2 * q + 1]);
+        ms[c.prof.cls[q]] += t;
+        launches[c.prof.cls[q]] += 1;
+    }
+    for (cudaEvent_t x : c.prof.ev) cudaEventDestroy(x);
+    c.prof.ev.clear();
+    c.prof.cls.clear();
+    if (e != cudaSuccess) return cuda_fail(e, "profiled steps");
+    SimDev s;
+    rc = read_sim(s);
+    if (rc != E4C_OK) return rc;
+    if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
+int e4c_last_error(char* buf, int len) {
+    if (!buf || len <= 0) return E4C_ERR_ARG;
+    std::strncpy(buf, g_ctx.last_error.c_str(), size_t(len) - 1);
+    buf[len - 1] = '\0';
+    return E4C_OK;
+}
+
+}  // extern "C"

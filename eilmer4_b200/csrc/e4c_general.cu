@@ -1,0 +1,781 @@
+// e4c_general.cu -- FP64 kernels of the general-geometry path.
+//
+// Compiled with -fmad=false: every multiply and add is rounded on its own,
+// as in the reference's D code, so the results match the reference algorithm
+// bit for bit (tests compare against the FP64 CPU oracle with ==).
+//
+// One face flux per thread (per direction), one cell update per thread.
+// Works for any structured grid, including curvilinear 2-D grids; the uniform
+// Cartesian 3-D case has its own fused kernel in e4c_fused.cu.
+#include <cfloat>
+
+#include "e4c_kernels.h"
+#include "e4c_physics.cuh"
+
+namespace e4c {
+
+__device__ __forceinline__ size_t pidx(const BlockView& b, int i, int j, int k) {
+    return (size_t(k) * b.njdim + j) * b.nidim + i;
+}
+
+__device__ __forceinline__ void set_status(SimDev* sim, int code) {
+    if (atomicCAS(&sim->status, 0, code) == 0) sim->status_step = sim->step;
+}
+
+// ---------------------------------------------------------------------------
+// Geometry (src/geom/elements/properties.d, src/eilmer/fvinterface.d:265-317)
+// ---------------------------------------------------------------------------
+struct Vd {
+    double x, y, z;
+};
+__device__ __forceinline__ Vd vload(const double* v, const BlockView& b, int i, int j, int k) {
+    // vertex of padded indices (i,j,k); the array is unpadded, i fastest
+    const int nvi = b.ni + 1, nvj = b.nj + 1;
+    size_t q = 3 * ((size_t(k - b.kmin) * nvj + (j - b.jmin)) * nvi + (i - b.imin));
+    return {v[q], v[q + 1], v[q + 2]};
+}
+__device__ __forceinline__ void vcross(Vd& v3, const Vd& v1, const Vd& v2) {
+    v3.x = v1.y * v2.z - v2.y * v1.z;  // vector3.d:604-609
+    v3.y = v2.x * v1.z - v1.x * v2.z;
+    v3.z = v1.x * v2.y - v2.x * v1.y;
+}
+__device__ __forceinline__ void vnormalize(Vd& v) {
+    double mag = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);  // vector3.d:386-404
+    if (mag > 0.0) { v.x /= mag; v.y /= mag; v.z /= mag; }
+    else { v.x = v.y = v.z = 0.0; }
+    if (fabs(v.x) < 1.0e-30) v.x = 0.0;
+    if (fabs(v.y) < 1.0e-30) v.y = 0.0;
+    if (fabs(v.z) < 1.0e-30) v.z = 0.0;
+}
+__device__ void quad_props(const Vd& p0, const Vd& p1, const Vd& p2, const Vd& p3, double* out) {
+    // quad_properties, properties.d:97-141
+    double p01x = p1.x - p0.x + p2.x - p3.x;
+    double p01y = p1.y - p0.y + p2.y - p3.y;
+    double p01z = p1.z - p0.z + p2.z - p3.z;
+    double p03x = p3.x - p0.x + p2.x - p1.x;
+    double p03y = p3.y - p0.y + p2.y - p1.y;
+    double p03z = p3.z - p0.z + p2.z - p1.z;
+    double vax = p01y * p03z - p01z * p03y;
+    double vay = p01z * p03x - p01x * p03z;
+    double vaz = p01x * p03y - p01y * p03x;
+    vax *= 0.25; vay *= 0.25; vaz *= 0.25;
+    double area = sqrt(vax * vax + vay * vay + vaz * vaz);
+    Vd n, t1, t2;
+    if (area > 1.0e-20) {
+        n = {vax / area, vay / area, vaz / area};
+        t1 = {p01x, p01y, p01z};
+        vnormalize(t1);
+        vcross(t2, n, t1);
+        vnormalize(t2);
+    } else {
+        n = {1.0, 0.0, 0.0}; t1 = {0.0, 1.0, 0.0}; t2 = {0.0, 0.0, 1.0};
+    }
+    out[0] = n.x; out[1] = n.y; out[2] = n.z;
+    out[3] = t1.x; out[4] = t1.y; out[5] = t1.z;
+    out[6] = t2.x; out[7] = t2.y; out[8] = t2.z;
+    out[9] = area;
+}
+__device__ void face2d_props(const Vd& A, const Vd& B, double* out) {
+    // FVInterface.update_2D_geometric_data, fvinterface.d:265-297 (planar)
+    double LAB = sqrt((B.x - A.x) * (B.x - A.x) + (B.y - A.y) * (B.y - A.y));
+    Vd n, t1, t2;
+    double area;
+    if (LAB > 1.0e-12) {
+        n = {(B.y - A.y) / LAB, -(B.x - A.x) / LAB, 0.0};
+        t2 = {0.0, 0.0, 1.0};
+        vcross(t1, n, t2);
+        area = LAB;
+    } else {
+        n = {1.0, 0.0, 0.0}; t2 = {0.0, 0.0, 1.0}; t1 = {0.0, 1.0, 0.0};
+        area = 0.0;
+    }
+    out[0] = n.x; out[1] = n.y; out[2] = n.z;
+    out[3] = t1.x; out[4] = t1.y; out[5] = t1.z;
+    out[6] = t2.x; out[7] = t2.y; out[8] = t2.z;
+    out[9] = area;
+}
+__device__ double tet_volume(const Vd& p0, const Vd& p1, const Vd& p2, const Vd& p3) {
+    // tetrahedron_volume, properties.d:293-304
+    double dx01 = p1.x - p0.x, dy01 = p1.y - p0.y, dz01 = p1.z - p0.z;
+    double dx02 = p2.x - p0.x, dy02 = p2.y - p0.y, dz02 = p2.z - p0.z;
+    double cx = dy01 * dz02 - dz01 * dy02;
+    double cy = dz01 * dx02 - dx01 * dz02;
+    double cz = dx01 * dy02 - dy01 * dx02;
+    double dx03 = p3.x - p0.x, dy03 = p3.y - p0.y, dz03 = p3.z - p0.z;
+    return (dx03 * cx + dy03 * cy + dz03 * cz) / 6.0;
+}
+__device__ double pyr_volume(const Vd& p0, const Vd& p1, const Vd& p2, const Vd& p3, const Vd& p4) {
+    // pyramid_properties, properties.d:390-419 (volume only)
+    Vd pmB{0.25 * (p0.x + p1.x + p2.x + p3.x), 0.25 * (p0.y + p1.y + p2.y + p3.y),
+           0.25 * (p0.z + p1.z + p2.z + p3.z)};
+    double volume = 0.0;
+    volume += tet_volume(p0, p1, pmB, p4);
+    volume += tet_volume(p1, p2, pmB, p4);
+    volume += tet_volume(p2, p3, pmB, p4);
+    volume += tet_volume(p3, p0, pmB, p4);
+    return volume;
+}
+__device__ Vd mid4(const Vd& a, const Vd& b, const Vd& c, const Vd& d) {
+    return {0.25 * (a.x + b.x + c.x + d.x), 0.25 * (a.y + b.y + c.y + d.y),
+            0.25 * (a.z + b.z + c.z + d.z)};
+}
+
+__global__ void k_geom_cells(BlockView b, const double* vtx) {
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        size_t c = pidx(b, i, j, k);
+        double vol, iL, jL, kL;
+        if (b.dim == 2) {
+            // xyplane_quad_cell_properties, properties.d:177-236
+            Vd p0 = vload(vtx, b, i, j, 0), p1 = vload(vtx, b, i + 1, j, 0);
+            Vd p2 = vload(vtx, b, i + 1, j + 1, 0), p3 = vload(vtx, b, i, j + 1, 0);
+            double xA = p1.x, yA = p1.y, xB = p2.x, yB = p2.y;
+            double xC = p3.x, yC = p3.y, xD = p0.x, yD = p0.y;
+            vol = 0.5 * ((xB + xA) * (yB - yA) + (xC + xB) * (yC - yB) + (xD + xC) * (yD - yC) +
+                         (xA + xD) * (yA - yD));
+            double xN = 0.5 * (xC + xB), yN = 0.5 * (yC + yB);
+            double xS = 0.5 * (xD + xA), yS = 0.5 * (yD + yA);
+            double xE = 0.5 * (xA + xB), yE = 0.5 * (yA + yB);
+            double xW = 0.5 * (xD + xC), yW = 0.5 * (yD + yC);
+            double dx = xN - xS, dy = yN - yS;
+            jL = sqrt(dx * dx + dy * dy);
+            dx = xE - xW; dy = yE - yW;
+            iL = sqrt(dx * dx + dy * dy);
+            kL = 0.0;
+        } else {
+            // hex_cell_properties, properties.d:568-648
+            Vd p[8] = {vload(vtx, b, i, j, k),         vload(vtx, b, i + 1, j, k),
+                       vload(vtx, b, i + 1, j + 1, k), vload(vtx, b, i, j + 1, k),
+                       vload(vtx, b, i, j, k + 1),     vload(vtx, b, i + 1, j, k + 1),
+                       vload(vtx, b, i + 1, j + 1, k + 1), vload(vtx, b, i, j + 1, k + 1)};
+            Vd cc{0.125 * (p[0].x + p[1].x + p[2].x + p[3].x + p[4].x + p[5].x + p[6].x + p[7].x),
+                  0.125 * (p[0].y + p[1].y + p[2].y + p[3].y + p[4].y + p[5].y + p[6].y + p[7].y),
+                  0.125 * (p[0].z + p[1].z + p[2].z + p[3].z + p[4].z + p[5].z + p[6].z + p[7].z)};
+            Vd pmN = mid4(p[3], p[2], p[6], p[7]), pmE = mid4(p[1], p[2], p[6], p[5]);
+            Vd pmS = mid4(p[0], p[1], p[5], p[4]), pmW = mid4(p[0], p[3], p[7], p[4]);
+            Vd pmT = mid4(p[4], p[5], p[6], p[7]), pmB = mid4(p[0], p[1], p[2], p[3]);
+            double dx, dy, dz;
+            dx = pmE.x - pmW.x; dy = pmE.y - pmW.y; dz = pmE.z - pmW.z;
+            iL = sqrt(dx * dx + dy * dy + dz * dz);
+            dx = pmN.x - pmS.x; dy = pmN.y - pmS.y; dz = pmN.z - pmS.z;
+            jL = sqrt(dx * dx + dy * dy + dz * dz);
+            dx = pmT.x - pmB.x; dy = pmT.y - pmB.y; dz = pmT.z - pmB.z;
+            kL = sqrt(dx * dx + dy * dy + dz * dz);
+            vol = 0.0;
+            vol += pyr_volume(p[6], p[7], p[3], p[2], cc);
+            vol += pyr_volume(p[5], p[6], p[2], p[1], cc);
+            vol += pyr_volume(p[4], p[5], p[1], p[0], cc);
+            vol += pyr_volume(p[7], p[4], p[0], p[3], cc);
+            vol += pyr_volume(p[7], p[6], p[5], p[4], cc);
+            vol += pyr_volume(p[0], p[1], p[2], p[3], cc);
+            if ((vol < 0.0 && fabs(vol) < 1.0e-12) || (vol >= 0.0 && vol < 1.0e-20)) vol = 0.0;
+        }
+        b.cgeom[0 * b.npad + c] = vol;
+        b.cgeom[1 * b.npad + c] = iL;
+        b.cgeom[2 * b.npad + c] = jL;
+        b.cgeom[3 * b.npad + c] = kL;
+    }
+}
+
+__global__ void k_geom_faces(BlockView b, const double* vtx, int dir) {
+    const int ni = b.ni + (dir == 0), nj = b.nj + (dir == 1), nk = b.nk + (dir == 2 && b.dim == 3);
+    const long long n = (long long)ni * nj * nk;
+    double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % ni);
+        int j = b.jmin + int((t / ni) % nj);
+        int k = b.kmin + int(t / ((long long)ni * nj));
+        double out[10];
+        if (b.dim == 2) {
+            if (dir == 0) face2d_props(vload(vtx, b, i, j, 0), vload(vtx, b, i, j + 1, 0), out);
+            else face2d_props(vload(vtx, b, i + 1, j, 0), vload(vtx, b, i, j, 0), out);
+        } else if (dir == 0) {
+            quad_props(vload(vtx, b, i, j, k), vload(vtx, b, i, j + 1, k),
+                       vload(vtx, b, i, j + 1, k + 1), vload(vtx, b, i, j, k + 1), out);
+        } else if (dir == 1) {
+            quad_props(vload(vtx, b, i, j, k), vload(vtx, b, i, j, k + 1),
+                       vload(vtx, b, i + 1, j, k + 1), vload(vtx, b, i + 1, j, k), out);
+        } else {
+            quad_props(vload(vtx, b, i, j, k), vload(vtx, b, i + 1, j, k),
+                       vload(vtx, b, i + 1, j + 1, k), vload(vtx, b, i, j + 1, k), out);
+        }
+        size_t f = pidx(b, i, j, k);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) fg[q * b.npad + f] = out[q];
+    }
+}
+
+// Ghost-cell lengths copied from the mirror interior cells (sfluidblock.d:675-712).
+__global__ void k_geom_ghost_lengths(BlockView b) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    auto copy = [&](size_t dst, size_t src) {
+        for (int q = 1; q < 4; ++q) b.cgeom[q * b.npad + dst] = b.cgeom[q * b.npad + src];
+    };
+    // i boundaries: over (j,k)
+    if (t < b.nj * b.nk) {
+        int j = b.jmin + t % b.nj, k = b.kmin + t / b.nj;
+        copy(pidx(b, b.imin - 1, j, k), pidx(b, b.imin, j, k));
+        copy(pidx(b, b.imin - 2, j, k), pidx(b, b.imin + 1, j, k));
+        copy(pidx(b, b.imax + 1, j, k), pidx(b, b.imax, j, k));
+        copy(pidx(b, b.imax + 2, j, k), pidx(b, b.imax - 1, j, k));
+    }
+    if (t < b.ni * b.nk) {
+        int i = b.imin + t % b.ni, k = b.kmin + t / b.ni;
+        copy(pidx(b, i, b.jmin - 1, k), pidx(b, i, b.jmin, k));
+        copy(pidx(b, i, b.jmin - 2, k), pidx(b, i, b.jmin + 1, k));
+        copy(pidx(b, i, b.jmax + 1, k), pidx(b, i, b.jmax, k));
+        copy(pidx(b, i, b.jmax + 2, k), pidx(b, i, b.jmax - 1, k));
+    }
+    if (b.dim == 3 && t < b.ni * b.nj) {
+        int i = b.imin + t % b.ni, j = b.jmin + t / b.ni;
+        copy(pidx(b, i, j, b.kmin - 1), pidx(b, i, j, b.kmin));
+        copy(pidx(b, i, j, b.kmin - 2), pidx(b, i, j, b.kmin + 1));
+        copy(pidx(b, i, j, b.kmax + 1), pidx(b, i, j, b.kmax));
+        copy(pidx(b, i, j, b.kmax + 2), pidx(b, i, j, b.kmax - 1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Upload: primitive SoA over interior cells -> padded W and encoded U0
+// (encode_conserved, src/eilmer/fvcell.d:494-560)
+// ---------------------------------------------------------------------------
+__global__ void k_upload(BlockView b, const double* prim) {
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const int nw = W_NBASE + (b.nsp > 1 ? b.nsp : 0);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        size_t c = pidx(b, i, j, k);
+        for (int q = 0; q < nw; ++q) b.W[q * b.npad + c] = prim[q * n + t];
+        double rho = prim[W_RHO * n + t];
+        double vx = prim[W_VX * n + t], vy = prim[W_VY * n + t], vz = prim[W_VZ * n + t];
+        double u = prim[W_U * n + t];
+        b.U0[0 * b.npad + c] = rho;
+        b.U0[1 * b.npad + c] = rho * vx;
+        b.U0[2 * b.npad + c] = rho * vy;
+        b.U0[3 * b.npad + c] = rho * vz;
+        double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
+        b.U0[4 * b.npad + c] = rho * (u + ke);
+        for (int s = 0; s < b.nv - 5; ++s) b.U0[(5 + s) * b.npad + c] = rho * prim[(W_NBASE + s) * n + t];
+    }
+}
+
+__global__ void k_download(BlockView b, double* prim, double* cons) {
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const int nw = W_NBASE + (b.nsp > 1 ? b.nsp : 0);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        size_t c = pidx(b, i, j, k);
+        if (prim)
+            for (int q = 0; q < nw; ++q) prim[q * n + t] = b.W[q * b.npad + c];
+        if (cons)
+            for (int q = 0; q < b.nv; ++q) cons[q * n + t] = b.U0[q * b.npad + c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ghost cells: slip wall, supersonic inflow, zero-order extrapolate outflow
+// (src/eilmer/bc/ghost_cell_effect/internal_copy_then_reflect.d:94+,
+//  flow_state_copy.d:66+, extrapolate_copy.d:82+, ghost_cell.d:34-44)
+// ---------------------------------------------------------------------------
+template <int NSP>
+__global__ void k_bc(BlockView b, const SimDev* sim) {
+    if (sim->status != 0 || sim->finished) return;
+    const int which = blockIdx.y;
+    if (b.dim == 2 && which >= 4) return;
+    int n1, n2;  // extent of the boundary layer of cells
+    if (which == NORTH || which == SOUTH) { n1 = b.ni; n2 = b.nk; }
+    else if (which == EAST || which == WEST) { n1 = b.nj; n2 = b.nk; }
+    else { n1 = b.ni; n2 = b.nj; }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n1 * n2) return;
+    const int a1 = t % n1, a2 = t / n1;
+    int i, j, k, di = 0, dj = 0, dk = 0;
+    switch (which) {
+        case NORTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmax; dj = 1; break;
+        case SOUTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmin; dj = -1; break;
+        case EAST: j = b.jmin + a1; k = b.kmin + a2; i = b.imax; di = 1; break;
+        case WEST: j = b.jmin + a1; k = b.kmin + a2; i = b.imin; di = -1; break;
+        case TOP: i = b.imin + a1; j = b.jmin + a2; k = b.kmax; dk = 1; break;
+        default: i = b.imin + a1; j = b.jmin + a2; k = b.kmin; dk = -1; break;
+    }
+    const size_t c0 = pidx(b, i, j, k);
+    const size_t c1 = pidx(b, i - di, j - dj, k - dk);
+    const size_t g1 = pidx(b, i + di, j + dj, k + dk);
+    const size_t g2 = pidx(b, i + 2 * di, j + 2 * dj, k + 2 * dk);
+    const int nw = W_NBASE + (NSP > 1 ? NSP : 0);
+    const int type = b.bc[which];
+    if (type == 1) {  // InFlowBC_Supersonic: both ghosts <- inflow FlowState
+        for (int q = 0; q < nw; ++q) {
+            b.W[q * b.npad + g1] = b.inflow[q];
+            b.W[q * b.npad + g2] = b.inflow[q];
+        }
+    } else if (type == 2) {  // OutFlowBC_SimpleExtrapolate, x_order 0
+        for (int q = 0; q < nw; ++q) {
+            double v = b.W[q * b.npad + c0];
+            b.W[q * b.npad + g1] = v;
+            b.W[q * b.npad + g2] = v;
+        }
+    } else {  // WallBC_WithSlip: copy then reflect the normal velocity
+        size_t f;
+        const double* fg;
+        switch (which) {
+            case NORTH: f = pidx(b, i, j + 1, k); fg = b.fgj; break;
+            case EAST: f = pidx(b, i + 1, j, k); fg = b.fgi; break;
+            case SOUTH: f = pidx(b, i, j, k); fg = b.fgj; break;
+            case WEST: f = pidx(b, i, j, k); fg = b.fgi; break;
+            case TOP: f = pidx(b, i, j, k + 1); fg = b.fgk; break;
+            default: f = pidx(b, i, j, k); fg = b.fgk; break;
+        }
+        Frame<double> fr;
+        fr.n = {fg[0 * b.npad + f], fg[1 * b.npad + f], fg[2 * b.npad + f]};
+        fr.t1 = {fg[3 * b.npad + f], fg[4 * b.npad + f], fg[5 * b.npad + f]};
+        fr.t2 = {fg[6 * b.npad + f], fg[7 * b.npad + f], fg[8 * b.npad + f]};
+        const size_t src[2] = {c0, c1}, dst[2] = {g1, g2};
+        for (int g = 0; g < 2; ++g) {
+            for (int q = 0; q < nw; ++q) b.W[q * b.npad + dst[g]] = b.W[q * b.npad + src[g]];
+            V3<double> v{b.W[W_VX * b.npad + src[g]], b.W[W_VY * b.npad + src[g]],
+                         b.W[W_VZ * b.npad + src[g]]};
+            to_local(v, fr.n, fr.t1, fr.t2);
+            v.x = -(v.x);
+            to_global(v, fr.n, fr.t1, fr.t2);
+            b.W[W_VX * b.npad + dst[g]] = v.x;
+            b.W[W_VY * b.npad + dst[g]] = v.y;
+            b.W[W_VZ * b.npad + dst[g]] = v.z;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Face flux: reconstruction + flux for one face
+// (sfluidblock.d:2190-2344, onedinterp.d:435-585, fluxcalc.d:26-128)
+// ---------------------------------------------------------------------------
+template <int NSP>
+__device__ __forceinline__ void load_prim(const BlockView& b, size_t c, Prim<double, NSP>& s) {
+    s.rho = b.W[W_RHO * b.npad + c];
+    s.vel = {b.W[W_VX * b.npad + c], b.W[W_VY * b.npad + c], b.W[W_VZ * b.npad + c]};
+    s.p = b.W[W_P * b.npad + c];
+    s.u = b.W[W_U * b.npad + c];
+    s.a = b.W[W_A * b.npad + c];
+    if (NSP > 1) {
+#pragma unroll
+        for (int q = 0; q < NSP; ++q) s.massf[q] = b.W[(W_NBASE + q) * b.npad + c];
+    } else {
+        s.massf[0] = 1.0;
+    }
+}
+
+template <int NSP, int FLUX>
+__global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
+    if (sim->status != 0 || sim->finished) return;
+    const int ni = b.ni + (dir == 0), nj = b.nj + (dir == 1), nk = b.nk + (dir == 2);
+    const long long n = (long long)ni * nj * nk;
+    const size_t stride = dir == 0 ? 1 : (dir == 1 ? size_t(b.nidim) : size_t(b.nidim) * b.njdim);
+    const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
+    double* Fo = dir == 0 ? b.Fi : (dir == 1 ? b.Fj : b.Fk);
+    constexpr int NSPC = NSP > 1 ? NSP : 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % ni);
+        int j = b.jmin + int((t / ni) % nj);
+        int k = b.kmin + int(t / ((long long)ni * nj));
+        const size_t f = pidx(b, i, j, k);
+        const size_t cR0 = f, cL0 = f - stride, cL1 = f - 2 * stride, cR1 = f + stride;
+        Frame<double> fr;
+        fr.n = {fg[0 * b.npad + f], fg[1 * b.npad + f], fg[2 * b.npad + f]};
+        fr.t1 = {fg[3 * b.npad + f], fg[4 * b.npad + f], fg[5 * b.npad + f]};
+        fr.t2 = {fg[6 * b.npad + f], fg[7 * b.npad + f], fg[8 * b.npad + f]};
+        Prim<double, NSP> sL1, sL0, sR0, sR1;
+        load_prim<NSP>(b, cL0, sL0);
+        load_prim<NSP>(b, cR0, sR0);
+        Prim<double, NSP> Lf = sL0, Rt = sR0;
+        if (o.order2) {
+            load_prim<NSP>(b, cL1, sL1);
+            load_prim<NSP>(b, cR1, sR1);
+            const double* len = b.cgeom + size_t(1 + dir) * b.npad;
+            if (o.local_frame) {
+                to_local(sL1.vel, fr.n, fr.t1, fr.t2);
+                to_local(sL0.vel, fr.n, fr.t1, fr.t2);
+                to_local(sR0.vel, fr.n, fr.t1, fr.t2);
+                to_local(sR1.vel, fr.n, fr.t1, fr.t2);
+            }
+            L2R2<double> r;
+            r.prepare(len[cL1], len[cL0], len[cR0], len[cR1]);
+            r.scalar(o.limiter, o.clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
+            r.scalar(o.limiter, o.clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
+            r.scalar(o.limiter, o.clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
+            if (NSP > 1) {
+#pragma unroll
+                for (int q = 0; q < NSP; ++q)
+                    r.scalar(o.limiter, o.clip, sL1.massf[q], sL0.massf[q], sR0.massf[q],
+                             sR1.massf[q], Lf.massf[q], Rt.massf[q]);
+                if (!scale_mass_fractions<double, NSP>(Lf.massf))
+                    for (int q = 0; q < NSP; ++q) Lf.massf[q] = sL0.massf[q];
+                if (!scale_mass_fractions<double, NSP>(Rt.massf))
+                    for (int q = 0; q < NSP; ++q) Rt.massf[q] = sR0.massf[q];
+            } else {
+                Lf.massf[0] = 1.0;
+                Rt.massf[0] = 1.0;
+            }
+            r.scalar(o.limiter, o.clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
+            r.scalar(o.limiter, o.clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
+            double T;
+            // codeForThermoUpdateBoth("rhou"), onedinterp.d:1039-1068
+            if (!ideal_rhou<double>(o.gas, Lf.rho, Lf.u, Lf.p, T)) Lf = sL0;
+            if (!ideal_rhou<double>(o.gas, Rt.rho, Rt.u, Rt.p, T)) Rt = sR0;
+            if (o.local_frame) {
+                to_global(Lf.vel, fr.n, fr.t1, fr.t2);
+                to_global(Rt.vel, fr.n, fr.t1, fr.t2);
+            }
+        }
+        // compute_interface_flux, fluxcalc.d:26-128 (fixed grid)
+        to_local(Lf.vel, fr.n, fr.t1, fr.t2);
+        to_local(Rt.vel, fr.n, fr.t1, fr.t2);
+        double F[5 + NSPC];
+        if (FLUX == 1) hllc<double, NSP, NSPC>(Lf, Rt, F);
+        else ausmdv<double, NSP, NSPC>(Lf, Rt, F);
+        V3<double> m{F[1], F[2], F[3]};
+        to_global(m, fr.n, fr.t1, fr.t2);
+        F[1] = m.x; F[2] = m.y; F[3] = m.z;
+#pragma unroll
+        for (int q = 0; q < 5 + NSPC; ++q) Fo[q * b.npad + f] = F[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cell update: time_derivatives + stage update + decode + validity check
+// (fvcell.d:735-875, 1153-1311, 563-732; fluidblock.d:433-499)
+// ---------------------------------------------------------------------------
+template <int NSP>
+__global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int final_stage) {
+    if (sim->status != 0 || sim->finished) return;
+    constexpr int NSPC = NSP > 1 ? NSP : 0;
+    constexpr int NV = 5 + NSPC;
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const double dt = sim->dt_global;
+    int bad = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        // faces north, east, south, west, top, bottom (sfluidblock.d:506-517)
+        const size_t sj = b.nidim, sk = size_t(b.nidim) * b.njdim;
+        const double* Fq[6] = {b.Fj, b.Fi, b.Fj, b.Fi, b.Fk, b.Fk};
+        const double* Gq[6] = {b.fgj, b.fgi, b.fgj, b.fgi, b.fgk, b.fgk};
+        const size_t fq[6] = {c + sj, c + 1, c, c, c + sk, c};
+        const double outsign[6] = {1.0, 1.0, -1.0, -1.0, 1.0, -1.0};
+        const int nf = (b.dim == 3) ? 6 : 4;
+        double integral[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) integral[v] = 0.0;
+        for (int q = 0; q < nf; ++q) {
+            double area = outsign[q] * Gq[q][9 * b.npad + fq[q]];
+            const double* F = Fq[q];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                if (v == 3 && b.dim != 3) continue;
+                integral[v] -= F[v * b.npad + fq[q]] * area;
+            }
+        }
+        double vol_inv = 1.0 / b.cgeom[c];
+        double Un[NV];
+        if (stage == 1) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double d0 = vol_inv * integral[v];
+                if (!final_stage) b.dUdt0[v * b.npad + c] = d0;
+                Un[v] = b.U0[v * b.npad + c] + dt * 1.0 * d0;
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double d1 = vol_inv * integral[v];
+                Un[v] = b.U0[v * b.npad + c] + dt * (0.5 * b.dUdt0[v * b.npad + c] + 0.5 * d1);
+            }
+        }
+        // decode_conserved (ideal gas; adjust_invalid_cell_data = false,
+        // ignore_low_T_thermo_update_failure = true, suggested_low_T_value = 200 K)
+        bool data_bad = false;
+        double rho = Un[0], vx = 0, vy = 0, vz = 0, u = 0, p = 0, T = 0, a = 0;
+        double massf[NSP];
+        massf[0] = 1.0;
+        if (!(Un[0] > 0.0)) {
+            set_status(sim, -5);
+            data_bad = true;
+        } else {
+            double dinv = 1.0 / rho;
+            vx = Un[1] * dinv; vy = Un[2] * dinv; vz = Un[3] * dinv;
+            u = Un[4] * dinv;
+            double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
+            u -= ke;
+            if (NSPC > 0) {
+#pragma unroll
+                for (int s = 0; s < NSPC; ++s) massf[s] = Un[5 + s] * dinv;
+                if (!scale_mass_fractions<double, NSP>(massf)) { set_status(sim, -6); data_bad = true; }
+            }
+            if (!ideal_rhou<double>(gas, rho, u, p, T)) {
+                T = 200.0;
+                p = rho * gas.Rgas * T;
+                u = gas.Cv * T;
+                // encode_conserved(gtl, ftl)
+                Un[0] = rho;
+                Un[1] = rho * vx; Un[2] = rho * vy; Un[3] = rho * vz;
+                double ke2 = 0.5 * (vx * vx + vy * vy + vz * vz);
+                Un[4] = rho * (u + ke2);
+#pragma unroll
+                for (int s = 0; s < NSPC; ++s) Un[5 + s] = rho * massf[s];
+            }
+            a = ideal_sound_speed<double>(gas, T);
+        }
+        // write the new state
+        double* W = b.W;
+        W[W_RHO * b.npad + c] = rho;
+        W[W_VX * b.npad + c] = vx; W[W_VY * b.npad + c] = vy; W[W_VZ * b.npad + c] = vz;
+        W[W_P * b.npad + c] = p; W[W_T * b.npad + c] = T;
+        W[W_U * b.npad + c] = u; W[W_A * b.npad + c] = a;
+#pragma unroll
+        for (int s = 0; s < NSPC; ++s) W[(W_NBASE + s) * b.npad + c] = massf[s];
+        if (final_stage) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) b.U0[v * b.npad + c] = Un[v];
+        }
+        // count_invalid_cells / FlowState.check_data (flowstate.d:345-388,
+        // gas_state.d:199-241, limits fvcore.d:20-27)
+        bool ok = !data_bad;
+        if (!isfinite(rho) || rho < 1.01 * 0.0) ok = false;
+        if (!isfinite(T) || T < 1.01 * 1.0) ok = false;
+        if (!isfinite(p)) ok = false;
+        if (!isfinite(a)) ok = false;
+        double fsum = 0.0;
+        for (int s = 0; s < NSP; ++s) fsum += massf[s];
+        if (fsum < 0.99 || fsum > 1.01 || !isfinite(fsum)) ok = false;
+        if (fabs(vx) > 30000.0 || fabs(vy) > 30000.0 || fabs(vz) > 30000.0) ok = false;
+        if (T < 0.0 || T > 50000.0) ok = false;
+        if (!ok) ++bad;
+    }
+    if (bad) atomicAdd(&sim->bad_cells, bad);
+}
+
+// ---------------------------------------------------------------------------
+// Time step: signal_frequency + block min/max (fvcell.d:1624-1705,
+// fluidblock.d:776-862)
+// ---------------------------------------------------------------------------
+__global__ void k_dt(BlockView b, const SimDev* sim, double cfl_value, const double* dt_current_p,
+                     unsigned long long* acc) {
+    // acc[0] = min dt_local, acc[1] = max cfl_local (as ordered bits), acc[2] = last signal
+    if (sim && (sim->status != 0 || sim->finished)) return;
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const double dt_current = *dt_current_p;
+    double dmin = DBL_MAX, cmax = 0.0;
+    bool any = false;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        V3<double> v{b.W[W_VX * b.npad + c], b.W[W_VY * b.npad + c], b.W[W_VZ * b.npad + c]};
+        const double a = b.W[W_A * b.npad + c];
+        const size_t sj = b.nidim, sk = size_t(b.nidim) * b.njdim;
+        const size_t fN = c + sj, fE = c + 1, fT = c + sk;
+        V3<double> nN{b.fgj[fN], b.fgj[b.npad + fN], b.fgj[2 * b.npad + fN]};
+        V3<double> nE{b.fgi[fE], b.fgi[b.npad + fE], b.fgi[2 * b.npad + fE]};
+        double un_N = fabs(dot3(v, nN));
+        double un_E = fabs(dot3(v, nE));
+        double un_T = 0.0;
+        if (b.dim == 3) {
+            V3<double> nT{b.fgk[fT], b.fgk[b.npad + fT], b.fgk[2 * b.npad + fT]};
+            un_T = fabs(dot3(v, nT));
+        }
+        double signal = 0.0;
+        signal = fmax(signal, (un_N + a) / b.cgeom[2 * b.npad + c]);
+        signal = fmax(signal, (un_E + a) / b.cgeom[1 * b.npad + c]);
+        if (b.dim == 3) signal = fmax(signal, (un_T + a) / b.cgeom[3 * b.npad + c]);
+        double cfl_local = dt_current * signal;
+        double dt_local = cfl_value / signal;
+        dmin = fmin(dmin, dt_local);
+        cmax = any ? fmax(cmax, cfl_local) : cfl_local;
+        any = true;
+        if (i == b.imax && j == b.jmax && k == b.kmax)
+            acc[2] = static_cast<unsigned long long>(__double_as_longlong(signal));
+    }
+    // warp reduction then one atomic per warp
+    for (int off = 16; off > 0; off >>= 1) {
+        dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
+        cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (dmin >= 0.0) atomicMin(&acc[0], dbits(dmin));
+        if (cmax >= 0.0) atomicMax(&acc[1], dbits(cmax));
+    }
+}
+
+__global__ void k_dt_reset(unsigned long long* acc, int nb) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nb) {
+        acc[3 * t + 0] = dbits(DBL_MAX);
+        acc[3 * t + 1] = 0ull;
+        acc[3 * t + 2] = 0ull;
+    }
+}
+
+// The simcore.d:1347-1452 logic over all blocks (one thread).
+__global__ void k_dt_finalize(SimDev* sim, const unsigned long long* acc, int nb, double cfl_allow,
+                              double dt_init, double dt_max, int check_cfl, int step0,
+                              double* out_dt_allow, double* out_cfl_max) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (sim && (sim->status != 0 || sim->finished)) return;
+    if (check_cfl < 0) {  // take SimState.step from the device-side loop
+        check_cfl = sim->step > 0;
+        step0 = sim->step == 0;
+    }
+    double dt_allow = DBL_MAX, cfl_max = 0.0;
+    for (int q = 0; q < nb; ++q) {
+        double d = __longlong_as_double(static_cast<long long>(acc[3 * q + 0]));
+        double c = __longlong_as_double(static_cast<long long>(acc[3 * q + 1]));
+        double last_signal = __longlong_as_double(static_cast<long long>(acc[3 * q + 2]));
+        if (check_cfl && (c < 0.0 || c > cfl_allow)) {
+            c = 0.5 * cfl_allow;
+            d = c / last_signal;
+        }
+        dt_allow = (d < dt_allow) ? d : dt_allow;
+        cfl_max = (c > cfl_max) ? c : cfl_max;
+    }
+    if (out_dt_allow) { *out_dt_allow = dt_allow; *out_cfl_max = cfl_max; }
+    if (!sim) return;
+    if (step0) dt_allow = fmin(dt_init, dt_allow);  // SimState.step == 0
+    if (dt_allow <= sim->dt_global) {
+        sim->dt_global = dt_allow;
+    } else {
+        double g = sim->dt_global * 1.5;
+        g = (dt_allow < g) ? dt_allow : g;
+        g = (dt_max < g) ? dt_max : g;
+        sim->dt_global = g;
+    }
+}
+
+__global__ void k_stage_check(SimDev* sim, int max_invalid_cells) {
+    if (sim->status == 0 && sim->bad_cells > max_invalid_cells) {
+        sim->status = -4;
+        sim->status_step = sim->step;
+    }
+}
+
+__global__ void k_reset_bad(SimDev* sim) { sim->bad_cells = 0; }
+
+__global__ void k_end_step(SimDev* sim) {
+    if (sim->status != 0 || sim->finished) return;
+    sim->time = sim->time + sim->dt_global;  // simcore.d:2951
+    sim->step = sim->step + 1;
+    if (sim->time >= sim->max_time) sim->finished = 1;  // simcore.d:1099
+}
+
+__global__ void k_begin_run(SimDev* sim, double max_time) {
+    sim->max_time = max_time;
+    sim->finished = (sim->time >= max_time) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launchers
+// ---------------------------------------------------------------------------
+static int grid_for(long long n, int threads) {
+    long long g = (n + threads - 1) / threads;
+    if (g > 148LL * 64) g = 148LL * 64;
+    if (g < 1) g = 1;
+    return int(g);
+}
+
+void launch_geometry(const BlockView& b, const double* vtx, cudaStream_t s) {
+    const int T = 256;
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_geom_cells<<<grid_for(n, T), T, 0, s>>>(b, vtx);
+    for (int d = 0; d < b.dim; ++d) {
+        long long nf = (long long)(b.ni + (d == 0)) * (b.nj + (d == 1)) * (b.nk + (d == 2));
+        k_geom_faces<<<grid_for(nf, T), T, 0, s>>>(b, vtx, d);
+    }
+    int m = b.ni * b.nj;
+    m = m > b.nj * b.nk ? m : b.nj * b.nk;
+    m = m > b.ni * b.nk ? m : b.ni * b.nk;
+    k_geom_ghost_lengths<<<(m + T - 1) / T, T, 0, s>>>(b);
+}
+
+void launch_upload(const BlockView& b, const double* prim, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_upload<<<grid_for(n, 256), 256, 0, s>>>(b, prim);
+}
+
+void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_download<<<grid_for(n, 256), 256, 0, s>>>(b, prim, cons);
+}
+
+void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s) {
+    int m = b.ni * b.nk;
+    m = m > b.nj * b.nk ? m : b.nj * b.nk;
+    m = m > b.ni * b.nj ? m : b.ni * b.nj;
+    dim3 grid((m + 127) / 128, 6);
+    if (b.nsp == 5) k_bc<5><<<grid, 128, 0, s>>>(b, sim);
+    else k_bc<1><<<grid, 128, 0, s>>>(b, sim);
+}
+
+void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
+                 cudaStream_t s) {
+    long long n = (long long)(b.ni + (dir == 0)) * (b.nj + (dir == 1)) * (b.nk + (dir == 2));
+    const int T = 128;
+    const int g = grid_for(n, T);
+    if (b.nsp == 5) {
+        if (o.flux == 1) k_flux<5, 1><<<g, T, 0, s>>>(b, sim, o, dir);
+        else k_flux<5, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+    } else {
+        if (o.flux == 1) k_flux<1, 1><<<g, T, 0, s>>>(b, sim, o, dir);
+        else k_flux<1, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+    }
+}
+
+void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
+                   int final_stage, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    const int T = 128;
+    if (b.nsp == 5) k_update<5><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
+    else k_update<1><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
+}
+
+void launch_dt_reset(unsigned long long* acc, int nb, cudaStream_t s) {
+    k_dt_reset<<<(nb + 127) / 128, 128, 0, s>>>(acc, nb);
+}
+
+void launch_dt(const BlockView& b, const SimDev* sim, double cfl_value, const double* dt_current,
+               unsigned long long* acc, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_dt<<<grid_for(n, 256), 256, 0, s>>>(b, sim, cfl_value, dt_current, acc);
+}
+
+void launch_dt_finalize(SimDev* sim, const unsigned long long* acc, int nb, double cfl_allow,
+                        double dt_init, double dt_max, int check_cfl, int step0,
+                        double* out_dt_allow, double* out_cfl_max, cudaStream_t s) {
+    k_dt_finalize<<<1, 32, 0, s>>>(sim, acc, nb, cfl_allow, dt_init, dt_max, check_cfl, step0,
+                                   out_dt_allow, out_cfl_max);
+}
+
+void launch_reset_bad(SimDev* sim, cudaStream_t s) { k_reset_bad<<<1, 1, 0, s>>>(sim); }
+void launch_stage_check(SimDev* sim, int max_invalid, cudaStream_t s) {
+    k_stage_check<<<1, 1, 0, s>>>(sim, max_invalid);
+}
+void launch_end_step(SimDev* sim, cudaStream_t s) { k_end_step<<<1, 1, 0, s>>>(sim); }
+void launch_begin_run(SimDev* sim, double max_time, cudaStream_t s) {
+    k_begin_run<<<1, 1, 0, s>>>(sim, max_time);
+}
+
+}  // namespace e4c

@@ -1,0 +1,68 @@
+// e4c_types.h -- plain structures shared by the host side of libe4cuda and
+// its kernels.  No CUDA or torch types appear here, so the host translation
+// units can include it with a plain C++ compiler.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace e4c {
+
+// Ideal-gas constants (src/gas/ideal_gas.d:66-69).
+struct GasConsts {
+    double Rgas, gamma, Cv, Cvinv, Cp;
+};
+
+// Boundary order north, east, south, west, top, bottom (src/eilmer/fvcore.d).
+enum Bnd { NORTH = 0, EAST = 1, SOUTH = 2, WEST = 3, TOP = 4, BOTTOM = 5 };
+
+// Number of primitive fields kept per padded cell on the general path:
+// rho, vel.x, vel.y, vel.z, p, T, u, a (then mass fractions).
+enum PrimField { W_RHO = 0, W_VX, W_VY, W_VZ, W_P, W_T, W_U, W_A, W_NBASE };
+
+// Device view of one structured block on the general-geometry path.  All
+// arrays use the reference's padded (i,j,k) index with two ghost layers,
+// (k*njdim + j)*nidim + i (src/eilmer/sfluidblock.d:205).
+struct BlockView {
+    int dim;
+    int ni, nj, nk;                 // interior cells
+    int nidim, njdim, nkdim;        // padded extents
+    int imin, imax, jmin, jmax, kmin, kmax;
+    size_t npad;                    // nidim*njdim*nkdim
+    int nsp;                        // species in the primitive state (1 for ideal gas)
+    int nv;                         // conserved components (5 [+nsp])
+    int bc[6];
+    // primitive state, (W_NBASE + nsp) arrays of npad
+    double* W;
+    // conserved state at the start of the step, and dUdt of stage 1 (nv x npad)
+    double* U0;
+    double* dUdt0;
+    // face fluxes per direction (nv x npad)
+    double* Fi;
+    double* Fj;
+    double* Fk;
+    // geometry: cells (vol, iLen, jLen, kLen) x npad; faces per direction
+    // (n.xyz, t1.xyz, t2.xyz, area) x npad
+    double* cgeom;
+    double* fgi;
+    double* fgj;
+    double* fgk;
+    // inflow FlowState (rho, vx, vy, vz, p, T, u, a, massf...)
+    double inflow[8 + 8];
+    int block_id;
+};
+
+// Device-resident simulation state (one per library context).
+struct SimDev {
+    double dt_global;
+    double time;
+    double max_time;                // the loop stops once time >= max_time
+    int step;
+    int status;                     // first error code seen, 0 if none
+    int status_step;                // step at which it was seen
+    int bad_cells;                  // invalid cells counted in the last stage
+    int finished;                   // set when time >= max_time
+    int pad_;
+};
+
+}  // namespace e4c

@@ -1,0 +1,137 @@
+"""Host-side driver over the libe4cuda C ABI.
+
+``Simulation`` plays the part of the D host's ``simcore`` for this path
+(src/eilmer/simcore.d): it owns the configuration, creates the blocks
+(``init_simulation`` :180), uploads the initial flow state (:305-322) and
+advances the solution with ``integrate_in_time`` (:791).  Every step runs on
+the GPU through the C ABI; nothing here computes flow physics.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .config import make_config
+
+
+@dataclass
+class RunInfo:
+    steps_taken: int
+    time: float
+    dt_global: float
+    status: int
+    status_step: int
+    bad_cells: int
+
+
+class Simulation:
+    """One set of structured blocks sharing dt_global, resident on one GPU."""
+
+    def __init__(self, config: dict | None = None, control: dict | None = None, *,
+                 precision: str = "fp64", device: int = 0, use_graphs: bool = True,
+                 gas: dict | None = None):
+        self.L = _lib.load()
+        self.cfg = make_config(config, control, precision=precision, device=device,
+                               use_graphs=use_graphs, gas=gas)
+        _lib.check(self.L.e4c_init(self.cfg))
+        self.blocks = []   # (ni, nj, nk)
+        self.nsp = 1
+
+    @classmethod
+    def from_workload(cls, wl, *, precision="fp64", control=None, use_graphs=True, **config):
+        cfgd = {"dimensions": wl.dimensions, "flux_calculator": wl.flux_calculator}
+        cfgd.update(config)
+        sim = cls(cfgd, control, precision=precision, use_graphs=use_graphs)
+        for b in wl.blocks:
+            h = sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+            sim.upload(h, b.prim)
+        return sim
+
+    def close(self):
+        if getattr(self, "L", None) is not None:
+            self.L.e4c_finalize()
+            self.L = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_block(self, ni, nj, nk, vtx, bc, inflow) -> int:
+        vtx = np.ascontiguousarray(vtx, dtype=np.float64)
+        inflow = np.ascontiguousarray(inflow, dtype=np.float64)
+        bca = (ctypes.c_int * 6)(*bc)
+        h = _lib.check(self.L.e4c_block_create(ni, nj, nk, _lib.dptr(vtx), bca, _lib.dptr(inflow)))
+        nk_eff = nk if self.cfg.dimensions == 3 else 1
+        self.blocks.append((ni, nj, nk_eff))
+        return h
+
+    def ncell(self, h):
+        ni, nj, nk = self.blocks[h]
+        return ni * nj * nk
+
+    def upload(self, h, prim):
+        """prim: (8, ncell) float64 numpy array or a contiguous (pinned) torch tensor."""
+        if not hasattr(prim, "data_ptr"):
+            prim = np.ascontiguousarray(prim, dtype=np.float64)
+            assert prim.shape[-1] == self.ncell(h)
+        _lib.check(self.L.e4c_block_upload(h, _lib.dptr(prim)))
+
+    def download(self, h, prim=None, cons=None, want_cons=True):
+        """Primitive (8, ncell) and conserved (5, ncell) state; the outputs may be
+        given (numpy arrays or contiguous pinned torch tensors)."""
+        n = self.ncell(h)
+        if prim is None:
+            prim = np.zeros((8, n))
+        if cons is None and want_cons:
+            cons = np.zeros((5, n))
+        _lib.check(self.L.e4c_block_download(h, _lib.dptr(prim),
+                                             _lib.dptr(cons) if cons is not None else None))
+        return prim, cons
+
+    def run(self, nsteps, max_time=1.0e300) -> RunInfo:
+        info = _lib.E4CRunInfo()
+        rc = self.L.e4c_integrate(int(nsteps), float(max_time), ctypes.byref(info))
+        _lib.check(rc)
+        return RunInfo(info.steps_taken, info.time, info.dt_global, info.status,
+                       info.status_step, info.bad_cells)
+
+    def dt_allow(self, hs, dt_current, check_cfl):
+        arr = (ctypes.c_int * len(hs))(*hs)
+        d, c = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.L.e4c_dt_allow(arr, len(hs), float(dt_current), int(bool(check_cfl)),
+                                       ctypes.byref(d), ctypes.byref(c)))
+        return d.value, c.value
+
+    def gasdynamic_step(self, hs, dt):
+        arr = (ctypes.c_int * len(hs))(*hs)
+        bad = ctypes.c_int()
+        _lib.check(self.L.e4c_gasdynamic_step(arr, len(hs), float(dt), ctypes.byref(bad)))
+        return bad.value
+
+    def state(self):
+        t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _lib.check(self.L.e4c_sim_state(ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))
+        return t.value, dt.value, st.value
+
+    def synchronize(self):
+        _lib.check(self.L.e4c_synchronize())
+
+    # -- timing hooks -------------------------------------------------------
+    def stream_handle(self) -> int:
+        """The cudaStream_t the library enqueues on (as an integer)."""
+        return int(self.L.e4c_stream() or 0)
+
+    def kernel_launches(self) -> int:
+        return int(self.L.e4c_kernel_launches())
+
+    def profile(self, nsteps):
+        """Per kernel class: (total ms, launches) over nsteps graph-free steps."""
+        ms = (ctypes.c_double * 6)()
+        nl = (ctypes.c_int * 6)()
+        _lib.check(self.L.e4c_profile_steps(int(nsteps), ms, nl))
+        return {name: (ms[q], nl[q]) for q, name in enumerate(_lib.KCLASS)}

@@ -1,0 +1,246 @@
+"""Grids and initial flow states for the structured-block workloads.
+
+These play the part of the reference's preparation step (``e4shared --prep``:
+``prep.lua`` builds the grid, evaluates the initial ``FlowState`` at each cell
+centroid and writes the flow file).  Flow states are built from (p, T) exactly
+as ``IdealGas.update_thermo_from_pT`` + ``update_sound_speed`` do
+(src/gas/ideal_gas.d:89-96, 137-144), in IEEE double arithmetic with the same
+operation order, so the library and any checker start from identical bits.
+
+Workloads (sizes as stated; all data synthetic, generated from a fixed seed):
+  * ``sod_2d``        2-D Sod shock tube, 256 x 64 cells on the unit square,
+                      slip walls all round (ausmdv, 1000 steps).
+  * ``sod_3d_tube``   the reference's own 3-D Sod regression deck
+                      (examples/eilmer/3D/sod-shock-tube/sg/sod.lua):
+                      100 x 2 x 2 cells on 1.0 x 0.1 x 0.1.
+  * ``inflow_3d``     256^3 ideal-air block on the unit cube, Mach 3 inflow at
+                      i-min, extrapolate outflow at i-max, slip walls elsewhere,
+                      density perturbed by 8 seeded random-phase sines.
+  * ``batched_blocks`` 64 independent 3-D blocks with edges drawn
+                      log-uniformly in [16, 96], each initialised like
+                      ``inflow_3d`` with its own seed offset.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+R_UNIVERSAL = 8.31451  # J/(mol.K), src/gas/physical_constants.d:13
+
+# Boundary order north, east, south, west, top, bottom (src/eilmer/fvcore.d Face).
+NORTH, EAST, SOUTH, WEST, TOP, BOTTOM = range(6)
+BC_SLIP_WALL = 0
+BC_INFLOW_SUPERSONIC = 1
+BC_OUTFLOW_EXTRAPOLATE = 2
+
+DEFAULT_SEED = 20261203
+
+# Primitive variable order used at the library boundary.
+PRIM_VARS = ("rho", "velx", "vely", "velz", "p", "T", "u", "a")
+
+
+def splitmix64(seed: int):
+    """The project RNG: SplitMix64 (Steele, Lea & Flood 2014), yields floats in [0,1)."""
+    state = seed & 0xFFFFFFFFFFFFFFFF
+    mask = 0xFFFFFFFFFFFFFFFF
+    while True:
+        state = (state + 0x9E3779B97F4A7C15) & mask
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z = z ^ (z >> 31)
+        yield (z >> 11) * (1.0 / (1 << 53))
+
+
+@dataclass
+class IdealGas:
+    """Ideal air as in src/gas/sample-data/ideal-air-gas-model.lua."""
+    mol_mass: float = 0.02896
+    gamma: float = 1.4
+
+    @property
+    def R(self):
+        return R_UNIVERSAL / self.mol_mass  # ideal_gas.d:66
+
+    @property
+    def Cv(self):
+        return self.R / (self.gamma - 1.0)
+
+    def from_pT(self, p, T):
+        """rho, u, a from p and T (ideal_gas.d:89-96 and :137-144)."""
+        p = np.asarray(p, dtype=np.float64)
+        T = np.asarray(T, dtype=np.float64)
+        rho = p / (T * self.R)
+        u = self.Cv * T
+        a = np.sqrt(self.gamma * self.R * T)
+        return rho, u, a
+
+    def from_rhop(self, rho, p):
+        """T, u, a from rho and p (ideal_gas.d:116-123 and :137-144)."""
+        rho = np.asarray(rho, dtype=np.float64)
+        p = np.asarray(p, dtype=np.float64)
+        T = p / (rho * self.R)
+        u = self.Cv * T
+        a = np.sqrt(self.gamma * self.R * T)
+        return T, u, a
+
+
+@dataclass
+class BlockSpec:
+    """One structured block: grid, boundary conditions and initial state."""
+    ni: int
+    nj: int
+    nk: int
+    vtx: np.ndarray            # ((nk+1)*(nj+1)*(ni+1), 3), i fastest; nk+1 -> 1 in 2-D
+    bc: tuple                  # 6 ints, order N, E, S, W, T, B
+    inflow: np.ndarray         # primitive FlowState used by inflow boundaries
+    prim: np.ndarray           # (8 [+nsp], ncell) primitive SoA over interior cells
+
+    @property
+    def ncell(self):
+        return self.ni * self.nj * self.nk
+
+
+@dataclass
+class Workload:
+    name: str
+    dimensions: int
+    blocks: list = field(default_factory=list)
+    flux_calculator: str = "ausmdv"
+    nsteps: int = 1
+    gas: IdealGas = field(default_factory=IdealGas)
+
+    @property
+    def ncell(self):
+        return sum(b.ncell for b in self.blocks)
+
+
+def box_vertices(ni, nj, nk, lx, ly, lz, dimensions, origin=(0.0, 0.0, 0.0)):
+    """Vertices of a Cartesian box; x = origin + lx*(i/ni) like a parametric map."""
+    xs = origin[0] + lx * (np.arange(ni + 1, dtype=np.float64) / ni)
+    ys = origin[1] + ly * (np.arange(nj + 1, dtype=np.float64) / nj)
+    if dimensions == 3:
+        zs = origin[2] + lz * (np.arange(nk + 1, dtype=np.float64) / nk)
+    else:
+        zs = np.zeros(1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1).copy()
+
+
+def cell_centres(vtx, ni, nj, nk, dimensions):
+    """Average of the cell's corner vertices (exact for dyadic Cartesian grids)."""
+    nvk = nk + 1 if dimensions == 3 else 1
+    V = vtx.reshape(nvk, nj + 1, ni + 1, 3)
+    if dimensions == 3:
+        c = (V[:-1, :-1, :-1] + V[:-1, :-1, 1:] + V[:-1, 1:, 1:] + V[:-1, 1:, :-1]
+             + V[1:, :-1, :-1] + V[1:, :-1, 1:] + V[1:, 1:, 1:] + V[1:, 1:, :-1]) * 0.125
+    else:
+        c = (V[:, :-1, :-1] + V[:, :-1, 1:] + V[:, 1:, 1:] + V[:, 1:, :-1]) * 0.25
+    return c.reshape(-1, 3)
+
+
+def prim_from(rho, vx, vy, vz, p, T, u, a):
+    n = np.broadcast(rho, vx, vy, vz, p, T, u, a).shape
+    out = np.empty((8,) + n, dtype=np.float64)
+    for q, v in enumerate((rho, vx, vy, vz, p, T, u, a)):
+        out[q] = v
+    return out.reshape(8, -1)
+
+
+def flowstate_pT(gas: IdealGas, p, T, vel=(0.0, 0.0, 0.0)):
+    rho, u, a = gas.from_pT(p, T)
+    return np.array([float(rho), vel[0], vel[1], vel[2], p, T, float(u), float(a)])
+
+
+def sod_2d(ni=256, nj=64, T_right=278.7, nsteps=1000) -> Workload:
+    gas = IdealGas()
+    vtx = box_vertices(ni, nj, 1, 1.0, 1.0, 0.0, 2)
+    xc = cell_centres(vtx, ni, nj, 1, 2)[:, 0]
+    left = xc < 0.5
+    p = np.where(left, 1.0e5, 1.0e4)
+    T = np.where(left, 348.4, 278.7 if T_right is None else T_right)
+    rho, u, a = gas.from_pT(p, T)
+    z = np.zeros_like(p)
+    prim = prim_from(rho, z, z, z, p, T, u, a)
+    bc = (BC_SLIP_WALL,) * 6
+    inflow = flowstate_pT(gas, 1.0e5, 300.0)
+    wl = Workload("sod_2d_%dx%d" % (ni, nj), 2, flux_calculator="ausmdv", nsteps=nsteps, gas=gas)
+    wl.blocks.append(BlockSpec(ni, nj, 1, vtx, bc, inflow, prim))
+    return wl
+
+
+def sod_3d_tube(ni=100, nj=2, nk=2, T_right=278.8) -> Workload:
+    """examples/eilmer/3D/sod-shock-tube/sg/sod.lua: 1.0 x 0.1 x 0.1, ausmdv."""
+    gas = IdealGas()
+    vtx = box_vertices(ni, nj, nk, 1.0, 0.1, 0.1, 3)
+    xc = cell_centres(vtx, ni, nj, nk, 3)[:, 0]
+    left = xc < 0.5
+    p = np.where(left, 1.0e5, 1.0e4)
+    T = np.where(left, 348.4, T_right)
+    rho, u, a = gas.from_pT(p, T)
+    z = np.zeros_like(p)
+    prim = prim_from(rho, z, z, z, p, T, u, a)
+    wl = Workload("sod_3d_tube", 3, flux_calculator="ausmdv", nsteps=600, gas=gas)
+    wl.blocks.append(BlockSpec(ni, nj, nk, vtx, (BC_SLIP_WALL,) * 6,
+                               flowstate_pT(gas, 1.0e5, 300.0), prim))
+    return wl
+
+
+def _perturbation(centres, seed):
+    rng = splitmix64(seed)
+    s = np.zeros(centres.shape[0])
+    for m in range(1, 9):
+        # random direction (uniform on the sphere) and phase for term m
+        cz = 2.0 * next(rng) - 1.0
+        phi = 2.0 * math.pi * next(rng)
+        sz = math.sqrt(max(0.0, 1.0 - cz * cz))
+        d = np.array([sz * math.cos(phi), sz * math.sin(phi), cz])
+        phase = 2.0 * math.pi * next(rng)
+        s += np.sin(2.0 * math.pi * m * (centres @ d) + phase)
+    return s
+
+
+def inflow_3d_block(ni, nj, nk, seed, spacing=None, mach=3.0, p_in=1.0e5, T_in=300.0,
+                    gas=None) -> BlockSpec:
+    """Mach-3 inflow block: inflow at i-min (west), outflow at i-max (east)."""
+    gas = gas or IdealGas()
+    if spacing is None:
+        lx, ly, lz = 1.0, 1.0, 1.0
+    else:
+        lx, ly, lz = ni * spacing, nj * spacing, nk * spacing
+    vtx = box_vertices(ni, nj, nk, lx, ly, lz, 3)
+    centres = cell_centres(vtx, ni, nj, nk, 3)
+    rho_in, u_in, a_in = gas.from_pT(p_in, T_in)
+    vx_in = mach * float(a_in)
+    inflow = np.array([float(rho_in), vx_in, 0.0, 0.0, p_in, T_in, float(u_in), float(a_in)])
+    rho = float(rho_in) * (1.0 + 0.05 * _perturbation(centres, seed))
+    p = np.full_like(rho, p_in)
+    T, u, a = gas.from_rhop(rho, p)
+    z = np.zeros_like(rho)
+    prim = prim_from(rho, np.full_like(rho, vx_in), z, z, p, T, u, a)
+    bc = [BC_SLIP_WALL] * 6
+    bc[WEST] = BC_INFLOW_SUPERSONIC
+    bc[EAST] = BC_OUTFLOW_EXTRAPOLATE
+    return BlockSpec(ni, nj, nk, vtx, tuple(bc), inflow, prim)
+
+
+def inflow_3d(n=256, seed=DEFAULT_SEED, flux="hllc", nsteps=500) -> Workload:
+    wl = Workload("inflow_3d_%d^3" % n, 3, flux_calculator=flux, nsteps=nsteps)
+    wl.blocks.append(inflow_3d_block(n, n, n, seed))
+    return wl
+
+
+def batched_blocks(nblocks=64, lo=16, hi=96, seed=DEFAULT_SEED, spacing=1.0 / 64.0,
+                   nsteps=200, flux="ausmdv") -> Workload:
+    """Independent blocks with log-uniform edges; cell spacing 1/64 keeps each
+    block's geometry exactly uniform."""
+    rng = splitmix64(seed ^ 0xB10C)
+    wl = Workload("batched_%d_blocks" % nblocks, 3, flux_calculator=flux, nsteps=nsteps)
+    for b in range(nblocks):
+        dims = [int(round(math.exp(math.log(lo) + (math.log(hi) - math.log(lo)) * next(rng))))
+                for _ in range(3)]
+        wl.blocks.append(inflow_3d_block(dims[0], dims[1], dims[2], seed + 1 + b,
+                                         spacing=spacing))
+    return wl

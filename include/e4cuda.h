@@ -1,0 +1,185 @@
+/*
+ * e4cuda.h -- C ABI of libe4cuda, the B200 (sm_100a) explicit structured-block
+ * gas-dynamic update for the Eilmer4 solver.
+ *
+ * The D host keeps its time loop, I/O and configuration; under a
+ * version(e4cuda) build the calls below replace, one for one:
+ *
+ *   e4c_init / e4c_finalize      GlobalConfig set-up and tear-down around
+ *                                init_simulation (src/eilmer/simcore.d:180) and
+ *                                finalize_simulation (simcore.d:3426)
+ *   e4c_block_create             SFluidBlock construction + geometry,
+ *                                compute_primary_cell_geometric_data
+ *                                (src/eilmer/sfluidblock.d:94-126, 650-842)
+ *                                and the boundary-condition set-up of
+ *                                bc.lua:528-551 (WallBC_WithSlip),
+ *                                :974-994 (InFlowBC_Supersonic),
+ *                                :1103-1121 (OutFlowBC_SimpleExtrapolate)
+ *   e4c_block_upload             read_solution + encode_conserved per block
+ *                                (simcore.d:305-322, sfluidblock.d:1778,
+ *                                src/eilmer/fvcell.d:494)
+ *   e4c_block_download           the state the host writes with
+ *                                write_solution_files (simcore.d:637)
+ *   e4c_dt_allow                 FluidBlock.determine_time_step_size over the
+ *                                given blocks (src/eilmer/fluidblock.d:776-862)
+ *   e4c_gasdynamic_step          gasdynamic_explicit_increment_with_fixed_grid
+ *                                (simcore.d:2303-2952)
+ *   e4c_integrate                the integrate_in_time loop (simcore.d:791-1110)
+ *                                restricted to dt control + gas dynamics,
+ *                                run on the device as CUDA graphs
+ *
+ * Conventions (after the gas_cwrap.d C ABI, src/gas/gas_cwrap.d:35-67):
+ * integer handles, plain pointers to host arrays borrowed for the duration
+ * of the call, return 0 on success and a negative E4C_ERR_* code on failure;
+ * e4c_last_error() gives the message.  The library never throws across the
+ * ABI, never aborts the process and never traps on the device.  It is not
+ * thread-safe: call it from one host thread.  All device memory belongs to
+ * the library (allocated at block creation, freed at e4c_finalize).
+ *
+ * Host arrays:
+ *   vertices    (ni+1)*(nj+1)*(nk+1) points, xyz each, i fastest (one k layer in 2-D)
+ *   primitive   SoA over interior cells (i fastest), variables
+ *               rho, vel.x, vel.y, vel.z, p, T, u, a [, massf[nsp]]
+ *   conserved   SoA: mass, x-, y-, z-momentum, total energy [, rho*massf[nsp]]
+ */
+#ifndef E4CUDA_H
+#define E4CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define E4C_OK 0
+#define E4C_ERR_ARG (-1)          /* bad argument or handle */
+#define E4C_ERR_CUDA (-2)         /* a CUDA runtime call failed */
+#define E4C_ERR_UNSUPPORTED (-3)  /* configuration outside the implemented path */
+#define E4C_ERR_BAD_CELLS (-4)    /* more invalid cells than max_invalid_cells (simcore.d:2480-2493) */
+#define E4C_ERR_BAD_MASS (-5)     /* non-positive density in decode (fvcell.d:570-590) */
+#define E4C_ERR_THERMO (-6)       /* thermodynamic update failed (fvcell.d:654-720) */
+#define E4C_ERR_CHEM (-7)         /* chemistry update failed (chemistry_update.d:213-270) */
+#define E4C_ERR_TIMEOUT (-8)      /* a bounded device wait ran out */
+#define E4C_ERR_STATE (-9)        /* call out of order (no e4c_init, no blocks, ...) */
+
+/* Boundary conditions (bc.lua names). */
+#define E4C_BC_WALL_WITH_SLIP 0
+#define E4C_BC_INFLOW_SUPERSONIC 1
+#define E4C_BC_OUTFLOW_SIMPLE_EXTRAPOLATE 2
+
+/* flux_calculator (src/eilmer/fvcore.d:184-228, plus the new "hllc"). */
+#define E4C_FLUX_AUSMDV 0
+#define E4C_FLUX_HLLC 1
+
+/* gasdynamic_update_scheme (fvcore.d:29-110). */
+#define E4C_UPDATE_EULER 0
+#define E4C_UPDATE_PC 1
+
+/* Arithmetic of the reconstruction and flux. */
+#define E4C_PREC_FP64 0       /* all FP64, same operation order as the reference */
+#define E4C_PREC_FP32_FLUX 1  /* FP32 reconstruction/flux, FP64 accumulation + decode */
+
+/* Gas models. */
+#define E4C_GAS_IDEAL 0
+#define E4C_GAS_THERM_PERF_5SP_AIR 1
+
+typedef struct e4c_config {
+    int dimensions;                 /* "dimensions" (globalconfig.d:1260) */
+    int flux_calculator;            /* "flux_calculator" (globalconfig.d:1329) */
+    int interpolation_order;        /* "interpolation_order" (globalconfig.d:1330) */
+    int apply_limiter;              /* "apply_limiter" (globalconfig.d:1338) */
+    int extrema_clipping;           /* "extrema_clipping" (globalconfig.d:568) */
+    int interpolate_in_local_frame; /* "interpolate_in_local_frame" (globalconfig.d:569) */
+    int gasdynamic_update_scheme;   /* "gasdynamic_update_scheme" (globalconfig.d:1281) */
+    double cfl_value;               /* control "cfl_value" */
+    double dt_init;                 /* control "dt_init" */
+    double dt_max;                  /* control "dt_max" */
+    int cfl_count;                  /* control "cfl_count" */
+    int max_invalid_cells;          /* "max_invalid_cells" (globalconfig.d:519) */
+    int gas_model;                  /* E4C_GAS_* */
+    double ideal_mol_mass;          /* IdealGas.mMass (kg/mol) */
+    double ideal_gamma;             /* IdealGas.gamma */
+    int reacting;                   /* "reacting" (globalconfig.d:1502) */
+    double T_frozen;                /* "T_frozen" (globalconfig.d:692) */
+    int precision;                  /* E4C_PREC_* */
+    int device;                     /* CUDA device ordinal */
+    int use_graphs;                 /* capture e4c_integrate steps in CUDA graphs */
+} e4c_config;
+
+typedef struct e4c_run_info {
+    int steps_taken;
+    double time;
+    double dt_global;
+    int status;                     /* 0 or the first E4C_ERR_* seen on the device */
+    int status_step;                /* step at which status was set */
+    int bad_cells;                  /* invalid cells in the last stage */
+} e4c_run_info;
+
+/* Fill cfg with the reference defaults (globalconfig.d:440-734). */
+int e4c_config_default(e4c_config* cfg);
+
+/* Select the device, check the configuration, create the context. */
+int e4c_init(const e4c_config* cfg);
+
+/* Free every device buffer and graph; the context may be re-initialised. */
+int e4c_finalize(void);
+
+/* Create a structured block; returns a handle >= 0 or an error code.
+ * bc_type[6] in the order north, east, south, west, top, bottom.
+ * inflow_prim is one primitive FlowState used by inflow boundaries. */
+int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* bc_type,
+                     const double* inflow_prim);
+
+/* Upload a block's primitive state and encode its conserved quantities. */
+int e4c_block_upload(int h, const double* prim);
+
+/* Download the primitive and/or conserved state (either pointer may be NULL). */
+int e4c_block_download(int h, double* prim, double* cons);
+
+/* Allowable time step over the blocks, as FluidBlock.determine_time_step_size
+ * followed by the min/max reduction over blocks (simcore.d:1362-1386);
+ * check_cfl corresponds to SimState.step > 0. */
+int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double* dt_allow,
+                 double* cfl_max);
+
+/* One explicit gas-dynamic step of size dt over the blocks; returns the
+ * invalid-cell count of the last stage in *bad_cells. */
+int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells);
+
+/* Run the time loop over all blocks for nsteps steps or until max_time:
+ * dt control every cfl_count steps, dt_init at step 0, x1.5 growth cap and
+ * dt_max, then the gas-dynamic step.  The loop stays on the device. */
+int e4c_integrate(int nsteps, double max_time, e4c_run_info* info);
+
+/* Simulation time, dt_global and step counter of the device-side loop. */
+int e4c_sim_state(double* time, double* dt_global, int* step);
+
+/* Wait for all queued device work. */
+int e4c_synchronize(void);
+
+/* The cudaStream_t the library enqueues all its work on (for event timing). */
+void* e4c_stream(void);
+
+/* Number of kernels the library has enqueued so far; a graph replay counts
+ * every kernel node it contains. */
+long long e4c_kernel_launches(void);
+
+/* Kernel classes timed by e4c_profile_steps. */
+#define E4C_KCLASS_DT 0        /* signal frequency + dt reduction */
+#define E4C_KCLASS_BC 1        /* ghost-cell fill (general path) */
+#define E4C_KCLASS_FLUX 2      /* reconstruction + flux (general path) */
+#define E4C_KCLASS_UPDATE 3    /* cell update + decode (general path) */
+#define E4C_KCLASS_STAGE 4     /* fused stage kernel (uniform path) */
+#define E4C_KCLASS_OTHER 5     /* bookkeeping kernels */
+#define E4C_NKCLASS 6
+
+/* Run nsteps time steps without graphs, timing each kernel class with CUDA
+ * events on the library stream: ms[c] = total milliseconds of class c and
+ * launches[c] = its launch count (arrays of E4C_NKCLASS). */
+int e4c_profile_steps(int nsteps, double* ms, int* launches);
+
+/* Copy the message of the last error into buf (always NUL-terminated). */
+int e4c_last_error(char* buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

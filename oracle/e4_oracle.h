@@ -1,0 +1,96 @@
+/*
+ * e4_oracle.h -- C API of the CPU FP64 oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The oracle is a plain C++ restatement of the
+ * Eilmer4 explicit structured-block update (the D code under src/eilmer,
+ * src/gas, src/geom, src/kinetics of the reference).  It exists to check the
+ * CUDA library and to time a CPU baseline.  Only tests/, the smoke() entry
+ * point and the bench's CPU-baseline leg may load it; the product path never
+ * does.
+ *
+ * Conventions follow the reference:
+ *   - cells of a structured block are indexed (i,j,k), i fastest;
+ *   - boundary order is north, east, south, west, top, bottom
+ *     (src/eilmer/fvcore.d Face enum);
+ *   - primitive arrays are SoA over interior cells with the variable order
+ *     rho, vel.x, vel.y, vel.z, p, T, u, a, massf[0..nsp-1];
+ *   - conserved arrays are SoA with the order mass, xmom, ymom, zmom,
+ *     total_energy, rho*massf[0..nsp-1] (only when nsp > 1).
+ */
+#ifndef E4_ORACLE_H
+#define E4_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { E4O_BC_SLIP_WALL = 0, E4O_BC_INFLOW_SUPERSONIC = 1, E4O_BC_OUTFLOW_EXTRAPOLATE = 2 };
+enum { E4O_FLUX_AUSMDV = 0, E4O_FLUX_HLLC = 1 };
+enum { E4O_UPDATE_EULER = 0, E4O_UPDATE_PC = 1 };
+enum { E4O_GAS_IDEAL = 0, E4O_GAS_THERM_PERF_5SP_AIR = 1 };
+
+typedef struct e4o_config {
+    int dimensions;                 /* 2 or 3 */
+    int flux_calculator;            /* E4O_FLUX_* */
+    int interpolation_order;        /* 1 or 2 */
+    int apply_limiter;
+    int extrema_clipping;
+    int interpolate_in_local_frame;
+    int update_scheme;              /* E4O_UPDATE_* */
+    double cfl_value;
+    double dt_init;
+    double dt_max;
+    int cfl_count;
+    int max_invalid_cells;
+    int gas_model;                  /* E4O_GAS_* */
+    double ideal_mol_mass;          /* kg/mol (ideal gas) */
+    double ideal_gamma;
+    int reacting;                   /* finite-rate chemistry after each step */
+    double T_frozen;
+    int n_threads;                  /* OpenMP threads; <=0 means all */
+} e4o_config;
+
+void e4o_default_config(e4o_config* cfg);
+
+void* e4o_sim_new(const e4o_config* cfg);
+void e4o_sim_free(void* sim);
+
+/* Add a structured block.  vtx holds (ni+1)*(nj+1)*(nk+1) points, 3 doubles
+ * each, i fastest (nk=1 and one vertex layer for 2D).  bc[6] uses the
+ * boundary order north, east, south, west, top, bottom.  inflow is a
+ * primitive FlowState (rho,vx,vy,vz,p,T,u,a,massf...) used by inflow BCs.
+ * Returns the block index, or a negative error code. */
+int e4o_add_block(void* sim, int ni, int nj, int nk, const double* vtx,
+                  const int* bc, const double* inflow);
+
+/* Set the interior flow state from a primitive SoA array and encode the
+ * conserved quantities (src/eilmer/fvcell.d encode_conserved). */
+int e4o_set_flow(void* sim, int blk, const double* prim);
+
+/* Read back the primitive and conserved arrays of a block (either may be NULL). */
+int e4o_get_flow(void* sim, int blk, double* prim, double* cons);
+
+/* Geometry of a block: cell volume, iLength, jLength, kLength per interior
+ * cell (4 x ncell SoA) and, per face direction d (0=i,1=j,2=k), for every
+ * face of that direction: n(3), t1(3), t2(3), area -> 10 doubles per face,
+ * face arrays laid out as the padded-index faces the reference iterates. */
+int e4o_get_cell_geometry(void* sim, int blk, double* out);
+
+/* Advance nsteps time steps (or until max_time), replaying
+ * src/eilmer/simcore.d integrate_in_time.  Returns 0 or a negative error. */
+int e4o_run(void* sim, int nsteps, double max_time);
+
+double e4o_time(void* sim);
+double e4o_dt_global(void* sim);
+int e4o_step_count(void* sim);
+int e4o_last_bad_cells(void* sim);
+const char* e4o_last_error(void* sim);
+
+/* Low-level pieces exposed for golden-vector tests. */
+int e4o_ideal_gas_pT(double mol_mass, double gamma, double p, double T,
+                     double* rho, double* u, double* a);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,189 @@
+"""ctypes wrapper of the CPU FP64 oracle (oracle/_build/libe4oracle.so).
+
+TEST INFRASTRUCTURE ONLY.  The oracle restates the reference's explicit
+structured-block update in plain C++ (see e4_oracle.cpp for the file:line map
+into the reference).  Only tests/, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` import this module; the product package never
+does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libe4oracle.so")
+
+BC_SLIP_WALL = 0
+BC_INFLOW_SUPERSONIC = 1
+BC_OUTFLOW_EXTRAPOLATE = 2
+FLUX_AUSMDV = 0
+FLUX_HLLC = 1
+UPDATE_EULER = 0
+UPDATE_PC = 1
+GAS_IDEAL = 0
+GAS_THERM_PERF_5SP_AIR = 1
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("dimensions", ctypes.c_int),
+        ("flux_calculator", ctypes.c_int),
+        ("interpolation_order", ctypes.c_int),
+        ("apply_limiter", ctypes.c_int),
+        ("extrema_clipping", ctypes.c_int),
+        ("interpolate_in_local_frame", ctypes.c_int),
+        ("update_scheme", ctypes.c_int),
+        ("cfl_value", ctypes.c_double),
+        ("dt_init", ctypes.c_double),
+        ("dt_max", ctypes.c_double),
+        ("cfl_count", ctypes.c_int),
+        ("max_invalid_cells", ctypes.c_int),
+        ("gas_model", ctypes.c_int),
+        ("ideal_mol_mass", ctypes.c_double),
+        ("ideal_gamma", ctypes.c_double),
+        ("reacting", ctypes.c_int),
+        ("T_frozen", ctypes.c_double),
+        ("n_threads", ctypes.c_int),
+    ]
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++, no GPU needed)."""
+    if force or not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = build()
+        L = ctypes.CDLL(path)
+        vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        P = ctypes.POINTER
+        L.e4o_default_config.argtypes = [P(Config)]
+        L.e4o_sim_new.argtypes = [P(Config)]
+        L.e4o_sim_new.restype = vp
+        L.e4o_sim_free.argtypes = [vp]
+        L.e4o_add_block.argtypes = [vp, ip, ip, ip, P(dp), P(ip), P(dp)]
+        L.e4o_add_block.restype = ip
+        L.e4o_set_flow.argtypes = [vp, ip, P(dp)]
+        L.e4o_get_flow.argtypes = [vp, ip, P(dp), P(dp)]
+        L.e4o_get_cell_geometry.argtypes = [vp, ip, P(dp)]
+        L.e4o_run.argtypes = [vp, ip, dp]
+        L.e4o_time.argtypes = [vp]
+        L.e4o_time.restype = dp
+        L.e4o_dt_global.argtypes = [vp]
+        L.e4o_dt_global.restype = dp
+        L.e4o_step_count.argtypes = [vp]
+        L.e4o_last_bad_cells.argtypes = [vp]
+        L.e4o_last_error.argtypes = [vp]
+        L.e4o_last_error.restype = ctypes.c_char_p
+        L.e4o_ideal_gas_pT.argtypes = [dp, dp, dp, dp, P(dp), P(dp), P(dp)]
+        _lib = L
+    return _lib
+
+
+def _dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def default_config(**kw) -> Config:
+    c = Config()
+    lib().e4o_default_config(ctypes.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class OracleSim:
+    """One simulation (a set of blocks sharing dt_global), as simcore.d runs it."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self._h = lib().e4o_sim_new(ctypes.byref(cfg))
+        self.blocks = []
+        self.nsp = 5 if cfg.gas_model == GAS_THERM_PERF_5SP_AIR else 1
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().e4o_sim_free(h)
+            self._h = None
+
+    def add_block(self, ni, nj, nk, vtx, bc, inflow):
+        vtx = np.ascontiguousarray(vtx, dtype=np.float64)
+        inflow = np.ascontiguousarray(inflow, dtype=np.float64)
+        bca = (ctypes.c_int * 6)(*bc)
+        b = lib().e4o_add_block(self._h, ni, nj, nk, _dptr(vtx), bca, _dptr(inflow))
+        if b < 0:
+            raise RuntimeError(f"e4o_add_block failed: {b}")
+        self.blocks.append((ni, nj, nk if self.cfg.dimensions == 3 else 1))
+        return b
+
+    def nvar_prim(self):
+        return 8 + (self.nsp if self.nsp > 1 else 0)
+
+    def nvar_cons(self):
+        return 5 + (self.nsp if self.nsp > 1 else 0)
+
+    def set_flow(self, b, prim):
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        rc = lib().e4o_set_flow(self._h, b, _dptr(prim))
+        if rc != 0:
+            raise RuntimeError(f"e4o_set_flow failed: {rc}")
+
+    def get_flow(self, b):
+        ni, nj, nk = self.blocks[b]
+        n = ni * nj * nk
+        prim = np.zeros((self.nvar_prim(), n))
+        cons = np.zeros((self.nvar_cons(), n))
+        lib().e4o_get_flow(self._h, b, _dptr(prim), _dptr(cons))
+        return prim, cons
+
+    def geometry(self, b):
+        ni, nj, nk = self.blocks[b]
+        n = ni * nj * nk
+        nf = (ni + 1) * nj * nk + ni * (nj + 1) * nk
+        if self.cfg.dimensions == 3:
+            nf += ni * nj * (nk + 1)
+        out = np.zeros(4 * n + 10 * nf)
+        lib().e4o_get_cell_geometry(self._h, b, _dptr(out))
+        return out[: 4 * n].reshape(4, n), out[4 * n:].reshape(nf, 10)
+
+    def run(self, nsteps, max_time=1.0e300):
+        rc = lib().e4o_run(self._h, nsteps, max_time)
+        return rc
+
+    @property
+    def time(self):
+        return lib().e4o_time(self._h)
+
+    @property
+    def dt_global(self):
+        return lib().e4o_dt_global(self._h)
+
+    @property
+    def step(self):
+        return lib().e4o_step_count(self._h)
+
+    @property
+    def last_bad_cells(self):
+        return lib().e4o_last_bad_cells(self._h)
+
+
+def ideal_gas_pT(mol_mass, gamma, p, T):
+    rho, u, a = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    rc = lib().e4o_ideal_gas_pT(mol_mass, gamma, p, T, ctypes.byref(rho), ctypes.byref(u),
+                                ctypes.byref(a))
+    if rc != 0:
+        raise ValueError("bad state")
+    return rho.value, u.value, a.value

@@ -1,0 +1,26 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import e4_oracle
+    e4_oracle.build()
+    return e4_oracle
+
+
+@pytest.fixture(scope="session")
+def e4lib():
+    from eilmer4_b200 import build, _lib
+    build.build()
+    return _lib.load()

@@ -1,0 +1,143 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle.
+
+The plain FP64 path keeps the reference's operation order with no fused
+multiply-adds, so the comparison is exact (==) on every primitive and
+conserved quantity, on the step count, simulation time and dt_global.
+"""
+import numpy as np
+import pytest
+
+from eilmer4_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FLUX = {"ausmdv": 0, "hllc": 1}
+
+
+def run_oracle(oracle, wl, nsteps, max_time=1.0e300, **cfgkw):
+    cfg = oracle.default_config(dimensions=wl.dimensions,
+                                flux_calculator=FLUX[wl.flux_calculator], n_threads=0, **cfgkw)
+    sim = oracle.OracleSim(cfg)
+    for b in wl.blocks:
+        h = sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+        sim.set_flow(h, b.prim)
+    rc = sim.run(nsteps, max_time)
+    out = [sim.get_flow(h) for h in range(len(wl.blocks))]
+    return rc, sim.step, sim.time, sim.dt_global, out
+
+
+def run_gpu(wl, nsteps, max_time=1.0e300, precision="fp64", use_graphs=True, **cfgkw):
+    from eilmer4_b200.simcore import Simulation
+    cfgd = {}
+    ctl = {}
+    for k, v in cfgkw.items():
+        if k in ("cfl_value", "cfl_count", "dt_init", "dt_max"):
+            ctl[k] = v
+        else:
+            cfgd[k] = v
+    with Simulation.from_workload(wl, precision=precision, control=ctl, use_graphs=use_graphs,
+                                  **cfgd) as sim:
+        info = sim.run(nsteps, max_time)
+        out = [sim.download(h) for h in range(len(wl.blocks))]
+        t, dt, st = sim.state()
+    return info, st, t, dt, out
+
+
+def assert_same(a, b, what):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if not np.array_equal(a, b):
+        bad = np.argwhere(a != b)
+        q = tuple(bad[0])
+        rel = np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))
+        raise AssertionError(f"{what}: {len(bad)} values differ; first at {q}: "
+                             f"gpu={a[q]!r} oracle={b[q]!r}; max rel {rel:.3e}")
+
+
+def compare(oracle, wl, nsteps, max_time=1.0e300, use_graphs=True, **kw):
+    orc, ost, otime, odt, oout = run_oracle(oracle, wl, nsteps, max_time,
+                                            **{k: v for k, v in kw.items() if k in
+                                               ("cfl_value", "update_scheme",
+                                                "interpolation_order", "cfl_count")})
+    assert orc == 0
+    gkw = {}
+    if "update_scheme" in kw:
+        gkw["gasdynamic_update_scheme"] = "euler" if kw["update_scheme"] == 0 else "pc"
+    if "interpolation_order" in kw:
+        gkw["interpolation_order"] = kw["interpolation_order"]
+    if "cfl_value" in kw:
+        gkw["cfl_value"] = kw["cfl_value"]
+    info, gst, gtime, gdt, gout = run_gpu(wl, nsteps, max_time, use_graphs=use_graphs, **gkw)
+    assert gst == ost, (gst, ost)
+    assert gtime == otime and gdt == odt, (gtime, otime, gdt, odt)
+    for b, ((gp, gc), (op, oc)) in enumerate(zip(gout, oout)):
+        assert_same(gc, oc, f"block {b} conserved")
+        assert_same(gp[:8], op[:8], f"block {b} primitive")
+    return info
+
+
+def test_sod_2d_small_bitexact(oracle, e4lib):
+    compare(oracle, W.sod_2d(64, 16), 120)
+
+
+def test_sod_tube_3d_reference_deck(oracle, e4lib):
+    # examples/eilmer/3D/sod-shock-tube/sg: run to t = 0.6 ms like the deck
+    info = compare(oracle, W.sod_3d_tube(), 600, max_time=0.6e-3)
+    assert abs(info.steps_taken - 75) < 3
+
+
+def test_inflow_3d_ausmdv_bitexact(oracle, e4lib):
+    wl = W.Workload("inflow3d", 3, flux_calculator="ausmdv")
+    wl.blocks.append(W.inflow_3d_block(20, 12, 10, seed=7))
+    compare(oracle, wl, 40)
+
+
+def test_inflow_3d_hllc_bitexact(oracle, e4lib):
+    wl = W.Workload("inflow3d", 3, flux_calculator="hllc")
+    wl.blocks.append(W.inflow_3d_block(16, 14, 12, seed=11))
+    compare(oracle, wl, 40)
+
+
+def test_multiblock_shared_dt(oracle, e4lib):
+    wl = W.batched_blocks(nblocks=3, lo=6, hi=12, nsteps=25)
+    compare(oracle, wl, 25)
+
+
+def test_euler_and_first_order(oracle, e4lib):
+    compare(oracle, W.sod_2d(40, 8), 30, update_scheme=0)
+    compare(oracle, W.sod_2d(40, 8), 30, interpolation_order=1)
+
+
+def test_without_graphs_matches(oracle, e4lib):
+    compare(oracle, W.sod_2d(32, 8), 25, use_graphs=False)
+
+
+def test_dt_allow_and_single_step_calls(oracle, e4lib):
+    """The per-call entry points a D host would use inside its own loop."""
+    from eilmer4_b200.simcore import Simulation
+    wl = W.sod_2d(32, 8)
+    with Simulation.from_workload(wl) as sim:
+        dt_allow, cfl_max = sim.dt_allow([0], 1.0e-3, False)
+        dt = min(1.0e-3, dt_allow)  # step 0: fmin(dt_init, dt_allow)
+        bad = sim.gasdynamic_step([0], dt)
+        assert bad == 0
+        gp, gc = sim.download(0)
+    _, ost, _, odt, oout = run_oracle(oracle, wl, 1)
+    assert dt == odt
+    assert_same(gc, oout[0][1], "conserved after one step")
+
+
+def test_bad_cells_reported(oracle, e4lib):
+    """A state past the velocity limit (flowstate.d:345-388) makes the stage
+    report E4C_ERR_BAD_CELLS, as the reference throws 'Too many bad cells'."""
+    from eilmer4_b200 import _lib
+    from eilmer4_b200.simcore import Simulation
+    wl = W.sod_2d(16, 4)
+    b = wl.blocks[0]
+    b.prim[1, 5] = 40000.0
+    with Simulation.from_workload(wl) as sim:
+        with pytest.raises(_lib.E4CError) as ei:
+            sim.run(3)
+        assert ei.value.code == _lib.E4C_ERR_BAD_CELLS
+    rc, *_ = run_oracle(oracle, wl, 3)
+    assert rc == -4
