@@ -58,6 +58,21 @@ void Ctx::release() {
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
     blocks.clear();
+    // every device pointer above is now dangling: forget them all
+    d_descs = nullptr;
+    descs_cap = 0;
+    nfused = 0;
+    fused_items = 0;
+    descs_valid = false;
+    max_cells_fused = 0;
+    d_hlist = nullptr;
+    hlist_cap = 0;
+    d_sim = nullptr;
+    d_scalars = nullptr;
+    d_dtacc = nullptr;
+    dtacc_cap = 0;
+    d_staging = nullptr;
+    staging_bytes = 0;
     initialised = false;
 }
 
@@ -83,13 +98,16 @@ static inline void launch_as(Ctx& c, int cls, int nkernels, F&& f) {
     if (c.prof.on) c.prof.end(c.stream);
 }
 
-// One stage over the given blocks (simcore.d:2325-2493 / 2529-2730).
+// One stage over the given blocks (simcore.d:2325-2493 / 2529-2730).  All
+// fused blocks go through one launch of the fused stage kernel.
 void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) {
     launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_reset_bad(d_sim, stream); });
+    bool any_fused = false;
+    for (int h : hs) any_fused = any_fused || blocks[h].fused;
+    if (any_fused) launch_as(*this, E4C_KCLASS_STAGE, 1, [&] { fused_stage_all(stage); });
     for (int h : hs) {
         const BlockHost& b = blocks[h];
-        if (b.fused) launch_as(*this, E4C_KCLASS_STAGE, 1, [&] { fused_stage(b, stage, final_stage); });
-        else launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc(b.v, d_sim, stream); });
+        if (!b.fused) launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc(b.v, d_sim, stream); });
     }
     for (int h : hs) {
         const BlockHost& b = blocks[h];
@@ -113,21 +131,24 @@ void Ctx::enqueue_gasdynamic(const std::vector<int>& hs) {
     launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_end_step(d_sim, stream); });
 }
 
-void Ctx::enqueue_dt(const std::vector<int>& hs, const double* dt_current, int check_cfl,
-                     int step0, SimDev* sim, double* out) {
-    launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_dt_reset(d_dtacc, int(hs.size()), stream); });
-    for (size_t q = 0; q < hs.size(); ++q) {
-        const BlockHost& b = blocks[hs[q]];
-        if (b.fused)
-            launch_as(*this, E4C_KCLASS_DT, 1, [&] { fused_dt(b, sim, dt_current, d_dtacc + 3 * q); });
-        else
-            launch_as(*this, E4C_KCLASS_DT, 1, [&] {
-                launch_dt(b.v, sim, cfg.cfl_value, dt_current, d_dtacc + 3 * q, stream);
-            });
+// dt control over the given blocks; accumulators are indexed by handle and
+// d_hl lists the handles of hs on the device.
+void Ctx::enqueue_dt(const std::vector<int>& hs, const int* d_hl, const double* dt_current,
+                     int check_cfl, int step0, SimDev* sim, double* out) {
+    launch_as(*this, E4C_KCLASS_OTHER, 1,
+              [&] { launch_dt_reset(d_dtacc, int(blocks.size()), stream); });
+    bool any_fused = false;
+    for (int h : hs) {
+        const BlockHost& b = blocks[h];
+        if (b.fused) { any_fused = true; continue; }
+        launch_as(*this, E4C_KCLASS_DT, 1, [&] {
+            launch_dt(b.v, sim, cfg.cfl_value, dt_current, d_dtacc + 3 * h, stream);
+        });
     }
+    if (any_fused) launch_as(*this, E4C_KCLASS_DT, 1, [&] { fused_dt_all(sim, dt_current); });
     const double cfl_allow = (cfg.gasdynamic_update_scheme == E4C_UPDATE_PC) ? 1.2 : 0.9;
     launch_as(*this, E4C_KCLASS_OTHER, 1, [&] {
-        launch_dt_finalize(sim, d_dtacc, int(hs.size()), cfl_allow, cfg.dt_init, cfg.dt_max,
+        launch_dt_finalize(sim, d_dtacc, d_hl, int(hs.size()), cfl_allow, cfg.dt_init, cfg.dt_max,
                            check_cfl, step0, out, out ? out + 1 : nullptr, stream);
     });
 }
@@ -184,8 +205,8 @@ int e4c_init(const e4c_config* cfg) {
         return fail(E4C_ERR_UNSUPPORTED, "gasdynamic_update_scheme must be euler or predictor-corrector");
     if (cfg->gas_model != E4C_GAS_IDEAL)
         return fail(E4C_ERR_UNSUPPORTED, "gas model not available in this build");
-    if (cfg->precision != E4C_PREC_FP64)
-        return fail(E4C_ERR_UNSUPPORTED, "precision not available in this build");
+    if (cfg->precision != E4C_PREC_FP64 && cfg->precision != E4C_PREC_FP32_FLUX)
+        return fail(E4C_ERR_UNSUPPORTED, "unknown precision");
     if (cfg->reacting) return fail(E4C_ERR_UNSUPPORTED, "reacting flow not available in this build");
     if (cfg->cfl_count < 1) return fail(E4C_ERR_ARG, "cfl_count must be >= 1");
     int ndev = 0;
@@ -255,8 +276,12 @@ int e4c_block_upload(int h, const double* prim) {
     BlockHost& b = c.blocks[h];
     size_t bytes = b.nprim_vars * b.ncell * sizeof(double);
     E4C_CUDA(cudaMemcpyAsync(c.d_staging, prim, bytes, cudaMemcpyHostToDevice, c.stream));
-    if (b.fused) c.fused_upload(b, c.d_staging);
-    else launch_upload(b.v, c.d_staging, c.stream);
+    if (b.fused) {
+        int rc = c.fused_upload(b, c.d_staging);
+        if (rc != E4C_OK) return rc;
+    } else {
+        launch_upload(b.v, c.d_staging, c.stream);
+    }
     E4C_CUDA(cudaGetLastError());
     E4C_CUDA(cudaStreamSynchronize(c.stream));
     return E4C_OK;
@@ -289,7 +314,12 @@ static int check_handles(const int* h, int nb, std::vector<int>& hs) {
     hs.assign(h, h + nb);
     for (int x : hs)
         if (x < 0 || x >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad block handle");
-    return c.ensure_dtacc(nb);
+    int rc = c.prepare_fused();
+    if (rc != E4C_OK) return rc;
+    if (!c.uses_all_fused(hs))
+        return fail(E4C_ERR_ARG, "blocks on the fused uniform path advance together: "
+                                 "pass all of them or none");
+    return c.set_hlist(hs);
 }
 
 int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double* dt_allow,
@@ -302,7 +332,8 @@ int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double*
     double* hp = static_cast<double*>(c.host_pinned);
     hp[0] = dt_current;
     E4C_CUDA(cudaMemcpyAsync(c.d_scalars, hp, sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    c.enqueue_dt(hs, c.d_scalars, check_cfl ? 1 : 0, 0, nullptr, c.d_scalars + 2);
+    c.enqueue_dt(hs, c.d_hlist + c.hlist_cap, c.d_scalars, check_cfl ? 1 : 0, 0, nullptr,
+                 c.d_scalars + 2);
     E4C_CUDA(cudaGetLastError());
     E4C_CUDA(cudaMemcpyAsync(hp + 2, c.d_scalars + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                              c.stream));
@@ -362,7 +393,7 @@ int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
     if (nsteps < 0) return fail(E4C_ERR_ARG, "negative step count");
     std::vector<int> hs = c.all_blocks();
-    int rc = c.ensure_dtacc(int(hs.size()));
+    int rc = c.prepare_fused();
     if (rc != E4C_OK) return rc;
     SimDev s0;
     rc = read_sim(s0);
@@ -418,7 +449,7 @@ int e4c_profile_steps(int nsteps, double* ms, int* launches) {
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
     if (!ms || !launches || nsteps < 0) return fail(E4C_ERR_ARG, "bad arguments");
     std::vector<int> hs = c.all_blocks();
-    int rc = c.ensure_dtacc(int(hs.size()));
+    int rc = c.prepare_fused();
     if (rc != E4C_OK) return rc;
     SimDev s0;
     rc = read_sim(s0);
@@ -427,7 +458,7 @@ int e4c_profile_steps(int nsteps, double* ms, int* launches) {
     c.prof.on = true;
     for (int q = 0; q < nsteps; ++q) {
         const bool dt_check = ((s0.step + q) % c.cfg.cfl_count) == 0;
-        if (dt_check) c.enqueue_dt(hs, &c.d_sim->dt_global, -1, -1, c.d_sim, nullptr);
+        if (dt_check) c.enqueue_dt(hs, c.d_hlist, &c.d_sim->dt_global, -1, -1, c.d_sim, nullptr);
         c.enqueue_gasdynamic(hs);
     }
     c.prof.on = false;

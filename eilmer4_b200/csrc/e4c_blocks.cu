@@ -1,4 +1,6 @@
-// e4c_blocks.cu -- block construction and the per-step launch sequence.
+// e4c_blocks.cu -- block construction, the fused-path bookkeeping and the
+// per-step launch sequence.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -12,14 +14,44 @@ namespace e4c {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
+void Ctx::dfree(void* p) {
+    auto it = std::find(allocations.begin(), allocations.end(), p);
+    if (it != allocations.end()) {
+        cudaFree(p);
+        allocations.erase(it);
+    }
+}
+
 int Ctx::ensure_dtacc(int nb) {
     if (nb <= dtacc_cap) return E4C_OK;
     int cap = nb < 64 ? 64 : nb;
     d_dtacc = static_cast<unsigned long long*>(dalloc(size_t(3) * cap * sizeof(unsigned long long)));
-    if (!d_dtacc) return fail(E4C_ERR_CUDA, "cudaMalloc of dt accumulators failed");
+    d_hlist = static_cast<int*>(dalloc(size_t(2) * cap * sizeof(int)));  // [all blocks | scratch]
+    if (!d_dtacc || !d_hlist) return fail(E4C_ERR_CUDA, "cudaMalloc of dt accumulators failed");
     dtacc_cap = cap;
+    hlist_cap = cap;
+    descs_valid = false;
     reset_graphs();
     return E4C_OK;
+}
+
+// Copy a list of block handles to the scratch half of d_hlist (synchronously,
+// so the pinned staging slot can be reused at once).
+int Ctx::set_hlist(const std::vector<int>& hs) {
+    int* hp = static_cast<int*>(host_pinned) + 256;  // a scratch slot past the scalars
+    if (hs.size() > 512) return fail(E4C_ERR_ARG, "too many blocks in one call");
+    for (size_t q = 0; q < hs.size(); ++q) hp[q] = hs[q];
+    E4C_CUDA(cudaMemcpyAsync(d_hlist + hlist_cap, hp, hs.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, stream));
+    E4C_CUDA(cudaStreamSynchronize(stream));
+    return E4C_OK;
+}
+
+bool Ctx::uses_all_fused(const std::vector<int>& hs) const {
+    int n = 0;
+    for (int h : hs)
+        if (blocks[h].fused) ++n;
+    return n == 0 || n == nfused;
 }
 
 int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
@@ -39,18 +71,13 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     for (int q = 0; q < 6; ++q) v.bc[q] = bc[q];
     for (int q = 0; q < 8; ++q) v.inflow[q] = inflow[q];
     const size_t np = v.npad;
-    const size_t nw = W_NBASE;
-    const size_t total = nw * np + 2 * size_t(v.nv) * np + 3 * size_t(v.nv) * np + 4 * np + 30 * np;
-    double* slab = static_cast<double*>(dalloc(total * sizeof(double)));
-    if (!slab) return fail(E4C_ERR_CUDA, "cudaMalloc of block storage failed");
-    E4C_CUDA(cudaMemsetAsync(slab, 0, total * sizeof(double), stream));
-    double* p = slab;
-    v.W = p; p += nw * np;
-    v.U0 = p; p += v.nv * np;
-    v.dUdt0 = p; p += v.nv * np;
-    v.Fi = p; p += v.nv * np;
-    v.Fj = p; p += v.nv * np;
-    v.Fk = p; p += v.nv * np;
+    // geometry arrays first (needed on either path), then the general-path state
+    const size_t ngeom = 4 * np + 30 * np;
+    const size_t nstate = W_NBASE * np + 2 * size_t(v.nv) * np + 3 * size_t(v.nv) * np;
+    double* geom = static_cast<double*>(dalloc(ngeom * sizeof(double)));
+    if (!geom) return fail(E4C_ERR_CUDA, "cudaMalloc of block geometry failed");
+    E4C_CUDA(cudaMemsetAsync(geom, 0, ngeom * sizeof(double), stream));
+    double* p = geom;
     v.cgeom = p; p += 4 * np;
     v.fgi = p; p += 10 * np;
     v.fgj = p; p += 10 * np;
@@ -58,33 +85,188 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     // geometry from the vertices (compute_primary_cell_geometric_data)
     const size_t nvtx = size_t(ni + 1) * (nj + 1) * ((dim == 3) ? nk + 1 : 1);
     double* d_vtx = nullptr;
-    E4C_CUDA(cudaMalloc(&d_vtx, nvtx * 3 * sizeof(double)));
+    E4C_CUDA(cudaMalloc(&d_vtx, nvtx * 3 * sizeof(double) + 64));
+    int* d_flag = reinterpret_cast<int*>(d_vtx + nvtx * 3);
     cudaError_t e = cudaMemcpyAsync(d_vtx, vtx, nvtx * 3 * sizeof(double), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(int), stream);
     if (e == cudaSuccess) {
         launch_geometry(v, d_vtx, stream);
+        launch_check_uniform(v, d_flag, stream);
         e = cudaGetLastError();
     }
+    int uniform_flag = 1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&uniform_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     cudaFree(d_vtx);
     if (e != cudaSuccess) return cuda_fail(e, "block geometry");
-    out.v = v;
+
     out.ncell = size_t(ni) * nj * v.nk;
     out.nprim_vars = 8;
-    out.fused = false;
+    const bool uniform = (uniform_flag == 0);
+    out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC;
+    if (cfg.precision == E4C_PREC_FP32_FLUX && !out.fused)
+        return fail(E4C_ERR_UNSUPPORTED,
+                    "the FP32-flux form needs a 3-D block with uniform geometry and the "
+                    "predictor-corrector scheme");
+    if (out.fused) {
+        // uniform constants: the first interior cell and its west/south/bottom faces
+        FusedDesc& f = out.f;
+        std::memset(&f, 0, sizeof(f));
+        f.ni = ni; f.nj = nj; f.nk = nk;
+        for (int q = 0; q < 6; ++q) f.bc[q] = bc[q];
+        const size_t c0 = (size_t(v.kmin) * v.njdim + v.jmin) * v.nidim + v.imin;
+        double g[4], fg[3][10];
+        for (int q = 0; q < 4; ++q)
+            E4C_CUDA(cudaMemcpy(&g[q], v.cgeom + q * np + c0, sizeof(double), cudaMemcpyDeviceToHost));
+        const double* fgs[3] = {v.fgi, v.fgj, v.fgk};
+        for (int d = 0; d < 3; ++d)
+            for (int q = 0; q < 10; ++q)
+                E4C_CUDA(cudaMemcpy(&fg[d][q], fgs[d] + q * np + c0, sizeof(double),
+                                    cudaMemcpyDeviceToHost));
+        f.vol = g[0];
+        for (int d = 0; d < 3; ++d) {
+            f.len[d] = g[1 + d];
+            f.area[d] = fg[d][9];
+            for (int q = 0; q < 3; ++q) {
+                f.fn[d][q] = fg[d][q];
+                f.ft1[d][q] = fg[d][3 + q];
+                f.ft2[d][q] = fg[d][6 + q];
+            }
+        }
+        // inflow FlowState: rho, vx, vy, vz, u, a
+        f.inflow[0] = inflow[0]; f.inflow[1] = inflow[1]; f.inflow[2] = inflow[2];
+        f.inflow[3] = inflow[3]; f.inflow[4] = inflow[6]; f.inflow[5] = inflow[7];
+        dfree(geom);
+        const size_t nc = out.ncell;
+        const size_t rsz = (cfg.precision == E4C_PREC_FP32_FLUX) ? sizeof(float) : sizeof(double);
+        char* s = static_cast<char*>(dalloc(2 * 5 * nc * rsz + (1 + 10) * nc * sizeof(double) + 256));
+        if (!s) return fail(E4C_ERR_CUDA, "cudaMalloc of fused block storage failed");
+        E4C_CUDA(cudaMemsetAsync(s, 0, 2 * 5 * nc * rsz + (1 + 10) * nc * sizeof(double) + 256, stream));
+        double* dp = reinterpret_cast<double*>(s);
+        f.U0 = dp; dp += 5 * nc;
+        f.dUdt0 = dp; dp += 5 * nc;
+        f.A0 = dp; dp += nc;
+        f.use_a0 = reinterpret_cast<int*>(dp); dp += 32;
+        char* rp = reinterpret_cast<char*>(dp);
+        f.WA = rp; rp += 5 * nc * rsz;
+        f.WB = rp;
+        v.W = v.U0 = v.dUdt0 = v.Fi = v.Fj = v.Fk = nullptr;
+        v.cgeom = v.fgi = v.fgj = v.fgk = nullptr;
+        max_cells_fused = std::max(max_cells_fused, int(nc));
+    } else {
+        double* slab = static_cast<double*>(dalloc(nstate * sizeof(double)));
+        if (!slab) return fail(E4C_ERR_CUDA, "cudaMalloc of block storage failed");
+        E4C_CUDA(cudaMemsetAsync(slab, 0, nstate * sizeof(double), stream));
+        double* q = slab;
+        v.W = q; q += W_NBASE * np;
+        v.U0 = q; q += v.nv * np;
+        v.dUdt0 = q; q += v.nv * np;
+        v.Fi = q; q += v.nv * np;
+        v.Fj = q; q += v.nv * np;
+        v.Fk = q; q += v.nv * np;
+    }
+    out.v = v;
     // staging area for uploads and downloads (primitive + conserved)
     const size_t need = (out.nprim_vars + size_t(v.nv)) * out.ncell * sizeof(double);
     if (need > staging_bytes) {
-        double* s = static_cast<double*>(dalloc(need));
-        if (!s) return fail(E4C_ERR_CUDA, "cudaMalloc of staging buffer failed");
-        d_staging = s;
+        double* st = static_cast<double*>(dalloc(need));
+        if (!st) return fail(E4C_ERR_CUDA, "cudaMalloc of staging buffer failed");
+        d_staging = st;
         staging_bytes = need;
     }
+    descs_valid = false;
     return E4C_OK;
+}
+
+// (Re)build the device descriptor array of the fused blocks and the
+// persistent grid of the fused stage kernel.
+int Ctx::prepare_fused() {
+    if (descs_valid) return E4C_OK;
+    int rc = ensure_dtacc(int(blocks.size()));
+    if (rc != E4C_OK) return rc;
+    {
+        // the "all blocks" handle list
+        int* hp = static_cast<int*>(host_pinned) + 256;
+        for (size_t q = 0; q < blocks.size(); ++q) hp[q] = int(q);
+        E4C_CUDA(cudaMemcpyAsync(d_hlist, hp, blocks.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                 stream));
+        E4C_CUDA(cudaStreamSynchronize(stream));
+    }
+    std::vector<FusedDesc> ds;
+    long long items = 0;
+    for (size_t h = 0; h < blocks.size(); ++h) {
+        BlockHost& b = blocks[h];
+        if (!b.fused) continue;
+        FusedDesc& f = b.f;
+        f.tiles_i = (f.ni + tile_ti - 1) / tile_ti;
+        f.tiles_j = (f.nj + tile_tj - 1) / tile_tj;
+        f.kchunks = (f.nk + tile_kc - 1) / tile_kc;
+        f.item0 = items;
+        f.acc = d_dtacc + 3 * h;
+        items += (long long)f.tiles_i * f.tiles_j * f.kchunks;
+        ds.push_back(f);
+    }
+    nfused = int(ds.size());
+    fused_items = items;
+    if (nfused > 0) {
+        if (nfused > descs_cap) {
+            d_descs = static_cast<FusedDesc*>(dalloc(sizeof(FusedDesc) * std::max(nfused, 64)));
+            if (!d_descs) return fail(E4C_ERR_CUDA, "cudaMalloc of block descriptors failed");
+            descs_cap = std::max(nfused, 64);
+        }
+        E4C_CUDA(cudaMemcpyAsync(d_descs, ds.data(), sizeof(FusedDesc) * nfused,
+                                 cudaMemcpyHostToDevice, stream));
+        E4C_CUDA(cudaStreamSynchronize(stream));
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg.device);
+        const int per_sm = (cfg.precision == E4C_PREC_FP32_FLUX)
+                               ? f32::fused_occupancy(cfg.flux_calculator, tile_ti, tile_tj)
+                               : f64::fused_occupancy(cfg.flux_calculator, tile_ti, tile_tj);
+        if (per_sm <= 0) return fail(E4C_ERR_UNSUPPORTED, "fused tile shape does not fit on the device");
+        long long g = (long long)nsm * per_sm;
+        fused_grid = int(std::min<long long>(g, items));
+    }
+    descs_valid = true;
+    reset_graphs();
+    return E4C_OK;
+}
+
+void Ctx::fused_stage_all(int stage) {
+    FusedLaunch L{d_descs, nfused, fused_items, tile_kc, tile_ti, tile_tj, fused_grid};
+    if (cfg.precision == E4C_PREC_FP32_FLUX) f32::fused_stage(L, d_sim, gas, fopts, stage, stream);
+    else f64::fused_stage(L, d_sim, gas, fopts, stage, stream);
+}
+
+void Ctx::fused_dt_all(SimDev* sim, const double* dt_current) {
+    int gx = (max_cells_fused + 255) / 256;
+    if (gx > 148 * 8) gx = 148 * 8;
+    if (gx < 1) gx = 1;
+    if (cfg.precision == E4C_PREC_FP32_FLUX)
+        f32::fused_dt(d_descs, nfused, gx, sim, gas, cfg.cfl_value, dt_current, stream);
+    else
+        f64::fused_dt(d_descs, nfused, gx, sim, gas, cfg.cfl_value, dt_current, stream);
+}
+
+int Ctx::fused_upload(BlockHost& b, const double* prim) {
+    FusedDesc& f = b.f;
+    if (cfg.precision == E4C_PREC_FP32_FLUX) f32::fused_upload(prim, b.ncell, f.WA, const_cast<double*>(f.A0), f.U0, stream);
+    else f64::fused_upload(prim, b.ncell, f.WA, const_cast<double*>(f.A0), f.U0, stream);
+    const int one = 1;
+    E4C_CUDA(cudaMemcpyAsync(f.use_a0, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    return E4C_OK;
+}
+
+void Ctx::fused_download(const BlockHost& b, double* prim, double* cons) {
+    const FusedDesc& f = b.f;
+    if (cfg.precision == E4C_PREC_FP32_FLUX)
+        f32::fused_download(f.WA, f.A0, f.use_a0, f.U0, b.ncell, gas, prim, cons, stream);
+    else
+        f64::fused_download(f.WA, f.A0, f.use_a0, f.U0, b.ncell, gas, prim, cons, stream);
 }
 
 int Ctx::run_step(const std::vector<int>& hs, bool dt_check) {
     auto enqueue = [&]() {
-        if (dt_check) enqueue_dt(hs, &d_sim->dt_global, -1, -1, d_sim, nullptr);
+        if (dt_check) enqueue_dt(hs, d_hlist, &d_sim->dt_global, -1, -1, d_sim, nullptr);
         enqueue_gasdynamic(hs);
     };
     if (!cfg.use_graphs) {
@@ -113,11 +295,5 @@ int Ctx::run_step(const std::vector<int>& hs, bool dt_check) {
     launches += gs.nkernels;
     return E4C_OK;
 }
-
-// The fused uniform path is not selected yet; these are never reached.
-void Ctx::fused_stage(const BlockHost&, int, int) {}
-void Ctx::fused_dt(const BlockHost&, SimDev*, const double*, unsigned long long*) {}
-void Ctx::fused_upload(BlockHost&, const double*) {}
-void Ctx::fused_download(const BlockHost&, double*, double*) {}
 
 }  // namespace e4c

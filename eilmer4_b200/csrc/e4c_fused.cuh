@@ -1,0 +1,430 @@
+// e4c_fused.cuh -- fused stage kernel for blocks with uniform, axis-aligned
+// geometry (every cell and every face of a direction has identical bits).
+//
+// One launch performs a whole predictor-corrector stage for every such block:
+// ghost cells (computed in the tile loader from the boundary condition),
+// MUSCL/van Albada reconstruction, the face flux, the flux divergence in the
+// reference's face order, the stage update and the conserved->primitive
+// decode.  CTAs are persistent over work items (block, i-j tile, k chunk);
+// within an item the CTA marches in k, keeping a ring of four halo planes of
+// the primitive state in shared memory, so each plane is read from HBM once
+// and each face flux is computed once.
+//
+// R = double: the plain FP64 form (compiled with -fmad=false; bit-identical
+//             to the general path and to the reference algorithm).
+// R = float:  the FP32 reconstruction/flux form; fluxes are accumulated,
+//             the state updated and decoded in FP64.
+#pragma once
+
+#include <cfloat>
+
+#include "e4c_kernels.h"
+#include "e4c_physics.cuh"
+
+namespace e4c {
+
+// Fields kept per cell in shared memory: rho, vx, vy, vz, u, a.
+constexpr int NF = 6;
+
+template <typename R, int TI, int TJ>
+struct FusedSmem {
+    static constexpr int PI = TI + 4, PJ = TJ + 4;
+    static constexpr int PLANE = NF * PI * PJ;
+    static constexpr size_t bytes() {
+        return sizeof(R) * (size_t(4) * PLANE + 5 * TJ * (TI + 1) + 5 * (TJ + 1) * TI);
+    }
+};
+
+template <typename R>
+__device__ __forceinline__ void reflect_normal(R& vx, R& vy, R& vz, const double* n,
+                                               const double* t1, const double* t2) {
+    // reflect_normal_velocity, ghost_cell.d:34-44
+    V3<R> v{vx, vy, vz};
+    Frame<R> fr{{R(n[0]), R(n[1]), R(n[2])}, {R(t1[0]), R(t1[1]), R(t1[2])},
+                {R(t2[0]), R(t2[1]), R(t2[2])}};
+    to_local(v, fr.n, fr.t1, fr.t2);
+    v.x = -(v.x);
+    to_global(v, fr.n, fr.t1, fr.t2);
+    vx = v.x; vy = v.y; vz = v.z;
+}
+
+// Load halo plane kk of a tile into shared-memory slot s.  Ghost cells are
+// built from the boundary condition of the face they lie beyond; corner
+// ghosts and cells beyond the second ghost layer are never read and skipped.
+template <typename R, int TI, int TJ>
+__device__ __forceinline__ void load_plane(const FusedDesc& d, const R* __restrict__ W, int use_a0,
+                                           const GasConsts& gas, R* plane, int i0, int j0,
+                                           int kk) {
+    constexpr int PI = TI + 4, PJ = TJ + 4;
+    const size_t nc = size_t(d.ni) * d.nj * d.nk;
+    for (int e = threadIdx.x; e < PI * PJ; e += blockDim.x) {
+        const int li = e % PI, lj = e / PI;
+        int gi = i0 - 2 + li, gj = j0 - 2 + lj, gk = kk;
+        const bool oi = gi < 0 || gi >= d.ni;
+        const bool oj = gj < 0 || gj >= d.nj;
+        const bool ok = gk < 0 || gk >= d.nk;
+        if (int(oi) + int(oj) + int(ok) > 1) continue;
+        int which = -1, layer = 0;  // boundary and ghost layer (0: first, 1: second)
+        if (oi) {
+            if (gi < 0) { which = WEST; layer = -gi - 1; }
+            else { which = EAST; layer = gi - d.ni; }
+        } else if (oj) {
+            if (gj < 0) { which = SOUTH; layer = -gj - 1; }
+            else { which = NORTH; layer = gj - d.nj; }
+        } else if (ok) {
+            if (gk < 0) { which = BOTTOM; layer = -gk - 1; }
+            else { which = TOP; layer = gk - d.nk; }
+        }
+        if (layer > 1) continue;
+        R rho, vx, vy, vz, u, a;
+        int type = which >= 0 ? d.bc[which] : -1;
+        if (type == 1) {  // supersonic inflow: both ghost layers hold the inflow state
+            rho = R(d.inflow[0]); vx = R(d.inflow[1]); vy = R(d.inflow[2]); vz = R(d.inflow[3]);
+            u = R(d.inflow[4]); a = R(d.inflow[5]);
+        } else {
+            // source cell: the mirror cell for a slip wall, the first interior
+            // cell for the zero-order extrapolation outflow
+            if (which >= 0) {
+                const int src = (type == 2) ? 0 : layer;
+                switch (which) {
+                    case WEST: gi = src; break;
+                    case EAST: gi = d.ni - 1 - src; break;
+                    case SOUTH: gj = src; break;
+                    case NORTH: gj = d.nj - 1 - src; break;
+                    case BOTTOM: gk = src; break;
+                    default: gk = d.nk - 1 - src; break;
+                }
+            }
+            const size_t c = (size_t(gk) * d.nj + gj) * d.ni + gi;
+            rho = W[0 * nc + c]; vx = W[1 * nc + c]; vy = W[2 * nc + c]; vz = W[3 * nc + c];
+            u = W[4 * nc + c];
+            if (use_a0) {
+                a = R(d.A0[c]);
+            } else {
+                // a of the decoded state: update_thermo_from_rhou then update_sound_speed
+                R T = u * R(gas.Cvinv);
+                a = sqrt(R(gas.gamma) * R(gas.Rgas) * T);
+            }
+            if (type == 0) {
+                const int dir = (which == WEST || which == EAST) ? 0 : ((which == SOUTH || which == NORTH) ? 1 : 2);
+                reflect_normal<R>(vx, vy, vz, d.fn[dir], d.ft1[dir], d.ft2[dir]);
+            }
+        }
+        R* p = plane + lj * PI + li;
+        constexpr int FS = PI * PJ;
+        p[0 * FS] = rho; p[1 * FS] = vx; p[2 * FS] = vy; p[3 * FS] = vz; p[4 * FS] = u; p[5 * FS] = a;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void get_cell(const R* plane, int off, int FS, const GasConsts& gas,
+                                         Prim<R, 1>& s) {
+    s.rho = plane[off];
+    s.vel = {plane[FS + off], plane[2 * FS + off], plane[3 * FS + off]};
+    s.u = plane[4 * FS + off];
+    s.a = plane[5 * FS + off];
+    s.p = R(0.0);  // filled in only when needed (cell_pressure)
+    s.massf[0] = R(1.0);
+    (void)gas;
+}
+
+// Cell-centre pressure of a decoded cell (update_thermo_from_rhou); read only
+// when a reconstructed state fails its thermo update and the reference falls
+// back to a copy of the cell-centre FlowState.
+template <typename R>
+__device__ __forceinline__ void cell_pressure(Prim<R, 1>& s, const GasConsts& gas) {
+    R T = s.u * R(gas.Cvinv);
+    s.p = s.rho * R(gas.Rgas) * T;
+}
+
+// Reconstruction + flux of one face from four cells (general-path semantics,
+// sfluidblock.d:2190-2344 with onedinterp.d:435-585 and fluxcalc.d:26-128).
+template <typename R, int FLUX>
+__device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R, 1> sR0,
+                                          Prim<R, 1> sR1, const L2R2<R>& w, const Frame<R>& fr,
+                                          const FluxOpts& o, R* F) {
+    Prim<R, 1> Lf = sL0, Rt = sR0;
+    if (o.order2) {
+        if (o.local_frame) {
+            to_local(sL1.vel, fr.n, fr.t1, fr.t2);
+            to_local(sL0.vel, fr.n, fr.t1, fr.t2);
+            to_local(sR0.vel, fr.n, fr.t1, fr.t2);
+            to_local(sR1.vel, fr.n, fr.t1, fr.t2);
+        }
+        const bool lim = o.limiter, clip = o.clip;
+        w.scalar(lim, clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
+        w.scalar(lim, clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
+        w.scalar(lim, clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
+        Lf.massf[0] = R(1.0);
+        Rt.massf[0] = R(1.0);
+        w.scalar(lim, clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
+        w.scalar(lim, clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
+        R T;
+        if (!ideal_rhou<R>(o.gas, Lf.rho, Lf.u, Lf.p, T)) { Lf = sL0; cell_pressure(Lf, o.gas); }
+        if (!ideal_rhou<R>(o.gas, Rt.rho, Rt.u, Rt.p, T)) { Rt = sR0; cell_pressure(Rt, o.gas); }
+        if (o.local_frame) {
+            to_global(Lf.vel, fr.n, fr.t1, fr.t2);
+            to_global(Rt.vel, fr.n, fr.t1, fr.t2);
+        }
+    } else {
+        cell_pressure(Lf, o.gas);
+        cell_pressure(Rt, o.gas);
+    }
+    to_local(Lf.vel, fr.n, fr.t1, fr.t2);
+    to_local(Rt.vel, fr.n, fr.t1, fr.t2);
+    if (FLUX == 1) hllc<R, 1, 0>(Lf, Rt, F);
+    else ausmdv<R, 1, 0>(Lf, Rt, F);
+    V3<R> m{F[1], F[2], F[3]};
+    to_global(m, fr.n, fr.t1, fr.t2);
+    F[1] = m.x; F[2] = m.y; F[3] = m.z;
+}
+
+template <typename R>
+__device__ __forceinline__ Frame<R> frame_of(const FusedDesc& d, int dir) {
+    Frame<R> f;
+    f.n = {R(d.fn[dir][0]), R(d.fn[dir][1]), R(d.fn[dir][2])};
+    f.t1 = {R(d.ft1[dir][0]), R(d.ft1[dir][1]), R(d.ft1[dir][2])};
+    f.t2 = {R(d.ft2[dir][0]), R(d.ft2[dir][1]), R(d.ft2[dir][2])};
+    return f;
+}
+
+__device__ __forceinline__ int find_block(const FusedDesc* descs, int nblocks, long long item) {
+    int lo = 0, hi = nblocks - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].item0 <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The fused stage.  stage 1: W=WA -> WB, writes dUdt0; stage 2: W=WB -> WA,
+// writes U0 (the end-of-step state).
+template <typename R, int FLUX, int TI, int TJ>
+__global__ void __launch_bounds__(TI* TJ)
+k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems, int kc,
+              SimDev* sim, GasConsts gas, FluxOpts o, int stage) {
+    if (sim->status != 0 || sim->finished) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using S = FusedSmem<R, TI, TJ>;
+    constexpr int PI = S::PI, PJ = S::PJ, FS = PI * PJ;
+    R* planes = reinterpret_cast<R*>(smem_raw);
+    R* Fi = planes + 4 * S::PLANE;              // [5][TJ][TI+1]
+    R* Fj = Fi + 5 * TJ * (TI + 1);             // [5][TJ+1][TI]
+    const int ti = threadIdx.x % TI, tj = threadIdx.x / TI;
+    const double dt = sim->dt_global;
+    int bad = 0;
+
+    for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int b = find_block(descs, nblocks, item);
+        const FusedDesc& d = descs[b];
+        long long local = item - d.item0;
+        const int kch = int(local % d.kchunks);
+        local /= d.kchunks;
+        const int tile_i = int(local % d.tiles_i), tile_j = int(local / d.tiles_i);
+        const int i0 = tile_i * TI, j0 = tile_j * TJ;
+        const int k0 = kch * kc, k1 = min(k0 + kc, d.nk);
+        const int i = i0 + ti, j = j0 + tj;
+        const bool active = i < d.ni && j < d.nj;
+        const size_t nc = size_t(d.ni) * d.nj * d.nk;
+        const R* __restrict__ Win = static_cast<const R*>(stage == 1 ? d.WA : d.WB);
+        R* __restrict__ Wout = static_cast<R*>(stage == 1 ? d.WB : d.WA);
+        const int use_a0 = (stage == 1) ? *d.use_a0 : 0;
+
+        // l2r2_prepare with the (uniform) cell lengths of each direction
+        L2R2<R> w[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) w[q].prepare(R(d.len[q]), R(d.len[q]), R(d.len[q]), R(d.len[q]));
+        const Frame<R> fr0 = frame_of<R>(d, 0), fr1 = frame_of<R>(d, 1), fr2 = frame_of<R>(d, 2);
+
+        // prologue: planes k0-2 .. k0+1
+        __syncthreads();
+        for (int kk = k0 - 2; kk <= k0 + 1; ++kk)
+            load_plane<R, TI, TJ>(d, Win, use_a0, gas, planes + ((kk + 8) & 3) * S::PLANE, i0, j0, kk);
+        __syncthreads();
+        R Fbot[5];
+        const int coff = (tj + 2) * PI + (ti + 2);
+        if (active) {
+            Prim<R, 1> c0, c1, c2, c3;
+            get_cell(planes + ((k0 - 2 + 8) & 3) * S::PLANE, coff, FS, gas, c0);
+            get_cell(planes + ((k0 - 1 + 8) & 3) * S::PLANE, coff, FS, gas, c1);
+            get_cell(planes + ((k0 + 8) & 3) * S::PLANE, coff, FS, gas, c2);
+            get_cell(planes + ((k0 + 1 + 8) & 3) * S::PLANE, coff, FS, gas, c3);
+            face_flux<R, FLUX>(c0, c1, c2, c3, w[2], fr2, o, Fbot);
+        }
+        __syncthreads();  // plane k0-2 is overwritten by the first load below
+        for (int k = k0; k < k1; ++k) {
+            // plane k+2 replaces plane k-2 (not read since the previous iteration)
+            load_plane<R, TI, TJ>(d, Win, use_a0, gas, planes + ((k + 2 + 8) & 3) * S::PLANE, i0, j0, k + 2);
+            __syncthreads();
+            const R* pk = planes + ((k + 8) & 3) * S::PLANE;
+            // i-faces of plane k: (TI+1) x TJ, face fi is the west face of cell i0+fi
+            for (int f = threadIdx.x; f < (TI + 1) * TJ; f += blockDim.x) {
+                const int fi = f % (TI + 1), fj = f / (TI + 1);
+                if (i0 + fi > d.ni || j0 + fj >= d.nj) continue;
+                const int off = (fj + 2) * PI + fi;
+                Prim<R, 1> a0, a1, a2, a3;
+                get_cell(pk, off, FS, gas, a0);
+                get_cell(pk, off + 1, FS, gas, a1);
+                get_cell(pk, off + 2, FS, gas, a2);
+                get_cell(pk, off + 3, FS, gas, a3);
+                R F[5];
+                face_flux<R, FLUX>(a0, a1, a2, a3, w[0], fr0, o, F);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) Fi[(v * TJ + fj) * (TI + 1) + fi] = F[v];
+            }
+            // j-faces of plane k: TI x (TJ+1), face fj is the south face of cell j0+fj
+            for (int f = threadIdx.x; f < TI * (TJ + 1); f += blockDim.x) {
+                const int fi = f % TI, fj = f / TI;
+                if (i0 + fi >= d.ni || j0 + fj > d.nj) continue;
+                const int off = fj * PI + (fi + 2);
+                Prim<R, 1> a0, a1, a2, a3;
+                get_cell(pk, off, FS, gas, a0);
+                get_cell(pk, off + PI, FS, gas, a1);
+                get_cell(pk, off + 2 * PI, FS, gas, a2);
+                get_cell(pk, off + 3 * PI, FS, gas, a3);
+                R F[5];
+                face_flux<R, FLUX>(a0, a1, a2, a3, w[1], fr1, o, F);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) Fj[(v * (TJ + 1) + fj) * TI + fi] = F[v];
+            }
+            // k-face on top of cell k, from planes k-1 .. k+2 of this column
+            R Ftop[5];
+            if (active) {
+                Prim<R, 1> c0, c1, c2, c3;
+                get_cell(planes + ((k - 1 + 8) & 3) * S::PLANE, coff, FS, gas, c0);
+                get_cell(pk, coff, FS, gas, c1);
+                get_cell(planes + ((k + 1 + 8) & 3) * S::PLANE, coff, FS, gas, c2);
+                get_cell(planes + ((k + 2 + 8) & 3) * S::PLANE, coff, FS, gas, c3);
+                face_flux<R, FLUX>(c0, c1, c2, c3, w[2], fr2, o, Ftop);
+            }
+            __syncthreads();
+            if (active) {
+                // time_derivatives: faces north, east, south, west, top, bottom
+                const double aN = d.area[1], aE = d.area[0], aT = d.area[2];
+                double integral[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    double s = 0.0;
+                    s -= double(Fj[(v * (TJ + 1) + tj + 1) * TI + ti]) * (1.0 * aN);
+                    s -= double(Fi[(v * TJ + tj) * (TI + 1) + ti + 1]) * (1.0 * aE);
+                    s -= double(Fj[(v * (TJ + 1) + tj) * TI + ti]) * (-1.0 * aN);
+                    s -= double(Fi[(v * TJ + tj) * (TI + 1) + ti]) * (-1.0 * aE);
+                    s -= double(Ftop[v]) * (1.0 * aT);
+                    s -= double(Fbot[v]) * (-1.0 * aT);
+                    integral[v] = s;
+                }
+                const double vol_inv = 1.0 / d.vol;
+                const size_t c = (size_t(k) * d.nj + j) * d.ni + i;
+                double Un[5];
+                if (stage == 1) {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) {
+                        const double d0 = vol_inv * integral[v];
+                        d.dUdt0[v * nc + c] = d0;
+                        Un[v] = d.U0[v * nc + c] + dt * 1.0 * d0;
+                    }
+                } else {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) {
+                        const double d1 = vol_inv * integral[v];
+                        Un[v] = d.U0[v * nc + c] + dt * (0.5 * d.dUdt0[v * nc + c] + 0.5 * d1);
+                    }
+                }
+                // decode_conserved (fvcell.d:563-732), ideal gas
+                bool ok = true;
+                double rho = Un[0], vx = 0.0, vy = 0.0, vz = 0.0, u = 0.0, p = 0.0, T = 0.0, a = 0.0;
+                if (!(Un[0] > 0.0)) {
+                    if (atomicCAS(&sim->status, 0, -5) == 0) sim->status_step = sim->step;
+                    ok = false;
+                } else {
+                    const double dinv = 1.0 / rho;
+                    vx = Un[1] * dinv; vy = Un[2] * dinv; vz = Un[3] * dinv;
+                    u = Un[4] * dinv;
+                    const double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
+                    u -= ke;
+                    if (!ideal_rhou<double>(gas, rho, u, p, T)) {
+                        T = 200.0;
+                        p = rho * gas.Rgas * T;
+                        u = gas.Cv * T;
+                        Un[0] = rho;
+                        Un[1] = rho * vx; Un[2] = rho * vy; Un[3] = rho * vz;
+                        const double ke2 = 0.5 * (vx * vx + vy * vy + vz * vz);
+                        Un[4] = rho * (u + ke2);
+                    }
+                    a = ideal_sound_speed<double>(gas, T);
+                }
+                Wout[0 * nc + c] = R(rho);
+                Wout[1 * nc + c] = R(vx); Wout[2 * nc + c] = R(vy); Wout[3 * nc + c] = R(vz);
+                Wout[4 * nc + c] = R(u);
+                if (stage == 2) {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) d.U0[v * nc + c] = Un[v];
+                }
+                // FlowState.check_data (flowstate.d:345-388)
+                if (!isfinite(rho) || rho < 0.0) ok = false;
+                if (!isfinite(T) || T < 1.01) ok = false;
+                if (!isfinite(p) || !isfinite(a)) ok = false;
+                if (fabs(vx) > 30000.0 || fabs(vy) > 30000.0 || fabs(vz) > 30000.0) ok = false;
+                if (T > 50000.0) ok = false;
+                if (!ok) ++bad;
+#pragma unroll
+                for (int v = 0; v < 5; ++v) Fbot[v] = Ftop[v];
+            }
+            __syncthreads();
+        }
+    }
+    if (stage == 2 && blockIdx.x == 0 && threadIdx.x == 0) {
+        // from now on the sound speed comes from the decoded state
+        for (int b = 0; b < nblocks; ++b) *descs[b].use_a0 = 0;
+    }
+    if (bad) atomicAdd(&sim->bad_cells, bad);
+}
+
+// signal_frequency + block min/max for the fused layout (fvcell.d:1624-1705,
+// fluidblock.d:776-862).  One launch over all fused blocks: blockIdx.y picks
+// the block, a warp reduction precedes one atomic per warp.
+template <typename R>
+__global__ void k_fused_dt(const FusedDesc* __restrict__ descs, SimDev* sim, GasConsts gas,
+                           double cfl_value, const double* dt_current_p) {
+    if (sim && (sim->status != 0 || sim->finished)) return;
+    const FusedDesc& d = descs[blockIdx.y];
+    const double dt_current = *dt_current_p;
+    const long long nc = (long long)d.ni * d.nj * d.nk;
+    const R* W = static_cast<const R*>(d.WA);
+    const V3<double> nN{d.fn[1][0], d.fn[1][1], d.fn[1][2]};
+    const V3<double> nE{d.fn[0][0], d.fn[0][1], d.fn[0][2]};
+    const V3<double> nT{d.fn[2][0], d.fn[2][1], d.fn[2][2]};
+    double dmin = DBL_MAX, cmax = 0.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
+         c += (long long)gridDim.x * blockDim.x) {
+        V3<double> v{double(W[1 * nc + c]), double(W[2 * nc + c]), double(W[3 * nc + c])};
+        double a;
+        if (*d.use_a0) {
+            a = d.A0[c];
+        } else {
+            double T = double(W[4 * nc + c]) * gas.Cvinv;
+            a = sqrt(gas.gamma * gas.Rgas * T);
+        }
+        const double un_N = fabs(dot3(v, nN));
+        const double un_E = fabs(dot3(v, nE));
+        const double un_T = fabs(dot3(v, nT));
+        double signal = 0.0;
+        signal = fmax(signal, (un_N + a) / d.len[1]);
+        signal = fmax(signal, (un_E + a) / d.len[0]);
+        signal = fmax(signal, (un_T + a) / d.len[2]);
+        dmin = fmin(dmin, cfl_value / signal);
+        cmax = fmax(cmax, dt_current * signal);
+        if (c == nc - 1) d.acc[2] = dbits(signal);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
+        cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&d.acc[0], dbits(dmin));
+        atomicMax(&d.acc[1], dbits(cmax));
+    }
+}
+
+}  // namespace e4c

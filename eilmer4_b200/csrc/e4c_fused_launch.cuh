@@ -1,0 +1,134 @@
+// e4c_fused_launch.cuh -- instantiations and launchers of the fused kernels
+// for one arithmetic type (included by e4c_fused.cu with double and by
+// e4c_fused32.cu with float; each file is its own translation unit with its
+// own floating-point contract).
+#pragma once
+
+#include "e4c_fused.cuh"
+
+#ifndef E4C_FUSED_R
+#error "define E4C_FUSED_R (double or float) before including this file"
+#endif
+
+namespace e4c {
+namespace E4C_FUSED_NS {
+
+using RT = E4C_FUSED_R;
+
+template <int FLUX, int TI, int TJ>
+static int launch_one(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o,
+                      int stage, cudaStream_t s) {
+    constexpr size_t smem = FusedSmem<RT, TI, TJ>::bytes();
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_fused_stage<RT, FLUX, TI, TJ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        attr_set = true;
+    }
+    k_fused_stage<RT, FLUX, TI, TJ><<<L.grid, TI * TJ, smem, s>>>(
+        static_cast<const FusedDesc*>(L.descs), L.nblocks, L.nitems, L.kc, sim, gas, o, stage);
+    return 0;
+}
+
+template <int FLUX, int TI, int TJ>
+static int occupancy_one() {
+    constexpr size_t smem = FusedSmem<RT, TI, TJ>::bytes();
+    cudaFuncSetAttribute(k_fused_stage<RT, FLUX, TI, TJ>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_stage<RT, FLUX, TI, TJ>, TI * TJ,
+                                                      smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+// Tile shapes available to the autotuner: (TI, TJ).
+#define E4C_TILES(X) X(32, 8) X(32, 4) X(16, 8) X(64, 4) X(16, 16)
+
+int fused_stage(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o,
+                int stage, cudaStream_t s) {
+#define E4C_CASE(TI_, TJ_)                                                        \
+    if (L.ti == TI_ && L.tj == TJ_) {                                            \
+        if (o.flux == 1) return launch_one<1, TI_, TJ_>(L, sim, gas, o, stage, s); \
+        return launch_one<0, TI_, TJ_>(L, sim, gas, o, stage, s);                  \
+    }
+    E4C_TILES(E4C_CASE)
+#undef E4C_CASE
+    return -1;
+}
+
+int fused_occupancy(int flux, int ti, int tj) {
+#define E4C_CASE(TI_, TJ_)                                          \
+    if (ti == TI_ && tj == TJ_) {                                  \
+        return flux == 1 ? occupancy_one<1, TI_, TJ_>() : occupancy_one<0, TI_, TJ_>(); \
+    }
+    E4C_TILES(E4C_CASE)
+#undef E4C_CASE
+    return 0;
+}
+
+void fused_dt(const void* descs, int nfused, int gx, SimDev* sim, const GasConsts& gas,
+              double cfl_value, const double* dt_current, cudaStream_t s) {
+    k_fused_dt<RT><<<dim3(gx, nfused), 256, 0, s>>>(static_cast<const FusedDesc*>(descs), sim, gas,
+                                                   cfl_value, dt_current);
+}
+
+// prim (rho, vx, vy, vz, p, T, u, a) -> W (R), A0 and the encoded U0
+// (encode_conserved, fvcell.d:494-560)
+__global__ void k_fused_upload(const double* prim, size_t nc, RT* W, double* A0, double* U0) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < nc;
+         c += size_t(gridDim.x) * blockDim.x) {
+        const double rho = prim[0 * nc + c], vx = prim[1 * nc + c], vy = prim[2 * nc + c];
+        const double vz = prim[3 * nc + c], u = prim[6 * nc + c], a = prim[7 * nc + c];
+        W[0 * nc + c] = RT(rho); W[1 * nc + c] = RT(vx); W[2 * nc + c] = RT(vy);
+        W[3 * nc + c] = RT(vz); W[4 * nc + c] = RT(u);
+        A0[c] = a;
+        U0[0 * nc + c] = rho;
+        U0[1 * nc + c] = rho * vx;
+        U0[2 * nc + c] = rho * vy;
+        U0[3 * nc + c] = rho * vz;
+        const double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
+        U0[4 * nc + c] = rho * (u + ke);
+    }
+}
+
+// W (R) -> prim with p, T, a from update_thermo_from_rhou + update_sound_speed
+__global__ void k_fused_download(const RT* W, const double* A0, const int* use_a0,
+                                 const double* U0, size_t nc, GasConsts gas, double* prim,
+                                 double* cons) {
+    const int a0 = *use_a0;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < nc;
+         c += size_t(gridDim.x) * blockDim.x) {
+        if (prim) {
+            const double rho = double(W[0 * nc + c]), u = double(W[4 * nc + c]);
+            const double T = u * gas.Cvinv;
+            prim[0 * nc + c] = rho;
+            prim[1 * nc + c] = double(W[1 * nc + c]);
+            prim[2 * nc + c] = double(W[2 * nc + c]);
+            prim[3 * nc + c] = double(W[3 * nc + c]);
+            prim[4 * nc + c] = rho * gas.Rgas * T;
+            prim[5 * nc + c] = T;
+            prim[6 * nc + c] = u;
+            prim[7 * nc + c] = a0 ? A0[c] : sqrt(gas.gamma * gas.Rgas * T);
+        }
+        if (cons)
+            for (int v = 0; v < 5; ++v) cons[v * nc + c] = U0[v * nc + c];
+    }
+}
+
+void fused_upload(const double* prim, size_t nc, void* W, double* A0, double* U0, cudaStream_t s) {
+    int g = int((nc + 255) / 256);
+    if (g > 148 * 32) g = 148 * 32;
+    k_fused_upload<<<g, 256, 0, s>>>(prim, nc, static_cast<RT*>(W), A0, U0);
+}
+
+void fused_download(const void* W, const double* A0, const int* use_a0, const double* U0,
+                    size_t nc, const GasConsts& gas, double* prim, double* cons, cudaStream_t s) {
+    int g = int((nc + 255) / 256);
+    if (g > 148 * 32) g = 148 * 32;
+    k_fused_download<<<g, 256, 0, s>>>(static_cast<const RT*>(W), A0, use_a0, U0, nc, gas, prim,
+                                        cons);
+}
+
+}  // namespace E4C_FUSED_NS
+}  // namespace e4c

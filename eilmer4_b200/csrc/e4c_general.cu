@@ -632,9 +632,9 @@ __global__ void k_dt_reset(unsigned long long* acc, int nb) {
 }
 
 // The simcore.d:1347-1452 logic over all blocks (one thread).
-__global__ void k_dt_finalize(SimDev* sim, const unsigned long long* acc, int nb, double cfl_allow,
-                              double dt_init, double dt_max, int check_cfl, int step0,
-                              double* out_dt_allow, double* out_cfl_max) {
+__global__ void k_dt_finalize(SimDev* sim, const unsigned long long* acc, const int* hlist, int nb,
+                              double cfl_allow, double dt_init, double dt_max, int check_cfl,
+                              int step0, double* out_dt_allow, double* out_cfl_max) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     if (sim && (sim->status != 0 || sim->finished)) return;
     if (check_cfl < 0) {  // take SimState.step from the device-side loop
@@ -643,9 +643,10 @@ __global__ void k_dt_finalize(SimDev* sim, const unsigned long long* acc, int nb
     }
     double dt_allow = DBL_MAX, cfl_max = 0.0;
     for (int q = 0; q < nb; ++q) {
-        double d = __longlong_as_double(static_cast<long long>(acc[3 * q + 0]));
-        double c = __longlong_as_double(static_cast<long long>(acc[3 * q + 1]));
-        double last_signal = __longlong_as_double(static_cast<long long>(acc[3 * q + 2]));
+        const int h = hlist[q];
+        double d = __longlong_as_double(static_cast<long long>(acc[3 * h + 0]));
+        double c = __longlong_as_double(static_cast<long long>(acc[3 * h + 1]));
+        double last_signal = __longlong_as_double(static_cast<long long>(acc[3 * h + 2]));
         if (check_cfl && (c < 0.0 || c > cfl_allow)) {
             c = 0.5 * cfl_allow;
             d = c / last_signal;
@@ -762,11 +763,42 @@ void launch_dt(const BlockView& b, const SimDev* sim, double cfl_value, const do
     k_dt<<<grid_for(n, 256), 256, 0, s>>>(b, sim, cfl_value, dt_current, acc);
 }
 
-void launch_dt_finalize(SimDev* sim, const unsigned long long* acc, int nb, double cfl_allow,
-                        double dt_init, double dt_max, int check_cfl, int step0,
+void launch_dt_finalize(SimDev* sim, const unsigned long long* acc, const int* hlist, int nb,
+                        double cfl_allow, double dt_init, double dt_max, int check_cfl, int step0,
                         double* out_dt_allow, double* out_cfl_max, cudaStream_t s) {
-    k_dt_finalize<<<1, 32, 0, s>>>(sim, acc, nb, cfl_allow, dt_init, dt_max, check_cfl, step0,
-                                   out_dt_allow, out_cfl_max);
+    k_dt_finalize<<<1, 32, 0, s>>>(sim, acc, hlist, nb, cfl_allow, dt_init, dt_max, check_cfl,
+                                   step0, out_dt_allow, out_cfl_max);
+}
+
+// Is the geometry uniform: every interior cell's (vol, iLen, jLen, kLen) and
+// every face's (n, t1, t2, area) of a direction identical to the first one?
+__global__ void k_check_uniform(BlockView b, int* flag) {
+    const size_t c0 = pidx(b, b.imin, b.jmin, b.kmin);
+    const long long nc = (long long)b.ni * b.nj * b.nk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nc;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        for (int q = 0; q < 4; ++q)
+            if (b.cgeom[q * b.npad + c] != b.cgeom[q * b.npad + c0]) atomicOr(flag, 1);
+        // the west, south and bottom faces of the cell, plus the far boundary faces
+        const double* fgs[3] = {b.fgi, b.fgj, b.fgk};
+        const size_t far[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
+        const bool at_far[3] = {i == b.imax, j == b.jmax, k == b.kmax};
+        for (int d = 0; d < b.dim; ++d)
+            for (int q = 0; q < 10; ++q) {
+                const double ref = fgs[d][q * b.npad + c0];
+                if (fgs[d][q * b.npad + c] != ref) atomicOr(flag, 1);
+                if (at_far[d] && fgs[d][q * b.npad + far[d]] != ref) atomicOr(flag, 1);
+            }
+    }
+}
+
+void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_check_uniform<<<grid_for(n, 256), 256, 0, s>>>(b, flag);
 }
 
 void launch_reset_bad(SimDev* sim, cudaStream_t s) { k_reset_bad<<<1, 1, 0, s>>>(sim); }

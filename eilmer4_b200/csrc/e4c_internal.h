@@ -12,42 +12,12 @@
 
 namespace e4c {
 
-// Constants of a block whose geometry is exactly uniform and axis aligned
-// (every cell and every face of a direction has the same bits).
-struct UniformGeom {
-    double vol;
-    double len[3];          // iLength, jLength, kLength
-    double area[3];         // face area per direction
-    double n[3][3], t1[3][3], t2[3][3];  // face frame per direction
-};
-
-// Device view of a block on the fused uniform path (e4c_fused.cu).
-struct FusedView {
-    int ni, nj, nk;
-    int bc[6];
-    size_t ncell;           // ni*nj*nk, interior only, i fastest
-    // primitive state rho, vx, vy, vz, u (FP64) -- 5 x ncell
-    double* W;
-    // sound speed as uploaded; used until the first decode, then unused
-    double* a0;
-    int use_a0;
-    // primitive state in FP32 for the FP32-flux form -- 5 x ncell
-    float* Wf;
-    double* U0;             // 5 x ncell
-    double* dUdt0;          // 5 x ncell
-    double* Wn;             // second primitive buffer (ping-pong), 5 x ncell
-    float* Wfn;
-    UniformGeom g;
-    double inflow[8];
-};
-
 struct BlockHost {
-    BlockView v{};
+    BlockView v{};          // general path (device arrays unset on the fused path)
     size_t ncell = 0;
     size_t nprim_vars = 8;
     bool fused = false;
-    FusedView f{};
-    int wsel = 0;           // which primitive buffer holds the current state (fused path)
+    FusedDesc f{};          // fused path: storage and uniform geometry
 };
 
 struct GraphSlot {
@@ -81,11 +51,27 @@ struct Ctx {
     std::vector<BlockHost> blocks;
     GraphSlot graphs[2];    // [0] plain step, [1] step with dt check
     int host_step = 0;
+    // fused path: descriptors of every fused block, rebuilt when blocks change
+    FusedDesc* d_descs = nullptr;
+    int descs_cap = 0;
+    int nfused = 0;
+    long long fused_items = 0;
+    bool descs_valid = false;
+    int tile_ti = 32, tile_tj = 8, tile_kc = 32;
+    int fused_grid = 0;
+    int max_cells_fused = 0;
+    // device list of block handles for the dt reduction
+    int* d_hlist = nullptr;
+    int hlist_cap = 0;
     long long launches = 0;   // kernels enqueued (graph replays add their node count)
     Profiler prof;
     std::string last_error;
 
     void* dalloc(size_t bytes);
+    void dfree(void* p);
+    int prepare_fused();
+    int set_hlist(const std::vector<int>& hs);
+    bool uses_all_fused(const std::vector<int>& hs) const;
     void release();
     void reset_graphs();
     int build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
@@ -94,14 +80,13 @@ struct Ctx {
     int run_step(const std::vector<int>& hs, bool dt_check);
     void enqueue_stage(const std::vector<int>& hs, int stage, int final_stage);
     void enqueue_gasdynamic(const std::vector<int>& hs);
-    void enqueue_dt(const std::vector<int>& hs, const double* dt_current, int check_cfl, int step0,
-                    SimDev* sim, double* out);
+    void enqueue_dt(const std::vector<int>& hs, const int* d_hl, const double* dt_current,
+                    int check_cfl, int step0, SimDev* sim, double* out);
     std::vector<int> all_blocks() const;
     // fused uniform path
-    void fused_stage(const BlockHost& b, int stage, int final_stage);
-    void fused_dt(const BlockHost& b, SimDev* sim, const double* dt_current,
-                  unsigned long long* acc);
-    void fused_upload(BlockHost& b, const double* prim);
+    void fused_stage_all(int stage);
+    void fused_dt_all(SimDev* sim, const double* dt_current);
+    int fused_upload(BlockHost& b, const double* prim);
     void fused_download(const BlockHost& b, double* prim, double* cons);
 };
 

@@ -25,14 +25,44 @@ void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int d
 void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
                    int final_stage, cudaStream_t s);
 void launch_dt_reset(unsigned long long* acc, int nb, cudaStream_t s);
+// dt accumulators are indexed by block handle; hlist lists the handles to reduce over
 void launch_dt(const BlockView& b, const SimDev* sim, double cfl_value, const double* dt_current,
                unsigned long long* acc, cudaStream_t s);
-void launch_dt_finalize(SimDev* sim, const unsigned long long* acc, int nb, double cfl_allow,
-                        double dt_init, double dt_max, int check_cfl, int step0,
+void launch_dt_finalize(SimDev* sim, const unsigned long long* acc, const int* hlist, int nb,
+                        double cfl_allow, double dt_init, double dt_max, int check_cfl, int step0,
                         double* out_dt_allow, double* out_cfl_max, cudaStream_t s);
 void launch_reset_bad(SimDev* sim, cudaStream_t s);
 void launch_stage_check(SimDev* sim, int max_invalid, cudaStream_t s);
 void launch_end_step(SimDev* sim, cudaStream_t s);
 void launch_begin_run(SimDev* sim, double max_time, cudaStream_t s);
+// compare every cell's and face's geometry with the first one; flag[0] != 0 if any differs
+void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
+
+// fused uniform path (e4c_fused.cu: FP64, e4c_fused32.cu: FP32 flux)
+struct FusedLaunch {
+    const void* descs;      // device array of FusedDesc
+    int nblocks;
+    long long nitems;       // (block, tile, k-chunk) work items
+    int kc;                 // k-chunk length
+    int ti, tj;             // tile shape
+    int grid;               // persistent CTAs
+};
+
+#define E4C_DECLARE_FUSED(NS)                                                                \
+    namespace NS {                                                                           \
+    int fused_stage(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o, \
+                    int stage, cudaStream_t s);                                              \
+    int fused_occupancy(int flux, int ti, int tj);                                           \
+    void fused_dt(const void* descs, int nfused, int gx, SimDev* sim, const GasConsts& gas,  \
+                  double cfl_value, const double* dt_current, cudaStream_t s);              \
+    void fused_upload(const double* prim, size_t nc, void* W, double* A0, double* U0,        \
+                      cudaStream_t s);                                                       \
+    void fused_download(const void* W, const double* A0, const int* use_a0, const double* U0, \
+                        size_t nc, const GasConsts& gas, double* prim, double* cons,        \
+                        cudaStream_t s);                                                     \
+    }
+E4C_DECLARE_FUSED(f64)
+E4C_DECLARE_FUSED(f32)
+#undef E4C_DECLARE_FUSED
 
 }  // namespace e4c

@@ -65,4 +65,26 @@ struct SimDev {
     int pad_;
 };
 
+// Per-block descriptor of the fused uniform path (device array, one entry per
+// fused block).  Geometry constants are those every cell and face of the
+// block shares; arrays are SoA over interior cells, i fastest.
+struct FusedDesc {
+    int ni, nj, nk;
+    int tiles_i, tiles_j, kchunks;
+    long long item0;            // first work item of this block
+    int bc[6];
+    int* use_a0;                // -> 1 while the uploaded sound speed is still in use
+    void* WA;                   // primitive state rho, vx, vy, vz, u (5 x ncell), R-typed
+    void* WB;                   // second buffer: stage 1 writes it, stage 2 reads it
+    const double* A0;           // uploaded sound speed (ncell)
+    double* U0;                 // conserved state (5 x ncell)
+    double* dUdt0;              // stage-1 derivative (5 x ncell)
+    unsigned long long* acc;    // dt accumulators of this block (3)
+    double vol;
+    double len[3];
+    double area[3];
+    double fn[3][3], ft1[3][3], ft2[3][3];
+    double inflow[6];           // rho, vx, vy, vz, u, a
+};
+
 }  // namespace e4c

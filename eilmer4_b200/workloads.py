@@ -117,12 +117,16 @@ class Workload:
         return sum(b.ncell for b in self.blocks)
 
 
-def box_vertices(ni, nj, nk, lx, ly, lz, dimensions, origin=(0.0, 0.0, 0.0)):
-    """Vertices of a Cartesian box; x = origin + lx*(i/ni) like a parametric map."""
-    xs = origin[0] + lx * (np.arange(ni + 1, dtype=np.float64) / ni)
-    ys = origin[1] + ly * (np.arange(nj + 1, dtype=np.float64) / nj)
+def box_vertices(ni, nj, nk, lx, ly, lz, dimensions, origin=(0.0, 0.0, 0.0), spacing=None):
+    """Vertices of a Cartesian box; x = origin + lx*(i/ni) like a parametric map,
+    or x = origin + i*spacing when a cell spacing is given."""
+    def axis(n, L, o):
+        r = np.arange(n + 1, dtype=np.float64)
+        return o + (r * spacing if spacing is not None else L * (r / n))
+    xs = axis(ni, lx, origin[0])
+    ys = axis(nj, ly, origin[1])
     if dimensions == 3:
-        zs = origin[2] + lz * (np.arange(nk + 1, dtype=np.float64) / nk)
+        zs = axis(nk, lz, origin[2])
     else:
         zs = np.zeros(1)
     Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
@@ -210,7 +214,7 @@ def inflow_3d_block(ni, nj, nk, seed, spacing=None, mach=3.0, p_in=1.0e5, T_in=3
         lx, ly, lz = 1.0, 1.0, 1.0
     else:
         lx, ly, lz = ni * spacing, nj * spacing, nk * spacing
-    vtx = box_vertices(ni, nj, nk, lx, ly, lz, 3)
+    vtx = box_vertices(ni, nj, nk, lx, ly, lz, 3, spacing=spacing)
     centres = cell_centres(vtx, ni, nj, nk, 3)
     rho_in, u_in, a_in = gas.from_pT(p_in, T_in)
     vx_in = mach * float(a_in)

@@ -141,3 +141,81 @@ def test_bad_cells_reported(oracle, e4lib):
         assert ei.value.code == _lib.E4C_ERR_BAD_CELLS
     rc, *_ = run_oracle(oracle, wl, 3)
     assert rc == -4
+
+
+# --- fused uniform path (dyadic Cartesian blocks) ---------------------------
+
+def uniform_block(ni, nj, nk, seed, spacing=1.0 / 64.0, all_walls=False, swirl=False):
+    b = W.inflow_3d_block(ni, nj, nk, seed, spacing=spacing)
+    if all_walls:
+        b.bc = (W.BC_SLIP_WALL,) * 6
+    if swirl:
+        c = W.cell_centres(b.vtx, ni, nj, nk, 3)
+        b.prim[2] = 120.0 * np.sin(9.0 * c[:, 0] + 2.0 * c[:, 2])
+        b.prim[3] = -80.0 * np.cos(7.0 * c[:, 1] + 3.0 * c[:, 0])
+    return b
+
+
+def test_fused_path_selected_for_uniform_blocks(e4lib):
+    from eilmer4_b200.simcore import Simulation
+    wl = W.Workload("u", 3, flux_calculator="hllc")
+    wl.blocks.append(uniform_block(40, 24, 20, 3))
+    with Simulation.from_workload(wl) as sim:
+        sim.run(2)
+        prof = sim.profile(2)
+    assert prof["stage"][1] == 4 and prof["flux"][1] == 0, prof
+
+
+def test_fused_fp64_ausmdv_bitexact(oracle, e4lib):
+    wl = W.Workload("u", 3, flux_calculator="ausmdv")
+    wl.blocks.append(uniform_block(40, 24, 20, 5))
+    compare(oracle, wl, 30)
+
+
+def test_fused_fp64_hllc_partial_tiles(oracle, e4lib):
+    # odd extents exercise partial tiles in i, j and k chunks
+    wl = W.Workload("u", 3, flux_calculator="hllc")
+    wl.blocks.append(uniform_block(37, 19, 41, 9, spacing=1.0 / 32.0))
+    compare(oracle, wl, 25)
+
+
+def test_fused_slip_walls_every_face(oracle, e4lib):
+    wl = W.Workload("u", 3, flux_calculator="hllc")
+    wl.blocks.append(uniform_block(24, 20, 18, 13, all_walls=True, swirl=True))
+    compare(oracle, wl, 40)
+
+
+def test_fused_multiblock(oracle, e4lib):
+    wl = W.batched_blocks(nblocks=4, lo=10, hi=28, nsteps=20)
+    compare(oracle, wl, 20)
+
+
+def test_fused_dt_allow_and_step_calls(oracle, e4lib):
+    from eilmer4_b200.simcore import Simulation
+    wl = W.Workload("u", 3, flux_calculator="hllc")
+    wl.blocks.append(uniform_block(32, 16, 16, 21))
+    with Simulation.from_workload(wl) as sim:
+        dt_allow, _ = sim.dt_allow([0], 1.0e-3, False)
+        dt = min(1.0e-3, dt_allow)
+        assert sim.gasdynamic_step([0], dt) == 0
+        gp, gc = sim.download(0)
+    _, _, _, odt, oout = run_oracle(oracle, wl, 1)
+    assert dt == odt
+    assert_same(gc, oout[0][1], "conserved after one step")
+
+
+def test_fp32_flux_form_error_vs_fp64(oracle, e4lib):
+    """FP32 reconstruction/flux with FP64 accumulation and decode: relative
+    density error against the FP64 oracle stays below 1e-5."""
+    wl = W.Workload("u", 3, flux_calculator="hllc")
+    wl.blocks.append(uniform_block(48, 32, 32, 17))
+    nsteps = 40
+    _, ost, otime, _, oout = run_oracle(oracle, wl, nsteps)
+    info, gst, gtime, _, gout = run_gpu(wl, nsteps, precision="fp32_flux")
+    assert gst == ost
+    assert abs(gtime - otime) / otime < 1e-5
+    rho_g, rho_o = gout[0][1][0], oout[0][1][0]
+    err = np.max(np.abs(rho_g - rho_o) / np.abs(rho_o))
+    assert err < 1.0e-5, err
+    E_g, E_o = gout[0][1][4], oout[0][1][4]
+    assert np.max(np.abs(E_g - E_o) / np.abs(E_o)) < 1.0e-5
