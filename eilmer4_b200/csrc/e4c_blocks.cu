@@ -124,6 +124,16 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
                 E4C_CUDA(cudaMemcpy(&fg[d][q], fgs[d] + q * np + c0, sizeof(double),
                                     cudaMemcpyDeviceToHost));
         f.vol = g[0];
+        // the fused kernel applies the face frames as permutations: require
+        // n, t1, t2 = (x,y,z), (y,z,x), (z,x,y) for the i, j, k faces
+        bool axis = true;
+        for (int d = 0; d < 3; ++d)
+            for (int q = 0; q < 3; ++q) {
+                const double en = (q == d) ? 1.0 : 0.0;
+                const double e1 = (q == (d + 1) % 3) ? 1.0 : 0.0;
+                const double e2 = (q == (d + 2) % 3) ? 1.0 : 0.0;
+                if (fg[d][q] != en || fg[d][3 + q] != e1 || fg[d][6 + q] != e2) axis = false;
+            }
         for (int d = 0; d < 3; ++d) {
             f.len[d] = g[1 + d];
             f.area[d] = fg[d][9];
@@ -133,9 +143,17 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
                 f.ft2[d][q] = fg[d][6 + q];
             }
         }
+        if (!axis) {
+            if (cfg.precision == E4C_PREC_FP32_FLUX)
+                return fail(E4C_ERR_UNSUPPORTED, "the FP32-flux form needs an axis-aligned Cartesian block");
+            out.fused = false;
+        }
         // inflow FlowState: rho, vx, vy, vz, u, a
         f.inflow[0] = inflow[0]; f.inflow[1] = inflow[1]; f.inflow[2] = inflow[2];
         f.inflow[3] = inflow[3]; f.inflow[4] = inflow[6]; f.inflow[5] = inflow[7];
+    }
+    if (out.fused) {
+        FusedDesc& f = out.f;
         dfree(geom);
         const size_t nc = out.ncell;
         const size_t rsz = (cfg.precision == E4C_PREC_FP32_FLUX) ? sizeof(float) : sizeof(double);

@@ -106,8 +106,11 @@ __device__ __forceinline__ void load_plane(const FusedDesc& d, const R* __restri
                 a = sqrt(R(gas.gamma) * R(gas.Rgas) * T);
             }
             if (type == 0) {
-                const int dir = (which == WEST || which == EAST) ? 0 : ((which == SOUTH || which == NORTH) ? 1 : 2);
-                reflect_normal<R>(vx, vy, vz, d.fn[dir], d.ft1[dir], d.ft2[dir]);
+                // reflect_normal_velocity (ghost_cell.d:34-44) with an axis frame:
+                // the normal component changes sign
+                if (which == WEST || which == EAST) vx = -vx;
+                else if (which == SOUTH || which == NORTH) vy = -vy;
+                else vz = -vz;
             }
         }
         R* p = plane + lj * PI + li;
@@ -138,18 +141,19 @@ __device__ __forceinline__ void cell_pressure(Prim<R, 1>& s, const GasConsts& ga
 }
 
 // Reconstruction + flux of one face from four cells (general-path semantics,
-// sfluidblock.d:2190-2344 with onedinterp.d:435-585 and fluxcalc.d:26-128).
-template <typename R, int FLUX>
+// sfluidblock.d:2190-2344 with onedinterp.d:435-585 and fluxcalc.d:26-128),
+// with the face frame of direction DIR applied as a permutation.
+template <typename R, int FLUX, int DIR>
 __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R, 1> sR0,
-                                          Prim<R, 1> sR1, const L2R2<R>& w, const Frame<R>& fr,
-                                          const FluxOpts& o, R* F) {
+                                          Prim<R, 1> sR1, const L2R2<R>& w, const FluxOpts& o,
+                                          R* F) {
     Prim<R, 1> Lf = sL0, Rt = sR0;
     if (o.order2) {
         if (o.local_frame) {
-            to_local(sL1.vel, fr.n, fr.t1, fr.t2);
-            to_local(sL0.vel, fr.n, fr.t1, fr.t2);
-            to_local(sR0.vel, fr.n, fr.t1, fr.t2);
-            to_local(sR1.vel, fr.n, fr.t1, fr.t2);
+            axis_to_local<DIR>(sL1.vel);
+            axis_to_local<DIR>(sL0.vel);
+            axis_to_local<DIR>(sR0.vel);
+            axis_to_local<DIR>(sR1.vel);
         }
         const bool lim = o.limiter, clip = o.clip;
         w.scalar(lim, clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
@@ -162,21 +166,39 @@ __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R
         R T;
         if (!ideal_rhou<R>(o.gas, Lf.rho, Lf.u, Lf.p, T)) { Lf = sL0; cell_pressure(Lf, o.gas); }
         if (!ideal_rhou<R>(o.gas, Rt.rho, Rt.u, Rt.p, T)) { Rt = sR0; cell_pressure(Rt, o.gas); }
-        if (o.local_frame) {
-            to_global(Lf.vel, fr.n, fr.t1, fr.t2);
-            to_global(Rt.vel, fr.n, fr.t1, fr.t2);
+        // transform back to the global frame (onedinterp.d:576-584) and into the
+        // face frame again (fluxcalc.d:50-52): together an identity here
+        if (!o.local_frame) {
+            axis_to_local<DIR>(Lf.vel);
+            axis_to_local<DIR>(Rt.vel);
         }
     } else {
         cell_pressure(Lf, o.gas);
         cell_pressure(Rt, o.gas);
+        axis_to_local<DIR>(Lf.vel);
+        axis_to_local<DIR>(Rt.vel);
     }
-    to_local(Lf.vel, fr.n, fr.t1, fr.t2);
-    to_local(Rt.vel, fr.n, fr.t1, fr.t2);
     if (FLUX == 1) hllc<R, 1, 0>(Lf, Rt, F);
     else ausmdv<R, 1, 0>(Lf, Rt, F);
     V3<R> m{F[1], F[2], F[3]};
-    to_global(m, fr.n, fr.t1, fr.t2);
+    axis_to_global<DIR>(m);
     F[1] = m.x; F[2] = m.y; F[3] = m.z;
+}
+
+// Face frames of a Cartesian block are exact cyclic unit permutations:
+// i-faces (x, y, z), j-faces (y, z, x), k-faces (z, x, y) as (n, t1, t2).
+// transform_to_local_frame / transform_to_global_frame with such a frame
+// reduce to a permutation: v.x*1 + v.y*0 + v.z*0 equals v.x up to the sign of
+// a zero, which no later operation turns into a different non-zero value.
+template <int DIR, typename R>
+__device__ __forceinline__ void axis_to_local(V3<R>& v) {
+    if (DIR == 1) { R t = v.x; v.x = v.y; v.y = v.z; v.z = t; }
+    if (DIR == 2) { R t = v.x; v.x = v.z; v.z = v.y; v.y = t; }
+}
+template <int DIR, typename R>
+__device__ __forceinline__ void axis_to_global(V3<R>& v) {
+    if (DIR == 1) { R t = v.z; v.z = v.y; v.y = v.x; v.x = t; }
+    if (DIR == 2) { R t = v.x; v.x = v.y; v.y = v.z; v.z = t; }
 }
 
 template <typename R>
@@ -235,7 +257,6 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
         L2R2<R> w[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) w[q].prepare(R(d.len[q]), R(d.len[q]), R(d.len[q]), R(d.len[q]));
-        const Frame<R> fr0 = frame_of<R>(d, 0), fr1 = frame_of<R>(d, 1), fr2 = frame_of<R>(d, 2);
 
         // prologue: planes k0-2 .. k0+1
         __syncthreads();
@@ -250,7 +271,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
             get_cell(planes + ((k0 - 1 + 8) & 3) * S::PLANE, coff, FS, gas, c1);
             get_cell(planes + ((k0 + 8) & 3) * S::PLANE, coff, FS, gas, c2);
             get_cell(planes + ((k0 + 1 + 8) & 3) * S::PLANE, coff, FS, gas, c3);
-            face_flux<R, FLUX>(c0, c1, c2, c3, w[2], fr2, o, Fbot);
+            face_flux<R, FLUX, 2>(c0, c1, c2, c3, w[2], o, Fbot);
         }
         __syncthreads();  // plane k0-2 is overwritten by the first load below
         for (int k = k0; k < k1; ++k) {
@@ -269,7 +290,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                 get_cell(pk, off + 2, FS, gas, a2);
                 get_cell(pk, off + 3, FS, gas, a3);
                 R F[5];
-                face_flux<R, FLUX>(a0, a1, a2, a3, w[0], fr0, o, F);
+                face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F);
 #pragma unroll
                 for (int v = 0; v < 5; ++v) Fi[(v * TJ + fj) * (TI + 1) + fi] = F[v];
             }
@@ -284,7 +305,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                 get_cell(pk, off + 2 * PI, FS, gas, a2);
                 get_cell(pk, off + 3 * PI, FS, gas, a3);
                 R F[5];
-                face_flux<R, FLUX>(a0, a1, a2, a3, w[1], fr1, o, F);
+                face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F);
 #pragma unroll
                 for (int v = 0; v < 5; ++v) Fj[(v * (TJ + 1) + fj) * TI + fi] = F[v];
             }
@@ -296,7 +317,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                 get_cell(pk, coff, FS, gas, c1);
                 get_cell(planes + ((k + 1 + 8) & 3) * S::PLANE, coff, FS, gas, c2);
                 get_cell(planes + ((k + 2 + 8) & 3) * S::PLANE, coff, FS, gas, c3);
-                face_flux<R, FLUX>(c0, c1, c2, c3, w[2], fr2, o, Ftop);
+                face_flux<R, FLUX, 2>(c0, c1, c2, c3, w[2], o, Ftop);
             }
             __syncthreads();
             if (active) {
