@@ -111,6 +111,9 @@ def load():
         "e4c_stream": ([], ctypes.c_void_p),
         "e4c_kernel_launches": ([], ctypes.c_longlong),
         "e4c_profile_steps": ([i, dp, ip], i),
+        "e4c_set_tile": ([i, i, i], i),
+        "e4c_get_tile": ([ip, ip, ip], i),
+        "e4c_autotune": ([i, ip, ip, ip, dp], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

@@ -31,7 +31,6 @@ UNITS = [
     ("e4c_api.cu", ["-fmad=false"]),
 ]
 
-HEADERS = ["e4c_physics.cuh", "e4c_types.h", "e4c_kernels.h", "e4c_internal.h"]
 
 
 def nvcc():
@@ -47,7 +46,8 @@ def _mtime(p):
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    hdr_time = max(_mtime(os.path.join(CSRC, h)) for h in HEADERS)
+    headers = [h for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
+    hdr_time = max(_mtime(os.path.join(CSRC, h)) for h in headers)
     hdr_time = max(hdr_time, _mtime(os.path.join(ROOT, "include", "e4cuda.h")))
     objs = []
     rebuilt = False

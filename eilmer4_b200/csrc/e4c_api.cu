@@ -481,6 +481,128 @@ int e4c_profile_steps(int nsteps, double* ms, int* launches) {
     return E4C_OK;
 }
 
+static bool tile_available(int ti, int tj) {
+    const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}};
+    for (auto& t : tiles)
+        if (t[0] == ti && t[1] == tj) return true;
+    return false;
+}
+
+int e4c_set_tile(int ti, int tj, int kc) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!tile_available(ti, tj) || kc < 1) return fail(E4C_ERR_ARG, "tile shape not available");
+    c.tile_ti = ti;
+    c.tile_tj = tj;
+    c.tile_kc = kc;
+    c.descs_valid = false;
+    c.reset_graphs();
+    return E4C_OK;
+}
+
+int e4c_get_tile(int* ti, int* tj, int* kc) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (ti) *ti = c.tile_ti;
+    if (tj) *tj = c.tile_tj;
+    if (kc) *kc = c.tile_kc;
+    return E4C_OK;
+}
+
+int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
+    if (nsteps < 1) return fail(E4C_ERR_ARG, "nsteps must be >= 1");
+    int rc = c.prepare_fused();
+    if (rc != E4C_OK) return rc;
+    if (c.nfused == 0) {
+        if (ti) *ti = c.tile_ti;
+        if (tj) *tj = c.tile_tj;
+        if (kc) *kc = c.tile_kc;
+        if (ms_per_step) *ms_per_step = 0.0;
+        return E4C_OK;
+    }
+    // snapshot everything a step changes: the primitive and conserved state of
+    // every block, the initial-sound-speed flags and the device clock
+    struct Saved { void* dst; const void* src; size_t bytes; };
+    std::vector<Saved> saved;
+    const size_t rsz = (c.cfg.precision == E4C_PREC_FP32_FLUX) ? sizeof(float) : sizeof(double);
+    for (BlockHost& b : c.blocks) {
+        if (b.fused) {
+            saved.push_back({nullptr, b.f.WA, 5 * b.ncell * rsz});
+            saved.push_back({nullptr, b.f.U0, 5 * b.ncell * sizeof(double)});
+            saved.push_back({nullptr, b.f.use_a0, sizeof(int)});
+        } else {
+            saved.push_back({nullptr, b.v.W, W_NBASE * b.v.npad * sizeof(double)});
+            saved.push_back({nullptr, b.v.U0, size_t(b.v.nv) * b.v.npad * sizeof(double)});
+        }
+    }
+    saved.push_back({nullptr, c.d_sim, sizeof(SimDev)});
+    size_t total = 0;
+    for (auto& x : saved) total += (x.bytes + 255) & ~size_t(255);
+    char* backup = nullptr;
+    E4C_CUDA(cudaMalloc(&backup, total));
+    size_t off = 0;
+    for (auto& x : saved) {
+        x.dst = backup + off;
+        off += (x.bytes + 255) & ~size_t(255);
+        E4C_CUDA(cudaMemcpyAsync(x.dst, x.src, x.bytes, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    auto restore = [&]() {
+        for (auto& x : saved)
+            cudaMemcpyAsync(const_cast<void*>(x.src), x.dst, x.bytes, cudaMemcpyDeviceToDevice,
+                            c.stream);
+    };
+    const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}};
+    const int kcs[] = {16, 32, 64, 128};
+    int best_ti = c.tile_ti, best_tj = c.tile_tj, best_kc = c.tile_kc;
+    double best = 1.0e300;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<int> hs = c.all_blocks();
+    const bool graphs = c.cfg.use_graphs != 0;
+    c.cfg.use_graphs = 0;
+    for (auto& t : tiles) {
+        for (int k : kcs) {
+            c.tile_ti = t[0]; c.tile_tj = t[1]; c.tile_kc = k;
+            c.descs_valid = false;
+            if (c.prepare_fused() != E4C_OK) { c.last_error.clear(); continue; }
+            restore();
+            launch_begin_run(c.d_sim, 1.0e300, c.stream);
+            // one untimed step, then the timed ones
+            c.run_step(hs, false);
+            cudaEventRecord(e0, c.stream);
+            for (int q = 0; q < nsteps; ++q) c.run_step(hs, false);
+            cudaEventRecord(e1, c.stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms / nsteps < best) {
+                best = ms / nsteps;
+                best_ti = t[0]; best_tj = t[1]; best_kc = k;
+            }
+        }
+    }
+    c.cfg.use_graphs = graphs ? 1 : 0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    restore();
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    cudaFree(backup);
+    if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    c.tile_ti = best_ti; c.tile_tj = best_tj; c.tile_kc = best_kc;
+    c.descs_valid = false;
+    rc = c.prepare_fused();
+    if (rc != E4C_OK) return rc;
+    if (ti) *ti = best_ti;
+    if (tj) *tj = best_tj;
+    if (kc) *kc = best_kc;
+    if (ms_per_step) *ms_per_step = best;
+    return E4C_OK;
+}
+
 int e4c_last_error(char* buf, int len) {
     if (!buf || len <= 0) return E4C_ERR_ARG;
     std::strncpy(buf, g_ctx.last_error.c_str(), size_t(len) - 1);

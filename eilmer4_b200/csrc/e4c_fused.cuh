@@ -119,6 +119,22 @@ __device__ __forceinline__ void load_plane(const FusedDesc& d, const R* __restri
     }
 }
 
+// Face frames of a Cartesian block are exact cyclic unit permutations:
+// i-faces (x, y, z), j-faces (y, z, x), k-faces (z, x, y) as (n, t1, t2).
+// transform_to_local_frame / transform_to_global_frame with such a frame
+// reduce to a permutation: v.x*1 + v.y*0 + v.z*0 equals v.x up to the sign of
+// a zero, which no later operation turns into a different non-zero value.
+template <int DIR, typename R>
+__device__ __forceinline__ void axis_to_local(V3<R>& v) {
+    if (DIR == 1) { R t = v.x; v.x = v.y; v.y = v.z; v.z = t; }
+    if (DIR == 2) { R t = v.x; v.x = v.z; v.z = v.y; v.y = t; }
+}
+template <int DIR, typename R>
+__device__ __forceinline__ void axis_to_global(V3<R>& v) {
+    if (DIR == 1) { R t = v.z; v.z = v.y; v.y = v.x; v.x = t; }
+    if (DIR == 2) { R t = v.x; v.x = v.y; v.y = v.z; v.z = t; }
+}
+
 template <typename R>
 __device__ __forceinline__ void get_cell(const R* plane, int off, int FS, const GasConsts& gas,
                                          Prim<R, 1>& s) {
@@ -185,22 +201,6 @@ __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R
     F[1] = m.x; F[2] = m.y; F[3] = m.z;
 }
 
-// Face frames of a Cartesian block are exact cyclic unit permutations:
-// i-faces (x, y, z), j-faces (y, z, x), k-faces (z, x, y) as (n, t1, t2).
-// transform_to_local_frame / transform_to_global_frame with such a frame
-// reduce to a permutation: v.x*1 + v.y*0 + v.z*0 equals v.x up to the sign of
-// a zero, which no later operation turns into a different non-zero value.
-template <int DIR, typename R>
-__device__ __forceinline__ void axis_to_local(V3<R>& v) {
-    if (DIR == 1) { R t = v.x; v.x = v.y; v.y = v.z; v.z = t; }
-    if (DIR == 2) { R t = v.x; v.x = v.z; v.z = v.y; v.y = t; }
-}
-template <int DIR, typename R>
-__device__ __forceinline__ void axis_to_global(V3<R>& v) {
-    if (DIR == 1) { R t = v.z; v.z = v.y; v.y = v.x; v.x = t; }
-    if (DIR == 2) { R t = v.x; v.x = v.y; v.y = v.z; v.z = t; }
-}
-
 template <typename R>
 __device__ __forceinline__ Frame<R> frame_of(const FusedDesc& d, int dir) {
     Frame<R> f;
@@ -220,10 +220,44 @@ __device__ __forceinline__ int find_block(const FusedDesc* descs, int nblocks, l
     return lo;
 }
 
+// Threads of a fused CTA: one per cell of the tile.
+template <int TI, int TJ>
+struct FusedThreads {
+    static constexpr int cells = TI * TJ;
+    static constexpr int total = TI * TJ;
+};
+
+// The i- and j-faces of a plane, (TI+1)*TJ + TI*(TJ+1) of them, are one list.
+// Full passes use every thread; the faces left over for the last pass are
+// shared out evenly across the warps, so every warp takes the same number of
+// passes and none waits at the plane barrier for one holding extra faces.
+template <int TI, int TJ>
+struct FaceList {
+    static constexpr int NT = TI * TJ;
+    static constexpr int NW = NT / 32;
+    static constexpr int N = (TI + 1) * TJ + TI * (TJ + 1);
+    static constexpr int FULL = N / NT;                 // passes with every thread
+    static constexpr int REM = N - FULL * NT;           // faces left for the last pass
+    static constexpr int SHARE = (REM + NW - 1) / NW;   // of them, per warp
+    __device__ static int face(int pass, int tid) {
+        if (pass < FULL) return pass * NT + tid;
+        const int lane = tid & 31, w = tid >> 5;
+        const int f = FULL * NT + w * SHARE + lane;
+        return (lane < SHARE && f < N) ? f : -1;
+    }
+    static constexpr int passes = FULL + (REM > 0 ? 1 : 0);
+};
+
+// Blocks per SM the launch bounds ask for: register budget of two CTAs in FP64.
+template <typename R>
+struct FusedMinBlocks {
+    static constexpr int value = sizeof(R) == 8 ? 2 : 3;
+};
+
 // The fused stage.  stage 1: W=WA -> WB, writes dUdt0; stage 2: W=WB -> WA,
 // writes U0 (the end-of-step state).
 template <typename R, int FLUX, int TI, int TJ>
-__global__ void __launch_bounds__(TI* TJ)
+__global__ void __launch_bounds__(FusedThreads<TI, TJ>::total, FusedMinBlocks<R>::value)
 k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems, int kc,
               SimDev* sim, GasConsts gas, FluxOpts o, int stage) {
     if (sim->status != 0 || sim->finished) return;
@@ -233,6 +267,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
     R* planes = reinterpret_cast<R*>(smem_raw);
     R* Fi = planes + 4 * S::PLANE;              // [5][TJ][TI+1]
     R* Fj = Fi + 5 * TJ * (TI + 1);             // [5][TJ+1][TI]
+    const bool cell_thread = threadIdx.x < FusedThreads<TI, TJ>::cells;
     const int ti = threadIdx.x % TI, tj = threadIdx.x / TI;
     const double dt = sim->dt_global;
     int bad = 0;
@@ -247,7 +282,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
         const int i0 = tile_i * TI, j0 = tile_j * TJ;
         const int k0 = kch * kc, k1 = min(k0 + kc, d.nk);
         const int i = i0 + ti, j = j0 + tj;
-        const bool active = i < d.ni && j < d.nj;
+        const bool active = cell_thread && i < d.ni && j < d.nj;
         const size_t nc = size_t(d.ni) * d.nj * d.nk;
         const R* __restrict__ Win = static_cast<const R*>(stage == 1 ? d.WA : d.WB);
         R* __restrict__ Wout = static_cast<R*>(stage == 1 ? d.WB : d.WA);
@@ -279,35 +314,41 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
             load_plane<R, TI, TJ>(d, Win, use_a0, gas, planes + ((k + 2 + 8) & 3) * S::PLANE, i0, j0, k + 2);
             __syncthreads();
             const R* pk = planes + ((k + 8) & 3) * S::PLANE;
-            // i-faces of plane k: (TI+1) x TJ, face fi is the west face of cell i0+fi
-            for (int f = threadIdx.x; f < (TI + 1) * TJ; f += blockDim.x) {
-                const int fi = f % (TI + 1), fj = f / (TI + 1);
-                if (i0 + fi > d.ni || j0 + fj >= d.nj) continue;
-                const int off = (fj + 2) * PI + fi;
-                Prim<R, 1> a0, a1, a2, a3;
-                get_cell(pk, off, FS, gas, a0);
-                get_cell(pk, off + 1, FS, gas, a1);
-                get_cell(pk, off + 2, FS, gas, a2);
-                get_cell(pk, off + 3, FS, gas, a3);
-                R F[5];
-                face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F);
+            // i-faces, (TI+1) x TJ (face fi is the west face of cell i0+fi), then
+            // j-faces, TI x (TJ+1) (face fj is the south face of cell j0+fj), as
+            // one list over all the CTA's threads
+            constexpr int NFI = (TI + 1) * TJ;
+            for (int pass = 0; pass < FaceList<TI, TJ>::passes; ++pass) {
+                const int f = FaceList<TI, TJ>::face(pass, threadIdx.x);
+                if (f < 0) continue;
+                if (f < NFI) {
+                    const int fi = f % (TI + 1), fj = f / (TI + 1);
+                    if (i0 + fi > d.ni || j0 + fj >= d.nj) continue;
+                    const int off = (fj + 2) * PI + fi;
+                    Prim<R, 1> a0, a1, a2, a3;
+                    get_cell(pk, off, FS, gas, a0);
+                    get_cell(pk, off + 1, FS, gas, a1);
+                    get_cell(pk, off + 2, FS, gas, a2);
+                    get_cell(pk, off + 3, FS, gas, a3);
+                    R F[5];
+                    face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F);
 #pragma unroll
-                for (int v = 0; v < 5; ++v) Fi[(v * TJ + fj) * (TI + 1) + fi] = F[v];
-            }
-            // j-faces of plane k: TI x (TJ+1), face fj is the south face of cell j0+fj
-            for (int f = threadIdx.x; f < TI * (TJ + 1); f += blockDim.x) {
-                const int fi = f % TI, fj = f / TI;
-                if (i0 + fi >= d.ni || j0 + fj > d.nj) continue;
-                const int off = fj * PI + (fi + 2);
-                Prim<R, 1> a0, a1, a2, a3;
-                get_cell(pk, off, FS, gas, a0);
-                get_cell(pk, off + PI, FS, gas, a1);
-                get_cell(pk, off + 2 * PI, FS, gas, a2);
-                get_cell(pk, off + 3 * PI, FS, gas, a3);
-                R F[5];
-                face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F);
+                    for (int v = 0; v < 5; ++v) Fi[(v * TJ + fj) * (TI + 1) + fi] = F[v];
+                } else {
+                    const int g = f - NFI;
+                    const int fi = g % TI, fj = g / TI;
+                    if (i0 + fi >= d.ni || j0 + fj > d.nj) continue;
+                    const int off = fj * PI + (fi + 2);
+                    Prim<R, 1> a0, a1, a2, a3;
+                    get_cell(pk, off, FS, gas, a0);
+                    get_cell(pk, off + PI, FS, gas, a1);
+                    get_cell(pk, off + 2 * PI, FS, gas, a2);
+                    get_cell(pk, off + 3 * PI, FS, gas, a3);
+                    R F[5];
+                    face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F);
 #pragma unroll
-                for (int v = 0; v < 5; ++v) Fj[(v * (TJ + 1) + fj) * TI + fi] = F[v];
+                    for (int v = 0; v < 5; ++v) Fj[(v * (TJ + 1) + fj) * TI + fi] = F[v];
+                }
             }
             // k-face on top of cell k, from planes k-1 .. k+2 of this column
             R Ftop[5];

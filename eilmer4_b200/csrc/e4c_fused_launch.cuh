@@ -25,7 +25,7 @@ static int launch_one(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, c
                              cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         attr_set = true;
     }
-    k_fused_stage<RT, FLUX, TI, TJ><<<L.grid, TI * TJ, smem, s>>>(
+    k_fused_stage<RT, FLUX, TI, TJ><<<L.grid, FusedThreads<TI, TJ>::total, smem, s>>>(
         static_cast<const FusedDesc*>(L.descs), L.nblocks, L.nitems, L.kc, sim, gas, o, stage);
     return 0;
 }
@@ -36,8 +36,8 @@ static int occupancy_one() {
     cudaFuncSetAttribute(k_fused_stage<RT, FLUX, TI, TJ>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_stage<RT, FLUX, TI, TJ>, TI * TJ,
-                                                      smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_stage<RT, FLUX, TI, TJ>,
+                                                      FusedThreads<TI, TJ>::total, smem) != cudaSuccess)
         return 0;
     return n;
 }

@@ -135,3 +135,21 @@ class Simulation:
         nl = (ctypes.c_int * 6)()
         _lib.check(self.L.e4c_profile_steps(int(nsteps), ms, nl))
         return {name: (ms[q], nl[q]) for q, name in enumerate(_lib.KCLASS)}
+
+    # -- fused-kernel tile shape -------------------------------------------
+    def set_tile(self, ti, tj, kc):
+        _lib.check(self.L.e4c_set_tile(int(ti), int(tj), int(kc)))
+
+    def get_tile(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.L.e4c_get_tile(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def autotune(self, nsteps=3):
+        """Pick the fastest fused tile shape on the current blocks; the flow
+        state and clock are left exactly as they were."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_double()
+        _lib.check(self.L.e4c_autotune(int(nsteps), ctypes.byref(a), ctypes.byref(b),
+                                       ctypes.byref(c), ctypes.byref(ms)))
+        return (a.value, b.value, c.value), ms.value

@@ -176,6 +176,18 @@ long long e4c_kernel_launches(void);
  * launches[c] = its launch count (arrays of E4C_NKCLASS). */
 int e4c_profile_steps(int nsteps, double* ms, int* launches);
 
+/* Tile shape of the fused stage kernel used for blocks with uniform
+ * Cartesian geometry: ti x tj cells per CTA in the i-j plane, marching kc
+ * planes in k.  Available (ti, tj): (32,8), (32,4), (16,8), (64,4), (16,16). */
+int e4c_set_tile(int ti, int tj, int kc);
+int e4c_get_tile(int* ti, int* tj, int* kc);
+
+/* Autotuner: time nsteps steps with every available tile shape and k-chunk
+ * length on the current blocks, keep the fastest, and restore the flow state
+ * and simulation clock exactly as they were before the trials.  Returns the
+ * chosen shape and its milliseconds per step. */
+int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step);
+
 /* Copy the message of the last error into buf (always NUL-terminated). */
 int e4c_last_error(char* buf, int len);
 

@@ -235,3 +235,28 @@ def test_fp32_flux_form_error_vs_fp64(oracle, e4lib):
     assert err < 1.0e-5, err
     E_g, E_o = gout[0][1][4], oout[0][1][4]
     assert np.max(np.abs(E_g - E_o) / np.abs(E_o)) < 1.0e-5
+
+
+def test_autotune_keeps_state_and_parity(oracle, e4lib):
+    """The autotuner's trial steps leave the flow state and clock untouched,
+    and every tile shape it may pick gives the same bits."""
+    from eilmer4_b200.simcore import Simulation
+    wl = W.Workload("u", 3, flux_calculator="hllc")
+    wl.blocks.append(uniform_block(36, 20, 28, 31))
+    nsteps = 12
+    _, ost, otime, odt, oout = run_oracle(oracle, wl, nsteps)
+    with Simulation.from_workload(wl) as sim:
+        (ti, tj, kc), ms = sim.autotune(2)
+        assert ms > 0.0 and (ti, tj) in ((32, 8), (32, 4), (16, 8), (64, 4), (16, 16))
+        t, dt, st = sim.state()
+        assert st == 0 and t == 0.0
+        sim.run(nsteps)
+        gp, gc = sim.download(0)
+        assert sim.state()[2] == ost
+    assert_same(gc, oout[0][1], "conserved after autotune + run")
+    for shape in ((16, 16, 16), (64, 4, 128), (32, 4, 7)):
+        with Simulation.from_workload(wl) as sim:
+            sim.set_tile(*shape)
+            sim.run(nsteps)
+            gp, gc = sim.download(0)
+        assert_same(gc, oout[0][1], f"conserved with tile {shape}")
