@@ -481,6 +481,8 @@ int e4c_profile_steps(int nsteps, double* ms, int* launches) {
     return E4C_OK;
 }
 
+static int read_sim(SimDev& s);
+
 static bool tile_available(int ti, int tj) {
     const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}};
     for (auto& t : tiles)
@@ -571,14 +573,18 @@ int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step) {
             if (c.prepare_fused() != E4C_OK) { c.last_error.clear(); continue; }
             restore();
             launch_begin_run(c.d_sim, 1.0e300, c.stream);
-            // one untimed step, then the timed ones
-            c.run_step(hs, false);
+            // one untimed step with the dt control (as at the start of a run),
+            // then the timed ones
+            c.run_step(hs, true);
             cudaEventRecord(e0, c.stream);
             for (int q = 0; q < nsteps; ++q) c.run_step(hs, false);
             cudaEventRecord(e1, c.stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) break;
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, e0, e1);
+            SimDev st;
+            if (read_sim(st) != E4C_OK) break;
+            if (st.status != 0) continue;  // a trial that failed says nothing about speed
             if (ms / nsteps < best) {
                 best = ms / nsteps;
                 best_ti = t[0]; best_tj = t[1]; best_kc = k;
