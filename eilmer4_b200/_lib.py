@@ -114,6 +114,7 @@ def load():
         "e4c_set_tile": ([i, i, i], i),
         "e4c_get_tile": ([ip, ip, ip], i),
         "e4c_autotune": ([i, ip, ip, ip, dp], i),
+        "e4c_dt_allow_noalloc": ([ip, i, d, i, dp, dp], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

@@ -32,6 +32,7 @@ UNITS = [
     ("e4c_fused32.cu", ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("e4c_blocks.cu", ["-fmad=false"]),
     ("e4c_api.cu", ["-fmad=false"]),
+    ("e4c_noalloc.cu", ["-fmad=false"]),
 ]
 
 

@@ -188,6 +188,25 @@ int e4c_get_tile(int* ti, int* tj, int* kc);
  * chosen shape and its milliseconds per step. */
 int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step);
 
+/* Most blocks one e4c_dt_allow_noalloc call can reduce over. */
+#define E4C_NOALLOC_MAX_BLOCKS 1024
+
+/* e4c_dt_allow without any device allocation.  No counterpart in the
+ * reference: it exists for hosts that cannot let a library call cudaMalloc
+ * inside their time loop -- a host that has given the whole GPU memory to its
+ * own pool or works to a fixed memory budget, where an allocation may fail or
+ * fragment the pool.  e4c_dt_allow may allocate its per-block accumulators on
+ * first use; this variant keeps its scratch (accumulators, block list, inputs
+ * and results, about 28 KB) in one fixed-size device array that lives in the
+ * library for as long as it is loaded, so it reduces over at most
+ * E4C_NOALLOC_MAX_BLOCKS blocks per call and returns E4C_ERR_ARG beyond that.
+ * Same inputs, outputs and results as e4c_dt_allow.  The first call on a
+ * device looks up the array's device address; make that first call before any
+ * stream capture.  The array is shared by all calls: calls that overlap on
+ * the GPU race (the library is single-threaded and uses one stream). */
+int e4c_dt_allow_noalloc(const int* h, int nb, double dt_current, int check_cfl,
+                         double* dt_allow, double* cfl_max);
+
 /* Copy the message of the last error into buf (always NUL-terminated). */
 int e4c_last_error(char* buf, int len);
 
