@@ -248,3 +248,33 @@ def batched_blocks(nblocks=64, lo=16, hi=96, seed=DEFAULT_SEED, spacing=1.0 / 64
         wl.blocks.append(inflow_3d_block(dims[0], dims[1], dims[2], seed + 1 + b,
                                          spacing=spacing))
     return wl
+
+
+def reacting_channel(ni=512, nj=256, nsteps=300, length=1.0, height=0.5, ramp_x=0.25,
+                     ramp_deg=15.0, mach=10.0, p_in=2000.0, T_in=300.0,
+                     massf=(0.767, 0.233, 0.0, 0.0, 0.0)):
+    """2-D hypersonic channel with a compression ramp on the lower wall:
+    5-species air (N2, O2, NO, N, O), Mach-10 inflow at i-min, extrapolate
+    outflow at i-max, slip walls below (ramp) and above.  Grid lines of
+    constant i are vertical; the lower wall rises at ramp_deg from ramp_x."""
+    from .thermochem import load_air5
+    tc = load_air5()
+    x = length * (np.arange(ni + 1, dtype=np.float64) / ni)
+    yw = np.where(x > ramp_x, (x - ramp_x) * math.tan(math.radians(ramp_deg)), 0.0)
+    eta = np.arange(nj + 1, dtype=np.float64) / nj
+    Y = yw[None, :] + (height - yw[None, :]) * eta[:, None]
+    X = np.broadcast_to(x[None, :], Y.shape)
+    vtx = np.stack([X.ravel(), Y.ravel(), np.zeros(X.size)], axis=1).copy()
+    rho, u, a = tc.state_pT(p_in, T_in, massf)
+    vx = mach * a
+    inflow = np.array([rho, vx, 0.0, 0.0, p_in, T_in, u, a] + list(massf))
+    n = ni * nj
+    prim = np.repeat(inflow[:, None], n, axis=1).copy()
+    bc = [BC_SLIP_WALL] * 6
+    bc[WEST] = BC_INFLOW_SUPERSONIC
+    bc[EAST] = BC_OUTFLOW_EXTRAPOLATE
+    wl = Workload("reacting_channel_%dx%d" % (ni, nj), 2, flux_calculator="ausmdv",
+                  nsteps=nsteps)
+    wl.blocks.append(BlockSpec(ni, nj, 1, vtx, tuple(bc), inflow, prim))
+    wl.thermochem = tc
+    return wl

@@ -50,6 +50,31 @@ typedef struct e4o_config {
     int n_threads;                  /* OpenMP threads; <=0 means all */
 } e4o_config;
 
+/* Thermally perfect mixture and reaction mechanism (plain arrays).
+ * Species thermo: NASA Glenn/CEA 9-coefficient curves with blending
+ * (src/gas/thermo/cea_thermo_curves.d).  Reactions: modified Arrhenius
+ * forward and backward rate constants in SI units, integer stoichiometric
+ * coefficients, optional third body with efficiencies. */
+#define E4O_MAXSP 8
+#define E4O_MAXSEG 4
+#define E4O_MAXR 8
+typedef struct e4o_thermochem {
+    int nsp;
+    double M[E4O_MAXSP];
+    int nseg[E4O_MAXSP];
+    double T_break[E4O_MAXSP][E4O_MAXSEG + 1];
+    double T_blend[E4O_MAXSP][E4O_MAXSEG];
+    double coeffs[E4O_MAXSP][E4O_MAXSEG][9];
+    int nreac;
+    double A_f[E4O_MAXR], n_f[E4O_MAXR], C_f[E4O_MAXR];
+    double A_b[E4O_MAXR], n_b[E4O_MAXR], C_b[E4O_MAXR];
+    int nu_r[E4O_MAXR][E4O_MAXSP];
+    int nu_p[E4O_MAXR][E4O_MAXSP];
+    int third_body[E4O_MAXR];
+    double eff[E4O_MAXR][E4O_MAXSP];
+    double T_lower, T_upper;
+} e4o_thermochem;
+
 void e4o_default_config(e4o_config* cfg);
 
 void* e4o_sim_new(const e4o_config* cfg);
@@ -85,6 +110,21 @@ double e4o_dt_global(void* sim);
 int e4o_step_count(void* sim);
 int e4o_last_bad_cells(void* sim);
 const char* e4o_last_error(void* sim);
+
+/* Install the thermally perfect mixture / mechanism (before adding blocks). */
+int e4o_set_thermochem(void* sim, const e4o_thermochem* tc);
+
+/* Thermally perfect gas state updates on one state (golden-vector tests):
+ * mode 0: from (p, T) -> rho, u;  1: from (rho, u) -> p, T (T holds the
+ * starting guess on entry);  2: from (rho, T) -> p, u.  a is the frozen
+ * sound speed.  Returns 0 or a negative error. */
+int e4o_tp_update(const e4o_thermochem* tc, int mode, const double* massf, double* rho,
+                  double* p, double* T, double* u, double* a);
+
+/* One chemistry update of one cell (constant rho, u): returns new mass
+ * fractions, T, u, p and the suggested chemistry step in *dt_chem. */
+int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double rho,
+                  double* T, double* u, double* p, double* massf, double* dt_chem);
 
 /* Low-level pieces exposed for golden-vector tests. */
 int e4o_ideal_gas_pT(double mol_mass, double gamma, double p, double T,

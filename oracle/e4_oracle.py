@@ -51,6 +51,31 @@ class Config(ctypes.Structure):
     ]
 
 
+MAXSP, MAXSEG, MAXR = 8, 4, 8
+
+
+class ThermoChem(ctypes.Structure):
+    _fields_ = [
+        ("nsp", ctypes.c_int),
+        ("M", ctypes.c_double * MAXSP),
+        ("nseg", ctypes.c_int * MAXSP),
+        ("T_break", (ctypes.c_double * (MAXSEG + 1)) * MAXSP),
+        ("T_blend", (ctypes.c_double * MAXSEG) * MAXSP),
+        ("coeffs", ((ctypes.c_double * 9) * MAXSEG) * MAXSP),
+        ("nreac", ctypes.c_int),
+        ("A_f", ctypes.c_double * MAXR), ("n_f", ctypes.c_double * MAXR),
+        ("C_f", ctypes.c_double * MAXR),
+        ("A_b", ctypes.c_double * MAXR), ("n_b", ctypes.c_double * MAXR),
+        ("C_b", ctypes.c_double * MAXR),
+        ("nu_r", (ctypes.c_int * MAXSP) * MAXR),
+        ("nu_p", (ctypes.c_int * MAXSP) * MAXR),
+        ("third_body", ctypes.c_int * MAXR),
+        ("eff", (ctypes.c_double * MAXSP) * MAXR),
+        ("T_lower", ctypes.c_double),
+        ("T_upper", ctypes.c_double),
+    ]
+
+
 def build(force: bool = False) -> str:
     """Compile the oracle with its Makefile (g++, no GPU needed)."""
     if force or not os.path.exists(_LIB_PATH):
@@ -87,6 +112,9 @@ def lib():
         L.e4o_last_error.argtypes = [vp]
         L.e4o_last_error.restype = ctypes.c_char_p
         L.e4o_ideal_gas_pT.argtypes = [dp, dp, dp, dp, P(dp), P(dp), P(dp)]
+        L.e4o_set_thermochem.argtypes = [vp, P(ThermoChem)]
+        L.e4o_tp_update.argtypes = [P(ThermoChem), ip, P(dp), P(dp), P(dp), P(dp), P(dp), P(dp)]
+        L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
         _lib = L
     return _lib
 
@@ -107,11 +135,14 @@ def default_config(**kw) -> Config:
 class OracleSim:
     """One simulation (a set of blocks sharing dt_global), as simcore.d runs it."""
 
-    def __init__(self, cfg: Config):
+    def __init__(self, cfg: Config, thermochem=None):
         self.cfg = cfg
         self._h = lib().e4o_sim_new(ctypes.byref(cfg))
         self.blocks = []
         self.nsp = 5 if cfg.gas_model == GAS_THERM_PERF_5SP_AIR else 1
+        if thermochem is not None:
+            self._tc = thermochem.fill(ThermoChem())
+            lib().e4o_set_thermochem(self._h, ctypes.byref(self._tc))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -187,3 +218,27 @@ def ideal_gas_pT(mol_mass, gamma, p, T):
     if rc != 0:
         raise ValueError("bad state")
     return rho.value, u.value, a.value
+
+
+def tp_update(thermochem, mode, massf, rho=0.0, p=0.0, T=0.0, u=0.0):
+    """Thermally perfect state update: mode 0 (p,T), 1 (rho,u; T = guess), 2 (rho,T)."""
+    tc = thermochem.fill(ThermoChem())
+    mf = np.ascontiguousarray(massf, dtype=np.float64)
+    r, pp, TT, uu, a = (ctypes.c_double(rho), ctypes.c_double(p), ctypes.c_double(T),
+                        ctypes.c_double(u), ctypes.c_double())
+    rc = lib().e4o_tp_update(ctypes.byref(tc), mode, _dptr(mf), ctypes.byref(r), ctypes.byref(pp),
+                             ctypes.byref(TT), ctypes.byref(uu), ctypes.byref(a))
+    if rc != 0:
+        raise ValueError(f"tp_update failed: {rc}")
+    return {"rho": r.value, "p": pp.value, "T": TT.value, "u": uu.value, "a": a.value}
+
+
+def chem_cell(thermochem, T_frozen, dt, rho, T, u, p, massf, dt_chem=-1.0):
+    """One chemistry update of one cell (thermochemical_increment)."""
+    tc = thermochem.fill(ThermoChem())
+    mf = np.array(massf, dtype=np.float64)
+    TT, uu, pp, dc = (ctypes.c_double(T), ctypes.c_double(u), ctypes.c_double(p),
+                      ctypes.c_double(dt_chem))
+    rc = lib().e4o_chem_cell(ctypes.byref(tc), T_frozen, dt, rho, ctypes.byref(TT),
+                             ctypes.byref(uu), ctypes.byref(pp), _dptr(mf), ctypes.byref(dc))
+    return rc, {"T": TT.value, "u": uu.value, "p": pp.value, "massf": mf, "dt_chem": dc.value}

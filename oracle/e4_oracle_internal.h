@@ -92,9 +92,8 @@ struct GasModel {
     int nsp = 1;
     // ideal gas
     double Rgas = 0.0, gamma = 1.4, Cv = 0.0, Cvinv = 0.0, Cp = 0.0;
-    // thermally perfect mixture (filled by init_therm_perf_air5)
-    double mol_mass[NSPMAX] = {};
-    double R_sp[NSPMAX] = {};
+    // thermally perfect mixture and mechanism (installed by e4o_set_thermochem)
+    e4o_thermochem tc{};
     void init_ideal(double mol_mass, double gamma);
     void init_therm_perf_air5();
     bool update_thermo_from_pT(GasState& Q) const;

@@ -93,3 +93,67 @@ def test_oracle_conserves_mass_in_closed_box(oracle):
     _, c1 = sim.get_flow(0)
     assert rel(c1[0].sum(), c0[0].sum()) < 1e-13
     assert rel(c1[4].sum(), c0[4].sum()) < 1e-13
+
+
+# --- thermally perfect 5-species air and chemistry ---------------------------
+
+def test_therm_perf_gas_golden(oracle):
+    """src/gas/therm_perf_gas.d:457-480 on the 5-species air deck (1e-6 relative)."""
+    from eilmer4_b200.thermochem import load_air5
+    tc = load_air5()
+    mf = [0.2] * 5
+    s = oracle.tp_update(tc, 0, mf, p=1.0e6, T=2000.0)
+    assert rel(s["u"], 11801825.6) < 1e-6 and rel(s["rho"], 1.2840117) < 1e-6
+    s = oracle.tp_update(tc, 1, mf, rho=2.0, u=14.0e6, T=2000.0)
+    assert rel(s["p"], 3373757.4) < 1e-6 and rel(s["T"], 4331.944) < 1e-6
+    s = oracle.tp_update(tc, 2, mf, rho=1.5, T=10000.0)
+    assert rel(s["p"], 5841068.3) < 1e-6 and rel(s["u"], 20340105.9) < 1e-6
+
+
+def test_portable_math_accuracy(oracle):
+    """The oracle's exp/log (also used on the GPU) stay within a few ulp of libm."""
+    import ctypes
+    L = oracle.lib()
+    # exercised through the thermo curves: u(T) and the rhou Newton round trip
+    from eilmer4_b200.thermochem import load_air5
+    tc = load_air5()
+    mf = [0.767, 0.233, 0.0, 0.0, 0.0]
+    for T in (250.0, 600.0, 1000.0, 2500.0, 7000.0, 15000.0):
+        s = oracle.tp_update(tc, 2, mf, rho=0.1, T=T)
+        ref_u = sum(m * (tc.h(i, T) - tc.R[i] * T) for i, m in enumerate(mf))
+        assert rel(s["u"], ref_u) < 1e-13, (T, s["u"], ref_u)
+        back = oracle.tp_update(tc, 1, mf, rho=0.1, u=s["u"], T=T * 1.3)
+        assert rel(back["T"], T) < 1e-9
+
+
+def test_chemistry_relaxes_towards_dissociation(oracle):
+    """Hot air at 6000 K dissociates O2 (and some N2); mass is conserved,
+    energy is kept (constant rho, u) and T drops."""
+    from eilmer4_b200.thermochem import load_air5
+    tc = load_air5()
+    mf = [0.767, 0.233, 0.0, 0.0, 0.0]
+    s = oracle.tp_update(tc, 0, mf, p=1.0e5, T=6000.0)
+    rc, out = oracle.chem_cell(tc, 300.0, 1.0e-6, s["rho"], 6000.0, s["u"], s["p"], mf)
+    assert rc == 0
+    y = out["massf"]
+    assert abs(sum(y) - 1.0) < 1e-12
+    assert y[4] > 1e-4 and y[1] < 0.233 and out["T"] < 6000.0
+    assert out["dt_chem"] > 0.0
+    # a frozen cell (T <= T_frozen) is left alone
+    rc, out2 = oracle.chem_cell(tc, 300.0, 1.0e-6, 1.0, 300.0, 2.0e5, 1.0e5, mf)
+    assert rc == 0 and list(out2["massf"]) == mf
+
+
+def test_reacting_channel_oracle_runs(oracle):
+    from eilmer4_b200 import workloads as W
+    wl = W.reacting_channel(ni=24, nj=12)
+    cfg = oracle.default_config(dimensions=2, flux_calculator=oracle.FLUX_AUSMDV,
+                                gas_model=oracle.GAS_THERM_PERF_5SP_AIR, reacting=1)
+    sim = oracle.OracleSim(cfg, wl.thermochem)
+    b = wl.blocks[0]
+    sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    sim.set_flow(0, b.prim)
+    assert sim.run(40) == 0
+    prim, cons = sim.get_flow(0)
+    assert np.all(np.isfinite(prim)) and prim[5].max() > 300.0
+    assert np.allclose(prim[8:].sum(axis=0), 1.0, atol=1e-12)
