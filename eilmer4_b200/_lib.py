@@ -22,7 +22,7 @@ E4C_ERR_CHEM = -7
 E4C_ERR_TIMEOUT = -8
 E4C_ERR_STATE = -9
 
-KCLASS = ("dt", "bc", "flux", "update", "stage", "other")
+KCLASS = ("dt", "bc", "flux", "update", "stage", "other", "chem")
 
 ERROR_NAMES = {
     E4C_ERR_ARG: "E4C_ERR_ARG", E4C_ERR_CUDA: "E4C_ERR_CUDA",
@@ -60,6 +60,31 @@ class E4CConfig(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
+    ]
+
+
+MAXSP, MAXSEG, MAXR = 8, 4, 8
+
+
+class E4CThermoChem(ctypes.Structure):
+    _fields_ = [
+        ("nsp", ctypes.c_int),
+        ("M", ctypes.c_double * MAXSP),
+        ("nseg", ctypes.c_int * MAXSP),
+        ("T_break", (ctypes.c_double * (MAXSEG + 1)) * MAXSP),
+        ("T_blend", (ctypes.c_double * MAXSEG) * MAXSP),
+        ("coeffs", ((ctypes.c_double * 9) * MAXSEG) * MAXSP),
+        ("nreac", ctypes.c_int),
+        ("A_f", ctypes.c_double * MAXR), ("n_f", ctypes.c_double * MAXR),
+        ("C_f", ctypes.c_double * MAXR),
+        ("A_b", ctypes.c_double * MAXR), ("n_b", ctypes.c_double * MAXR),
+        ("C_b", ctypes.c_double * MAXR),
+        ("nu_r", (ctypes.c_int * MAXSP) * MAXR),
+        ("nu_p", (ctypes.c_int * MAXSP) * MAXR),
+        ("third_body", ctypes.c_int * MAXR),
+        ("eff", (ctypes.c_double * MAXSP) * MAXR),
+        ("T_lower", ctypes.c_double),
+        ("T_upper", ctypes.c_double),
     ]
 
 
@@ -115,6 +140,8 @@ def load():
         "e4c_get_tile": ([ip, ip, ip], i),
         "e4c_autotune": ([i, ip, ip, ip, dp], i),
         "e4c_dt_allow_noalloc": ([ip, i, d, i, dp, dp], i),
+        "e4c_set_thermochem": ([P(E4CThermoChem)], i),
+        "e4c_chemistry_step": ([ip, i, d], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

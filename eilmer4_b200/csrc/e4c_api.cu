@@ -125,9 +125,19 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
               [&] { launch_stage_check(d_sim, cfg.max_invalid_cells, stream); });
 }
 
+void Ctx::enqueue_chemistry(const std::vector<int>& hs, const double* dt) {
+    for (int h : hs) {
+        const BlockHost& b = blocks[h];
+        launch_as(*this, E4C_KCLASS_CHEM, 1,
+                  [&] { launch_chem(b.v, d_sim, cfg.T_frozen, dt, nreac, stream); });
+    }
+}
+
 void Ctx::enqueue_gasdynamic(const std::vector<int>& hs) {
     const int nstages = (cfg.gasdynamic_update_scheme == E4C_UPDATE_PC) ? 2 : 1;
     for (int s = 1; s <= nstages; ++s) enqueue_stage(hs, s, s == nstages);
+    // chemistry_step(dt_global) after the gas-dynamic increment (simcore.d:903-907)
+    if (cfg.reacting) enqueue_chemistry(hs, &d_sim->dt_global);
     launch_as(*this, E4C_KCLASS_OTHER, 1, [&] { launch_end_step(d_sim, stream); });
 }
 
@@ -164,6 +174,9 @@ std::vector<int> Ctx::all_blocks() const {
 using namespace e4c;
 
 extern "C" {
+
+static int read_sim(SimDev& s);
+static int status_error(const SimDev& s);
 
 int e4c_config_default(e4c_config* c) {
     if (!c) return fail(E4C_ERR_ARG, "e4c_config_default: null config");
@@ -203,11 +216,14 @@ int e4c_init(const e4c_config* cfg) {
     if (cfg->gasdynamic_update_scheme != E4C_UPDATE_EULER &&
         cfg->gasdynamic_update_scheme != E4C_UPDATE_PC)
         return fail(E4C_ERR_UNSUPPORTED, "gasdynamic_update_scheme must be euler or predictor-corrector");
-    if (cfg->gas_model != E4C_GAS_IDEAL)
-        return fail(E4C_ERR_UNSUPPORTED, "gas model not available in this build");
+    if (cfg->gas_model != E4C_GAS_IDEAL && cfg->gas_model != E4C_GAS_THERM_PERF_5SP_AIR)
+        return fail(E4C_ERR_UNSUPPORTED, "unknown gas model");
     if (cfg->precision != E4C_PREC_FP64 && cfg->precision != E4C_PREC_FP32_FLUX)
         return fail(E4C_ERR_UNSUPPORTED, "unknown precision");
-    if (cfg->reacting) return fail(E4C_ERR_UNSUPPORTED, "reacting flow not available in this build");
+    if (cfg->reacting && cfg->gas_model != E4C_GAS_THERM_PERF_5SP_AIR)
+        return fail(E4C_ERR_UNSUPPORTED, "reacting flow needs the thermally perfect mixture");
+    if (cfg->gas_model != E4C_GAS_IDEAL && cfg->precision != E4C_PREC_FP64)
+        return fail(E4C_ERR_UNSUPPORTED, "the FP32-flux form is for the ideal gas");
     if (cfg->cfl_count < 1) return fail(E4C_ERR_ARG, "cfl_count must be >= 1");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -240,6 +256,8 @@ int e4c_init(const e4c_config* cfg) {
     E4C_CUDA(cudaMemcpyAsync(c.d_sim, &s0, sizeof(SimDev), cudaMemcpyHostToDevice, c.stream));
     E4C_CUDA(cudaStreamSynchronize(c.stream));
     c.host_step = 0;
+    c.have_thermochem = false;
+    c.nreac = 0;
     c.initialised = true;
     return E4C_OK;
 }
@@ -249,10 +267,51 @@ int e4c_finalize(void) {
     return E4C_OK;
 }
 
+int e4c_set_thermochem(const e4c_thermochem* tc) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!tc) return fail(E4C_ERR_ARG, "null thermochem");
+    if (c.cfg.gas_model != E4C_GAS_THERM_PERF_5SP_AIR)
+        return fail(E4C_ERR_STATE, "the configured gas model is not the thermally perfect mixture");
+    if (tc->nsp != 5 || tc->nreac != 5)
+        return fail(E4C_ERR_UNSUPPORTED, "this build carries 5 species and 5 reactions");
+    for (int i = 0; i < tc->nsp; ++i)
+        if (tc->nseg[i] < 2 || tc->nseg[i] > E4C_MAXSEG || !(tc->M[i] > 0.0))
+            return fail(E4C_ERR_ARG, "bad species thermo data");
+    if (!c.blocks.empty()) return fail(E4C_ERR_STATE, "set the mixture before creating blocks");
+    if (set_thermochem_constants(*tc) != 0) return fail(E4C_ERR_CUDA, "copy of the mixture failed");
+    c.have_thermochem = true;
+    c.nreac = tc->nreac;
+    return E4C_OK;
+}
+
+int e4c_chemistry_step(const int* h, int nb, double dt) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.cfg.reacting || !c.have_thermochem) return fail(E4C_ERR_STATE, "not a reacting configuration");
+    if (!h || nb <= 0) return fail(E4C_ERR_ARG, "no blocks given");
+    std::vector<int> hs(h, h + nb);
+    for (int x : hs)
+        if (x < 0 || x >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad block handle");
+    double* hp = static_cast<double*>(c.host_pinned);
+    hp[9] = dt;
+    E4C_CUDA(cudaMemcpyAsync(c.d_scalars + 4, hp + 9, sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    launch_begin_run(c.d_sim, 1.0e300, c.stream);
+    c.enqueue_chemistry(hs, c.d_scalars + 4);
+    E4C_CUDA(cudaGetLastError());
+    SimDev s;
+    int rc = read_sim(s);
+    if (rc != E4C_OK) return rc;
+    if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
 int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* bc_type,
                      const double* inflow_prim) {
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "e4c_block_create before e4c_init");
+    if (c.cfg.gas_model == E4C_GAS_THERM_PERF_5SP_AIR && !c.have_thermochem)
+        return fail(E4C_ERR_STATE, "call e4c_set_thermochem before creating blocks");
     if (!vtx_xyz || !bc_type || !inflow_prim) return fail(E4C_ERR_ARG, "null pointer");
     const int dim = c.cfg.dimensions;
     if (dim == 2) nk = 1;

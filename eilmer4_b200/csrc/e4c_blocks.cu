@@ -66,14 +66,16 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     if (dim == 3) { v.kmin = 2; v.kmax = v.kmin + nk - 1; }
     else { v.kmin = 0; v.kmax = 0; }
     v.npad = size_t(v.nidim) * v.njdim * v.nkdim;
-    v.nsp = 1;
-    v.nv = 5;
+    v.nsp = (cfg.gas_model == E4C_GAS_THERM_PERF_5SP_AIR) ? 5 : 1;
+    v.nv = 5 + (v.nsp > 1 ? v.nsp : 0);
     for (int q = 0; q < 6; ++q) v.bc[q] = bc[q];
-    for (int q = 0; q < 8; ++q) v.inflow[q] = inflow[q];
+    for (int q = 0; q < 8 + (v.nsp > 1 ? v.nsp : 0); ++q) v.inflow[q] = inflow[q];
     const size_t np = v.npad;
     // geometry arrays first (needed on either path), then the general-path state
     const size_t ngeom = 4 * np + 30 * np;
-    const size_t nstate = W_NBASE * np + 2 * size_t(v.nv) * np + 3 * size_t(v.nv) * np;
+    const size_t nw = W_NBASE + (v.nsp > 1 ? size_t(v.nsp) : 0);
+    const size_t nstate = nw * np + 2 * size_t(v.nv) * np + 3 * size_t(v.nv) * np +
+                          (cfg.reacting ? np : 0);
     double* geom = static_cast<double*>(dalloc(ngeom * sizeof(double)));
     if (!geom) return fail(E4C_ERR_CUDA, "cudaMalloc of block geometry failed");
     E4C_CUDA(cudaMemsetAsync(geom, 0, ngeom * sizeof(double), stream));
@@ -88,22 +90,23 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     E4C_CUDA(cudaMalloc(&d_vtx, nvtx * 3 * sizeof(double) + 64));
     int* d_flag = reinterpret_cast<int*>(d_vtx + nvtx * 3);
     cudaError_t e = cudaMemcpyAsync(d_vtx, vtx, nvtx * 3 * sizeof(double), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, sizeof(int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, 2 * sizeof(int), stream);
     if (e == cudaSuccess) {
         launch_geometry(v, d_vtx, stream);
         launch_check_uniform(v, d_flag, stream);
         e = cudaGetLastError();
     }
-    int uniform_flag = 1;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&uniform_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    int flags[2] = {1, 1};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     cudaFree(d_vtx);
     if (e != cudaSuccess) return cuda_fail(e, "block geometry");
 
     out.ncell = size_t(ni) * nj * v.nk;
-    out.nprim_vars = 8;
-    const bool uniform = (uniform_flag == 0);
-    out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC;
+    out.nprim_vars = nw;
+    v.axis_frames = (flags[1] == 0) ? 1 : 0;
+    const bool uniform = (flags[0] == 0);
+    out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC && v.nsp == 1;
     if (cfg.precision == E4C_PREC_FP32_FLUX && !out.fused)
         return fail(E4C_ERR_UNSUPPORTED,
                     "the FP32-flux form needs a 3-D block with uniform geometry and the "
@@ -176,12 +179,13 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
         if (!slab) return fail(E4C_ERR_CUDA, "cudaMalloc of block storage failed");
         E4C_CUDA(cudaMemsetAsync(slab, 0, nstate * sizeof(double), stream));
         double* q = slab;
-        v.W = q; q += W_NBASE * np;
+        v.W = q; q += nw * np;
         v.U0 = q; q += v.nv * np;
         v.dUdt0 = q; q += v.nv * np;
         v.Fi = q; q += v.nv * np;
         v.Fj = q; q += v.nv * np;
         v.Fk = q; q += v.nv * np;
+        v.dt_chem = cfg.reacting ? q : nullptr;  // zero: no suggestion yet, as dt_chem = -1
     }
     out.v = v;
     // staging area for uploads and downloads (primitive + conserved)

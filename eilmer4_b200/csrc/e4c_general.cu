@@ -11,8 +11,16 @@
 
 #include "e4c_kernels.h"
 #include "e4c_physics.cuh"
+#include "e4c_thermo.cuh"
 
 namespace e4c {
+
+// Thermally perfect mixture and mechanism of the context (e4c_set_thermochem).
+__constant__ e4c_thermochem c_tc;
+
+int set_thermochem_constants(const e4c_thermochem& tc) {
+    return cudaMemcpyToSymbol(c_tc, &tc, sizeof(tc)) == cudaSuccess ? 0 : -1;
+}
 
 __device__ __forceinline__ size_t pidx(const BlockView& b, int i, int j, int k) {
     return (size_t(k) * b.njdim + j) * b.nidim + i;
@@ -367,6 +375,7 @@ __device__ __forceinline__ void load_prim(const BlockView& b, size_t c, Prim<dou
     s.p = b.W[W_P * b.npad + c];
     s.u = b.W[W_U * b.npad + c];
     s.a = b.W[W_A * b.npad + c];
+    s.T = b.W[W_T * b.npad + c];
     if (NSP > 1) {
 #pragma unroll
         for (int q = 0; q < NSP; ++q) s.massf[q] = b.W[(W_NBASE + q) * b.npad + c];
@@ -375,7 +384,79 @@ __device__ __forceinline__ void load_prim(const BlockView& b, size_t c, Prim<dou
     }
 }
 
-template <int NSP, int FLUX>
+// interp_l2r2 rotates the velocities of its four stencil cells into the face
+// frame and back again in place (onedinterp.d:445-454, 576-584), so a cell
+// enters each face with the round-off of every earlier face, in the loop order
+// of sfluidblock.d:2190-2344, that it took part in.  For frames made of signed
+// unit axes a round trip is exact (up to the sign of a zero) and is skipped.
+__device__ __forceinline__ bool frame_is_axis(const double* fg, size_t npad, size_t f) {
+    for (int v = 0; v < 3; ++v) {
+        int ones = 0;
+        for (int c = 0; c < 3; ++c) {
+            const double x = fg[(3 * v + c) * npad + f];
+            if (x == 1.0 || x == -1.0) ++ones;
+            else if (x != 0.0) return false;
+        }
+        if (ones != 1) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void roundtrip(V3<double>& v, const double* fg, size_t npad, size_t f) {
+    if (frame_is_axis(fg, npad, f)) return;
+    const V3<double> n{fg[0 * npad + f], fg[1 * npad + f], fg[2 * npad + f]};
+    const V3<double> t1{fg[3 * npad + f], fg[4 * npad + f], fg[5 * npad + f]};
+    const V3<double> t2{fg[6 * npad + f], fg[7 * npad + f], fg[8 * npad + f]};
+    to_local(v, n, t1, t2);
+    to_global(v, n, t1, t2);
+}
+
+// Velocity of stencil cell (ci,cj,ck) as the reference holds it when it
+// reaches the face of direction dir at index fpos along dir.
+__device__ void replay_roundtrips(const BlockView& b, int dir, int fpos, int ci, int cj, int ck,
+                                  V3<double>& v) {
+    const int c[3] = {ci, cj, ck};
+    const int lo[3] = {b.imin, b.jmin, b.kmin}, hi[3] = {b.imax, b.jmax, b.kmax};
+    const double* fgs[3] = {b.fgi, b.fgj, b.fgk};
+    // faces of the earlier directions (their loops cover interior rows only)
+    if (c[dir] >= lo[dir] && c[dir] <= hi[dir]) {
+        for (int d = 0; d < dir; ++d)
+            for (int g = c[d] - 1; g <= c[d] + 2; ++g) {
+                if (g < lo[d] || g > hi[d] + 1) continue;
+                int p[3] = {c[0], c[1], c[2]};
+                p[d] = g;
+                roundtrip(v, fgs[d], b.npad, pidx(b, p[0], p[1], p[2]));
+            }
+    }
+    // earlier faces of this direction in the same row
+    for (int g = c[dir] - 1; g <= c[dir] + 2 && g < fpos; ++g) {
+        if (g < lo[dir] || g > hi[dir] + 1) continue;
+        int p[3] = {c[0], c[1], c[2]};
+        p[dir] = g;
+        roundtrip(v, fgs[dir], b.npad, pidx(b, p[0], p[1], p[2]));
+    }
+}
+
+// update_thermo_from_rhou of a reconstructed state: ideal gas, or the
+// thermally perfect mixture started from the cell-centre temperature (the
+// state was copied from the cell, onedinterp.d / sfluidblock.d:2199-2208)
+template <int NSP, int GAS>
+__device__ __forceinline__ bool rhou_update(const FluxOpts& o, Prim<double, NSP>& s) {
+    if (GAS == 0) {
+        double T;
+        return ideal_rhou<double>(o.gas, s.rho, s.u, s.p, T);
+    }
+    TPState<NSP> Q;
+    Q.rho = s.rho; Q.u = s.u; Q.T = s.T; Q.p = s.p; Q.a = s.a;
+#pragma unroll
+    for (int i = 0; i < NSP; ++i) Q.massf[i] = s.massf[i];
+    TPGas<NSP> g(c_tc);
+    if (!g.rhou(Q)) return false;
+    s.p = Q.p; s.T = Q.T; s.u = Q.u;
+    return true;
+}
+
+template <int NSP, int FLUX, int GAS>
 __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
     if (sim->status != 0 || sim->finished) return;
     const int ni = b.ni + (dir == 0), nj = b.nj + (dir == 1), nk = b.nk + (dir == 2);
@@ -402,6 +483,14 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
         if (o.order2) {
             load_prim<NSP>(b, cL1, sL1);
             load_prim<NSP>(b, cR1, sR1);
+            if (o.local_frame && !b.axis_frames) {
+                const int fpos = dir == 0 ? i : (dir == 1 ? j : k);
+                const int di = dir == 0, dj = dir == 1, dk = dir == 2;
+                replay_roundtrips(b, dir, fpos, i - 2 * di, j - 2 * dj, k - 2 * dk, sL1.vel);
+                replay_roundtrips(b, dir, fpos, i - di, j - dj, k - dk, sL0.vel);
+                replay_roundtrips(b, dir, fpos, i, j, k, sR0.vel);
+                replay_roundtrips(b, dir, fpos, i + di, j + dj, k + dk, sR1.vel);
+            }
             const double* len = b.cgeom + size_t(1 + dir) * b.npad;
             if (o.local_frame) {
                 to_local(sL1.vel, fr.n, fr.t1, fr.t2);
@@ -429,10 +518,9 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
             }
             r.scalar(o.limiter, o.clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
             r.scalar(o.limiter, o.clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
-            double T;
             // codeForThermoUpdateBoth("rhou"), onedinterp.d:1039-1068
-            if (!ideal_rhou<double>(o.gas, Lf.rho, Lf.u, Lf.p, T)) Lf = sL0;
-            if (!ideal_rhou<double>(o.gas, Rt.rho, Rt.u, Rt.p, T)) Rt = sR0;
+            if (!rhou_update<NSP, GAS>(o, Lf)) Lf = sL0;
+            if (!rhou_update<NSP, GAS>(o, Rt)) Rt = sR0;
             if (o.local_frame) {
                 to_global(Lf.vel, fr.n, fr.t1, fr.t2);
                 to_global(Rt.vel, fr.n, fr.t1, fr.t2);
@@ -456,7 +544,7 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
 // Cell update: time_derivatives + stage update + decode + validity check
 // (fvcell.d:735-875, 1153-1311, 563-732; fluidblock.d:433-499)
 // ---------------------------------------------------------------------------
-template <int NSP>
+template <int NSP, int GAS>
 __global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int final_stage) {
     if (sim->status != 0 || sim->finished) return;
     constexpr int NSPC = NSP > 1 ? NSP : 0;
@@ -525,10 +613,33 @@ __global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int
                 for (int s = 0; s < NSPC; ++s) massf[s] = Un[5 + s] * dinv;
                 if (!scale_mass_fractions<double, NSP>(massf)) { set_status(sim, -6); data_bad = true; }
             }
-            if (!ideal_rhou<double>(gas, rho, u, p, T)) {
+            bool ok_thermo;
+            if (GAS == 0) {
+                ok_thermo = ideal_rhou<double>(gas, rho, u, p, T);
+            } else {
+                // thermally perfect: the Newton starts from the cell's previous T
+                TPState<NSP> Q;
+                Q.rho = rho; Q.u = u; Q.T = b.W[W_T * b.npad + c];
+#pragma unroll
+                for (int s = 0; s < NSP; ++s) Q.massf[s] = massf[s];
+                TPGas<NSP> g(c_tc);
+                ok_thermo = g.rhou(Q);
+                p = Q.p; T = Q.T; u = Q.u;
+            }
+            if (!ok_thermo) {
                 T = 200.0;
-                p = rho * gas.Rgas * T;
-                u = gas.Cv * T;
+                if (GAS == 0) {
+                    p = rho * gas.Rgas * T;
+                    u = gas.Cv * T;
+                } else {
+                    TPState<NSP> Q;
+                    Q.rho = rho; Q.T = T;
+#pragma unroll
+                    for (int s = 0; s < NSP; ++s) Q.massf[s] = massf[s];
+                    TPGas<NSP> g(c_tc);
+                    g.rhoT(Q);
+                    p = Q.p; u = Q.u;
+                }
                 // encode_conserved(gtl, ftl)
                 Un[0] = rho;
                 Un[1] = rho * vx; Un[2] = rho * vy; Un[3] = rho * vz;
@@ -537,7 +648,12 @@ __global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int
 #pragma unroll
                 for (int s = 0; s < NSPC; ++s) Un[5 + s] = rho * massf[s];
             }
-            a = ideal_sound_speed<double>(gas, T);
+            if (GAS == 0) {
+                a = ideal_sound_speed<double>(gas, T);
+            } else {
+                TPGas<NSP> g(c_tc);
+                a = g.sound_speed(massf, T);
+            }
         }
         // write the new state
         double* W = b.W;
@@ -566,6 +682,49 @@ __global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int
         if (!ok) ++bad;
     }
     if (bad) atomicAdd(&sim->bad_cells, bad);
+}
+
+// ---------------------------------------------------------------------------
+// Chemistry: FVCell.thermochemical_increment for every interior cell
+// (simcore.d:1489-1505, fvcell.d:1510-1621), one cell per thread
+// ---------------------------------------------------------------------------
+template <int NSP, int NR>
+__global__ void k_chem(BlockView b, SimDev* sim, double T_frozen, const double* dt_p) {
+    if (sim->status != 0 || sim->finished) return;
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const double dt = *dt_p;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = b.imin + int(t % b.ni);
+        const int j = b.jmin + int((t / b.ni) % b.nj);
+        const int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        TPState<NSP> Q;
+        Q.rho = b.W[W_RHO * b.npad + c];
+        Q.p = b.W[W_P * b.npad + c];
+        Q.T = b.W[W_T * b.npad + c];
+        Q.u = b.W[W_U * b.npad + c];
+        Q.a = b.W[W_A * b.npad + c];
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) Q.massf[s] = b.W[(W_NBASE + s) * b.npad + c];
+        if (Q.T <= T_frozen) continue;
+        double dt_chem = b.dt_chem[c];
+        int rc = thermochemical_increment_d<NSP, NR>(c_tc, T_frozen, Q, dt, dt_chem, nullptr, nullptr);
+        if (rc != 0) {
+            set_status(sim, rc);
+            continue;
+        }
+        b.dt_chem[c] = dt_chem;
+        b.W[W_P * b.npad + c] = Q.p;
+        b.W[W_T * b.npad + c] = Q.T;
+        b.W[W_U * b.npad + c] = Q.u;
+        b.W[W_A * b.npad + c] = Q.a;
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) {
+            b.W[(W_NBASE + s) * b.npad + c] = Q.massf[s];
+            b.U0[(5 + s) * b.npad + c] = Q.rho * Q.massf[s];
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -737,11 +896,11 @@ void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int d
     const int T = 128;
     const int g = grid_for(n, T);
     if (b.nsp == 5) {
-        if (o.flux == 1) k_flux<5, 1><<<g, T, 0, s>>>(b, sim, o, dir);
-        else k_flux<5, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+        if (o.flux == 1) k_flux<5, 1, 1><<<g, T, 0, s>>>(b, sim, o, dir);
+        else k_flux<5, 0, 1><<<g, T, 0, s>>>(b, sim, o, dir);
     } else {
-        if (o.flux == 1) k_flux<1, 1><<<g, T, 0, s>>>(b, sim, o, dir);
-        else k_flux<1, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+        if (o.flux == 1) k_flux<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+        else k_flux<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, dir);
     }
 }
 
@@ -749,8 +908,17 @@ void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int st
                    int final_stage, cudaStream_t s) {
     long long n = (long long)b.ni * b.nj * b.nk;
     const int T = 128;
-    if (b.nsp == 5) k_update<5><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
-    else k_update<1><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
+    if (b.nsp == 5) k_update<5, 1><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
+    else k_update<1, 0><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
+}
+
+int launch_chem(const BlockView& b, SimDev* sim, double T_frozen, const double* dt, int nreac,
+                cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    const int T = 64;
+    if (b.nsp != 5 || nreac != 5) return -1;
+    k_chem<5, 5><<<grid_for(n, T), T, 0, s>>>(b, sim, T_frozen, dt);
+    return 0;
 }
 
 void launch_dt_reset(unsigned long long* acc, int nb, cudaStream_t s) {
@@ -787,12 +955,15 @@ __global__ void k_check_uniform(BlockView b, int* flag) {
         const double* fgs[3] = {b.fgi, b.fgj, b.fgk};
         const size_t far[3] = {pidx(b, i + 1, j, k), pidx(b, i, j + 1, k), pidx(b, i, j, k + 1)};
         const bool at_far[3] = {i == b.imax, j == b.jmax, k == b.kmax};
-        for (int d = 0; d < b.dim; ++d)
+        for (int d = 0; d < b.dim; ++d) {
             for (int q = 0; q < 10; ++q) {
                 const double ref = fgs[d][q * b.npad + c0];
                 if (fgs[d][q * b.npad + c] != ref) atomicOr(flag, 1);
                 if (at_far[d] && fgs[d][q * b.npad + far[d]] != ref) atomicOr(flag, 1);
             }
+            if (!frame_is_axis(fgs[d], b.npad, c)) atomicOr(flag + 1, 1);
+            if (at_far[d] && !frame_is_axis(fgs[d], b.npad, far[d])) atomicOr(flag + 1, 1);
+        }
     }
 }
 

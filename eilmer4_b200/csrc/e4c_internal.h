@@ -51,6 +51,8 @@ struct Ctx {
     std::vector<BlockHost> blocks;
     GraphSlot graphs[2];    // [0] plain step, [1] step with dt check
     int host_step = 0;
+    bool have_thermochem = false;
+    int nreac = 0;
     // fused path: descriptors of every fused block, rebuilt when blocks change
     FusedDesc* d_descs = nullptr;
     int descs_cap = 0;
@@ -80,6 +82,7 @@ struct Ctx {
     int run_step(const std::vector<int>& hs, bool dt_check);
     void enqueue_stage(const std::vector<int>& hs, int stage, int final_stage);
     void enqueue_gasdynamic(const std::vector<int>& hs);
+    void enqueue_chemistry(const std::vector<int>& hs, const double* dt);
     void enqueue_dt(const std::vector<int>& hs, const int* d_hl, const double* dt_current,
                     int check_cfl, int step0, SimDev* sim, double* out);
     std::vector<int> all_blocks() const;

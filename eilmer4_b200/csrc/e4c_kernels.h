@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/e4cuda.h"
 #include "e4c_types.h"
 
 namespace e4c {
@@ -35,8 +36,13 @@ void launch_reset_bad(SimDev* sim, cudaStream_t s);
 void launch_stage_check(SimDev* sim, int max_invalid, cudaStream_t s);
 void launch_end_step(SimDev* sim, cudaStream_t s);
 void launch_begin_run(SimDev* sim, double max_time, cudaStream_t s);
-// compare every cell's and face's geometry with the first one; flag[0] != 0 if any differs
+// compare every cell's and face's geometry with the first one; flag[0] != 0 if any
+// differs, flag[1] != 0 if some face frame is not made of signed unit axes
 void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
+// thermally perfect mixture / mechanism into constant memory; chemistry of one block
+int set_thermochem_constants(const e4c_thermochem& tc);
+int launch_chem(const BlockView& b, SimDev* sim, double T_frozen, const double* dt, int nreac,
+                cudaStream_t s);
 
 // fused uniform path (e4c_fused.cu: FP64, e4c_fused32.cu: FP32 flux)
 struct FusedLaunch {

@@ -53,6 +53,7 @@ struct Frame {
 template <typename R, int NSP>
 struct Prim {
     R rho, p, u, a;
+    R T;  // the starting guess of a thermally perfect rhou update
     V3<R> vel;
     R massf[NSP];
 };

@@ -1,0 +1,556 @@
+// e4c_thermo.cuh -- thermally perfect mixture and finite-rate chemistry on the device.
+//
+// Reference code reproduced (paths in the reference project):
+//   CEA thermo curves   src/gas/thermo/cea_thermo_curves.d:49-167
+//   mixture EOS         src/gas/therm_perf_gas.d:182-191, 345-396,
+//                       src/gas/thermo/therm_perf_gas_mix_eos.d:63-150,
+//                       src/gas/thermo/perf_gas_mix_eos.d:43-62, gas_model.d:45-46, 196-230, 330-338
+//   T Newton            src/nm/newton.d:40-99 (rtsafe with bisection); note that it leaves
+//                       Q.u at the energy of the last evaluated iterate, as the reference does
+//   rates               src/kinetics/rate_constant.d:71-75, reaction.d:79-114, 275-400,
+//                       reaction_mechanism.d:47-82, 127-170
+//   sub-cycling         src/kinetics/chemistry_update.d:119-307
+//   cell increment      src/eilmer/fvcell.d:1510-1621
+// The point-implicit step (backward Euler solved by Newton iteration with the
+// analytic Jacobian) has no counterpart in the reference.
+//
+// exp and log are portable implementations written with + - * / only (Cody-
+// Waite reduction + Taylor polynomial for exp; atanh series for log).  With
+// -fmad=false they give the same bits as the CPU oracle's copies of the same
+// methods (within a few ulp of libm).
+#pragma once
+
+#include <cfloat>
+#include <math_constants.h>
+
+#include "../../include/e4cuda.h"
+
+namespace e4c {
+
+// ---------------------------------------------------------------------------
+// Portable exp / log / pow
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double pm_log(double x) {
+    if (!(x > 0.0)) return (x == 0.0) ? -HUGE_VAL : CUDART_NAN;
+    if (isinf(x)) return x;
+    int k;
+    double m = frexp(x, &k);
+    if (m < 0.70710678118654752440) { m = m * 2.0; k = k - 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double s2 = s * s;
+    double p = 1.0 / 23.0;
+    p = p * s2 + 1.0 / 21.0;
+    p = p * s2 + 1.0 / 19.0;
+    p = p * s2 + 1.0 / 17.0;
+    p = p * s2 + 1.0 / 15.0;
+    p = p * s2 + 1.0 / 13.0;
+    p = p * s2 + 1.0 / 11.0;
+    p = p * s2 + 1.0 / 9.0;
+    p = p * s2 + 1.0 / 7.0;
+    p = p * s2 + 1.0 / 5.0;
+    p = p * s2 + 1.0 / 3.0;
+    p = p * s2 + 1.0;
+    const double ln2_hi = 6.93147180369123816490e-01;
+    const double ln2_lo = 1.90821492927058770002e-10;
+    double kd = double(k);
+    return kd * ln2_hi + (2.0 * s * p + kd * ln2_lo);
+}
+
+__device__ __forceinline__ double pm_exp(double x) {
+    if (x != x) return x;
+    if (x > 709.78) return HUGE_VAL;
+    if (x < -745.2) return 0.0;
+    const double inv_ln2 = 1.44269504088896338700e+00;
+    const double ln2_hi = 6.93147180369123816490e-01;
+    const double ln2_lo = 1.90821492927058770002e-10;
+    double kd = floor(x * inv_ln2 + 0.5);
+    double r = (x - kd * ln2_hi) - kd * ln2_lo;
+    double p = 1.0 / 6227020800.0;
+    p = p * r + 1.0 / 479001600.0;
+    p = p * r + 1.0 / 39916800.0;
+    p = p * r + 1.0 / 3628800.0;
+    p = p * r + 1.0 / 362880.0;
+    p = p * r + 1.0 / 40320.0;
+    p = p * r + 1.0 / 5040.0;
+    p = p * r + 1.0 / 720.0;
+    p = p * r + 1.0 / 120.0;
+    p = p * r + 1.0 / 24.0;
+    p = p * r + 1.0 / 6.0;
+    p = p * r + 0.5;
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    return ldexp(p, int(kd));
+}
+
+__device__ __forceinline__ double pm_pow(double x, double n) {
+    if (n == 0.0) return 1.0;
+    if (n == 1.0) return x;
+    if (n == -1.0) return 1.0 / x;
+    if (n == 2.0) return x * x;
+    if (n == 0.5) return sqrt(x);
+    if (n == -0.5) return 1.0 / sqrt(x);
+    if (n == 1.5) return x * sqrt(x);
+    if (n == -1.5) return 1.0 / (x * sqrt(x));
+    return pm_exp(n * pm_log(x));
+}
+
+// ---------------------------------------------------------------------------
+// CEA thermo curves
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cea_coefficients(const e4c_thermochem& tc, int isp, double T,
+                                                 double a[9]) {
+    const int nseg = tc.nseg[isp];
+    const double* tb = tc.T_break[isp];
+    const double* bl = tc.T_blend[isp];
+    if (T < (tb[1] - 0.5 * bl[0])) {
+        for (int j = 0; j < 9; ++j) a[j] = tc.coeffs[isp][0][j];
+        return;
+    }
+    if (T > (tb[nseg - 1] + 0.5 * bl[nseg - 2])) {
+        for (int j = 0; j < 9; ++j) a[j] = tc.coeffs[isp][nseg - 1][j];
+        return;
+    }
+    for (int i = 1; i < nseg; ++i) {
+        double T_blend_low = tb[i] - 0.5 * bl[i - 1];
+        double T_blend_high = tb[i] + 0.5 * bl[i - 1];
+        if (T >= T_blend_low && T <= T_blend_high) {
+            double wB = (1. / bl[i - 1]) * (T - T_blend_low);
+            double wA = 1.0 - wB;
+            for (int j = 0; j < 9; ++j) a[j] = wA * tc.coeffs[isp][i - 1][j] + wB * tc.coeffs[isp][i][j];
+            return;
+        }
+        if (T > T_blend_high && T < (tb[i + 1] - 0.5 * bl[i])) {
+            for (int j = 0; j < 9; ++j) a[j] = tc.coeffs[isp][i][j];
+            return;
+        }
+    }
+    for (int j = 0; j < 9; ++j) a[j] = CUDART_NAN;
+}
+
+__device__ __forceinline__ double cea_Cp(const e4c_thermochem& tc, int isp, double R, double T) {
+    const int nseg = tc.nseg[isp];
+    if (T < tc.T_break[isp][0]) T = tc.T_break[isp][0];
+    if (T > tc.T_break[isp][nseg]) T = tc.T_break[isp][nseg];
+    double a[9];
+    cea_coefficients(tc, isp, T, a);
+    double Cp_on_R = a[0] / (T * T) + a[1] / T + a[2] + a[3] * T;
+    Cp_on_R += a[4] * T * T + a[5] * T * T * T + a[6] * T * T * T * T;
+    return R * Cp_on_R;
+}
+
+__device__ __forceinline__ double cea_h_in_range(const e4c_thermochem& tc, int isp, double R,
+                                                 double T) {
+    double a[9];
+    cea_coefficients(tc, isp, T, a);
+    double h_on_RT = -a[0] / (T * T) + a[1] / T * pm_log(T) + a[2] + a[3] * T / 2.0;
+    h_on_RT += a[4] * T * T / 3.0 + a[5] * T * T * T / 4.0 + a[6] * T * T * T * T / 5.0 + a[7] / T;
+    return R * T * h_on_RT;
+}
+
+__device__ __forceinline__ double cea_h(const e4c_thermochem& tc, int isp, double R, double T) {
+    const int nseg = tc.nseg[isp];
+    if (T < tc.T_break[isp][0]) {
+        double T_low = tc.T_break[isp][0];
+        double h_low = cea_h_in_range(tc, isp, R, T_low);
+        double Cp_low = cea_Cp(tc, isp, R, T_low);
+        return h_low - Cp_low * (T_low - T);
+    }
+    if (T > tc.T_break[isp][nseg]) {
+        double T_high = tc.T_break[isp][nseg];
+        double h_high = cea_h_in_range(tc, isp, R, T_high);
+        double Cp_high = cea_Cp(tc, isp, R, T_high);
+        return h_high + Cp_high * (T - T_high);
+    }
+    return cea_h_in_range(tc, isp, R, T);
+}
+
+// ---------------------------------------------------------------------------
+// Thermally perfect mixture
+// ---------------------------------------------------------------------------
+template <int NSP>
+struct TPState {
+    double rho, p, T, u, a;
+    double massf[NSP];
+};
+
+template <int NSP>
+struct TPGas {
+    const e4c_thermochem& tc;
+    double R[NSP];
+    __device__ explicit TPGas(const e4c_thermochem& t) : tc(t) {
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) R[i] = 8.31451 / tc.M[i];
+    }
+    __device__ double mass_average(const double* massf, const double* phi) const {
+        double result = 0.0;
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) result += massf[i] * phi[i];
+        return result;
+    }
+    __device__ double Rmix(const double* massf) const { return mass_average(massf, R); }
+    __device__ double energy(const double* massf, double T) const {
+        double e[NSP];
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], T) - R[i] * T;
+        return mass_average(massf, e);
+    }
+    __device__ double dudT(const double* massf, double T) const {
+        double v[NSP];
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) v[i] = cea_Cp(tc, i, R[i], T) - R[i];
+        return -1.0 * mass_average(massf, v);
+    }
+    // nm/newton.d:40-99, f(T) = e_tgt - u(T); Q.T and Q.u follow every evaluation
+    __device__ bool solve_T(TPState<NSP>& Q, double e_tgt, double x0, double xMin, double xMax,
+                            double tol, double& root) const {
+        const int MAXIT = 30;
+        double xL = xMin, xH = xMax;
+        Q.T = xL; Q.u = energy(Q.massf, Q.T);
+        double fL = e_tgt - Q.u;
+        Q.T = xH; Q.u = energy(Q.massf, Q.T);
+        double fH = e_tgt - Q.u;
+        if ((fL > 0.0 && fH > 0.0) || (fL < 0.0 && fH < 0.0)) return false;
+        if (fL == 0.0) { root = xMin; return true; }
+        if (fH == 0.0) { root = xMax; return true; }
+        if (fL < 0.0) { xL = xMin; xH = xMax; }
+        else { xH = xMin; xL = xMax; }
+        double rts = x0;
+        double dxold = (xMax - xMin);
+        double dx = dxold;
+        Q.T = rts; Q.u = energy(Q.massf, Q.T);
+        double f0 = e_tgt - Q.u;
+        double df0 = dudT(Q.massf, rts);
+        for (int j = 0; j < MAXIT; ++j) {
+            if ((((rts - xH) * df0 - f0) * ((rts - xL) * df0 - f0) > 0.0) ||
+                (fabs(2.0 * f0) > fabs(dxold * df0))) {
+                dxold = dx;
+                dx = 0.5 * (xH - xL);
+                rts = xL + dx;
+                if (xL == rts) { root = rts; return true; }
+            } else {
+                dxold = dx;
+                dx = f0 / df0;
+                double tmp = rts;
+                rts -= dx;
+                if (tmp == rts) { root = rts; return true; }
+            }
+            if (fabs(dx) < tol) { root = rts; return true; }
+            Q.T = rts; Q.u = energy(Q.massf, Q.T);
+            f0 = e_tgt - Q.u;
+            df0 = dudT(Q.massf, rts);
+            if (f0 < 0.0) xL = rts;
+            else xH = rts;
+        }
+        return false;
+    }
+    // ThermallyPerfectGasMixEOS.update_temperature (therm_perf_gas_mix_eos.d:70-150)
+    __device__ bool update_temperature(TPState<NSP>& Q) const {
+        double Tsave = Q.T;
+        double e_tgt = Q.u;
+        double T1 = fmax(Q.T - 0.5 * 1000.0, 20.0);
+        double T2 = T1 + 1000.0;
+        double root;
+        if (solve_T(Q, e_tgt, Tsave, T1, T2, 1.0e-6, root)) { Q.T = root; return true; }
+        if (solve_T(Q, e_tgt, Tsave, 20.0, 100000.0, 1.0e-6, root)) { Q.T = root; return true; }
+        Q.T = Tsave;
+        Q.u = energy(Q.massf, Q.T);
+        return false;
+    }
+    __device__ bool rhou(TPState<NSP>& Q) const {
+        if (!update_temperature(Q)) return false;
+        Q.p = Q.rho * Rmix(Q.massf) * Q.T;
+        return true;
+    }
+    __device__ void rhoT(TPState<NSP>& Q) const {
+        Q.u = energy(Q.massf, Q.T);
+        Q.p = Q.rho * Rmix(Q.massf) * Q.T;
+    }
+    __device__ double sound_speed(const double* massf, double T) const {
+        double cp[NSP], cv[NSP];
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) {
+            double c = cea_Cp(tc, i, R[i], T);
+            cp[i] = c;
+            cv[i] = c - R[i];
+        }
+        double gamma = mass_average(massf, cp) / mass_average(massf, cv);
+        double dpdrho = Rmix(massf) * T;
+        return sqrt(gamma * dpdrho);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Reaction rates and the chemistry update
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double ipow_d(double c, int n) {
+    return (n == 1) ? c : ((n == 2) ? c * c : (n == 0 ? 1.0 : pm_pow(c, double(n))));
+}
+
+template <int NSP, int NR>
+struct MechD {
+    const e4c_thermochem& tc;
+    double kf[NR], kb[NR];
+    __device__ explicit MechD(const e4c_thermochem& t) : tc(t) {}
+    __device__ void rate_constants(double T) {
+        if (T < tc.T_lower) T = tc.T_lower;
+        if (T > tc.T_upper) T = tc.T_upper;
+        for (int r = 0; r < NR; ++r) {
+            kf[r] = tc.A_f[r] * pm_pow(T, tc.n_f[r]) * pm_exp(-tc.C_f[r] / T);
+            kb[r] = tc.A_b[r] * pm_pow(T, tc.n_b[r]) * pm_exp(-tc.C_b[r] / T);
+        }
+    }
+    __device__ void rates(int r, const double* c, double& wf, double& wb) const {
+        if (tc.third_body[r]) {
+            double M = 0.0;
+            for (int i = 0; i < NSP; ++i) M += tc.eff[r][i] * c[i];
+            wf = kf[r] * M;
+            wb = kb[r] * M;
+        } else {
+            wf = kf[r];
+            wb = kb[r];
+        }
+        for (int i = 0; i < NSP; ++i)
+            if (tc.nu_r[r][i] > 0) wf *= ipow_d(c[i], tc.nu_r[r][i]);
+        for (int i = 0; i < NSP; ++i)
+            if (tc.nu_p[r][i] > 0) wb *= ipow_d(c[i], tc.nu_p[r][i]);
+    }
+    __device__ void split_rates(const double* c, double* q, double* L) const {
+        for (int i = 0; i < NSP; ++i) { q[i] = 0.0; L[i] = 0.0; }
+        for (int r = 0; r < NR; ++r) {
+            double wf, wb;
+            rates(r, c, wf, wb);
+            for (int i = 0; i < NSP; ++i) {
+                if (tc.nu_r[r][i] == 0 && tc.nu_p[r][i] == 0) continue;
+                const double nu = double(tc.nu_p[r][i] - tc.nu_r[r][i]);
+                double prod = 0.0, loss = 0.0;
+                if (nu > 0.0) { prod = nu * wf; loss = nu * wb; }
+                else if (nu < 0.0) { prod = -nu * wb; loss = -nu * wf; }
+                q[i] += prod;
+                L[i] += loss;
+            }
+        }
+    }
+    __device__ void jacobian(const double* c, double J[NSP][NSP]) const {
+        for (int i = 0; i < NSP; ++i)
+            for (int j = 0; j < NSP; ++j) J[i][j] = 0.0;
+        for (int r = 0; r < NR; ++r) {
+            double Pf = 1.0, Pb = 1.0;
+            for (int i = 0; i < NSP; ++i) {
+                if (tc.nu_r[r][i] > 0) Pf *= ipow_d(c[i], tc.nu_r[r][i]);
+                if (tc.nu_p[r][i] > 0) Pb *= ipow_d(c[i], tc.nu_p[r][i]);
+            }
+            double M = 1.0;
+            if (tc.third_body[r]) {
+                M = 0.0;
+                for (int i = 0; i < NSP; ++i) M += tc.eff[r][i] * c[i];
+            }
+            for (int j = 0; j < NSP; ++j) {
+                double dPf = 0.0, dPb = 0.0;
+                const int aj = tc.nu_r[r][j], bj = tc.nu_p[r][j];
+                if (aj > 0) {
+                    dPf = double(aj) * ipow_d(c[j], aj - 1);
+                    for (int i = 0; i < NSP; ++i)
+                        if (i != j && tc.nu_r[r][i] > 0) dPf *= ipow_d(c[i], tc.nu_r[r][i]);
+                }
+                if (bj > 0) {
+                    dPb = double(bj) * ipow_d(c[j], bj - 1);
+                    for (int i = 0; i < NSP; ++i)
+                        if (i != j && tc.nu_p[r][i] > 0) dPb *= ipow_d(c[i], tc.nu_p[r][i]);
+                }
+                double ef = tc.third_body[r] ? tc.eff[r][j] : 0.0;
+                double dwf = kf[r] * (M * dPf + ef * Pf);
+                double dwb = kb[r] * (M * dPb + ef * Pb);
+                for (int i = 0; i < NSP; ++i) {
+                    const double nu = double(tc.nu_p[r][i] - tc.nu_r[r][i]);
+                    if (nu != 0.0) J[i][j] += nu * (dwf - dwb);
+                }
+            }
+        }
+    }
+    __device__ double estimate_step_size(const double* c) const {
+        double q[NSP], L[NSP];
+        split_rates(c, q, L);
+        double min_dt = 1.0e6;
+        for (int i = 0; i < NSP; ++i) {
+            if (c[i] > 0.0 && (fabs(q[i] - L[i]) > 1.0e-30)) {
+                double dt;
+                if (q[i] > 10000.0 * L[i]) dt = c[i] / (L[i] + 1.0e-50);
+                else dt = fabs(c[i] / (q[i] - L[i]));
+                min_dt = fmin(min_dt, dt);
+            }
+        }
+        double dt_chem = 1.0e-3 * min_dt;
+        dt_chem = fmin(dt_chem, 1.0e-10);
+        dt_chem = fmax(dt_chem, 1.0e-15);
+        return dt_chem;
+    }
+};
+
+template <int N>
+__device__ bool solve_dense_d(double A[N][N], double* b) {
+    for (int col = 0; col < N; ++col) {
+        int piv = col;
+        double best = fabs(A[col][col]);
+        for (int r = col + 1; r < N; ++r)
+            if (fabs(A[r][col]) > best) { best = fabs(A[r][col]); piv = r; }
+        if (!(best > 0.0)) return false;
+        if (piv != col) {
+            for (int j = 0; j < N; ++j) { double t = A[col][j]; A[col][j] = A[piv][j]; A[piv][j] = t; }
+            double t = b[col]; b[col] = b[piv]; b[piv] = t;
+        }
+        for (int r = col + 1; r < N; ++r) {
+            double f = A[r][col] / A[col][col];
+            for (int j = col; j < N; ++j) A[r][j] = A[r][j] - f * A[col][j];
+            b[r] = b[r] - f * b[col];
+        }
+    }
+    for (int r = N - 1; r >= 0; --r) {
+        double s = b[r];
+        for (int j = r + 1; j < N; ++j) s = s - A[r][j] * b[j];
+        b[r] = s / A[r][r];
+    }
+    return true;
+}
+
+// Backward-Euler step solved by Newton iteration from the guess x0 (the start
+// state c0 on the plain path).  Converged when max|F_i| / sum(c0) <= 1e-8.
+template <int NSP, int NR>
+__device__ bool point_implicit_step(const MechD<NSP, NR>& m, const double* c0, const double* x0,
+                                    double h, double* cOut, double& h_suggest, int& iters) {
+    double cscale = 0.0;
+    for (int i = 0; i < NSP; ++i) cscale += c0[i];
+    if (!(cscale > 0.0)) return false;
+    double x[NSP];
+    for (int i = 0; i < NSP; ++i) x[i] = x0[i];
+    bool converged = false;
+    iters = 0;
+    for (int it = 0; it < 10; ++it) {
+        double q[NSP], L[NSP], F[NSP];
+        m.split_rates(x, q, L);
+        double res = 0.0;
+        for (int i = 0; i < NSP; ++i) {
+            F[i] = x[i] - c0[i] - h * (q[i] - L[i]);
+            res = fmax(res, fabs(F[i]));
+        }
+        if (res / cscale <= 1.0e-8) { converged = true; break; }
+        double J[NSP][NSP], A[NSP][NSP];
+        m.jacobian(x, J);
+        for (int i = 0; i < NSP; ++i)
+            for (int j = 0; j < NSP; ++j) A[i][j] = ((i == j) ? 1.0 : 0.0) - h * J[i][j];
+        double dx[NSP];
+        for (int i = 0; i < NSP; ++i) dx[i] = -F[i];
+        if (!solve_dense_d<NSP>(A, dx)) return false;
+        for (int i = 0; i < NSP; ++i) {
+            x[i] = x[i] + dx[i];
+            if (x[i] < 0.0) x[i] = 0.0;
+        }
+        ++iters;
+    }
+    if (!converged) return false;
+    double q0[NSP], L0[NSP];
+    m.split_rates(c0, q0, L0);
+    double err = 0.0;
+    for (int i = 0; i < NSP; ++i) {
+        double xe = c0[i] + h * (q0[i] - L0[i]);
+        double sc = 1.0e-12 * cscale + 1.0e-3 * fmax(fabs(x[i]), fabs(c0[i]));
+        err = fmax(err, fabs(x[i] - xe) / sc);
+    }
+    double fac = (err > 0.0) ? 0.9 / sqrt(err) : 5.0;
+    fac = fmin(5.0, fmax(0.2, fac));
+    h_suggest = h * fac;
+    for (int i = 0; i < NSP; ++i) cOut[i] = x[i];
+    return err <= 1.0;
+}
+
+// ChemistryUpdate.opCall with the point-implicit step.  guess (optional):
+// a prediction of the concentrations at the end of the interval, used as the
+// Newton start of the first sub-step when that sub-step spans the interval.
+// Returns 0, or E4C_ERR_CHEM with Q restored.  *newton counts the Newton
+// iterations taken.
+template <int NSP, int NR>
+__device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, double tInterval,
+                                  double& dtChemSuggest, const double* guess, int* newton) {
+    TPState<NSP> Qinit = Q;
+    double conc0[NSP], concOut[NSP];
+    if (isnan(Q.rho) || Q.rho <= 0.0) return E4C_ERR_CHEM;
+    for (int i = 0; i < NSP; ++i) {
+        conc0[i] = Q.massf[i] * Q.rho / tc.M[i];
+        if (conc0[i] < 1.0e-30) conc0[i] = 0.0;
+        concOut[i] = conc0[i];
+    }
+    MechD<NSP, NR> m(tc);
+    m.rate_constants(Q.T);
+    double t = 0.0, h, dtSave = dtChemSuggest;
+    if (dtChemSuggest > tInterval) h = tInterval;
+    else if (dtChemSuggest <= 0.0) h = m.estimate_step_size(conc0);
+    else h = dtChemSuggest;
+    int cycle = 0;
+    for (; cycle < 10000; ++cycle) {
+        dtSave = dtChemSuggest;
+        h = fmin(h, tInterval - t);
+        int attempt = 0;
+        for (; attempt < 4; ++attempt) {
+            int iters = 0;
+            const bool seeded = guess && cycle == 0 && attempt == 0 && h == tInterval;
+            bool ok = point_implicit_step<NSP, NR>(m, conc0, seeded ? guess : conc0, h, concOut,
+                                                   dtChemSuggest, iters);
+            if (newton) *newton += iters;
+            bool massf_ok = true;
+            if (ok) {
+                double total = 0.0;
+                for (int i = 0; i < NSP; ++i) {
+                    Q.massf[i] = concOut[i] * tc.M[i] / Q.rho;
+                    if (Q.massf[i] < 1.0e-30) Q.massf[i] = 0.0;
+                    total += Q.massf[i];
+                }
+                if (fabs(total - 1.0) > 1.0e-3) massf_ok = false;
+            }
+            if (ok && massf_ok) {
+                t += h;
+                for (int i = 0; i < NSP; ++i) conc0[i] = concOut[i];
+                double hMax = h * (1.0 + 10.0 / 100.0);
+                if (dtChemSuggest > h) h = fmin(dtChemSuggest, hMax);
+                break;
+            } else {
+                h /= 10.0;
+                if (h < 1.0e-15) { Q = Qinit; return E4C_ERR_CHEM; }
+            }
+        }
+        if (attempt == 4) { Q = Qinit; return E4C_ERR_CHEM; }
+        if (t >= tInterval) {
+            if (cycle == 0) dtSave = dtChemSuggest;
+            break;
+        }
+    }
+    if (cycle == 10000) { Q = Qinit; return E4C_ERR_CHEM; }
+    double total = 0.0;
+    for (int i = 0; i < NSP; ++i) {
+        Q.massf[i] = concOut[i] * tc.M[i] / Q.rho;
+        if (Q.massf[i] < 1.0e-30) Q.massf[i] = 0.0;
+        total += Q.massf[i];
+    }
+    for (int i = 0; i < NSP; ++i) Q.massf[i] /= total;
+    dtChemSuggest = dtSave;
+    return 0;
+}
+
+// FVCell.thermochemical_increment (fvcell.d:1510-1621): chemistry at constant
+// rho and u, then T, p, a from the new composition.
+template <int NSP, int NR>
+__device__ int thermochemical_increment_d(const e4c_thermochem& tc, double T_frozen,
+                                          TPState<NSP>& Q, double dt, double& dt_chem,
+                                          const double* guess, int* newton) {
+    if (Q.T <= T_frozen) return 0;
+    int rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, guess, newton);
+    if (rc != 0) {
+        dt_chem = -1.0;
+        rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, nullptr, newton);
+        if (rc != 0) return rc;
+    }
+    TPGas<NSP> g(tc);
+    if (!g.rhou(Q)) return E4C_ERR_THERMO;
+    Q.a = g.sound_speed(Q.massf, Q.T);
+    return 0;
+}
+
+}  // namespace e4c

@@ -50,6 +50,8 @@ struct BlockView {
     // inflow FlowState (rho, vx, vy, vz, p, T, u, a, massf...)
     double inflow[8 + 8];
     int block_id;
+    int axis_frames;                // every face frame is made of signed unit axes
+    double* dt_chem;                // per-cell chemistry step suggestion (reacting blocks)
 };
 
 // Device-resident simulation state (one per library context).

@@ -32,19 +32,26 @@ class Simulation:
 
     def __init__(self, config: dict | None = None, control: dict | None = None, *,
                  precision: str = "fp64", device: int = 0, use_graphs: bool = True,
-                 gas: dict | None = None):
+                 gas: dict | None = None, thermochem=None):
         self.L = _lib.load()
+        if thermochem is not None:
+            gas = dict(gas or {}, model="therm_perf_5sp_air")
         self.cfg = make_config(config, control, precision=precision, device=device,
                                use_graphs=use_graphs, gas=gas)
         _lib.check(self.L.e4c_init(self.cfg))
         self.blocks = []   # (ni, nj, nk)
         self.nsp = 1
+        if thermochem is not None:
+            self._tc = thermochem.fill(_lib.E4CThermoChem())
+            _lib.check(self.L.e4c_set_thermochem(ctypes.byref(self._tc)))
+            self.nsp = thermochem.nsp
 
     @classmethod
     def from_workload(cls, wl, *, precision="fp64", control=None, use_graphs=True, **config):
         cfgd = {"dimensions": wl.dimensions, "flux_calculator": wl.flux_calculator}
         cfgd.update(config)
-        sim = cls(cfgd, control, precision=precision, use_graphs=use_graphs)
+        tc = getattr(wl, "thermochem", None)
+        sim = cls(cfgd, control, precision=precision, use_graphs=use_graphs, thermochem=tc)
         for b in wl.blocks:
             h = sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
             sim.upload(h, b.prim)
@@ -85,10 +92,11 @@ class Simulation:
         """Primitive (8, ncell) and conserved (5, ncell) state; the outputs may be
         given (numpy arrays or contiguous pinned torch tensors)."""
         n = self.ncell(h)
+        ns = self.nsp if self.nsp > 1 else 0
         if prim is None:
-            prim = np.zeros((8, n))
+            prim = np.zeros((8 + ns, n))
         if cons is None and want_cons:
-            cons = np.zeros((5, n))
+            cons = np.zeros((5 + ns, n))
         _lib.check(self.L.e4c_block_download(h, _lib.dptr(prim),
                                              _lib.dptr(cons) if cons is not None else None))
         return prim, cons
@@ -113,6 +121,10 @@ class Simulation:
         _lib.check(self.L.e4c_gasdynamic_step(arr, len(hs), float(dt), ctypes.byref(bad)))
         return bad.value
 
+    def chemistry_step(self, hs, dt):
+        arr = (ctypes.c_int * len(hs))(*hs)
+        _lib.check(self.L.e4c_chemistry_step(arr, len(hs), float(dt)))
+
     def state(self):
         t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         _lib.check(self.L.e4c_sim_state(ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))
@@ -131,8 +143,8 @@ class Simulation:
 
     def profile(self, nsteps):
         """Per kernel class: (total ms, launches) over nsteps graph-free steps."""
-        ms = (ctypes.c_double * 6)()
-        nl = (ctypes.c_int * 6)()
+        ms = (ctypes.c_double * 7)()
+        nl = (ctypes.c_int * 7)()
         _lib.check(self.L.e4c_profile_steps(int(nsteps), ms, nl))
         return {name: (ms[q], nl[q]) for q, name in enumerate(_lib.KCLASS)}
 

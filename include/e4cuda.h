@@ -113,11 +113,49 @@ typedef struct e4c_run_info {
     int bad_cells;                  /* invalid cells in the last stage */
 } e4c_run_info;
 
+/* Thermally perfect mixture and finite-rate mechanism (the data a gas-model
+ * file and a reaction file carry): NASA Glenn/CEA 9-coefficient curves with
+ * blend ranges per species (src/gas/thermo/cea_thermo_curves.d), modified
+ * Arrhenius forward/backward rate constants in SI units
+ * (src/kinetics/rate_constant.d:71-75, reaction.lua:20-36), integer
+ * stoichiometric coefficients, third-body efficiencies and the rate-constant
+ * temperature limits (reaction_mechanism.d:47-57). */
+#define E4C_MAXSP 8
+#define E4C_MAXSEG 4
+#define E4C_MAXR 8
+typedef struct e4c_thermochem {
+    int nsp;
+    double M[E4C_MAXSP];
+    int nseg[E4C_MAXSP];
+    double T_break[E4C_MAXSP][E4C_MAXSEG + 1];
+    double T_blend[E4C_MAXSP][E4C_MAXSEG];
+    double coeffs[E4C_MAXSP][E4C_MAXSEG][9];
+    int nreac;
+    double A_f[E4C_MAXR], n_f[E4C_MAXR], C_f[E4C_MAXR];
+    double A_b[E4C_MAXR], n_b[E4C_MAXR], C_b[E4C_MAXR];
+    int nu_r[E4C_MAXR][E4C_MAXSP];
+    int nu_p[E4C_MAXR][E4C_MAXSP];
+    int third_body[E4C_MAXR];
+    double eff[E4C_MAXR][E4C_MAXSP];
+    double T_lower, T_upper;
+} e4c_thermochem;
+
 /* Fill cfg with the reference defaults (globalconfig.d:440-734). */
 int e4c_config_default(e4c_config* cfg);
 
 /* Select the device, check the configuration, create the context. */
 int e4c_init(const e4c_config* cfg);
+
+/* Install the thermally perfect mixture and mechanism (gas_model
+ * E4C_GAS_THERM_PERF_5SP_AIR; call after e4c_init, before creating blocks).
+ * Replaces the gas-model construction of src/gas/therm_perf_gas.d and the
+ * ChemistryUpdate set-up of src/kinetics/chemistry_update.d:35-117. */
+int e4c_set_thermochem(const e4c_thermochem* tc);
+
+/* One chemistry update of every cell of the blocks over dt (chemistry_step,
+ * src/eilmer/simcore.d:1489-1505, i.e. FVCell.thermochemical_increment per
+ * cell); e4c_integrate calls it after each gas-dynamic step when reacting. */
+int e4c_chemistry_step(const int* h, int nb, double dt);
 
 /* Free every device buffer and graph; the context may be re-initialised. */
 int e4c_finalize(void);
@@ -169,7 +207,8 @@ long long e4c_kernel_launches(void);
 #define E4C_KCLASS_UPDATE 3    /* cell update + decode (general path) */
 #define E4C_KCLASS_STAGE 4     /* fused stage kernel (uniform path) */
 #define E4C_KCLASS_OTHER 5     /* bookkeeping kernels */
-#define E4C_NKCLASS 6
+#define E4C_KCLASS_CHEM 6      /* chemistry cell update */
+#define E4C_NKCLASS 7
 
 /* Run nsteps time steps without graphs, timing each kernel class with CUDA
  * events on the library stream: ms[c] = total milliseconds of class c and
