@@ -584,6 +584,8 @@ int Sim::chemistry_step(double dt) {
             for (int j = b->jmin; j <= b->jmax; ++j)
                 for (int i = b->imin; i <= b->imax; ++i) {
                     Cell& c = b->cell(i, j, k);
+                    // fvcell.d:1514: frozen cells return before U.massf is touched
+                    if (c.fs.gas.T <= cfg.T_frozen) continue;
                     int rc = thermochemical_increment(gm.tc, cfg.T_frozen, c.fs.gas, dt, c.dt_chem);
                     if (rc != 0) { err = std::min(err, rc); continue; }
                     for (int s = 0; s < nsp_cons; ++s) c.U[0][5 + s] = c.fs.gas.rho * c.fs.gas.massf[s];
