@@ -7,11 +7,22 @@ CFL 0.5.  A bench "step" is one full time step (both predictor-corrector
 stages, ghost cells, decode and the dt control every 10 steps) over the block.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32_flux]
-                  [--impl ours|reference] [--n 256] [--flux hllc|ausmdv]
+                  [--impl ours|reference] [--n 256] [--flux hllc|ausmdv] [--headline-only]
 
-Prints one JSON line (rank 0).  --impl reference times the CPU FP64
-restatement of the reference algorithm (the D solver itself cannot be built:
-no D compiler) on the host cores, on a bounded sample of the same workload.
+Prints one JSON line (rank 0).  The headline (value, roofline, e2e, clocks,
+gpu_launches) is the --precision form of the 256^3 block.  On one GPU the
+same line also carries, each timed the same way on its own simulation:
+  "fp32_flux" (or "plain_fp64"): the other precision form of the 256^3 block,
+      its speed-up over FP64 and its max relative density difference from the
+      FP64 run after the same steps;
+  "batched": 64 uneven blocks (edges log-uniform in [16, 96]) in one
+      persistent launch per stage inside a CUDA graph, autotuned tiles;
+  "reacting": the 512x256 5-species reacting ramp channel, 300 steps, with
+      reacting cells/s, Newton iterations per reacting cell and the chemistry
+      share of the step.
+--impl reference times the CPU FP64 restatement of the reference algorithm
+(the D solver itself cannot be built: no D compiler) on the host cores, on a
+bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -24,6 +35,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -32,6 +45,13 @@ UNIT = "cell-updates/s"
 # Algorithmic bytes per cell-update (both stages): FP64 W (5) + U (5) per
 # stage read/write as laid out in DESIGN.md: 45 doubles; FP32-flux form 280 B.
 BYTES_PER_CELL_UPDATE = {"fp64": 360.0, "fp32_flux": 280.0}
+# chemistry of one reacting cell: read rho, u, T, massf x5, dt_chem; write
+# massf x5, T, p, u, a, dt_chem and rho*massf x5 (doubles)
+BYTES_PER_REACTING_CELL = 8.0 * (9 + 15)
+# DRAM bytes per launch of the fused stage kernel from ncu captures of the
+# 256^3 workload (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
+# (precision, kernel class); None where no capture exists
+TRAFFIC = {}
 
 
 def peaks():
@@ -144,11 +164,200 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local_rank):
+def _timed_steps(sim, ext, steps, dist=None, clocks=None):
+    """Device time of `steps` time steps on the library stream (CUDA events),
+    max over ranks; returns (ms, kernel launches)."""
+    import torch
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    l0 = sim.kernel_launches()
+    ev0.record(ext)
+    sim.run(steps)
+    ev1.record(ext)
+    ev1.synchronize()
+    launches = sim.kernel_launches() - l0
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms, launches
+
+
+def _roofline_stage(sim, ncell, bpc, profile_steps):
+    """Achieved GB/s of the dominant kernel class from a graph-free profile."""
+    prof = sim.profile(profile_steps)
+    cls = max(prof, key=lambda k: prof[k][0])
+    cls_ms, cls_n = prof[cls]
+    step_ms = sum(v[0] for v in prof.values()) / profile_steps
+    if cls == "stage":
+        # one fused launch per stage: stage 1 moves 4/9, stage 2 5/9 of the
+        # step's bytes; the average launch moves half
+        per_launch_bytes = bpc / 2.0 * ncell
+    else:
+        per_launch_bytes = bpc * ncell * (cls_ms / profile_steps) / step_ms / max(
+            1, cls_n // profile_steps)
+    achieved = per_launch_bytes / (cls_ms / cls_n * 1e-3) / 1e9
+    return cls, achieved, prof
+
+
+def euler_case(args, precision, local_rank, dist, world, headline):
+    """256^3 (or --n) Mach-3 inflow block; returns a result dict and the
+    downloaded density after warm-up + timed steps."""
     import torch
 
     from eilmer4_b200 import workloads as W
     from eilmer4_b200.simcore import Simulation
+
+    wl = W.inflow_3d(n=args.n, flux=args.flux)
+    blk = wl.blocks[0]
+    ncell = blk.ncell
+    sim = Simulation.from_workload(wl, precision=precision, device=local_rank)
+    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
+    tile = sim.get_tile()
+    if not args.no_autotune:
+        # project autotuner: fastest fused tile shape; the state is restored
+        tile, _ = sim.autotune(3)
+    for _ in range(args.warmup):
+        sim.run(1)
+    sim.synchronize()
+    clocks = ClockSampler(local_rank) if headline else None
+    ms, launches = _timed_steps(sim, ext, args.steps, dist, clocks)
+    clk = clocks.stop() if clocks else None
+    rho = sim.download(0, want_cons=False)[0][0].copy()
+    ms_per_step = ms / args.steps
+    value = world * ncell * args.steps / (ms * 1e-3)
+    bpc = BYTES_PER_CELL_UPDATE[precision]
+    cls, achieved, prof = _roofline_stage(sim, ncell, bpc, args.profile_steps)
+    hbm, peak_kind = peaks()
+    step_achieved = bpc * ncell / (ms_per_step * 1e-3) / 1e9
+    res = {
+        "value": value, "unit": UNIT, "ms_per_step": ms_per_step, "steps": args.steps,
+        "dtype": "f64" if precision == "fp64" else "f32-flux/f64-accum",
+        "tile": {"ti": tile[0], "tj": tile[1], "kc": tile[2], "autotuned": not args.no_autotune},
+        "roofline": {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "traffic": TRAFFIC.get((precision, cls)),
+                     "step_achieved": step_achieved, "step_frac": step_achieved / hbm,
+                     "bytes_per_cell_update": bpc},
+        "profile_ms": {k: round(v[0] / args.profile_steps, 4) for k, v in prof.items()},
+        "gpu_launches": launches,
+    }
+    if clk is not None:
+        res["clocks"] = clk
+    if headline:
+        # end to end through the C ABI with host buffers: upload the state
+        # from pinned memory, one step, download the state to pinned memory
+        host_in = torch.from_numpy(blk.prim).pin_memory()
+        host_out = torch.empty((8, ncell), dtype=torch.float64).pin_memory()
+        e2e_steps = max(2, min(args.steps, 5))
+        sim.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sim.upload(0, host_in)
+            sim.run(1)
+            sim.download(0, prim=host_out, want_cons=False)
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        res["e2e"] = {"value": world * ncell * e2e_steps / e2e_s, "unit": UNIT,
+                      "h2d_bytes_per_step": 8 * 8 * ncell, "d2h_bytes_per_step": 8 * 8 * ncell}
+    sim.close()
+    return res, rho
+
+
+def batched_case(args, local_rank):
+    """64 uneven blocks (edges log-uniform in [16, 96]) in one persistent launch."""
+    import torch
+
+    from eilmer4_b200 import workloads as W
+    from eilmer4_b200.simcore import Simulation
+
+    wl = W.batched_blocks()
+    ncell = wl.ncell
+    sim = Simulation.from_workload(wl, device=local_rank)
+    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
+    tile, _ = sim.autotune(3)
+    for _ in range(args.warmup):
+        sim.run(1)
+    sim.synchronize()
+    ms, launches = _timed_steps(sim, ext, args.batched_steps)
+    bpc = BYTES_PER_CELL_UPDATE["fp64"]
+    cls, achieved, prof = _roofline_stage(sim, ncell, bpc, args.profile_steps)
+    hbm, _ = peaks()
+    sim.close()
+    return {
+        "workload": f"{len(wl.blocks)} uneven 3-D blocks, edges log-uniform in [16,96], "
+                    "ausmdv, CFL 0.5, fp64, one persistent launch per stage, CUDA graph",
+        "cells": ncell, "steps": args.batched_steps,
+        "value": ncell * args.batched_steps / (ms * 1e-3), "unit": UNIT,
+        "ms_per_step": ms / args.batched_steps,
+        "tile": {"ti": tile[0], "tj": tile[1], "kc": tile[2], "autotuned": True},
+        "roofline": {"kernel": cls, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm},
+        "gpu_launches": launches,
+    }
+
+
+def reacting_case(args, local_rank):
+    """512x256 5-species reacting ramp channel: gas dynamics + point-implicit
+    chemistry every step."""
+    import torch
+
+    from eilmer4_b200 import workloads as W
+    from eilmer4_b200.simcore import Simulation
+
+    wl = W.reacting_channel()
+    ncell = wl.ncell
+    sim = Simulation.from_workload(wl, reacting=True, device=local_rank)
+    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
+    for _ in range(args.warmup):
+        sim.run(1)
+    sim.synchronize()
+    sim.chemistry_counters(reset=True)
+    ms, launches = _timed_steps(sim, ext, args.reacting_steps)
+    cells, newton, recovered = sim.chemistry_counters(reset=True)
+    prof = sim.profile(args.profile_steps)
+    pcells, _, _ = sim.chemistry_counters(reset=True)
+    chem_ms = prof["chem"][0]
+    step_ms = sum(v[0] for v in prof.values())
+    prim = sim.download(0, want_cons=False)[0]
+    sim.close()
+    hbm, _ = peaks()
+    chem_rate = pcells / (chem_ms * 1e-3) if chem_ms > 0 else None
+    out = {
+        "workload": "reacting_channel 512x256, 5-species air, 5 reactions, M10 2 kPa 300 K, "
+                    "15-deg ramp, ausmdv, PC, point-implicit chemistry every step",
+        "cells": ncell, "steps": args.reacting_steps,
+        "ms_per_step": ms / args.reacting_steps,
+        "cell_updates_per_s": ncell * args.reacting_steps / (ms * 1e-3),
+        "reacting_cells_per_s": cells / (ms * 1e-3),
+        "reacting_cells_per_step": cells / args.reacting_steps,
+        "newton_per_reacting_cell": newton / max(cells, 1),
+        "recovered_cells": recovered,
+        "chem_share": chem_ms / step_ms if step_ms > 0 else None,
+        "chem_kernel": {"reacting_cells_per_s": chem_rate,
+                        "achieved_GBps": (BYTES_PER_REACTING_CELL * pcells / (chem_ms * 1e-3)
+                                          / 1e9) if chem_ms > 0 else None,
+                        "peak_GBps": hbm, "bound": "fp64 latency"},
+        "T_max": float(prim[5].max()),
+        "gpu_launches": launches,
+    }
+    return out, prim
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -158,81 +367,18 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    wl = W.inflow_3d(n=args.n, flux=args.flux)
-    blk = wl.blocks[0]
-    ncell = blk.ncell
-    sim = Simulation.from_workload(wl, precision=args.precision, device=local_rank)
-    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
-    tile = sim.get_tile()
-    if not args.no_autotune:
-        # project autotuner: fastest fused tile shape; the state is restored
-        tile, _ = sim.autotune(3)
-
-    for _ in range(args.warmup):
-        sim.run(1)
-    sim.synchronize()
-
-    # timed region: K full time steps, all on the device
-    clocks = ClockSampler(local_rank)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    time.sleep(0.3)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    l0 = sim.kernel_launches()
-    ev0.record(ext)
-    sim.run(args.steps)
-    ev1.record(ext)
-    ev1.synchronize()
-    launches = sim.kernel_launches() - l0
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    clk = clocks.stop()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    ms_per_step = ms / args.steps
-    value = world * ncell * args.steps / (ms * 1e-3)
-
-    # dominant kernel: per-class device time over a few graph-free steps
-    prof = sim.profile(args.profile_steps)
-    cls = max(prof, key=lambda k: prof[k][0])
-    cls_ms, cls_n = prof[cls]
-    step_ms = sum(v[0] for v in prof.values()) / args.profile_steps
-    hbm, peak_kind = peaks()
-    bpc = BYTES_PER_CELL_UPDATE[args.precision]
-    if cls == "stage":
-        # stage 1 moves 20 doubles/cell, stage 2 25 doubles/cell (FP64 form)
-        per_launch_bytes = bpc / 2.0 * ncell
-    else:
-        # unfused path: the step's algorithmic bytes over the whole step
-        per_launch_bytes = bpc * ncell * (cls_ms / args.profile_steps) / step_ms / max(
-            1, cls_n // args.profile_steps)
-    achieved = per_launch_bytes / (cls_ms / cls_n * 1e-3) / 1e9
-    step_achieved = bpc * ncell / (ms_per_step * 1e-3) / 1e9
-
-    # end to end through the C ABI with host buffers: upload the state from
-    # pinned memory, one step, download the state to pinned memory
-    n = ncell
-    host_in = torch.from_numpy(blk.prim).pin_memory()
-    host_out = torch.empty((8, n), dtype=torch.float64).pin_memory()
-    e2e_steps = max(2, min(args.steps, 5))
-    sim.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        sim.upload(0, host_in)
-        sim.run(1)
-        sim.download(0, prim=host_out, want_cons=False)
-    e2e_s = time.perf_counter() - t0
-    e2e_value = world * ncell * e2e_steps / e2e_s if world == 1 else None
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = world * ncell * e2e_steps / float(t.item())
+    head, rho_head = euler_case(args, args.precision, local_rank, dist, world, headline=True)
+    extra = {}
+    if not args.headline_only and world == 1:
+        other = "fp32_flux" if args.precision == "fp64" else "fp64"
+        res, rho_other = euler_case(args, other, local_rank, dist, world, headline=False)
+        rho64, rho32 = (rho_head, rho_other) if args.precision == "fp64" else (rho_other, rho_head)
+        res["rel_density_err_vs_fp64"] = float(np.max(np.abs(rho32 - rho64) / np.abs(rho64)))
+        res["speedup_vs_fp64"] = (res["value"] / head["value"] if other == "fp32_flux"
+                                  else head["value"] / res["value"])
+        extra["fp32_flux" if other == "fp32_flux" else "plain_fp64"] = res
+        extra["batched"] = batched_case(args, local_rank)
+        extra["reacting"], _ = reacting_case(args, local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -241,33 +387,26 @@ def run_ours(args, rank, world, local_rank):
                "sample": f"{args.cpu_sample}^3 block of the same workload, {args.cpu_steps} steps "
                          f"({secs:.1f} s), CPU FP64 restatement, OpenMP"}
 
-    sim.close()
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-accum",
-            "data": "synthetic",
+            "dtype": head["dtype"], "data": "synthetic",
             "config": {"workload": f"inflow_3d {args.n}^3 ideal air, {args.flux}, MUSCL/vanAlbada, "
                                    f"PC, CFL 0.5, {args.precision}",
-                       "cells": ncell, "l2": "inputs larger than L2 (each 5-double state array "
-                       f"{5 * 8 * ncell / 1e6:.0f} MB > 126 MB)",
+                       "cells": args.n ** 3, "l2": "inputs larger than L2 (each 5-double state "
+                       f"array {5 * 8 * args.n ** 3 / 1e6:.0f} MB > 126 MB)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single"},
-            "tile": {"ti": tile[0], "tj": tile[1], "kc": tile[2],
-                     "autotuned": not args.no_autotune},
-            "roofline": {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                         "traffic": None, "step_achieved": step_achieved,
-                         "step_frac": step_achieved / hbm,
-                         "bytes_per_cell_update": bpc},
-            "profile_ms": {k: round(v[0] / args.profile_steps, 4) for k, v in prof.items()},
-            "gpu_launches": launches,
-            "clocks": clk,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * 8 * ncell,
-                    "d2h_bytes_per_step": 8 * 8 * ncell},
+            "tile": head["tile"],
+            "roofline": head["roofline"],
+            "profile_ms": head["profile_ms"],
+            "gpu_launches": head["gpu_launches"],
+            "clocks": head.get("clocks"),
+            "e2e": head["e2e"],
             "cpu_baseline": cpu,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -288,6 +427,10 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the --precision 256^3 line, no FP32/batched/reacting parts")
+    ap.add_argument("--batched-steps", type=int, default=20)
+    ap.add_argument("--reacting-steps", type=int, default=300)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

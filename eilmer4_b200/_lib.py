@@ -142,6 +142,7 @@ def load():
         "e4c_dt_allow_noalloc": ([ip, i, d, i, dp, dp], i),
         "e4c_set_thermochem": ([P(E4CThermoChem)], i),
         "e4c_chemistry_step": ([ip, i, d], i),
+        "e4c_chemistry_counters": ([P(ctypes.c_longlong), i], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

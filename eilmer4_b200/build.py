@@ -54,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     hdr_time = max(_mtime(os.path.join(CSRC, h)) for h in headers)
     hdr_time = max(hdr_time, _mtime(os.path.join(ROOT, "include", "e4cuda.h")))
     objs = []
-    rebuilt = False
+    cmds = []
     for src, flags in UNITS:
         sp = os.path.join(CSRC, src)
         if not os.path.exists(sp):
@@ -66,8 +66,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
-            rebuilt = True
+            cmds.append((cmd, op))
+    # the translation units compile concurrently, one nvcc process each
+    procs = [(subprocess.Popen(cmd), op) for cmd, op in cmds]
+    failed = []
+    for pr, op in procs:
+        if pr.wait() != 0:
+            failed.append(op)
+    for op in failed:
+        if os.path.exists(op):
+            os.remove(op)
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc", output=" ".join(failed))
+    rebuilt = bool(cmds)
     if force or rebuilt or _mtime(LIB) < max(_mtime(o) for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl",
                "-lpthread"]

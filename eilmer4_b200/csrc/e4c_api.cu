@@ -69,6 +69,7 @@ void Ctx::release() {
     hlist_cap = 0;
     d_sim = nullptr;
     d_scalars = nullptr;
+    d_chem_stats = nullptr;
     d_dtacc = nullptr;
     dtacc_cap = 0;
     d_staging = nullptr;
@@ -129,7 +130,8 @@ void Ctx::enqueue_chemistry(const std::vector<int>& hs, const double* dt) {
     for (int h : hs) {
         const BlockHost& b = blocks[h];
         launch_as(*this, E4C_KCLASS_CHEM, 1,
-                  [&] { launch_chem(b.v, d_sim, cfg.T_frozen, dt, nreac, stream); });
+                  [&] { launch_chem(b.v, d_sim, cfg.T_frozen, dt, nreac, nullptr, d_chem_stats,
+                                    stream); });
     }
 }
 
@@ -248,7 +250,9 @@ int e4c_init(const e4c_config* cfg) {
     c.d_dtacc = nullptr;
     c.dtacc_cap = 0;
     c.d_scalars = static_cast<double*>(c.dalloc(8 * sizeof(double)));
-    if (!c.d_sim || !c.d_scalars) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    c.d_chem_stats = static_cast<unsigned long long*>(c.dalloc(4 * sizeof(unsigned long long)));
+    if (!c.d_sim || !c.d_scalars || !c.d_chem_stats) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    E4C_CUDA(cudaMemsetAsync(c.d_chem_stats, 0, 4 * sizeof(unsigned long long), c.stream));
     E4C_CUDA(cudaMallocHost(&c.host_pinned, 4096));
     SimDev s0{};
     s0.dt_global = cfg->dt_init;  // simcore.d:562
@@ -303,6 +307,20 @@ int e4c_chemistry_step(const int* h, int nb, double dt) {
     int rc = read_sim(s);
     if (rc != E4C_OK) return rc;
     if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
+int e4c_chemistry_counters(long long* out, int reset) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!out) return fail(E4C_ERR_ARG, "null output");
+    unsigned long long* hp = static_cast<unsigned long long*>(c.host_pinned) + 32;
+    E4C_CUDA(cudaMemcpyAsync(hp, c.d_chem_stats, 3 * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, c.stream));
+    if (reset)
+        E4C_CUDA(cudaMemsetAsync(c.d_chem_stats, 0, 4 * sizeof(unsigned long long), c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    for (int q = 0; q < 3; ++q) out[q] = (long long)hp[q];
     return E4C_OK;
 }
 

@@ -689,10 +689,16 @@ __global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int
 // (simcore.d:1489-1505, fvcell.d:1510-1621), one cell per thread
 // ---------------------------------------------------------------------------
 template <int NSP, int NR>
-__global__ void k_chem(BlockView b, SimDev* sim, double T_frozen, const double* dt_p) {
+__global__ void k_chem(BlockView b, SimDev* sim, double T_frozen, const double* dt_p,
+                       const double* guess, unsigned long long* stats) {
+    // guess (optional): [NSP + 1][ncell] over the interior cells in (i, j, k)
+    // order, predicted end concentrations and temperature.  stats (optional):
+    // reacting cells, Newton iterations, cells that needed the sub-cycled
+    // recovery, accumulated.
     if (sim->status != 0 || sim->finished) return;
     const long long n = (long long)b.ni * b.nj * b.nk;
     const double dt = *dt_p;
+    unsigned int my_cells = 0, my_newton = 0, my_recovered = 0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = b.imin + int(t % b.ni);
@@ -708,8 +714,18 @@ __global__ void k_chem(BlockView b, SimDev* sim, double T_frozen, const double* 
 #pragma unroll
         for (int s = 0; s < NSP; ++s) Q.massf[s] = b.W[(W_NBASE + s) * b.npad + c];
         if (Q.T <= T_frozen) continue;
+        double g[NSP + 1];
+        if (guess) {
+#pragma unroll
+            for (int s = 0; s <= NSP; ++s) g[s] = guess[s * n + t];
+        }
         double dt_chem = b.dt_chem[c];
-        int rc = thermochemical_increment_d<NSP, NR>(c_tc, T_frozen, Q, dt, dt_chem, nullptr, nullptr);
+        ChemCount cnt;
+        int rc = thermochemical_increment_d<NSP, NR>(c_tc, T_frozen, Q, dt, dt_chem,
+                                                     guess ? g : nullptr, &cnt);
+        my_cells += 1;
+        my_newton += cnt.newton;
+        my_recovered += cnt.recovered;
         if (rc != 0) {
             set_status(sim, rc);
             continue;
@@ -723,6 +739,16 @@ __global__ void k_chem(BlockView b, SimDev* sim, double T_frozen, const double* 
         for (int s = 0; s < NSP; ++s) {
             b.W[(W_NBASE + s) * b.npad + c] = Q.massf[s];
             b.U0[(5 + s) * b.npad + c] = Q.rho * Q.massf[s];
+        }
+    }
+    if (stats) {
+        my_cells = __reduce_add_sync(0xffffffffu, my_cells);
+        my_newton = __reduce_add_sync(0xffffffffu, my_newton);
+        my_recovered = __reduce_add_sync(0xffffffffu, my_recovered);
+        if ((threadIdx.x & 31) == 0 && my_cells > 0) {
+            atomicAdd(stats + 0, (unsigned long long)my_cells);
+            atomicAdd(stats + 1, (unsigned long long)my_newton);
+            atomicAdd(stats + 2, (unsigned long long)my_recovered);
         }
     }
 }
@@ -913,11 +939,11 @@ void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int st
 }
 
 int launch_chem(const BlockView& b, SimDev* sim, double T_frozen, const double* dt, int nreac,
-                cudaStream_t s) {
+                const double* guess, unsigned long long* stats, cudaStream_t s) {
     long long n = (long long)b.ni * b.nj * b.nk;
     const int T = 64;
     if (b.nsp != 5 || nreac != 5) return -1;
-    k_chem<5, 5><<<grid_for(n, T), T, 0, s>>>(b, sim, T_frozen, dt);
+    k_chem<5, 5><<<grid_for(n, T), T, 0, s>>>(b, sim, T_frozen, dt, guess, stats);
     return 0;
 }
 

@@ -53,6 +53,8 @@ struct Ctx {
     int host_step = 0;
     bool have_thermochem = false;
     int nreac = 0;
+    // chemistry counters: reacting cells, Newton iterations, recovered cells
+    unsigned long long* d_chem_stats = nullptr;
     // fused path: descriptors of every fused block, rebuilt when blocks change
     FusedDesc* d_descs = nullptr;
     int descs_cap = 0;

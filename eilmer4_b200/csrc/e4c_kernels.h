@@ -42,6 +42,7 @@ void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
 // thermally perfect mixture / mechanism into constant memory; chemistry of one block
 int set_thermochem_constants(const e4c_thermochem& tc);
 int launch_chem(const BlockView& b, SimDev* sim, double T_frozen, const double* dt, int nreac,
+                const double* guess, unsigned long long* stats,
                 cudaStream_t s);
 
 // fused uniform path (e4c_fused.cu: FP64, e4c_fused32.cu: FP32 flux)

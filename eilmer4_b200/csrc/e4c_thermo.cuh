@@ -462,14 +462,86 @@ __device__ bool point_implicit_step(const MechD<NSP, NR>& m, const double* c0, c
     return err <= 1.0;
 }
 
-// ChemistryUpdate.opCall with the point-implicit step.  guess (optional):
-// a prediction of the concentrations at the end of the interval, used as the
-// Newton start of the first sub-step when that sub-step spans the interval.
-// Returns 0, or E4C_ERR_CHEM with Q restored.  *newton counts the Newton
-// iterations taken.
+// One backward-Euler step over the whole interval h by Newton iteration
+// (at most 12 iterations, the convergence test of point_implicit_step, no
+// error control): the point-implicit update proper.  The iteration starts
+// from c0; with a guess (a prediction of the end concentrations; ignored
+// unless every entry is finite and non-negative) it starts from whichever of
+// c0 and the guess has the smaller residual.  Without a guess the operations are exactly the
+// CPU oracle's.
+template <int NSP, int NR>
+__device__ bool point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
+                                     const double* guess, double h, double* cOut, int& iters) {
+    double cscale = 0.0;
+    for (int i = 0; i < NSP; ++i) cscale += c0[i];
+    iters = 0;
+    if (!(cscale > 0.0)) return false;
+    double x[NSP];
+    for (int i = 0; i < NSP; ++i) x[i] = c0[i];
+    for (int it = 0; it <= 12; ++it) {
+        double q[NSP], L[NSP], F[NSP];
+        m.split_rates(x, q, L);
+        double res = 0.0;
+        for (int i = 0; i < NSP; ++i) {
+            F[i] = x[i] - c0[i] - h * (q[i] - L[i]);
+            res = fmax(res, fabs(F[i]));
+        }
+        bool use_guess = (it == 0 && guess != nullptr);
+        if (use_guess)
+            for (int i = 0; i < NSP; ++i)
+                if (!(guess[i] >= 0.0) || isinf(guess[i])) use_guess = false;
+        if (use_guess) {
+            double xg[NSP], Fg[NSP];
+            for (int i = 0; i < NSP; ++i) xg[i] = guess[i];
+            m.split_rates(xg, q, L);
+            double resg = 0.0;
+            for (int i = 0; i < NSP; ++i) {
+                Fg[i] = xg[i] - c0[i] - h * (q[i] - L[i]);
+                resg = fmax(resg, fabs(Fg[i]));
+            }
+            if (resg < res) {
+                res = resg;
+                for (int i = 0; i < NSP; ++i) { x[i] = xg[i]; F[i] = Fg[i]; }
+            }
+        }
+        if (res / cscale <= 1.0e-8) {
+            for (int i = 0; i < NSP; ++i) cOut[i] = x[i];
+            return true;
+        }
+        if (it == 12) break;
+        double J[NSP][NSP], A[NSP][NSP];
+        m.jacobian(x, J);
+        for (int i = 0; i < NSP; ++i)
+            for (int j = 0; j < NSP; ++j) A[i][j] = ((i == j) ? 1.0 : 0.0) - h * J[i][j];
+        double dx[NSP];
+        for (int i = 0; i < NSP; ++i) dx[i] = -F[i];
+        if (!solve_dense_d<NSP>(A, dx)) return false;
+        for (int i = 0; i < NSP; ++i) {
+            x[i] = x[i] + dx[i];
+            if (x[i] < 0.0) x[i] = 0.0;
+        }
+        ++iters;
+    }
+    return false;
+}
+
+// Per-cell chemistry counters: Newton iterations of the whole-interval step
+// and of the recovery sub-steps, and whether the recovery ran.
+struct ChemCount {
+    int newton = 0;
+    int recovered = 0;
+};
+
+// The chemistry update of one cell over tInterval at the cell's temperature:
+// the point-implicit step over the whole interval; when its Newton iteration
+// does not converge, ChemistryUpdate.opCall's sub-cycling
+// (chemistry_update.d:119-307) with error-controlled point-implicit sub-steps
+// and the dt_chem warm start.  guess (optional): predicted end
+// concentrations for the whole-interval step.  Returns 0, or E4C_ERR_CHEM
+// with Q restored.
 template <int NSP, int NR>
 __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, double tInterval,
-                                  double& dtChemSuggest, const double* guess, int* newton) {
+                                  double& dtChemSuggest, const double* guess, ChemCount* cnt) {
     TPState<NSP> Qinit = Q;
     double conc0[NSP], concOut[NSP];
     if (isnan(Q.rho) || Q.rho <= 0.0) return E4C_ERR_CHEM;
@@ -480,6 +552,26 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
     }
     MechD<NSP, NR> m(tc);
     m.rate_constants(Q.T);
+    {
+        int iters = 0;
+        bool ok = point_implicit_whole<NSP, NR>(m, conc0, guess, tInterval, concOut, iters);
+        if (cnt) cnt->newton += iters;
+        if (ok) {
+            double total = 0.0;
+            for (int i = 0; i < NSP; ++i) {
+                Q.massf[i] = concOut[i] * tc.M[i] / Q.rho;
+                if (Q.massf[i] < 1.0e-30) Q.massf[i] = 0.0;
+                total += Q.massf[i];
+            }
+            if (fabs(total - 1.0) <= 1.0e-3) {
+                for (int i = 0; i < NSP; ++i) Q.massf[i] /= total;
+                return 0;
+            }
+            for (int i = 0; i < NSP; ++i) Q.massf[i] = Qinit.massf[i];
+            for (int i = 0; i < NSP; ++i) concOut[i] = conc0[i];
+        }
+    }
+    if (cnt) cnt->recovered = 1;
     double t = 0.0, h, dtSave = dtChemSuggest;
     if (dtChemSuggest > tInterval) h = tInterval;
     else if (dtChemSuggest <= 0.0) h = m.estimate_step_size(conc0);
@@ -491,10 +583,9 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
         int attempt = 0;
         for (; attempt < 4; ++attempt) {
             int iters = 0;
-            const bool seeded = guess && cycle == 0 && attempt == 0 && h == tInterval;
-            bool ok = point_implicit_step<NSP, NR>(m, conc0, seeded ? guess : conc0, h, concOut,
-                                                   dtChemSuggest, iters);
-            if (newton) *newton += iters;
+            bool ok = point_implicit_step<NSP, NR>(m, conc0, conc0, h, concOut, dtChemSuggest,
+                                                   iters);
+            if (cnt) cnt->newton += iters;
             bool massf_ok = true;
             if (ok) {
                 double total = 0.0;
@@ -535,19 +626,37 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
 }
 
 // FVCell.thermochemical_increment (fvcell.d:1510-1621): chemistry at constant
-// rho and u, then T, p, a from the new composition.
+// rho and u, then T, p, a from the new composition.  guess (optional): six
+// values, the predicted end concentrations and end temperature; the
+// temperature only starts the rhou Newton iteration (when it lies within
+// 500 K of the cell's temperature), so it changes T by no more than that
+// iteration's tolerance.
 template <int NSP, int NR>
 __device__ int thermochemical_increment_d(const e4c_thermochem& tc, double T_frozen,
                                           TPState<NSP>& Q, double dt, double& dt_chem,
-                                          const double* guess, int* newton) {
+                                          const double* guess, ChemCount* cnt) {
     if (Q.T <= T_frozen) return 0;
-    int rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, guess, newton);
+    const double T0 = Q.T;
+    int rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, guess, cnt);
     if (rc != 0) {
         dt_chem = -1.0;
-        rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, nullptr, newton);
+        rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, nullptr, cnt);
         if (rc != 0) return rc;
     }
     TPGas<NSP> g(tc);
+    if (guess != nullptr) {
+        const double Tg = guess[NSP];
+        if (Tg > 20.0 && Tg < 1.0e5 && fabs(Tg - T0) < 500.0) {
+            const double u0 = Q.u;
+            Q.T = Tg;
+            if (g.rhou(Q)) {
+                Q.a = g.sound_speed(Q.massf, Q.T);
+                return 0;
+            }
+            Q.T = T0;
+            Q.u = u0;
+        }
+    }
     if (!g.rhou(Q)) return E4C_ERR_THERMO;
     Q.a = g.sound_speed(Q.massf, Q.T);
     return 0;

@@ -125,6 +125,13 @@ class Simulation:
         arr = (ctypes.c_int * len(hs))(*hs)
         _lib.check(self.L.e4c_chemistry_step(arr, len(hs), float(dt)))
 
+    def chemistry_counters(self, reset=False):
+        """(reacting cells, Newton iterations, recovered cells) accumulated by
+        the chemistry updates since the last reset."""
+        out = (ctypes.c_longlong * 3)()
+        _lib.check(self.L.e4c_chemistry_counters(out, int(bool(reset))))
+        return tuple(int(x) for x in out)
+
     def state(self):
         t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         _lib.check(self.L.e4c_sim_state(ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st)))

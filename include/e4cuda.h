@@ -154,8 +154,19 @@ int e4c_set_thermochem(const e4c_thermochem* tc);
 
 /* One chemistry update of every cell of the blocks over dt (chemistry_step,
  * src/eilmer/simcore.d:1489-1505, i.e. FVCell.thermochemical_increment per
- * cell); e4c_integrate calls it after each gas-dynamic step when reacting. */
+ * cell); e4c_integrate calls it after each gas-dynamic step when reacting.
+ * Each cell hotter than T_frozen takes one point-implicit (backward-Euler)
+ * step over dt, solved by Newton iteration with the analytic Jacobian; when
+ * that iteration does not converge, ChemistryUpdate.opCall's sub-cycling
+ * (src/kinetics/chemistry_update.d:119-307) with error-controlled
+ * point-implicit sub-steps takes over for that cell. */
 int e4c_chemistry_step(const int* h, int nb, double dt);
+
+/* Chemistry counters accumulated since e4c_init or the last reset: out[0]
+ * reacting cells updated, out[1] Newton iterations, out[2] cells that needed
+ * the sub-cycled recovery.  reset != 0 zeroes them after reading.  No
+ * counterpart in the reference (diagnostics of the point-implicit update). */
+int e4c_chemistry_counters(long long* out, int reset);
 
 /* Free every device buffer and graph; the context may be re-initialised. */
 int e4c_finalize(void);

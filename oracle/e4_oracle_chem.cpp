@@ -493,7 +493,57 @@ static bool point_implicit_step(const Mech& m, const double* c0, double h, doubl
     return err <= 1.0;
 }
 
-// ChemistryUpdate.opCall (chemistry_update.d:119-307) with the point-implicit step.
+// One backward-Euler step over the whole interval h, x = c0 + h w(x), by
+// Newton iteration from the start x = c0 (at most PI_WHOLE_MAXIT iterations,
+// same convergence test as point_implicit_step, no error control).  This is
+// the point-implicit update proper; the sub-cycled recovery below runs only
+// when it does not converge.
+static const int PI_WHOLE_MAXIT = 12;
+
+static bool point_implicit_whole(const Mech& m, const double* c0, double h, double* cOut,
+                                 int& iters) {
+    const int n = m.tc.nsp;
+    double cscale = 0.0;
+    for (int i = 0; i < n; ++i) cscale += c0[i];
+    iters = 0;
+    if (!(cscale > 0.0)) return false;
+    double x[E4O_MAXSP];
+    for (int i = 0; i < n; ++i) x[i] = c0[i];
+    for (int it = 0; it <= PI_WHOLE_MAXIT; ++it) {
+        double q[E4O_MAXSP], L[E4O_MAXSP], F[E4O_MAXSP];
+        m.split_rates(x, q, L);
+        double res = 0.0;
+        for (int i = 0; i < n; ++i) {
+            F[i] = x[i] - c0[i] - h * (q[i] - L[i]);
+            res = std::fmax(res, std::fabs(F[i]));
+        }
+        if (res / cscale <= PI_NEWTON_TOL) {
+            for (int i = 0; i < n; ++i) cOut[i] = x[i];
+            return true;
+        }
+        if (it == PI_WHOLE_MAXIT) break;
+        double J[E4O_MAXSP][E4O_MAXSP], A[E4O_MAXSP][E4O_MAXSP];
+        m.jacobian(x, J);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) A[i][j] = ((i == j) ? 1.0 : 0.0) - h * J[i][j];
+        double dx[E4O_MAXSP];
+        for (int i = 0; i < n; ++i) dx[i] = -F[i];
+        if (!solve_dense(n, A, dx)) return false;
+        for (int i = 0; i < n; ++i) {
+            x[i] = x[i] + dx[i];
+            if (x[i] < 0.0) x[i] = 0.0;
+        }
+        ++iters;
+    }
+    return false;
+}
+
+// The chemistry update of one cell over tInterval at the cell's temperature:
+// first the point-implicit step over the whole interval; if its Newton
+// iteration does not converge (or the mass fractions stop summing to one),
+// ChemistryUpdate.opCall's sub-cycling (chemistry_update.d:119-307) takes
+// over, with error-controlled point-implicit sub-steps and the per-cell
+// dt_chem warm start.
 static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInterval,
                             double& dtChemSuggest) {
     const int n = tc.nsp;
@@ -507,6 +557,23 @@ static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInter
     for (int i = 0; i < n; ++i) concOut[i] = conc0[i];
     Mech m(tc);
     m.eval_rate_constants(Q.T);
+    {
+        int iters;
+        if (point_implicit_whole(m, conc0, tInterval, concOut, iters)) {
+            double total = 0.0;
+            for (int i = 0; i < n; ++i) {
+                Q.massf[i] = concOut[i] * tc.M[i] / Q.rho;
+                if (Q.massf[i] < 1.0e-30) Q.massf[i] = 0.0;
+                total += Q.massf[i];
+            }
+            if (std::fabs(total - 1.0) <= 1.0e-3) {
+                for (int i = 0; i < n; ++i) Q.massf[i] /= total;
+                return 0;
+            }
+            for (int i = 0; i < n; ++i) Q.massf[i] = Qinit.massf[i];
+            for (int i = 0; i < n; ++i) concOut[i] = conc0[i];
+        }
+    }
     double t = 0.0, h, dtSave;
     if (dtChemSuggest > tInterval) h = tInterval;
     else if (dtChemSuggest <= 0.0) h = m.estimate_step_size(conc0);
