@@ -19,7 +19,12 @@ same line also carries, each timed the same way on its own simulation:
       persistent launch per stage inside a CUDA graph, autotuned tiles;
   "reacting": the 512x256 5-species reacting ramp channel, 300 steps, with
       reacting cells/s, Newton iterations per reacting cell and the chemistry
-      share of the step.
+      share of the step;
+  "learned": the high-enthalpy variant of that channel (Mach 10 at 2000 K,
+      20 kPa, where the air dissociates) with the learned chemistry seed:
+      training on 1e7 pairs from the plain update, then the same run timed
+      plain and seeded, Newton iterations, chemistry speed-up and the
+      mass-fraction difference from the plain update.
 --impl reference times the CPU FP64 restatement of the reference algorithm
 (the D solver itself cannot be built: no D compiler) on the host cores, on a
 bounded sample of the same workload.
@@ -326,9 +331,9 @@ def reacting_case(args, local_rank):
     sim.synchronize()
     sim.chemistry_counters(reset=True)
     ms, launches = _timed_steps(sim, ext, args.reacting_steps)
-    cells, newton, recovered = sim.chemistry_counters(reset=True)
+    cells, newton, recovered, active = sim.chemistry_counters(reset=True)
     prof = sim.profile(args.profile_steps)
-    pcells, _, _ = sim.chemistry_counters(reset=True)
+    pcells = sim.chemistry_counters(reset=True)[0]
     chem_ms = prof["chem"][0]
     step_ms = sum(v[0] for v in prof.values())
     prim = sim.download(0, want_cons=False)[0]
@@ -344,6 +349,7 @@ def reacting_case(args, local_rank):
         "reacting_cells_per_s": cells / (ms * 1e-3),
         "reacting_cells_per_step": cells / args.reacting_steps,
         "newton_per_reacting_cell": newton / max(cells, 1),
+        "newton_active_cells_per_step": active / args.reacting_steps,
         "recovered_cells": recovered,
         "chem_share": chem_ms / step_ms if step_ms > 0 else None,
         "chem_kernel": {"reacting_cells_per_s": chem_rate,
@@ -354,6 +360,104 @@ def reacting_case(args, local_rank):
         "gpu_launches": launches,
     }
     return out, prim
+
+
+def learned_case(args, local_rank):
+    """High-enthalpy reacting channel (Mach 10 at 2000 K, 20 kPa): the plain
+    point-implicit chemistry against the learned seed.  The network is trained
+    here, on the device, on pairs that the plain update produces from the
+    states of a plain run (sampled every 10 steps); then the same run is timed
+    plain and seeded from the same initial state."""
+    import torch
+
+    from eilmer4_b200 import workloads as W
+    from eilmer4_b200.simcore import Simulation
+
+    nsteps = args.reacting_steps
+    wl = W.reacting_channel_hot()
+    ncell = wl.ncell
+    t0 = time.perf_counter()
+    sim = Simulation.from_workload(wl, reacting=True, device=local_rank)
+    nsnap = max(1, nsteps // 10)
+    per = max(1, args.seed_pairs // nsnap)
+    for q in range(nsnap):
+        sim.run(10)
+        _, dt, _ = sim.state()
+        sim.seed_collect([0], dt, per, seed=1000 + q)
+    sim.synchronize()
+    t_collect = time.perf_counter() - t0
+    rep = sim.seed_train(epochs=args.seed_epochs, batch=args.seed_batch, lr=args.seed_lr, seed=1)
+    params, norm = sim.seed_get()
+    sim.close()
+
+    runs = {}
+    for seeded in (False, True):
+        sim = Simulation.from_workload(wl, reacting=True, device=local_rank)
+        if seeded:
+            sim.seed_set(params, norm)
+            sim.seed_enable(True)
+        ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
+        for _ in range(args.warmup):
+            sim.run(1)
+        sim.synchronize()
+        sim.chemistry_counters(reset=True)
+        ms, launches = _timed_steps(sim, ext, nsteps)
+        cells, newton, recovered, active = sim.chemistry_counters(reset=True)
+        prof = sim.profile(args.profile_steps)
+        pcells = sim.chemistry_counters(reset=True)[0]
+        prim = sim.download(0, want_cons=False)[0]
+        chem_ms = prof["chem"][0] + prof["seed"][0]
+        runs[seeded] = {
+            "ms_per_step": ms / nsteps,
+            "cell_updates_per_s": ncell * nsteps / (ms * 1e-3),
+            "reacting_cells_per_s": cells / (ms * 1e-3),
+            "newton_per_reacting_cell": newton / max(cells, 1),
+            "newton_active_cells_per_step": active / nsteps,
+            "newton_per_active_cell": newton / max(active, 1),
+            "recovered_cells": recovered,
+            "chem_ms_per_step": chem_ms / args.profile_steps,
+            "seed_ms_per_step": prof["seed"][0] / args.profile_steps,
+            "chem_kernel_reacting_cells_per_s": pcells / (chem_ms * 1e-3) if chem_ms > 0 else None,
+            "gpu_launches": launches,
+            "_prim": prim,
+        }
+        sim.close()
+    plain, seeded = runs[False], runs[True]
+    # the chemistry update of one state (the plain run's last) with and
+    # without the network: the surrogate's error against the plain update
+    prim0 = plain["_prim"]
+    sim = Simulation.from_workload(wl, reacting=True, device=local_rank)
+    sim.seed_set(params, norm)
+    out = {}
+    for on in (False, True):
+        sim.upload(0, prim0)
+        sim.seed_enable(on)
+        sim.chemistry_counters(reset=True)
+        sim.chemistry_step([0], args.learned_check_dt)
+        c = sim.chemistry_counters(reset=True)
+        out[on] = (sim.download(0, want_cons=False)[0], c)
+    sim.close()
+    one_step_err = float(np.abs(out[True][0][8:] - out[False][0][8:]).max())
+    run_err = float(np.abs(seeded["_prim"][8:] - plain["_prim"][8:]).max())
+    for r in runs.values():
+        r.pop("_prim")
+    return {
+        "workload": "reacting_channel_hot 512x256 (Mach 10 at 2000 K, 20 kPa), 5-species air, "
+                    f"5 reactions, ausmdv, PC, {nsteps} steps",
+        "cells": ncell, "steps": nsteps,
+        "training": {"pairs": rep["n_train"] + rep["n_val"], "epochs": args.seed_epochs,
+                     "batch": args.seed_batch, "train_loss": rep["train_loss"],
+                     "val_loss": rep["val_loss"], "train_s": rep["seconds"],
+                     "collect_s": t_collect, "optimizer_steps": rep["steps"]},
+        "plain": plain, "seeded": seeded,
+        "chem_speedup": plain["chem_ms_per_step"] / seeded["chem_ms_per_step"],
+        "step_speedup": plain["ms_per_step"] / seeded["ms_per_step"],
+        "massf_err_one_update": one_step_err,
+        "newton_one_update": {"plain": out[False][1][1], "seeded": out[True][1][1],
+                              "reacting_cells": out[False][1][0],
+                              "active_cells": out[False][1][3]},
+        "massf_diff_after_run": run_err,
+    }
 
 
 def run_ours(args, rank, world, local_rank):
@@ -379,6 +483,8 @@ def run_ours(args, rank, world, local_rank):
         extra["fp32_flux" if other == "fp32_flux" else "plain_fp64"] = res
         extra["batched"] = batched_case(args, local_rank)
         extra["reacting"], _ = reacting_case(args, local_rank)
+        if not args.no_learned:
+            extra["learned"] = learned_case(args, local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -431,6 +537,12 @@ def main():
                     help="only the --precision 256^3 line, no FP32/batched/reacting parts")
     ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--reacting-steps", type=int, default=300)
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--seed-pairs", type=int, default=10_000_000)
+    ap.add_argument("--seed-epochs", type=int, default=8)
+    ap.add_argument("--seed-batch", type=int, default=4096)
+    ap.add_argument("--seed-lr", type=float, default=2.0e-3)
+    ap.add_argument("--learned-check-dt", type=float, default=1.0e-7)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

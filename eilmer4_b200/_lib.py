@@ -22,7 +22,7 @@ E4C_ERR_CHEM = -7
 E4C_ERR_TIMEOUT = -8
 E4C_ERR_STATE = -9
 
-KCLASS = ("dt", "bc", "flux", "update", "stage", "other", "chem")
+KCLASS = ("dt", "bc", "flux", "update", "stage", "other", "chem", "seed")
 
 ERROR_NAMES = {
     E4C_ERR_ARG: "E4C_ERR_ARG", E4C_ERR_CUDA: "E4C_ERR_CUDA",
@@ -143,6 +143,15 @@ def load():
         "e4c_set_thermochem": ([P(E4CThermoChem)], i),
         "e4c_chemistry_step": ([ip, i, d], i),
         "e4c_chemistry_counters": ([P(ctypes.c_longlong), i], i),
+        "e4c_seed_collect": ([ip, i, d, ctypes.c_longlong, ctypes.c_ulonglong], i),
+        "e4c_seed_dataset": ([P(ctypes.c_longlong)], i),
+        "e4c_seed_clear": ([], i),
+        "e4c_seed_train": ([i, i, d, ctypes.c_ulonglong, dp], i),
+        "e4c_seed_get": ([P(ctypes.c_float), dp], i),
+        "e4c_seed_set": ([P(ctypes.c_float), dp], i),
+        "e4c_seed_enable": ([i], i),
+        "e4c_seed_predict": ([dp, ctypes.c_longlong, dp], i),
+        "e4c_seed_loss_grad": ([P(ctypes.c_float), P(ctypes.c_float), i, dp, P(ctypes.c_float)], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -162,6 +171,16 @@ def check(rc: int) -> int:
     if rc < 0:
         raise E4CError(rc, last_error())
     return rc
+
+
+SEED_NPARAM = 9286
+SEED_NNORM = 30
+
+
+def fptr(a):
+    """ctypes float* of a C-contiguous float32 numpy array."""
+    assert a.dtype.name == "float32" and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
 def dptr(a):

@@ -25,6 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, extra flags)
 UNITS = [
     ("e4c_general.cu", ["-fmad=false"]),
+    ("e4c_tp.cu", ["-fmad=false"]),
     ("e4c_fused.cu", ["-fmad=false"]),
     # FP32 reconstruction/flux: approximate FP32 division and square root
     # (the form is checked against FP64 with a tolerance); FP64 arithmetic in
@@ -33,6 +34,8 @@ UNITS = [
     ("e4c_blocks.cu", ["-fmad=false"]),
     ("e4c_api.cu", ["-fmad=false"]),
     ("e4c_noalloc.cu", ["-fmad=false"]),
+    # learned chemistry seed: BF16 tensor-core MLP, FP32 arithmetic
+    ("e4c_seed.cu", []),
 ]
 
 

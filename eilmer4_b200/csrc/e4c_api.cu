@@ -70,6 +70,10 @@ void Ctx::release() {
     d_sim = nullptr;
     d_scalars = nullptr;
     d_chem_stats = nullptr;
+    d_chem_work = nullptr;
+    d_chem_nwork = nullptr;
+    chem_work_cap = 0;
+    seed = SeedNet{};
     d_dtacc = nullptr;
     dtacc_cap = 0;
     d_staging = nullptr;
@@ -129,10 +133,36 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
 void Ctx::enqueue_chemistry(const std::vector<int>& hs, const double* dt) {
     for (int h : hs) {
         const BlockHost& b = blocks[h];
-        launch_as(*this, E4C_KCLASS_CHEM, 1,
-                  [&] { launch_chem(b.v, d_sim, cfg.T_frozen, dt, nreac, nullptr, d_chem_stats,
-                                    stream); });
+        cudaMemsetAsync(d_chem_nwork, 0, sizeof(int), stream);
+        launch_as(*this, E4C_KCLASS_CHEM, 1, [&] {
+            launch_chem(b.v, d_sim, cfg.T_frozen, dt, nreac, d_chem_work, d_chem_nwork,
+                        d_chem_stats, stream);
+        });
+        const double* guess = nullptr;
+        if (seed.enabled && seed.d_guess && b.ncell <= seed.guess_cap) {
+            launch_as(*this, E4C_KCLASS_SEED, 1,
+                      [&] { seed_infer(b.v, dt, d_chem_work, d_chem_nwork); });
+            guess = seed.d_guess;
+        }
+        launch_as(*this, E4C_KCLASS_CHEM, 1, [&] {
+            launch_chem_work(b.v, d_sim, cfg.T_frozen, dt, nreac, d_chem_work, d_chem_nwork,
+                             guess, d_chem_stats, stream);
+        });
     }
+}
+
+int Ctx::ensure_chem_work(size_t ncell) {
+    if (ncell <= chem_work_cap) return E4C_OK;
+    dfree(d_chem_work);
+    d_chem_work = static_cast<int*>(dalloc((ncell + 16) * sizeof(int)));
+    if (!d_chem_work) {
+        chem_work_cap = 0;
+        d_chem_nwork = nullptr;
+        return fail(E4C_ERR_CUDA, "cudaMalloc of the chemistry work list failed");
+    }
+    d_chem_nwork = d_chem_work + ncell;
+    chem_work_cap = ncell;
+    return E4C_OK;
 }
 
 void Ctx::enqueue_gasdynamic(const std::vector<int>& hs) {
@@ -286,6 +316,7 @@ int e4c_set_thermochem(const e4c_thermochem* tc) {
     if (set_thermochem_constants(*tc) != 0) return fail(E4C_ERR_CUDA, "copy of the mixture failed");
     c.have_thermochem = true;
     c.nreac = tc->nreac;
+    for (int i = 0; i < 5; ++i) c.seed.mol.M[i] = tc->M[i];
     return E4C_OK;
 }
 
@@ -315,12 +346,12 @@ int e4c_chemistry_counters(long long* out, int reset) {
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (!out) return fail(E4C_ERR_ARG, "null output");
     unsigned long long* hp = static_cast<unsigned long long*>(c.host_pinned) + 32;
-    E4C_CUDA(cudaMemcpyAsync(hp, c.d_chem_stats, 3 * sizeof(unsigned long long),
+    E4C_CUDA(cudaMemcpyAsync(hp, c.d_chem_stats, 4 * sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost, c.stream));
     if (reset)
         E4C_CUDA(cudaMemsetAsync(c.d_chem_stats, 0, 4 * sizeof(unsigned long long), c.stream));
     E4C_CUDA(cudaStreamSynchronize(c.stream));
-    for (int q = 0; q < 3; ++q) out[q] = (long long)hp[q];
+    for (int q = 0; q < 4; ++q) out[q] = (long long)hp[q];
     return E4C_OK;
 }
 
@@ -340,6 +371,10 @@ int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* b
     BlockHost b;
     int rc = c.build_block(ni, nj, nk, vtx_xyz, bc_type, inflow_prim, b);
     if (rc != E4C_OK) return rc;
+    if (c.cfg.reacting) {
+        rc = c.ensure_chem_work(b.ncell);
+        if (rc != E4C_OK) return rc;
+    }
     c.blocks.push_back(b);
     c.blocks.back().v.block_id = int(c.blocks.size()) - 1;
     c.reset_graphs();

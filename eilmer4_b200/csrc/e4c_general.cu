@@ -9,26 +9,9 @@
 // Cartesian 3-D case has its own fused kernel in e4c_fused.cu.
 #include <cfloat>
 
-#include "e4c_kernels.h"
-#include "e4c_physics.cuh"
-#include "e4c_thermo.cuh"
+#include "e4c_cells.cuh"
 
 namespace e4c {
-
-// Thermally perfect mixture and mechanism of the context (e4c_set_thermochem).
-__constant__ e4c_thermochem c_tc;
-
-int set_thermochem_constants(const e4c_thermochem& tc) {
-    return cudaMemcpyToSymbol(c_tc, &tc, sizeof(tc)) == cudaSuccess ? 0 : -1;
-}
-
-__device__ __forceinline__ size_t pidx(const BlockView& b, int i, int j, int k) {
-    return (size_t(k) * b.njdim + j) * b.nidim + i;
-}
-
-__device__ __forceinline__ void set_status(SimDev* sim, int code) {
-    if (atomicCAS(&sim->status, 0, code) == 0) sim->status_step = sim->step;
-}
 
 // ---------------------------------------------------------------------------
 // Geometry (src/geom/elements/properties.d, src/eilmer/fvinterface.d:265-317)
@@ -365,395 +348,6 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
 }
 
 // ---------------------------------------------------------------------------
-// Face flux: reconstruction + flux for one face
-// (sfluidblock.d:2190-2344, onedinterp.d:435-585, fluxcalc.d:26-128)
-// ---------------------------------------------------------------------------
-template <int NSP>
-__device__ __forceinline__ void load_prim(const BlockView& b, size_t c, Prim<double, NSP>& s) {
-    s.rho = b.W[W_RHO * b.npad + c];
-    s.vel = {b.W[W_VX * b.npad + c], b.W[W_VY * b.npad + c], b.W[W_VZ * b.npad + c]};
-    s.p = b.W[W_P * b.npad + c];
-    s.u = b.W[W_U * b.npad + c];
-    s.a = b.W[W_A * b.npad + c];
-    s.T = b.W[W_T * b.npad + c];
-    if (NSP > 1) {
-#pragma unroll
-        for (int q = 0; q < NSP; ++q) s.massf[q] = b.W[(W_NBASE + q) * b.npad + c];
-    } else {
-        s.massf[0] = 1.0;
-    }
-}
-
-// interp_l2r2 rotates the velocities of its four stencil cells into the face
-// frame and back again in place (onedinterp.d:445-454, 576-584), so a cell
-// enters each face with the round-off of every earlier face, in the loop order
-// of sfluidblock.d:2190-2344, that it took part in.  For frames made of signed
-// unit axes a round trip is exact (up to the sign of a zero) and is skipped.
-__device__ __forceinline__ bool frame_is_axis(const double* fg, size_t npad, size_t f) {
-    for (int v = 0; v < 3; ++v) {
-        int ones = 0;
-        for (int c = 0; c < 3; ++c) {
-            const double x = fg[(3 * v + c) * npad + f];
-            if (x == 1.0 || x == -1.0) ++ones;
-            else if (x != 0.0) return false;
-        }
-        if (ones != 1) return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ void roundtrip(V3<double>& v, const double* fg, size_t npad, size_t f) {
-    if (frame_is_axis(fg, npad, f)) return;
-    const V3<double> n{fg[0 * npad + f], fg[1 * npad + f], fg[2 * npad + f]};
-    const V3<double> t1{fg[3 * npad + f], fg[4 * npad + f], fg[5 * npad + f]};
-    const V3<double> t2{fg[6 * npad + f], fg[7 * npad + f], fg[8 * npad + f]};
-    to_local(v, n, t1, t2);
-    to_global(v, n, t1, t2);
-}
-
-// Velocity of stencil cell (ci,cj,ck) as the reference holds it when it
-// reaches the face of direction dir at index fpos along dir.
-__device__ void replay_roundtrips(const BlockView& b, int dir, int fpos, int ci, int cj, int ck,
-                                  V3<double>& v) {
-    const int c[3] = {ci, cj, ck};
-    const int lo[3] = {b.imin, b.jmin, b.kmin}, hi[3] = {b.imax, b.jmax, b.kmax};
-    const double* fgs[3] = {b.fgi, b.fgj, b.fgk};
-    // faces of the earlier directions (their loops cover interior rows only)
-    if (c[dir] >= lo[dir] && c[dir] <= hi[dir]) {
-        for (int d = 0; d < dir; ++d)
-            for (int g = c[d] - 1; g <= c[d] + 2; ++g) {
-                if (g < lo[d] || g > hi[d] + 1) continue;
-                int p[3] = {c[0], c[1], c[2]};
-                p[d] = g;
-                roundtrip(v, fgs[d], b.npad, pidx(b, p[0], p[1], p[2]));
-            }
-    }
-    // earlier faces of this direction in the same row
-    for (int g = c[dir] - 1; g <= c[dir] + 2 && g < fpos; ++g) {
-        if (g < lo[dir] || g > hi[dir] + 1) continue;
-        int p[3] = {c[0], c[1], c[2]};
-        p[dir] = g;
-        roundtrip(v, fgs[dir], b.npad, pidx(b, p[0], p[1], p[2]));
-    }
-}
-
-// update_thermo_from_rhou of a reconstructed state: ideal gas, or the
-// thermally perfect mixture started from the cell-centre temperature (the
-// state was copied from the cell, onedinterp.d / sfluidblock.d:2199-2208)
-template <int NSP, int GAS>
-__device__ __forceinline__ bool rhou_update(const FluxOpts& o, Prim<double, NSP>& s) {
-    if (GAS == 0) {
-        double T;
-        return ideal_rhou<double>(o.gas, s.rho, s.u, s.p, T);
-    }
-    TPState<NSP> Q;
-    Q.rho = s.rho; Q.u = s.u; Q.T = s.T; Q.p = s.p; Q.a = s.a;
-#pragma unroll
-    for (int i = 0; i < NSP; ++i) Q.massf[i] = s.massf[i];
-    TPGas<NSP> g(c_tc);
-    if (!g.rhou(Q)) return false;
-    s.p = Q.p; s.T = Q.T; s.u = Q.u;
-    return true;
-}
-
-template <int NSP, int FLUX, int GAS>
-__global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
-    if (sim->status != 0 || sim->finished) return;
-    const int ni = b.ni + (dir == 0), nj = b.nj + (dir == 1), nk = b.nk + (dir == 2);
-    const long long n = (long long)ni * nj * nk;
-    const size_t stride = dir == 0 ? 1 : (dir == 1 ? size_t(b.nidim) : size_t(b.nidim) * b.njdim);
-    const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
-    double* Fo = dir == 0 ? b.Fi : (dir == 1 ? b.Fj : b.Fk);
-    constexpr int NSPC = NSP > 1 ? NSP : 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i = b.imin + int(t % ni);
-        int j = b.jmin + int((t / ni) % nj);
-        int k = b.kmin + int(t / ((long long)ni * nj));
-        const size_t f = pidx(b, i, j, k);
-        const size_t cR0 = f, cL0 = f - stride, cL1 = f - 2 * stride, cR1 = f + stride;
-        Frame<double> fr;
-        fr.n = {fg[0 * b.npad + f], fg[1 * b.npad + f], fg[2 * b.npad + f]};
-        fr.t1 = {fg[3 * b.npad + f], fg[4 * b.npad + f], fg[5 * b.npad + f]};
-        fr.t2 = {fg[6 * b.npad + f], fg[7 * b.npad + f], fg[8 * b.npad + f]};
-        Prim<double, NSP> sL1, sL0, sR0, sR1;
-        load_prim<NSP>(b, cL0, sL0);
-        load_prim<NSP>(b, cR0, sR0);
-        Prim<double, NSP> Lf = sL0, Rt = sR0;
-        if (o.order2) {
-            load_prim<NSP>(b, cL1, sL1);
-            load_prim<NSP>(b, cR1, sR1);
-            if (o.local_frame && !b.axis_frames) {
-                const int fpos = dir == 0 ? i : (dir == 1 ? j : k);
-                const int di = dir == 0, dj = dir == 1, dk = dir == 2;
-                replay_roundtrips(b, dir, fpos, i - 2 * di, j - 2 * dj, k - 2 * dk, sL1.vel);
-                replay_roundtrips(b, dir, fpos, i - di, j - dj, k - dk, sL0.vel);
-                replay_roundtrips(b, dir, fpos, i, j, k, sR0.vel);
-                replay_roundtrips(b, dir, fpos, i + di, j + dj, k + dk, sR1.vel);
-            }
-            const double* len = b.cgeom + size_t(1 + dir) * b.npad;
-            if (o.local_frame) {
-                to_local(sL1.vel, fr.n, fr.t1, fr.t2);
-                to_local(sL0.vel, fr.n, fr.t1, fr.t2);
-                to_local(sR0.vel, fr.n, fr.t1, fr.t2);
-                to_local(sR1.vel, fr.n, fr.t1, fr.t2);
-            }
-            L2R2<double> r;
-            r.prepare(len[cL1], len[cL0], len[cR0], len[cR1]);
-            r.scalar(o.limiter, o.clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
-            r.scalar(o.limiter, o.clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
-            r.scalar(o.limiter, o.clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
-            if (NSP > 1) {
-#pragma unroll
-                for (int q = 0; q < NSP; ++q)
-                    r.scalar(o.limiter, o.clip, sL1.massf[q], sL0.massf[q], sR0.massf[q],
-                             sR1.massf[q], Lf.massf[q], Rt.massf[q]);
-                if (!scale_mass_fractions<double, NSP>(Lf.massf))
-                    for (int q = 0; q < NSP; ++q) Lf.massf[q] = sL0.massf[q];
-                if (!scale_mass_fractions<double, NSP>(Rt.massf))
-                    for (int q = 0; q < NSP; ++q) Rt.massf[q] = sR0.massf[q];
-            } else {
-                Lf.massf[0] = 1.0;
-                Rt.massf[0] = 1.0;
-            }
-            r.scalar(o.limiter, o.clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
-            r.scalar(o.limiter, o.clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
-            // codeForThermoUpdateBoth("rhou"), onedinterp.d:1039-1068
-            if (!rhou_update<NSP, GAS>(o, Lf)) Lf = sL0;
-            if (!rhou_update<NSP, GAS>(o, Rt)) Rt = sR0;
-            if (o.local_frame) {
-                to_global(Lf.vel, fr.n, fr.t1, fr.t2);
-                to_global(Rt.vel, fr.n, fr.t1, fr.t2);
-            }
-        }
-        // compute_interface_flux, fluxcalc.d:26-128 (fixed grid)
-        to_local(Lf.vel, fr.n, fr.t1, fr.t2);
-        to_local(Rt.vel, fr.n, fr.t1, fr.t2);
-        double F[5 + NSPC];
-        if (FLUX == 1) hllc<double, NSP, NSPC>(Lf, Rt, F);
-        else ausmdv<double, NSP, NSPC>(Lf, Rt, F);
-        V3<double> m{F[1], F[2], F[3]};
-        to_global(m, fr.n, fr.t1, fr.t2);
-        F[1] = m.x; F[2] = m.y; F[3] = m.z;
-#pragma unroll
-        for (int q = 0; q < 5 + NSPC; ++q) Fo[q * b.npad + f] = F[q];
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Cell update: time_derivatives + stage update + decode + validity check
-// (fvcell.d:735-875, 1153-1311, 563-732; fluidblock.d:433-499)
-// ---------------------------------------------------------------------------
-template <int NSP, int GAS>
-__global__ void k_update(BlockView b, SimDev* sim, GasConsts gas, int stage, int final_stage) {
-    if (sim->status != 0 || sim->finished) return;
-    constexpr int NSPC = NSP > 1 ? NSP : 0;
-    constexpr int NV = 5 + NSPC;
-    const long long n = (long long)b.ni * b.nj * b.nk;
-    const double dt = sim->dt_global;
-    int bad = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i = b.imin + int(t % b.ni);
-        int j = b.jmin + int((t / b.ni) % b.nj);
-        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
-        const size_t c = pidx(b, i, j, k);
-        // faces north, east, south, west, top, bottom (sfluidblock.d:506-517)
-        const size_t sj = b.nidim, sk = size_t(b.nidim) * b.njdim;
-        const double* Fq[6] = {b.Fj, b.Fi, b.Fj, b.Fi, b.Fk, b.Fk};
-        const double* Gq[6] = {b.fgj, b.fgi, b.fgj, b.fgi, b.fgk, b.fgk};
-        const size_t fq[6] = {c + sj, c + 1, c, c, c + sk, c};
-        const double outsign[6] = {1.0, 1.0, -1.0, -1.0, 1.0, -1.0};
-        const int nf = (b.dim == 3) ? 6 : 4;
-        double integral[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) integral[v] = 0.0;
-        for (int q = 0; q < nf; ++q) {
-            double area = outsign[q] * Gq[q][9 * b.npad + fq[q]];
-            const double* F = Fq[q];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                if (v == 3 && b.dim != 3) continue;
-                integral[v] -= F[v * b.npad + fq[q]] * area;
-            }
-        }
-        double vol_inv = 1.0 / b.cgeom[c];
-        double Un[NV];
-        if (stage == 1) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                double d0 = vol_inv * integral[v];
-                if (!final_stage) b.dUdt0[v * b.npad + c] = d0;
-                Un[v] = b.U0[v * b.npad + c] + dt * 1.0 * d0;
-            }
-        } else {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                double d1 = vol_inv * integral[v];
-                Un[v] = b.U0[v * b.npad + c] + dt * (0.5 * b.dUdt0[v * b.npad + c] + 0.5 * d1);
-            }
-        }
-        // decode_conserved (ideal gas; adjust_invalid_cell_data = false,
-        // ignore_low_T_thermo_update_failure = true, suggested_low_T_value = 200 K)
-        bool data_bad = false;
-        double rho = Un[0], vx = 0, vy = 0, vz = 0, u = 0, p = 0, T = 0, a = 0;
-        double massf[NSP];
-        massf[0] = 1.0;
-        if (!(Un[0] > 0.0)) {
-            set_status(sim, -5);
-            data_bad = true;
-        } else {
-            double dinv = 1.0 / rho;
-            vx = Un[1] * dinv; vy = Un[2] * dinv; vz = Un[3] * dinv;
-            u = Un[4] * dinv;
-            double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
-            u -= ke;
-            if (NSPC > 0) {
-#pragma unroll
-                for (int s = 0; s < NSPC; ++s) massf[s] = Un[5 + s] * dinv;
-                if (!scale_mass_fractions<double, NSP>(massf)) { set_status(sim, -6); data_bad = true; }
-            }
-            bool ok_thermo;
-            if (GAS == 0) {
-                ok_thermo = ideal_rhou<double>(gas, rho, u, p, T);
-            } else {
-                // thermally perfect: the Newton starts from the cell's previous T
-                TPState<NSP> Q;
-                Q.rho = rho; Q.u = u; Q.T = b.W[W_T * b.npad + c];
-#pragma unroll
-                for (int s = 0; s < NSP; ++s) Q.massf[s] = massf[s];
-                TPGas<NSP> g(c_tc);
-                ok_thermo = g.rhou(Q);
-                p = Q.p; T = Q.T; u = Q.u;
-            }
-            if (!ok_thermo) {
-                T = 200.0;
-                if (GAS == 0) {
-                    p = rho * gas.Rgas * T;
-                    u = gas.Cv * T;
-                } else {
-                    TPState<NSP> Q;
-                    Q.rho = rho; Q.T = T;
-#pragma unroll
-                    for (int s = 0; s < NSP; ++s) Q.massf[s] = massf[s];
-                    TPGas<NSP> g(c_tc);
-                    g.rhoT(Q);
-                    p = Q.p; u = Q.u;
-                }
-                // encode_conserved(gtl, ftl)
-                Un[0] = rho;
-                Un[1] = rho * vx; Un[2] = rho * vy; Un[3] = rho * vz;
-                double ke2 = 0.5 * (vx * vx + vy * vy + vz * vz);
-                Un[4] = rho * (u + ke2);
-#pragma unroll
-                for (int s = 0; s < NSPC; ++s) Un[5 + s] = rho * massf[s];
-            }
-            if (GAS == 0) {
-                a = ideal_sound_speed<double>(gas, T);
-            } else {
-                TPGas<NSP> g(c_tc);
-                a = g.sound_speed(massf, T);
-            }
-        }
-        // write the new state
-        double* W = b.W;
-        W[W_RHO * b.npad + c] = rho;
-        W[W_VX * b.npad + c] = vx; W[W_VY * b.npad + c] = vy; W[W_VZ * b.npad + c] = vz;
-        W[W_P * b.npad + c] = p; W[W_T * b.npad + c] = T;
-        W[W_U * b.npad + c] = u; W[W_A * b.npad + c] = a;
-#pragma unroll
-        for (int s = 0; s < NSPC; ++s) W[(W_NBASE + s) * b.npad + c] = massf[s];
-        if (final_stage) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) b.U0[v * b.npad + c] = Un[v];
-        }
-        // count_invalid_cells / FlowState.check_data (flowstate.d:345-388,
-        // gas_state.d:199-241, limits fvcore.d:20-27)
-        bool ok = !data_bad;
-        if (!isfinite(rho) || rho < 1.01 * 0.0) ok = false;
-        if (!isfinite(T) || T < 1.01 * 1.0) ok = false;
-        if (!isfinite(p)) ok = false;
-        if (!isfinite(a)) ok = false;
-        double fsum = 0.0;
-        for (int s = 0; s < NSP; ++s) fsum += massf[s];
-        if (fsum < 0.99 || fsum > 1.01 || !isfinite(fsum)) ok = false;
-        if (fabs(vx) > 30000.0 || fabs(vy) > 30000.0 || fabs(vz) > 30000.0) ok = false;
-        if (T < 0.0 || T > 50000.0) ok = false;
-        if (!ok) ++bad;
-    }
-    if (bad) atomicAdd(&sim->bad_cells, bad);
-}
-
-// ---------------------------------------------------------------------------
-// Chemistry: FVCell.thermochemical_increment for every interior cell
-// (simcore.d:1489-1505, fvcell.d:1510-1621), one cell per thread
-// ---------------------------------------------------------------------------
-template <int NSP, int NR>
-__global__ void k_chem(BlockView b, SimDev* sim, double T_frozen, const double* dt_p,
-                       const double* guess, unsigned long long* stats) {
-    // guess (optional): [NSP + 1][ncell] over the interior cells in (i, j, k)
-    // order, predicted end concentrations and temperature.  stats (optional):
-    // reacting cells, Newton iterations, cells that needed the sub-cycled
-    // recovery, accumulated.
-    if (sim->status != 0 || sim->finished) return;
-    const long long n = (long long)b.ni * b.nj * b.nk;
-    const double dt = *dt_p;
-    unsigned int my_cells = 0, my_newton = 0, my_recovered = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = b.imin + int(t % b.ni);
-        const int j = b.jmin + int((t / b.ni) % b.nj);
-        const int k = b.kmin + int(t / ((long long)b.ni * b.nj));
-        const size_t c = pidx(b, i, j, k);
-        TPState<NSP> Q;
-        Q.rho = b.W[W_RHO * b.npad + c];
-        Q.p = b.W[W_P * b.npad + c];
-        Q.T = b.W[W_T * b.npad + c];
-        Q.u = b.W[W_U * b.npad + c];
-        Q.a = b.W[W_A * b.npad + c];
-#pragma unroll
-        for (int s = 0; s < NSP; ++s) Q.massf[s] = b.W[(W_NBASE + s) * b.npad + c];
-        if (Q.T <= T_frozen) continue;
-        double g[NSP + 1];
-        if (guess) {
-#pragma unroll
-            for (int s = 0; s <= NSP; ++s) g[s] = guess[s * n + t];
-        }
-        double dt_chem = b.dt_chem[c];
-        ChemCount cnt;
-        int rc = thermochemical_increment_d<NSP, NR>(c_tc, T_frozen, Q, dt, dt_chem,
-                                                     guess ? g : nullptr, &cnt);
-        my_cells += 1;
-        my_newton += cnt.newton;
-        my_recovered += cnt.recovered;
-        if (rc != 0) {
-            set_status(sim, rc);
-            continue;
-        }
-        b.dt_chem[c] = dt_chem;
-        b.W[W_P * b.npad + c] = Q.p;
-        b.W[W_T * b.npad + c] = Q.T;
-        b.W[W_U * b.npad + c] = Q.u;
-        b.W[W_A * b.npad + c] = Q.a;
-#pragma unroll
-        for (int s = 0; s < NSP; ++s) {
-            b.W[(W_NBASE + s) * b.npad + c] = Q.massf[s];
-            b.U0[(5 + s) * b.npad + c] = Q.rho * Q.massf[s];
-        }
-    }
-    if (stats) {
-        my_cells = __reduce_add_sync(0xffffffffu, my_cells);
-        my_newton = __reduce_add_sync(0xffffffffu, my_newton);
-        my_recovered = __reduce_add_sync(0xffffffffu, my_recovered);
-        if ((threadIdx.x & 31) == 0 && my_cells > 0) {
-            atomicAdd(stats + 0, (unsigned long long)my_cells);
-            atomicAdd(stats + 1, (unsigned long long)my_newton);
-            atomicAdd(stats + 2, (unsigned long long)my_recovered);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Time step: signal_frequency + block min/max (fvcell.d:1624-1705,
 // fluidblock.d:776-862)
 // ---------------------------------------------------------------------------
@@ -922,8 +516,7 @@ void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int d
     const int T = 128;
     const int g = grid_for(n, T);
     if (b.nsp == 5) {
-        if (o.flux == 1) k_flux<5, 1, 1><<<g, T, 0, s>>>(b, sim, o, dir);
-        else k_flux<5, 0, 1><<<g, T, 0, s>>>(b, sim, o, dir);
+        launch_flux_tp(b, sim, o, dir, g, T, s);
     } else {
         if (o.flux == 1) k_flux<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, dir);
         else k_flux<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, dir);
@@ -934,17 +527,8 @@ void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int st
                    int final_stage, cudaStream_t s) {
     long long n = (long long)b.ni * b.nj * b.nk;
     const int T = 128;
-    if (b.nsp == 5) k_update<5, 1><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
+    if (b.nsp == 5) launch_update_tp(b, sim, gas, stage, final_stage, grid_for(n, T), T, s);
     else k_update<1, 0><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
-}
-
-int launch_chem(const BlockView& b, SimDev* sim, double T_frozen, const double* dt, int nreac,
-                const double* guess, unsigned long long* stats, cudaStream_t s) {
-    long long n = (long long)b.ni * b.nj * b.nk;
-    const int T = 64;
-    if (b.nsp != 5 || nreac != 5) return -1;
-    k_chem<5, 5><<<grid_for(n, T), T, 0, s>>>(b, sim, T_frozen, dt, guess, stats);
-    return 0;
 }
 
 void launch_dt_reset(unsigned long long* acc, int nb, cudaStream_t s) {

@@ -20,6 +20,27 @@ struct BlockHost {
     FusedDesc f{};          // fused path: storage and uniform geometry
 };
 
+// The learned chemistry seed (e4c_seed.cu): network, training set, guesses.
+struct SeedNet {
+    float* d_params = nullptr;     // FP32 master parameters
+    float* d_grad = nullptr;       // gradient, Adam moments (same layout)
+    float* d_m = nullptr;
+    float* d_v = nullptr;
+    uint16_t* d_packed = nullptr;  // BF16 image used by the tensor-core kernels
+    double* d_norm = nullptr;
+    float* d_loss = nullptr;
+    double norm[E4C_SEED_NNORM] = {};
+    bool have_weights = false;
+    bool enabled = false;
+    int adam_t = 0;
+    double* d_feat = nullptr;      // training pairs: features [n][8], targets [n][6]
+    double* d_targ = nullptr;
+    long long n = 0, cap = 0;
+    double* d_guess = nullptr;     // per-cell guesses of the chemistry step [6][ncell]
+    size_t guess_cap = 0;
+    SeedMolar mol{};
+};
+
 struct GraphSlot {
     cudaGraphExec_t exec = nullptr;
     long long nkernels = 0;   // kernel nodes in the graph
@@ -55,6 +76,11 @@ struct Ctx {
     int nreac = 0;
     // chemistry counters: reacting cells, Newton iterations, recovered cells
     unsigned long long* d_chem_stats = nullptr;
+    // chemistry work list (cells needing Newton work) and its length
+    int* d_chem_work = nullptr;
+    int* d_chem_nwork = nullptr;
+    size_t chem_work_cap = 0;
+    SeedNet seed;
     // fused path: descriptors of every fused block, rebuilt when blocks change
     FusedDesc* d_descs = nullptr;
     int descs_cap = 0;
@@ -85,6 +111,13 @@ struct Ctx {
     void enqueue_stage(const std::vector<int>& hs, int stage, int final_stage);
     void enqueue_gasdynamic(const std::vector<int>& hs);
     void enqueue_chemistry(const std::vector<int>& hs, const double* dt);
+    // learned chemistry seed
+    int seed_alloc_net();
+    int seed_pack();
+    int seed_dataset_reserve(long long n);
+    int seed_guess_reserve(size_t ncell);
+    void seed_infer(const BlockView& v, const double* dt, const int* work, const int* nwork);
+    int ensure_chem_work(size_t ncell);
     void enqueue_dt(const std::vector<int>& hs, const int* d_hl, const double* dt_current,
                     int check_cfl, int step0, SimDev* sim, double* out);
     std::vector<int> all_blocks() const;

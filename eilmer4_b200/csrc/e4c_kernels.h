@@ -41,9 +41,25 @@ void launch_begin_run(SimDev* sim, double max_time, cudaStream_t s);
 void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
 // thermally perfect mixture / mechanism into constant memory; chemistry of one block
 int set_thermochem_constants(const e4c_thermochem& tc);
+// thermally perfect face fluxes / cell updates (e4c_tp.cu)
+void launch_flux_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, int g,
+                    int T, cudaStream_t s);
+void launch_update_tp(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
+                      int final_stage, int g, int T, cudaStream_t s);
+// training pairs of the chemistry seed: list of the cells needing Newton work
+// over dt, then sampled plain chemistry updates (features [n][8], targets [n][6])
+void launch_seed_active_list(const BlockView& b, double T_frozen, double dt, int* list,
+                             int* count, cudaStream_t s);
+void launch_seed_collect(const BlockView& b, const int* hot, int nhot, long long n,
+                         unsigned long long seed, double dt, double T_frozen, double* feat,
+                         double* targ, cudaStream_t s);
+// chemistry: pass 1 (every cell; lists cells needing Newton work) and
+// pass 2 (the listed cells, optionally from a guess)
 int launch_chem(const BlockView& b, SimDev* sim, double T_frozen, const double* dt, int nreac,
-                const double* guess, unsigned long long* stats,
-                cudaStream_t s);
+                int* work, int* nwork, unsigned long long* stats, cudaStream_t s);
+int launch_chem_work(const BlockView& b, SimDev* sim, double T_frozen, const double* dt,
+                     int nreac, const int* work, const int* nwork, const double* guess,
+                     unsigned long long* stats, cudaStream_t s);
 
 // fused uniform path (e4c_fused.cu: FP64, e4c_fused32.cu: FP32 flux)
 struct FusedLaunch {

@@ -1,0 +1,1027 @@
+// e4c_seed.cu -- the learned chemistry seed: a small multilayer perceptron
+// that predicts the end state of a cell's chemistry update, used as the
+// Newton starting point of the point-implicit step.  No counterpart in the
+// reference.
+//
+// Network: input (log T, log p, Y[5], log dt) normalised by the training-set
+// mean and spread; three hidden layers of 64 units with the tanh-form GELU
+// (Hendrycks & Gimpel 2016); output 6 values, the normalised transforms
+// asinh(dY_s / sY) (5 species) and asinh(dT / sT).  Weights are kept in FP32
+// (master copy for Adam) and run as BF16 on the tensor cores with FP32
+// accumulation: mma.sync m16n8k16, one warp per 16 samples, the activations
+// of one layer passed to the next in registers (the accumulator fragment of
+// two adjacent 8-column tiles is exactly the A fragment of one 16-column
+// k-tile).  Training runs forward and backward in one kernel per mini-batch
+// of 64-sample tiles, with weight gradients accumulated over the tile by
+// tensor-core products of the stored activations and output gradients.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <vector>
+
+#include "e4c_internal.h"
+
+namespace e4c {
+
+#define E4C_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Parameter layout (FP32 master vector) and the packed BF16 image
+// ---------------------------------------------------------------------------
+constexpr int P_W1 = 0;               // [64][8]
+constexpr int P_B1 = P_W1 + 64 * 8;   // [64]
+constexpr int P_W2 = P_B1 + 64;       // [64][64]
+constexpr int P_B2 = P_W2 + 64 * 64;
+constexpr int P_W3 = P_B2 + 64;       // [64][64]
+constexpr int P_B3 = P_W3 + 64 * 64;
+constexpr int P_W4 = P_B3 + 64;       // [6][64]
+constexpr int P_B4 = P_W4 + 6 * 64;   // [6]
+constexpr int P_N = P_B4 + 6;
+static_assert(P_N == E4C_SEED_NPARAM, "parameter count");
+
+// Packed image (bf16 elements), copied as is into shared memory.  Row strides
+// of 24 and 72 elements keep the fragment loads free of bank conflicts.
+constexpr int S16 = 24, S64 = 72;
+constexpr int OFF_W1 = 0;                      // W1  [64][24], cols 8.. zero
+constexpr int OFF_W2 = OFF_W1 + 64 * S16;      // W2  [64][72]
+constexpr int OFF_W3 = OFF_W2 + 64 * S64;      // W3  [64][72]
+constexpr int OFF_W4 = OFF_W3 + 64 * S64;      // W4  [8][72], rows 6, 7 zero
+constexpr int OFF_W2T = OFF_W4 + 8 * S64;      // W2^T [64][72]
+constexpr int OFF_W3T = OFF_W2T + 64 * S64;    // W3^T [64][72]
+constexpr int OFF_W4T = OFF_W3T + 64 * S64;    // W4^T [64][24], cols 6.. zero
+constexpr int PACKED_N = OFF_W4T + 64 * S16;   // 22080
+constexpr int PACKED_FWD = OFF_W2T;            // the forward part
+static_assert((PACKED_N * 2) % 16 == 0 && (PACKED_FWD * 2) % 16 == 0, "uint4 copies");
+constexpr int NBIAS = 200;                     // b1, b2, b3 (64 each), b4 (6) + 2 zeros
+
+// Norm vector: mu_in[8], sd_in[8], mu_out[6], sd_out[6], sY, sT.
+constexpr int N_MU_IN = 0, N_SD_IN = 8, N_MU_OUT = 16, N_SD_OUT = 22, N_SY = 28, N_ST = 29;
+static_assert(E4C_SEED_NNORM == 30, "norm layout");
+
+constexpr int TILE = 64;                 // samples per CTA in training
+constexpr int SMEM_TRAIN = PACKED_N * 2 + NBIAS * 4 + (2 * 64 * S16 + 6 * 64 * S64) * 2;
+
+// ---------------------------------------------------------------------------
+// Fragment helpers (PTX ISA, mma.m16n8k16 with .bf16 inputs): g = lane/4,
+// t = lane%4; A (16x16, row) regs {A[g][2t..], A[g+8][2t..], A[g][2t+8..],
+// A[g+8][2t+8..]}; B (16x8, col) regs {B[2t..][g], B[2t+8..][g]};
+// C (16x8) {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ uint32_t pack_raw(uint16_t lo, uint16_t hi) {
+    return uint32_t(lo) | (uint32_t(hi) << 16);
+}
+
+__device__ __forceinline__ float bf16_to_f(uint16_t r) {
+    return __uint_as_float(uint32_t(r) << 16);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// B fragment of the weight matrix M stored [n][k] (row n contiguous in k).
+__device__ __forceinline__ void load_b(const uint16_t* M, int S, int n0, int k0, int lane,
+                                       uint32_t& b0, uint32_t& b1) {
+    const uint16_t* p = M + (n0 + (lane >> 2)) * S + k0 + 2 * (lane & 3);
+    b0 = *reinterpret_cast<const uint32_t*>(p);
+    b1 = *reinterpret_cast<const uint32_t*>(p + 8);
+}
+
+// acc[j] (16 x 8 tile j of 64 outputs) = A (16 x 16*KT) * M^T + bias.
+template <int KT>
+__device__ __forceinline__ void dense64(const uint32_t (&a)[KT][4], const uint16_t* M, int S,
+                                        const float* bias, float (&acc)[8][4], int lane) {
+    const int t = lane & 3;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const float bl = bias ? bias[8 * j + 2 * t] : 0.0f;
+        const float bh = bias ? bias[8 * j + 2 * t + 1] : 0.0f;
+        acc[j][0] = bl;
+        acc[j][1] = bh;
+        acc[j][2] = bl;
+        acc[j][3] = bh;
+#pragma unroll
+        for (int kk = 0; kk < KT; ++kk) {
+            uint32_t b0, b1;
+            load_b(M, S, 8 * j, 16 * kk, lane, b0, b1);
+            mma_bf16(acc[j], a[kk], b0, b1);
+        }
+    }
+}
+
+// Output layer: 8 columns (6 used), K = 64.
+__device__ __forceinline__ void dense_out(const uint32_t (&a)[4][4], const uint16_t* M,
+                                          const float* bias, float (&acc)[4], int lane) {
+    const int t = lane & 3;
+    acc[0] = bias[2 * t];
+    acc[1] = bias[2 * t + 1];
+    acc[2] = acc[0];
+    acc[3] = acc[1];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        uint32_t b0, b1;
+        load_b(M, S64, 0, 16 * kk, lane, b0, b1);
+        mma_bf16(acc, a[kk], b0, b1);
+    }
+}
+
+__device__ __forceinline__ float gelu_f(float x) {
+    const float c = 0.7978845608028654f;  // sqrt(2/pi)
+    const float u = c * (x + 0.044715f * x * x * x);
+    return 0.5f * x * (1.0f + tanhf(u));
+}
+
+__device__ __forceinline__ float gelu_grad_f(float x) {
+    const float c = 0.7978845608028654f;
+    const float x2 = x * x;
+    const float th = tanhf(c * (x + 0.044715f * x2 * x));
+    return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * c * (1.0f + 3.0f * 0.044715f * x2);
+}
+
+// GELU in place (keeping the derivative when dg is given), then the BF16 A
+// fragments of the next layer.
+__device__ __forceinline__ void gelu_to_a(float (&z)[8][4], uint32_t (&a)[4][4],
+                                          float (*dg)[4]) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (dg) dg[j][e] = gelu_grad_f(z[j][e]);
+            z[j][e] = gelu_f(z[j][e]);
+        }
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        a[kk][0] = pack_bf16(z[2 * kk][0], z[2 * kk][1]);
+        a[kk][1] = pack_bf16(z[2 * kk][2], z[2 * kk][3]);
+        a[kk][2] = pack_bf16(z[2 * kk + 1][0], z[2 * kk + 1][1]);
+        a[kk][3] = pack_bf16(z[2 * kk + 1][2], z[2 * kk + 1][3]);
+    }
+}
+
+// Backward through GELU: dZ = dH * GELU'(Z), as A fragments.
+__device__ __forceinline__ void times_to_a(const float (&dh)[8][4], const float (&dg)[8][4],
+                                           uint32_t (&a)[4][4]) {
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        a[kk][0] = pack_bf16(dh[2 * kk][0] * dg[2 * kk][0], dh[2 * kk][1] * dg[2 * kk][1]);
+        a[kk][1] = pack_bf16(dh[2 * kk][2] * dg[2 * kk][2], dh[2 * kk][3] * dg[2 * kk][3]);
+        a[kk][2] = pack_bf16(dh[2 * kk + 1][0] * dg[2 * kk + 1][0],
+                             dh[2 * kk + 1][1] * dg[2 * kk + 1][1]);
+        a[kk][3] = pack_bf16(dh[2 * kk + 1][2] * dg[2 * kk + 1][2],
+                             dh[2 * kk + 1][3] * dg[2 * kk + 1][3]);
+    }
+}
+
+// Store a warp's 16 x 64 A fragments (BF16) as rows row0.. of a [.][S] array.
+__device__ __forceinline__ void store_a(uint16_t* H, int S, int row0, const uint32_t (&a)[4][4],
+                                        int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+        uint32_t* r0 = reinterpret_cast<uint32_t*>(H + (row0 + g) * S + 16 * kk + 2 * t);
+        uint32_t* r8 = reinterpret_cast<uint32_t*>(H + (row0 + g + 8) * S + 16 * kk + 2 * t);
+        r0[0] = a[kk][0];
+        r8[0] = a[kk][1];
+        r0[4] = a[kk][2];
+        r8[4] = a[kk][3];
+    }
+}
+
+__device__ __forceinline__ void load_weights(uint16_t* sw, float* sb, const uint16_t* packed,
+                                             const float* params, int nelem) {
+    const uint4* src = reinterpret_cast<const uint4*>(packed);
+    uint4* dst = reinterpret_cast<uint4*>(sw);
+    for (int q = threadIdx.x; q < nelem / 8; q += blockDim.x) dst[q] = src[q];
+    for (int q = threadIdx.x; q < NBIAS; q += blockDim.x) {
+        float v = 0.0f;
+        if (q < 64) v = params[P_B1 + q];
+        else if (q < 128) v = params[P_B2 + q - 64];
+        else if (q < 192) v = params[P_B3 + q - 128];
+        else if (q < 198) v = params[P_B4 + q - 192];
+        sb[q] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+// FP32 master parameters -> packed BF16 image (forward and transposed copies).
+__global__ void k_seed_pack(const float* __restrict__ w, uint16_t* __restrict__ packed) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < PACKED_N; e += gridDim.x * blockDim.x) {
+        float v = 0.0f;
+        if (e < OFF_W2) {
+            const int r = (e - OFF_W1) / S16, c = (e - OFF_W1) % S16;
+            if (c < 8) v = w[P_W1 + r * 8 + c];
+        } else if (e < OFF_W3) {
+            const int r = (e - OFF_W2) / S64, c = (e - OFF_W2) % S64;
+            if (c < 64) v = w[P_W2 + r * 64 + c];
+        } else if (e < OFF_W4) {
+            const int r = (e - OFF_W3) / S64, c = (e - OFF_W3) % S64;
+            if (c < 64) v = w[P_W3 + r * 64 + c];
+        } else if (e < OFF_W2T) {
+            const int r = (e - OFF_W4) / S64, c = (e - OFF_W4) % S64;
+            if (r < 6 && c < 64) v = w[P_W4 + r * 64 + c];
+        } else if (e < OFF_W3T) {
+            const int r = (e - OFF_W2T) / S64, c = (e - OFF_W2T) % S64;
+            if (c < 64) v = w[P_W2 + c * 64 + r];
+        } else if (e < OFF_W4T) {
+            const int r = (e - OFF_W3T) / S64, c = (e - OFF_W3T) % S64;
+            if (c < 64) v = w[P_W3 + c * 64 + r];
+        } else {
+            const int r = (e - OFF_W4T) / S16, c = (e - OFF_W4T) % S16;
+            if (c < 6) v = w[P_W4 + c * 64 + r];
+        }
+        __nv_bfloat16 b = __float2bfloat16_rn(v);
+        packed[e] = *reinterpret_cast<uint16_t*>(&b);
+    }
+}
+
+// One mini-batch: rows idx[0..nbatch) of the normalised inputs X [.][8] and
+// targets Y [.][6].  Loss = sum over rows and outputs of (z - y)^2 * inv_count;
+// its gradient is added to grad (FP32, master layout) when backward is set.
+__global__ void __launch_bounds__(128) k_seed_train(const float* __restrict__ params,
+                                                    const uint16_t* __restrict__ packed,
+                                                    const float* __restrict__ X,
+                                                    const float* __restrict__ Y,
+                                                    const int* __restrict__ idx, int nbatch,
+                                                    float inv_count, int backward,
+                                                    float* __restrict__ grad,
+                                                    float* __restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint16_t* sw = reinterpret_cast<uint16_t*>(smem);
+    float* sb = reinterpret_cast<float*>(smem + PACKED_N * 2);
+    uint16_t* sH0 = reinterpret_cast<uint16_t*>(smem + PACKED_N * 2 + NBIAS * 4);  // [64][24]
+    uint16_t* sH1 = sH0 + 64 * S16;   // [64][72]
+    uint16_t* sH2 = sH1 + 64 * S64;
+    uint16_t* sH3 = sH2 + 64 * S64;
+    uint16_t* sD1 = sH3 + 64 * S64;
+    uint16_t* sD2 = sD1 + 64 * S64;
+    uint16_t* sD3 = sD2 + 64 * S64;
+    uint16_t* sD4 = sD3 + 64 * S64;   // [64][24]
+    load_weights(sw, sb, packed, params, PACKED_N);
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int row0 = warp * 16;
+    const int ra = blockIdx.x * TILE + row0 + g, rb = ra + 8;
+    const bool va = ra < nbatch, vb = rb < nbatch;
+    const int sa = va ? idx[ra] : 0, sbi = vb ? idx[rb] : 0;
+
+    uint32_t a0[1][4];
+    a0[0][0] = pack_bf16(va ? X[sa * 8 + 2 * t] : 0.0f, va ? X[sa * 8 + 2 * t + 1] : 0.0f);
+    a0[0][1] = pack_bf16(vb ? X[sbi * 8 + 2 * t] : 0.0f, vb ? X[sbi * 8 + 2 * t + 1] : 0.0f);
+    a0[0][2] = 0u;
+    a0[0][3] = 0u;
+    *reinterpret_cast<uint32_t*>(sH0 + (row0 + g) * S16 + 2 * t) = a0[0][0];
+    *reinterpret_cast<uint32_t*>(sH0 + (row0 + g + 8) * S16 + 2 * t) = a0[0][1];
+
+    float acc[8][4];
+    float dg1[8][4], dg2[8][4], dg3[8][4];
+    uint32_t a[4][4];
+    dense64<1>(a0, sw + OFF_W1, S16, sb, acc, lane);
+    gelu_to_a(acc, a, dg1);
+    store_a(sH1, S64, row0, a, lane);
+    dense64<4>(a, sw + OFF_W2, S64, sb + 64, acc, lane);
+    gelu_to_a(acc, a, dg2);
+    store_a(sH2, S64, row0, a, lane);
+    dense64<4>(a, sw + OFF_W3, S64, sb + 128, acc, lane);
+    gelu_to_a(acc, a, dg3);
+    store_a(sH3, S64, row0, a, lane);
+    float z4[4];
+    dense_out(a, sw + OFF_W4, sb + 192, z4, lane);
+
+    // squared error on the 6 outputs and its derivative
+    float d4[4];
+    float lsum = 0.0f;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int col = 2 * t + (e & 1);
+        const bool row_ok = (e < 2) ? va : vb;
+        const int s = (e < 2) ? sa : sbi;
+        if (row_ok && col < 6) {
+            const float diff = z4[e] - Y[s * 6 + col];
+            lsum += diff * diff;
+            d4[e] = 2.0f * diff * inv_count;
+        } else {
+            d4[e] = 0.0f;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if (lane == 0) atomicAdd(loss, lsum * inv_count);
+    if (!backward) return;
+
+    uint32_t ad4[1][4];
+    ad4[0][0] = pack_bf16(d4[0], d4[1]);
+    ad4[0][1] = pack_bf16(d4[2], d4[3]);
+    ad4[0][2] = 0u;
+    ad4[0][3] = 0u;
+    {
+        uint32_t* r0 = reinterpret_cast<uint32_t*>(sD4 + (row0 + g) * S16 + 2 * t);
+        uint32_t* r8 = reinterpret_cast<uint32_t*>(sD4 + (row0 + g + 8) * S16 + 2 * t);
+        r0[0] = ad4[0][0];
+        r8[0] = ad4[0][1];
+        r0[4] = 0u;
+        r8[4] = 0u;
+    }
+    // dH3 = dZ4 W4, dZ3 = dH3 GELU'(Z3), ... down to dZ1
+    dense64<1>(ad4, sw + OFF_W4T, S16, nullptr, acc, lane);
+    times_to_a(acc, dg3, a);
+    store_a(sD3, S64, row0, a, lane);
+    dense64<4>(a, sw + OFF_W3T, S64, nullptr, acc, lane);
+    times_to_a(acc, dg2, a);
+    store_a(sD2, S64, row0, a, lane);
+    dense64<4>(a, sw + OFF_W2T, S64, nullptr, acc, lane);
+    times_to_a(acc, dg1, a);
+    store_a(sD1, S64, row0, a, lane);
+    __syncthreads();
+
+    // weight gradients over the tile: dW[out][in] = sum_s dZ[s][out] H[s][in],
+    // as (out x samples) x (samples x in) products on the tensor cores
+    for (int tile = warp; tile < 76; tile += 4) {
+        const uint16_t *D, *H;
+        int SD, SH, m0, n0, ldg, mmax;
+        float* G;
+        if (tile < 4) {
+            D = sD1; SD = S64; H = sH0; SH = S16; m0 = 16 * tile; n0 = 0;
+            G = grad + P_W1; ldg = 8; mmax = 64;
+        } else if (tile < 36) {
+            const int q = tile - 4;
+            D = sD2; SD = S64; H = sH1; SH = S64; m0 = 16 * (q >> 3); n0 = 8 * (q & 7);
+            G = grad + P_W2; ldg = 64; mmax = 64;
+        } else if (tile < 68) {
+            const int q = tile - 36;
+            D = sD3; SD = S64; H = sH2; SH = S64; m0 = 16 * (q >> 3); n0 = 8 * (q & 7);
+            G = grad + P_W3; ldg = 64; mmax = 64;
+        } else {
+            const int q = tile - 68;
+            D = sD4; SD = S16; H = sH3; SH = S64; m0 = 0; n0 = 8 * q;
+            G = grad + P_W4; ldg = 64; mmax = 6;
+        }
+        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const int k0 = 16 * ks;
+            uint32_t af[4];
+            af[0] = pack_raw(D[(k0 + 2 * t) * SD + m0 + g], D[(k0 + 2 * t + 1) * SD + m0 + g]);
+            af[1] = pack_raw(D[(k0 + 2 * t) * SD + m0 + g + 8], D[(k0 + 2 * t + 1) * SD + m0 + g + 8]);
+            af[2] = pack_raw(D[(k0 + 2 * t + 8) * SD + m0 + g], D[(k0 + 2 * t + 9) * SD + m0 + g]);
+            af[3] = pack_raw(D[(k0 + 2 * t + 8) * SD + m0 + g + 8],
+                             D[(k0 + 2 * t + 9) * SD + m0 + g + 8]);
+            const uint32_t b0 =
+                pack_raw(H[(k0 + 2 * t) * SH + n0 + g], H[(k0 + 2 * t + 1) * SH + n0 + g]);
+            const uint32_t b1 =
+                pack_raw(H[(k0 + 2 * t + 8) * SH + n0 + g], H[(k0 + 2 * t + 9) * SH + n0 + g]);
+            mma_bf16(c, af, b0, b1);
+        }
+        if (m0 + g < mmax) {
+            atomicAdd(G + (m0 + g) * ldg + n0 + 2 * t, c[0]);
+            atomicAdd(G + (m0 + g) * ldg + n0 + 2 * t + 1, c[1]);
+        }
+        if (m0 + g + 8 < mmax) {
+            atomicAdd(G + (m0 + g + 8) * ldg + n0 + 2 * t, c[2]);
+            atomicAdd(G + (m0 + g + 8) * ldg + n0 + 2 * t + 1, c[3]);
+        }
+    }
+    // bias gradients: column sums of dZ
+    for (int q = threadIdx.x; q < 198; q += blockDim.x) {
+        const uint16_t* D;
+        int S, col;
+        float* G;
+        if (q < 64) { D = sD1; S = S64; col = q; G = grad + P_B1; }
+        else if (q < 128) { D = sD2; S = S64; col = q - 64; G = grad + P_B2; }
+        else if (q < 192) { D = sD3; S = S64; col = q - 128; G = grad + P_B3; }
+        else { D = sD4; S = S16; col = q - 192; G = grad + P_B4; }
+        float s = 0.0f;
+        for (int r = 0; r < TILE; ++r) s += bf16_to_f(D[r * S + col]);
+        atomicAdd(G + col, s);
+    }
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master parameters; clears the gradient.
+__global__ void k_seed_adam(float* __restrict__ w, float* __restrict__ grad, float* __restrict__ m,
+                            float* __restrict__ v, int n, float lr, float beta1, float beta2,
+                            float eps, float bc1, float bc2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = grad[i];
+        const float mi = beta1 * m[i] + (1.0f - beta1) * gi;
+        const float vi = beta2 * v[i] + (1.0f - beta2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+        grad[i] = 0.0f;
+    }
+}
+
+// Cell source for inference: a structured block's primitive state.
+struct BlockCells {
+    const double* W;
+    size_t npad;
+    int ni, nj, imin, jmin, kmin, nidim, njdim;
+    __device__ size_t cell(long long q) const {
+        const int i = imin + int(q % ni);
+        const int j = jmin + int((q / ni) % nj);
+        const int k = kmin + int(q / ((long long)ni * nj));
+        return (size_t(k) * njdim + j) * nidim + i;
+    }
+};
+
+// Forward pass of one warp over 16 rows whose normalised features are in
+// xs[16][8]; writes the 6 normalised outputs of each row to os[16][8].
+__device__ __forceinline__ void warp_forward(const uint16_t* sw, const float* sb,
+                                             const float (*xs)[8], float (*os)[8], int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    uint32_t a0[1][4];
+    a0[0][0] = pack_bf16(xs[g][2 * t], xs[g][2 * t + 1]);
+    a0[0][1] = pack_bf16(xs[g + 8][2 * t], xs[g + 8][2 * t + 1]);
+    a0[0][2] = 0u;
+    a0[0][3] = 0u;
+    float acc[8][4];
+    uint32_t a[4][4];
+    dense64<1>(a0, sw + OFF_W1, S16, sb, acc, lane);
+    gelu_to_a(acc, a, nullptr);
+    dense64<4>(a, sw + OFF_W2, S64, sb + 64, acc, lane);
+    gelu_to_a(acc, a, nullptr);
+    dense64<4>(a, sw + OFF_W3, S64, sb + 128, acc, lane);
+    gelu_to_a(acc, a, nullptr);
+    float z4[4];
+    dense_out(a, sw + OFF_W4, sb + 192, z4, lane);
+    os[g][2 * t] = z4[0];
+    os[g][2 * t + 1] = z4[1];
+    os[g + 8][2 * t] = z4[2];
+    os[g + 8][2 * t + 1] = z4[3];
+}
+
+__device__ __forceinline__ void seed_features(double T, double p, const double* Y, double dt,
+                                              const double* norm, float* x) {
+    double f[8] = {log(T), log(p), Y[0], Y[1], Y[2], Y[3], Y[4], log(dt)};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x[q] = float((f[q] - norm[N_MU_IN + q]) / norm[N_SD_IN + q]);
+}
+
+// Guess for the chemistry step of the cells in the work list (interior
+// indices work[0..*nwork)): guess[s * n + q] (s < 5) = predicted end
+// concentration of species s of the q-th listed cell, guess[5 * n + q] =
+// its predicted end temperature (n = interior cells of the block).
+__global__ void __launch_bounds__(128) k_seed_infer(BlockCells b, long long n,
+                                                    const int* __restrict__ work,
+                                                    const int* __restrict__ nwork,
+                                                    const float* __restrict__ params,
+                                                    const uint16_t* __restrict__ packed,
+                                                    const double* __restrict__ norm,
+                                                    const double* __restrict__ dt_p, SeedMolar mol,
+                                                    double* __restrict__ guess) {
+    __shared__ __align__(16) uint16_t sw[PACKED_FWD];
+    __shared__ float sb[NBIAS];
+    __shared__ float xs[4][16][8];
+    __shared__ float os[4][16][8];
+    const long long nw = *nwork;
+    if ((long long)blockIdx.x * 64 >= nw) return;
+    load_weights(sw, sb, packed, params, PACKED_FWD);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double dt = *dt_p;
+    for (long long base = (long long)blockIdx.x * 64 + warp * 16; base < nw;
+         base += (long long)gridDim.x * 64) {
+        const long long q = base + lane;
+        double rho = 0.0, T = 0.0, Y[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (lane < 16) {
+            float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (q < nw) {
+                const size_t c = b.cell(work[q]);
+                rho = b.W[W_RHO * b.npad + c];
+                T = b.W[W_T * b.npad + c];
+                const double p = b.W[W_P * b.npad + c];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) Y[s] = b.W[(W_NBASE + s) * b.npad + c];
+                seed_features(T, p, Y, dt, norm, x);
+            }
+#pragma unroll
+            for (int f = 0; f < 8; ++f) xs[warp][lane][f] = x[f];
+        }
+        __syncwarp();
+        warp_forward(sw, sb, xs[warp], os[warp], lane);
+        __syncwarp();
+        if (lane < 16 && q < nw) {
+#pragma unroll
+            for (int s = 0; s < 5; ++s) {
+                const double z = double(os[warp][lane][s]) * norm[N_SD_OUT + s] + norm[N_MU_OUT + s];
+                const double y = Y[s] + norm[N_SY] * sinh(z);
+                guess[s * n + q] = fmax(y, 0.0) * rho / mol.M[s];
+            }
+            const double zT = double(os[warp][lane][5]) * norm[N_SD_OUT + 5] + norm[N_MU_OUT + 5];
+            guess[5 * n + q] = T + norm[N_ST] * sinh(zT);
+        }
+        __syncwarp();
+    }
+}
+
+// Prediction for rows (T, p, Y[5], dt) -> (dY[5], dT), through the same
+// forward pass as k_seed_infer.
+__global__ void __launch_bounds__(128) k_seed_predict(const double* __restrict__ rows, long long n,
+                                                      const float* __restrict__ params,
+                                                      const uint16_t* __restrict__ packed,
+                                                      const double* __restrict__ norm,
+                                                      double* __restrict__ out) {
+    __shared__ __align__(16) uint16_t sw[PACKED_FWD];
+    __shared__ float sb[NBIAS];
+    __shared__ float xs[4][16][8];
+    __shared__ float os[4][16][8];
+    load_weights(sw, sb, packed, params, PACKED_FWD);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * 64 + warp * 16; base < n;
+         base += (long long)gridDim.x * 64) {
+        const long long q = base + lane;
+        if (lane < 16) {
+            float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (q < n) {
+                const double* r = rows + q * 8;
+                seed_features(r[0], r[1], r + 2, r[7], norm, x);
+            }
+#pragma unroll
+            for (int f = 0; f < 8; ++f) xs[warp][lane][f] = x[f];
+        }
+        __syncwarp();
+        warp_forward(sw, sb, xs[warp], os[warp], lane);
+        __syncwarp();
+        if (lane < 16 && q < n) {
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                const double z = double(os[warp][lane][s]) * norm[N_SD_OUT + s] + norm[N_MU_OUT + s];
+                out[q * 6 + s] = norm[s < 5 ? N_SY : N_ST] * sinh(z);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Sums over the valid samples (first feature finite) of the features, the
+// transformed targets asinh(d / s) and their squares: acc[0..13] sums,
+// acc[14..27] sums of squares, acc[28] count.
+__global__ void k_seed_stats(const double* __restrict__ feat, const double* __restrict__ targ,
+                             long long n, double sY, double sT, double* __restrict__ acc) {
+    __shared__ double red[29][8];
+    double loc[29];
+    for (int q = 0; q < 29; ++q) loc[q] = 0.0;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+         r += (long long)gridDim.x * blockDim.x) {
+        if (!isfinite(feat[r * 8])) continue;
+        for (int q = 0; q < 8; ++q) {
+            const double v = feat[r * 8 + q];
+            loc[q] += v;
+            loc[14 + q] += v * v;
+        }
+        for (int q = 0; q < 6; ++q) {
+            const double v = asinh(targ[r * 6 + q] / (q < 5 ? sY : sT));
+            loc[8 + q] += v;
+            loc[22 + q] += v * v;
+        }
+        loc[28] += 1.0;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = 0; q < 29; ++q) {
+        double v = loc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[q][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 29) {
+        double v = 0.0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+        atomicAdd(acc + threadIdx.x, v);
+    }
+}
+
+// Normalised FP32 training arrays of the valid samples, compacted.
+__global__ void k_seed_normalize(const double* __restrict__ feat, const double* __restrict__ targ,
+                                 long long n, const double* __restrict__ norm,
+                                 float* __restrict__ X, float* __restrict__ Y,
+                                 int* __restrict__ count) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+         r += (long long)gridDim.x * blockDim.x) {
+        if (!isfinite(feat[r * 8])) continue;
+        const int o = atomicAdd(count, 1);
+        for (int q = 0; q < 8; ++q)
+            X[(long long)o * 8 + q] =
+                float((feat[r * 8 + q] - norm[N_MU_IN + q]) / norm[N_SD_IN + q]);
+        for (int q = 0; q < 6; ++q) {
+            const double v = asinh(targ[r * 6 + q] / norm[q < 5 ? N_SY : N_ST]);
+            Y[(long long)o * 6 + q] = float((v - norm[N_MU_OUT + q]) / norm[N_SD_OUT + q]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static int grid_of(long long n, int threads, int cap) {
+    long long g = (n + threads - 1) / threads;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return int(g);
+}
+
+int Ctx::seed_alloc_net() {
+    SeedNet& s = seed;
+    if (s.d_params) return E4C_OK;
+    s.d_params = static_cast<float*>(dalloc(4 * P_N * sizeof(float)));
+    s.d_packed = static_cast<uint16_t*>(dalloc(PACKED_N * sizeof(uint16_t)));
+    s.d_norm = static_cast<double*>(dalloc(64 * sizeof(double)));
+    s.d_loss = static_cast<float*>(dalloc(64 * sizeof(float)));
+    if (!s.d_params || !s.d_packed || !s.d_norm || !s.d_loss)
+        return fail(E4C_ERR_CUDA, "cudaMalloc of the seed network failed");
+    s.d_grad = s.d_params + P_N;
+    s.d_m = s.d_params + 2 * P_N;
+    s.d_v = s.d_params + 3 * P_N;
+    E4C_CUDA(cudaMemsetAsync(s.d_params, 0, 4 * P_N * sizeof(float), stream));
+    E4C_CUDA(cudaMemsetAsync(s.d_loss, 0, 64 * sizeof(float), stream));
+    return E4C_OK;
+}
+
+int Ctx::seed_pack() {
+    k_seed_pack<<<grid_of(PACKED_N, 256, 148), 256, 0, stream>>>(seed.d_params, seed.d_packed);
+    E4C_CUDA(cudaGetLastError());
+    return E4C_OK;
+}
+
+int Ctx::seed_dataset_reserve(long long n) {
+    SeedNet& s = seed;
+    if (n <= s.cap) return E4C_OK;
+    long long cap = std::max(n, 2 * s.cap);
+    double* f = static_cast<double*>(dalloc(size_t(cap) * 8 * sizeof(double)));
+    double* t = static_cast<double*>(dalloc(size_t(cap) * 6 * sizeof(double)));
+    if (!f || !t) {
+        dfree(f);
+        dfree(t);
+        return fail(E4C_ERR_CUDA, "cudaMalloc of the seed training set failed");
+    }
+    if (s.n > 0) {
+        E4C_CUDA(cudaMemcpyAsync(f, s.d_feat, size_t(s.n) * 8 * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, stream));
+        E4C_CUDA(cudaMemcpyAsync(t, s.d_targ, size_t(s.n) * 6 * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, stream));
+    }
+    E4C_CUDA(cudaStreamSynchronize(stream));
+    dfree(s.d_feat);
+    dfree(s.d_targ);
+    s.d_feat = f;
+    s.d_targ = t;
+    s.cap = cap;
+    return E4C_OK;
+}
+
+int Ctx::seed_guess_reserve(size_t ncell) {
+    SeedNet& s = seed;
+    if (ncell <= s.guess_cap) return E4C_OK;
+    dfree(s.d_guess);
+    s.d_guess = static_cast<double*>(dalloc(ncell * 6 * sizeof(double)));
+    if (!s.d_guess) {
+        s.guess_cap = 0;
+        return fail(E4C_ERR_CUDA, "cudaMalloc of the seed guess buffer failed");
+    }
+    s.guess_cap = ncell;
+    return E4C_OK;
+}
+
+void Ctx::seed_infer(const BlockView& v, const double* dt, const int* work, const int* nwork) {
+    BlockCells bc{v.W, v.npad, v.ni, v.nj, v.imin, v.jmin, v.kmin, v.nidim, v.njdim};
+    const long long n = (long long)v.ni * v.nj * v.nk;
+    // the list length is known only on the device: CTAs past its end return
+    k_seed_infer<<<grid_of(n, 64, 148 * 4), 128, 0, stream>>>(
+        bc, n, work, nwork, seed.d_params, seed.d_packed, seed.d_norm, dt, seed.mol, seed.d_guess);
+}
+
+}  // namespace e4c
+
+using namespace e4c;
+
+extern "C" {
+
+int e4c_seed_collect(const int* h, int nb, double dt, long long nsamples, unsigned long long rng_seed) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.cfg.reacting || !c.have_thermochem) return fail(E4C_ERR_STATE, "not a reacting configuration");
+    if (!h || nb <= 0 || nsamples <= 0 || !(dt > 0.0)) return fail(E4C_ERR_ARG, "bad arguments");
+    for (int q = 0; q < nb; ++q)
+        if (h[q] < 0 || h[q] >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad block handle");
+    // cells needing Newton work over dt in each block
+    size_t maxcell = 0;
+    for (int q = 0; q < nb; ++q) maxcell = std::max(maxcell, c.blocks[h[q]].ncell);
+    int* d_list = static_cast<int*>(c.dalloc(maxcell * sizeof(int) + 64));
+    if (!d_list) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    int* d_count = d_list + maxcell;
+    std::vector<long long> hot(nb, 0);
+    int* hp = static_cast<int*>(c.host_pinned) + 512;
+    for (int q = 0; q < nb; ++q) {
+        E4C_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int), c.stream));
+        launch_seed_active_list(c.blocks[h[q]].v, c.cfg.T_frozen, dt, d_list, d_count, c.stream);
+        E4C_CUDA(cudaMemcpyAsync(hp, d_count, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+        E4C_CUDA(cudaStreamSynchronize(c.stream));
+        hot[q] = hp[0];
+    }
+    long long total_hot = 0;
+    for (long long x : hot) total_hot += x;
+    if (total_hot == 0) {   // no cell needs Newton work: nothing to learn from
+        c.dfree(d_list);
+        return E4C_OK;
+    }
+    int rc = c.seed_dataset_reserve(c.seed.n + nsamples);
+    if (rc != E4C_OK) {
+        c.dfree(d_list);
+        return rc;
+    }
+    long long done = 0;
+    for (int q = 0; q < nb; ++q) {
+        if (hot[q] == 0) continue;
+        long long ns = (q == nb - 1) ? nsamples - done : nsamples * hot[q] / total_hot;
+        if (ns <= 0) continue;
+        E4C_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int), c.stream));
+        launch_seed_active_list(c.blocks[h[q]].v, c.cfg.T_frozen, dt, d_list, d_count, c.stream);
+        launch_seed_collect(c.blocks[h[q]].v, d_list, int(hot[q]), ns, rng_seed + 0x9E37ull * q, dt,
+                            c.cfg.T_frozen, c.seed.d_feat + c.seed.n * 8,
+                            c.seed.d_targ + c.seed.n * 6, c.stream);
+        E4C_CUDA(cudaGetLastError());
+        c.seed.n += ns;
+        done += ns;
+    }
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    c.dfree(d_list);
+    return E4C_OK;
+}
+
+int e4c_seed_dataset(long long* n) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!n) return fail(E4C_ERR_ARG, "null output");
+    *n = c.seed.n;
+    return E4C_OK;
+}
+
+int e4c_seed_clear(void) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    c.seed.n = 0;
+    return E4C_OK;
+}
+
+int e4c_seed_train(int epochs, int batch, double lr, unsigned long long rng_seed, double* report) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (epochs < 1 || batch < 64 || !(lr > 0.0)) return fail(E4C_ERR_ARG, "bad training arguments");
+    SeedNet& s = c.seed;
+    if (s.n < 256) return fail(E4C_ERR_STATE, "collect at least 256 training pairs first");
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = c.seed_alloc_net();
+    s.adam_t = 0;
+    if (rc != E4C_OK) return rc;
+    // normalisation from the valid samples
+    double* d_acc = static_cast<double*>(c.dalloc(32 * sizeof(double)));
+    float* d_X = static_cast<float*>(c.dalloc(size_t(s.n) * 8 * sizeof(float)));
+    float* d_Y = static_cast<float*>(c.dalloc(size_t(s.n) * 6 * sizeof(float)));
+    int* d_idx = static_cast<int*>(c.dalloc(size_t(s.n) * sizeof(int) + 64));
+    if (!d_acc || !d_X || !d_Y || !d_idx) {
+        c.dfree(d_acc); c.dfree(d_X); c.dfree(d_Y); c.dfree(d_idx);
+        return fail(E4C_ERR_CUDA, "cudaMalloc of the training arrays failed");
+    }
+    auto cleanup = [&] { c.dfree(d_acc); c.dfree(d_X); c.dfree(d_Y); c.dfree(d_idx); };
+    const double sY = 1.0e-9, sT = 1.0e-3;
+    E4C_CUDA(cudaMemsetAsync(d_acc, 0, 32 * sizeof(double), c.stream));
+    k_seed_stats<<<grid_of(s.n, 256, 148 * 4), 256, 0, c.stream>>>(s.d_feat, s.d_targ, s.n, sY, sT,
+                                                                   d_acc);
+    double acc[32];
+    E4C_CUDA(cudaMemcpyAsync(acc, d_acc, 29 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    const double cnt = acc[28];
+    if (cnt < 256) { cleanup(); return fail(E4C_ERR_STATE, "too few valid training pairs"); }
+    double norm[E4C_SEED_NNORM];
+    for (int q = 0; q < 14; ++q) {
+        const double mu = acc[q] / cnt;
+        double var = acc[14 + q] / cnt - mu * mu;
+        double sd = var > 0.0 ? std::sqrt(var) : 0.0;
+        if (!(sd > 1.0e-6)) sd = 1.0;   // a constant input or output
+        if (q < 8) { norm[N_MU_IN + q] = mu; norm[N_SD_IN + q] = sd; }
+        else { norm[N_MU_OUT + q - 8] = mu; norm[N_SD_OUT + q - 8] = sd; }
+    }
+    norm[N_SY] = sY;
+    norm[N_ST] = sT;
+    std::memcpy(s.norm, norm, sizeof(norm));
+    E4C_CUDA(cudaMemcpyAsync(s.d_norm, s.norm, sizeof(norm), cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaMemsetAsync(d_idx + s.n, 0, sizeof(int), c.stream));
+    k_seed_normalize<<<grid_of(s.n, 256, 148 * 8), 256, 0, c.stream>>>(
+        s.d_feat, s.d_targ, s.n, s.d_norm, d_X, d_Y, d_idx + s.n);
+    int nvalid = 0;
+    E4C_CUDA(cudaMemcpyAsync(&nvalid, d_idx + s.n, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    const int nval = std::max(64, nvalid / 50);
+    const int ntrain = nvalid - nval;
+    // initial weights: uniform in +-1/sqrt(fan_in) (weights and biases)
+    std::mt19937_64 gen(rng_seed);
+    std::vector<float> w(P_N);
+    auto init = [&](int off, int count, int fan_in) {
+        std::uniform_real_distribution<float> u(-1.0f / std::sqrt(float(fan_in)),
+                                                1.0f / std::sqrt(float(fan_in)));
+        for (int q = 0; q < count; ++q) w[off + q] = u(gen);
+    };
+    init(P_W1, 64 * 8 + 64, 8);
+    init(P_W2, 64 * 64 + 64, 64);
+    init(P_W3, 64 * 64 + 64, 64);
+    init(P_W4, 6 * 64 + 6, 64);
+    E4C_CUDA(cudaMemcpyAsync(s.d_params, w.data(), P_N * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaMemsetAsync(s.d_grad, 0, 3 * P_N * sizeof(float), c.stream));
+    rc = c.seed_pack();
+    if (rc != E4C_OK) { cleanup(); return rc; }
+    E4C_CUDA(cudaFuncSetAttribute(k_seed_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  SMEM_TRAIN));
+    std::vector<int> perm(ntrain), vidx(nval);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::iota(vidx.begin(), vidx.end(), ntrain);
+    const long long steps_per_epoch = (ntrain + batch - 1) / batch;
+    const long long total = steps_per_epoch * epochs;
+    long long step = 0;
+    double train_loss = 0.0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), gen);
+        E4C_CUDA(cudaMemcpyAsync(d_idx, perm.data(), size_t(ntrain) * sizeof(int),
+                                 cudaMemcpyHostToDevice, c.stream));
+        E4C_CUDA(cudaMemsetAsync(s.d_loss, 0, sizeof(float), c.stream));
+        for (long long b = 0; b < steps_per_epoch; ++b) {
+            const int off = int(b * batch);
+            const int nb = std::min(batch, ntrain - off);
+            // cosine decay to 1 % of lr
+            const double frac = double(step) / double(total);
+            const float lr_t = float(lr * (0.01 + 0.99 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac))));
+            ++step;
+            k_seed_train<<<(nb + TILE - 1) / TILE, 128, SMEM_TRAIN, c.stream>>>(
+                s.d_params, s.d_packed, d_X, d_Y, d_idx + off, nb, 1.0f / float(nb * 6), 1,
+                s.d_grad, s.d_loss);
+            ++s.adam_t;
+            const float bc1 = float(1.0 - std::pow(0.9, double(s.adam_t)));
+            const float bc2 = float(1.0 - std::pow(0.999, double(s.adam_t)));
+            k_seed_adam<<<grid_of(P_N, 256, 64), 256, 0, c.stream>>>(
+                s.d_params, s.d_grad, s.d_m, s.d_v, P_N, lr_t, 0.9f, 0.999f, 1.0e-8f, bc1, bc2);
+            k_seed_pack<<<grid_of(PACKED_N, 256, 148), 256, 0, c.stream>>>(s.d_params, s.d_packed);
+            c.launches += 3;
+        }
+        E4C_CUDA(cudaGetLastError());
+        float lsum = 0.0f;
+        E4C_CUDA(cudaMemcpyAsync(&lsum, s.d_loss, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+        E4C_CUDA(cudaStreamSynchronize(c.stream));
+        train_loss = lsum / double(steps_per_epoch);
+    }
+    // validation loss (no gradient)
+    E4C_CUDA(cudaMemcpyAsync(d_idx, vidx.data(), size_t(nval) * sizeof(int),
+                             cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaMemsetAsync(s.d_loss, 0, sizeof(float), c.stream));
+    k_seed_train<<<(nval + TILE - 1) / TILE, 128, SMEM_TRAIN, c.stream>>>(
+        s.d_params, s.d_packed, d_X, d_Y, d_idx, nval, 1.0f / float(nval * 6), 0, s.d_grad,
+        s.d_loss);
+    float vloss = 0.0f;
+    E4C_CUDA(cudaMemcpyAsync(&vloss, s.d_loss, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    E4C_CUDA(cudaGetLastError());
+    cleanup();
+    s.have_weights = true;
+    c.reset_graphs();
+    const double secs =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (report) {
+        report[0] = train_loss;
+        report[1] = vloss;
+        report[2] = ntrain;
+        report[3] = nval;
+        report[4] = secs;
+        report[5] = double(step);
+    }
+    return E4C_OK;
+}
+
+int e4c_seed_get(float* params, double* norm) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.seed.have_weights) return fail(E4C_ERR_STATE, "no trained or installed network");
+    if (params)
+        E4C_CUDA(cudaMemcpyAsync(params, c.seed.d_params, P_N * sizeof(float),
+                                 cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    if (norm) std::memcpy(norm, c.seed.norm, sizeof(c.seed.norm));
+    return E4C_OK;
+}
+
+int e4c_seed_set(const float* params, const double* norm) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!params || !norm) return fail(E4C_ERR_ARG, "null pointer");
+    for (int q = 0; q < E4C_SEED_NNORM; ++q)
+        if (!std::isfinite(norm[q])) return fail(E4C_ERR_ARG, "non-finite normalisation constant");
+    for (int q = 0; q < 6; ++q)
+        if (!(norm[N_SD_IN + q] > 0.0) || !(norm[N_SD_OUT + q] > 0.0))
+            return fail(E4C_ERR_ARG, "non-positive spread in the normalisation constants");
+    int rc = c.seed_alloc_net();
+    if (rc != E4C_OK) return rc;
+    std::memcpy(c.seed.norm, norm, sizeof(c.seed.norm));
+    E4C_CUDA(cudaMemcpyAsync(c.seed.d_params, params, P_N * sizeof(float), cudaMemcpyHostToDevice,
+                             c.stream));
+    E4C_CUDA(cudaMemcpyAsync(c.seed.d_norm, c.seed.norm, sizeof(c.seed.norm),
+                             cudaMemcpyHostToDevice, c.stream));
+    rc = c.seed_pack();
+    if (rc != E4C_OK) return rc;
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    c.seed.have_weights = true;
+    c.reset_graphs();
+    return E4C_OK;
+}
+
+int e4c_seed_enable(int on) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (on && !c.seed.have_weights) return fail(E4C_ERR_STATE, "no trained or installed network");
+    if (on && (!c.cfg.reacting || !c.have_thermochem))
+        return fail(E4C_ERR_STATE, "not a reacting configuration");
+    if (on) {
+        size_t maxcell = 0;
+        for (const BlockHost& b : c.blocks) maxcell = std::max(maxcell, b.ncell);
+        int rc = c.seed_guess_reserve(std::max<size_t>(maxcell, 1));
+        if (rc != E4C_OK) return rc;
+    }
+    c.seed.enabled = on != 0;
+    c.reset_graphs();
+    return E4C_OK;
+}
+
+int e4c_seed_predict(const double* rows, long long n, double* out) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.seed.have_weights) return fail(E4C_ERR_STATE, "no trained or installed network");
+    if (!rows || !out || n <= 0) return fail(E4C_ERR_ARG, "bad arguments");
+    double* d = static_cast<double*>(c.dalloc(size_t(n) * 14 * sizeof(double)));
+    if (!d) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    E4C_CUDA(cudaMemcpyAsync(d, rows, size_t(n) * 8 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    k_seed_predict<<<grid_of(n, 64, 148 * 8), 128, 0, c.stream>>>(d, n, c.seed.d_params,
+                                                                  c.seed.d_packed, c.seed.d_norm,
+                                                                  d + n * 8);
+    c.launches += 1;
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaMemcpyAsync(out, d + n * 8, size_t(n) * 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                             c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    c.dfree(d);
+    return E4C_OK;
+}
+
+int e4c_seed_loss_grad(const float* x, const float* y, int n, double* loss, float* grad) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.seed.have_weights) return fail(E4C_ERR_STATE, "no trained or installed network");
+    if (!x || !y || n <= 0 || !loss || !grad) return fail(E4C_ERR_ARG, "bad arguments");
+    const size_t bytes = size_t(n) * (8 + 6) * sizeof(float) + size_t(n) * sizeof(int) +
+                         P_N * sizeof(float) + 64;
+    char* d = static_cast<char*>(c.dalloc(bytes));
+    if (!d) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    float* dX = reinterpret_cast<float*>(d);
+    float* dY = dX + size_t(n) * 8;
+    float* dG = dY + size_t(n) * 6;
+    float* dL = dG + P_N;
+    int* dI = reinterpret_cast<int*>(dL + 4);
+    std::vector<int> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    E4C_CUDA(cudaMemcpyAsync(dX, x, size_t(n) * 8 * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaMemcpyAsync(dY, y, size_t(n) * 6 * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaMemcpyAsync(dI, idx.data(), size_t(n) * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    E4C_CUDA(cudaMemsetAsync(dG, 0, (P_N + 4) * sizeof(float), c.stream));
+    E4C_CUDA(cudaFuncSetAttribute(k_seed_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  SMEM_TRAIN));
+    k_seed_train<<<(n + TILE - 1) / TILE, 128, SMEM_TRAIN, c.stream>>>(
+        c.seed.d_params, c.seed.d_packed, dX, dY, dI, n, 1.0f / float(n * 6), 1, dG, dL);
+    c.launches += 1;
+    E4C_CUDA(cudaGetLastError());
+    float l = 0.0f;
+    E4C_CUDA(cudaMemcpyAsync(grad, dG, P_N * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaMemcpyAsync(&l, dL, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    *loss = l;
+    c.dfree(d);
+    return E4C_OK;
+}
+
+}  // extern "C"

@@ -462,20 +462,30 @@ __device__ bool point_implicit_step(const MechD<NSP, NR>& m, const double* c0, c
     return err <= 1.0;
 }
 
+// Outcomes of point_implicit_whole.
+constexpr int PI_FAILED = 0;      // no convergence: the sub-cycled recovery takes over
+constexpr int PI_CONVERGED = 1;
+constexpr int PI_MORE = 2;        // probe: the start state is not converged
+// thermochemical_increment_d in probe mode: the cell needs Newton work
+constexpr int CHEM_NEEDS_WORK = 1;
+
 // One backward-Euler step over the whole interval h by Newton iteration
 // (at most 12 iterations, the convergence test of point_implicit_step, no
-// error control): the point-implicit update proper.  The iteration starts
+// error control): the point-implicit update proper.  In probe mode it
+// returns PI_MORE, before anything else, unless the start state c0 already
+// satisfies the convergence test.  The iteration starts
 // from c0; with a guess (a prediction of the end concentrations; ignored
 // unless every entry is finite and non-negative) it starts from whichever of
 // c0 and the guess has the smaller residual.  Without a guess the operations are exactly the
 // CPU oracle's.
 template <int NSP, int NR>
-__device__ bool point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
-                                     const double* guess, double h, double* cOut, int& iters) {
+__device__ int point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
+                                    const double* guess, double h, double* cOut, int& iters,
+                                    bool probe) {
     double cscale = 0.0;
     for (int i = 0; i < NSP; ++i) cscale += c0[i];
     iters = 0;
-    if (!(cscale > 0.0)) return false;
+    if (!(cscale > 0.0)) return probe ? PI_MORE : PI_FAILED;
     double x[NSP];
     for (int i = 0; i < NSP; ++i) x[i] = c0[i];
     for (int it = 0; it <= 12; ++it) {
@@ -486,6 +496,7 @@ __device__ bool point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
             F[i] = x[i] - c0[i] - h * (q[i] - L[i]);
             res = fmax(res, fabs(F[i]));
         }
+        if (it == 0 && probe && !(res / cscale <= 1.0e-8)) return PI_MORE;
         bool use_guess = (it == 0 && guess != nullptr);
         if (use_guess)
             for (int i = 0; i < NSP; ++i)
@@ -506,7 +517,7 @@ __device__ bool point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
         }
         if (res / cscale <= 1.0e-8) {
             for (int i = 0; i < NSP; ++i) cOut[i] = x[i];
-            return true;
+            return PI_CONVERGED;
         }
         if (it == 12) break;
         double J[NSP][NSP], A[NSP][NSP];
@@ -515,14 +526,14 @@ __device__ bool point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
             for (int j = 0; j < NSP; ++j) A[i][j] = ((i == j) ? 1.0 : 0.0) - h * J[i][j];
         double dx[NSP];
         for (int i = 0; i < NSP; ++i) dx[i] = -F[i];
-        if (!solve_dense_d<NSP>(A, dx)) return false;
+        if (!solve_dense_d<NSP>(A, dx)) return PI_FAILED;
         for (int i = 0; i < NSP; ++i) {
             x[i] = x[i] + dx[i];
             if (x[i] < 0.0) x[i] = 0.0;
         }
         ++iters;
     }
-    return false;
+    return PI_FAILED;
 }
 
 // Per-cell chemistry counters: Newton iterations of the whole-interval step
@@ -541,7 +552,8 @@ struct ChemCount {
 // with Q restored.
 template <int NSP, int NR>
 __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, double tInterval,
-                                  double& dtChemSuggest, const double* guess, ChemCount* cnt) {
+                                  double& dtChemSuggest, const double* guess, ChemCount* cnt,
+                                  bool probe = false) {
     TPState<NSP> Qinit = Q;
     double conc0[NSP], concOut[NSP];
     if (isnan(Q.rho) || Q.rho <= 0.0) return E4C_ERR_CHEM;
@@ -554,9 +566,11 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
     m.rate_constants(Q.T);
     {
         int iters = 0;
-        bool ok = point_implicit_whole<NSP, NR>(m, conc0, guess, tInterval, concOut, iters);
+        const int st =
+            point_implicit_whole<NSP, NR>(m, conc0, guess, tInterval, concOut, iters, probe);
+        if (st == PI_MORE) return CHEM_NEEDS_WORK;   // Q untouched
         if (cnt) cnt->newton += iters;
-        if (ok) {
+        if (st == PI_CONVERGED) {
             double total = 0.0;
             for (int i = 0; i < NSP; ++i) {
                 Q.massf[i] = concOut[i] * tc.M[i] / Q.rho;
@@ -626,7 +640,10 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
 }
 
 // FVCell.thermochemical_increment (fvcell.d:1510-1621): chemistry at constant
-// rho and u, then T, p, a from the new composition.  guess (optional): six
+// rho and u, then T, p, a from the new composition.  probe: return
+// CHEM_NEEDS_WORK, with Q untouched, for a cell whose start state does not
+// already satisfy the point-implicit convergence test; every other cell is
+// updated exactly as without probe.  guess (optional): six
 // values, the predicted end concentrations and end temperature; the
 // temperature only starts the rhou Newton iteration (when it lies within
 // 500 K of the cell's temperature), so it changes T by no more than that
@@ -634,10 +651,12 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
 template <int NSP, int NR>
 __device__ int thermochemical_increment_d(const e4c_thermochem& tc, double T_frozen,
                                           TPState<NSP>& Q, double dt, double& dt_chem,
-                                          const double* guess, ChemCount* cnt) {
+                                          const double* guess, ChemCount* cnt,
+                                          bool probe = false) {
     if (Q.T <= T_frozen) return 0;
     const double T0 = Q.T;
-    int rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, guess, cnt);
+    int rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, guess, cnt, probe);
+    if (rc == CHEM_NEEDS_WORK) return rc;
     if (rc != 0) {
         dt_chem = -1.0;
         rc = chemistry_update_d<NSP, NR>(tc, Q, dt, dt_chem, nullptr, cnt);

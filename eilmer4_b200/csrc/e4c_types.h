@@ -89,4 +89,9 @@ struct FusedDesc {
     double inflow[6];           // rho, vx, vy, vz, u, a
 };
 
+// Molar masses of the five species, for the chemistry seed's guesses.
+struct SeedMolar {
+    double M[5];
+};
+
 }  // namespace e4c

@@ -48,10 +48,12 @@ class Simulation:
 
     @classmethod
     def from_workload(cls, wl, *, precision="fp64", control=None, use_graphs=True, **config):
+        device = int(config.pop("device", 0))
         cfgd = {"dimensions": wl.dimensions, "flux_calculator": wl.flux_calculator}
         cfgd.update(config)
         tc = getattr(wl, "thermochem", None)
-        sim = cls(cfgd, control, precision=precision, use_graphs=use_graphs, thermochem=tc)
+        sim = cls(cfgd, control, precision=precision, device=device, use_graphs=use_graphs,
+                  thermochem=tc)
         for b in wl.blocks:
             h = sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
             sim.upload(h, b.prim)
@@ -126,11 +128,63 @@ class Simulation:
         _lib.check(self.L.e4c_chemistry_step(arr, len(hs), float(dt)))
 
     def chemistry_counters(self, reset=False):
-        """(reacting cells, Newton iterations, recovered cells) accumulated by
-        the chemistry updates since the last reset."""
-        out = (ctypes.c_longlong * 3)()
+        """(reacting cells, Newton iterations, recovered cells, Newton-active
+        cells) accumulated by the chemistry updates since the last reset."""
+        out = (ctypes.c_longlong * 4)()
         _lib.check(self.L.e4c_chemistry_counters(out, int(bool(reset))))
         return tuple(int(x) for x in out)
+
+    # -- learned chemistry seed ---------------------------------------------
+    def seed_collect(self, hs, dt, nsamples, seed=1):
+        """Add nsamples (state, dt) -> plain-update pairs from the blocks' hot cells."""
+        arr = (ctypes.c_int * len(hs))(*hs)
+        _lib.check(self.L.e4c_seed_collect(arr, len(hs), float(dt), int(nsamples), int(seed)))
+
+    def seed_dataset(self):
+        n = ctypes.c_longlong()
+        _lib.check(self.L.e4c_seed_dataset(ctypes.byref(n)))
+        return n.value
+
+    def seed_clear(self):
+        _lib.check(self.L.e4c_seed_clear())
+
+    def seed_train(self, epochs=8, batch=2048, lr=2.0e-3, seed=1):
+        """Train on the collected pairs; returns the training report."""
+        rep = (ctypes.c_double * 6)()
+        _lib.check(self.L.e4c_seed_train(int(epochs), int(batch), float(lr), int(seed), rep))
+        keys = ("train_loss", "val_loss", "n_train", "n_val", "seconds", "steps")
+        return dict(zip(keys, list(rep)))
+
+    def seed_get(self):
+        p = np.zeros(_lib.SEED_NPARAM, dtype=np.float32)
+        norm = np.zeros(_lib.SEED_NNORM)
+        _lib.check(self.L.e4c_seed_get(_lib.fptr(p), _lib.dptr(norm)))
+        return p, norm
+
+    def seed_set(self, params, norm):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        nm = np.ascontiguousarray(norm, dtype=np.float64)
+        assert p.size == _lib.SEED_NPARAM and nm.size == _lib.SEED_NNORM
+        _lib.check(self.L.e4c_seed_set(_lib.fptr(p), _lib.dptr(nm)))
+
+    def seed_enable(self, on=True):
+        _lib.check(self.L.e4c_seed_enable(int(bool(on))))
+
+    def seed_predict(self, rows):
+        """rows (n, 8): T, p, Y[5], dt -> (n, 6): predicted dY[5], dT."""
+        r = np.ascontiguousarray(rows, dtype=np.float64)
+        out = np.zeros((r.shape[0], 6))
+        _lib.check(self.L.e4c_seed_predict(_lib.dptr(r), r.shape[0], _lib.dptr(out)))
+        return out
+
+    def seed_loss_grad(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.zeros(_lib.SEED_NPARAM, dtype=np.float32)
+        loss = ctypes.c_double()
+        _lib.check(self.L.e4c_seed_loss_grad(_lib.fptr(x), _lib.fptr(y), x.shape[0],
+                                             ctypes.byref(loss), _lib.fptr(g)))
+        return loss.value, g
 
     def state(self):
         t, dt, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
@@ -150,8 +204,8 @@ class Simulation:
 
     def profile(self, nsteps):
         """Per kernel class: (total ms, launches) over nsteps graph-free steps."""
-        ms = (ctypes.c_double * 7)()
-        nl = (ctypes.c_int * 7)()
+        ms = (ctypes.c_double * len(_lib.KCLASS))()
+        nl = (ctypes.c_int * len(_lib.KCLASS))()
         _lib.check(self.L.e4c_profile_steps(int(nsteps), ms, nl))
         return {name: (ms[q], nl[q]) for q, name in enumerate(_lib.KCLASS)}
 

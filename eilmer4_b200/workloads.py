@@ -278,3 +278,14 @@ def reacting_channel(ni=512, nj=256, nsteps=300, length=1.0, height=0.5, ramp_x=
     wl.blocks.append(BlockSpec(ni, nj, 1, vtx, tuple(bc), inflow, prim))
     wl.thermochem = tc
     return wl
+
+
+def reacting_channel_hot(ni=512, nj=256, nsteps=300):
+    """The reacting channel with a high-enthalpy free stream: Mach 10 at
+    2000 K and 20 kPa.  Behind the ramp shock the air reaches about 6000 K and
+    dissociates within a few flow steps; the 300 K, 2 kPa free stream of
+    reacting_channel stays below 1000 K behind the shock, where the chemistry
+    is frozen over a flow step."""
+    wl = reacting_channel(ni, nj, nsteps, T_in=2000.0, p_in=2.0e4)
+    wl.name = "reacting_channel_hot_%dx%d" % (ni, nj)
+    return wl

@@ -163,10 +163,56 @@ int e4c_set_thermochem(const e4c_thermochem* tc);
 int e4c_chemistry_step(const int* h, int nb, double dt);
 
 /* Chemistry counters accumulated since e4c_init or the last reset: out[0]
- * reacting cells updated, out[1] Newton iterations, out[2] cells that needed
- * the sub-cycled recovery.  reset != 0 zeroes them after reading.  No
- * counterpart in the reference (diagnostics of the point-implicit update). */
+ * reacting cells updated (hotter than T_frozen), out[1] Newton iterations,
+ * out[2] cells that needed the sub-cycled recovery, out[3] cells whose start
+ * state did not already satisfy the convergence test (the Newton-active
+ * cells).  reset != 0 zeroes them after reading.  No counterpart in the
+ * reference (diagnostics of the point-implicit update). */
 int e4c_chemistry_counters(long long* out, int reset);
+
+/* ---- Learned chemistry seed (no counterpart in the reference) ----------
+ * A small multilayer perceptron, input (log T, log p, Y[5], log dt), three
+ * hidden layers of 64 GELU units, output the change of the five mass
+ * fractions and of T over dt, with BF16 weights run on the tensor cores
+ * (FP32 accumulation).  When enabled, each chemistry update first evaluates
+ * it for every cell and starts the point-implicit Newton iteration from the
+ * predicted end concentrations (or from the start state, whichever has the
+ * smaller residual), and the temperature Newton iteration from the predicted
+ * end temperature.  The converged result is that of the plain update to
+ * within the Newton tolerances; the plain update is also the fallback. */
+#define E4C_SEED_NPARAM 9286   /* FP32 parameters: W1[64][8] b1 W2[64][64] b2 W3 b3 W4[6][64] b4 */
+#define E4C_SEED_NNORM 30      /* mu_in[8] sd_in[8] mu_out[6] sd_out[6] sY sT */
+
+/* Add nsamples training pairs to the library's training set: cells drawn
+ * uniformly from the blocks' Newton-active cells (hotter than T_frozen, start
+ * state not already converged over dt; current state), steps dt * f with
+ * log f uniform in [log 1/4, log 4], each advanced by the plain chemistry
+ * update on the device.  Adds nothing when no cell is active. */
+int e4c_seed_collect(const int* h, int nb, double dt, long long nsamples, unsigned long long seed);
+int e4c_seed_dataset(long long* n);
+int e4c_seed_clear(void);
+
+/* Train the network on the collected pairs with the library's forward and
+ * backward tensor-core kernels and Adam (cosine learning-rate decay to 1 % of
+ * lr), 2 % of the pairs held out.  report (optional, 6 doubles): final
+ * training loss, validation loss, training pairs, validation pairs, seconds,
+ * optimiser steps. */
+int e4c_seed_train(int epochs, int batch, double lr, unsigned long long seed, double* report);
+
+/* Read or install the network: params[E4C_SEED_NPARAM], norm[E4C_SEED_NNORM]. */
+int e4c_seed_get(float* params, double* norm);
+int e4c_seed_set(const float* params, const double* norm);
+
+/* Use (on != 0) or stop using the network in the chemistry updates. */
+int e4c_seed_enable(int on);
+
+/* Network output for n rows (T, p, Y[5], dt): out[n][6] = predicted dY[5], dT
+ * (the inference kernel of the chemistry step, on host data). */
+int e4c_seed_predict(const double* rows, long long n, double* out);
+
+/* Loss and gradient of the training kernel on n normalised rows x[n][8],
+ * targets y[n][6]: loss = mean of the squared errors, grad[E4C_SEED_NPARAM]. */
+int e4c_seed_loss_grad(const float* x, const float* y, int n, double* loss, float* grad);
 
 /* Free every device buffer and graph; the context may be re-initialised. */
 int e4c_finalize(void);
@@ -219,7 +265,8 @@ long long e4c_kernel_launches(void);
 #define E4C_KCLASS_STAGE 4     /* fused stage kernel (uniform path) */
 #define E4C_KCLASS_OTHER 5     /* bookkeeping kernels */
 #define E4C_KCLASS_CHEM 6      /* chemistry cell update */
-#define E4C_NKCLASS 7
+#define E4C_KCLASS_SEED 7      /* learned chemistry seed (inference) */
+#define E4C_NKCLASS 8
 
 /* Run nsteps time steps without graphs, timing each kernel class with CUDA
  * events on the library stream: ms[c] = total milliseconds of class c and
