@@ -169,6 +169,23 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """Max of a host number over all ranks of the process group (x itself
+    without one).  Every rank must call it at the same point."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank in (the max over ranks of) `seconds`."""
+    return world * units_per_rank / seconds
+
+
 def _timed_steps(sim, ext, steps, dist=None, clocks=None):
     """Device time of `steps` time steps on the library stream (CUDA events),
     max over ranks; returns (ms, kernel launches)."""
@@ -188,11 +205,8 @@ def _timed_steps(sim, ext, steps, dist=None, clocks=None):
     ev1.synchronize()
     launches = sim.kernel_launches() - l0
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     return ms, launches
 
@@ -239,7 +253,7 @@ def euler_case(args, precision, local_rank, dist, world, headline):
     clk = clocks.stop() if clocks else None
     rho = sim.download(0, want_cons=False)[0][0].copy()
     ms_per_step = ms / args.steps
-    value = world * ncell * args.steps / (ms * 1e-3)
+    value = replica_rate(ncell * args.steps, world, ms * 1e-3)
     bpc = BYTES_PER_CELL_UPDATE[precision]
     cls, achieved, prof = _roofline_stage(sim, ncell, bpc, args.profile_steps)
     hbm, peak_kind = peaks()
@@ -270,12 +284,8 @@ def euler_case(args, precision, local_rank, dist, world, headline):
             sim.upload(0, host_in)
             sim.run(1)
             sim.download(0, prim=host_out, want_cons=False)
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        res["e2e"] = {"value": world * ncell * e2e_steps / e2e_s, "unit": UNIT,
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+        res["e2e"] = {"value": replica_rate(ncell * e2e_steps, world, e2e_s), "unit": UNIT,
                       "h2d_bytes_per_step": 8 * 8 * ncell, "d2h_bytes_per_step": 8 * 8 * ncell}
     sim.close()
     return res, rho
@@ -471,6 +481,14 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.part != "all":
+        # one part alone (profiling runs): its own JSON line
+        fn = {"reacting": lambda: reacting_case(args, local_rank)[0],
+              "learned": lambda: learned_case(args, local_rank),
+              "batched": lambda: batched_case(args, local_rank)}[args.part]
+        if rank == 0:
+            print(json.dumps({"part": args.part, **fn()}), flush=True)
+        return
     head, rho_head = euler_case(args, args.precision, local_rank, dist, world, headline=True)
     extra = {}
     if not args.headline_only and world == 1:
@@ -538,6 +556,8 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=20)
     ap.add_argument("--reacting-steps", type=int, default=300)
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--part", default="all", choices=["all", "reacting", "learned", "batched"],
+                    help="run one sub-part alone (for profiling)")
     ap.add_argument("--seed-pairs", type=int, default=10_000_000)
     ap.add_argument("--seed-epochs", type=int, default=8)
     ap.add_argument("--seed-batch", type=int, default=4096)
