@@ -143,6 +143,28 @@ def cpu_oracle_rate(n, steps, flux, threads=0, seed=None):
     return n ** 3 * steps / dt, cores, dt
 
 
+def cpu_oracle_reacting(wl, steps):
+    """Cell-updates/s of the CPU FP64 oracle (OpenMP, all cores) on the full
+    reacting channel: `steps` time steps after the first (dt set-up)."""
+    from oracle import e4_oracle as O
+    O.build()
+    cfg = O.default_config(dimensions=2, flux_calculator=O.FLUX_AUSMDV,
+                           gas_model=O.GAS_THERM_PERF_5SP_AIR, reacting=1, n_threads=0)
+    sim = O.OracleSim(cfg, wl.thermochem)
+    b = wl.blocks[0]
+    sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    sim.set_flow(0, b.prim)
+    sim.run(1)
+    t0 = time.perf_counter()
+    rc = sim.run(steps)
+    secs = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(f"oracle failed: {rc}")
+    return {"value": b.ncell * steps / secs, "unit": UNIT, "cores": os.cpu_count() or 1,
+            "kind": "port", "sample": f"the full {b.ni}x{b.nj} channel, steps 2-{steps + 1} "
+                                       f"({secs:.1f} s), CPU FP64 restatement, OpenMP"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -350,6 +372,9 @@ def reacting_case(args, local_rank):
     sim.close()
     hbm, _ = peaks()
     chem_rate = pcells / (chem_ms * 1e-3) if chem_ms > 0 else None
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_oracle_reacting(wl, args.cpu_reacting_steps)
     out = {
         "workload": "reacting_channel 512x256, 5-species air, 5 reactions, M10 2 kPa 300 K, "
                     "15-deg ramp, ausmdv, PC, point-implicit chemistry every step",
@@ -368,6 +393,7 @@ def reacting_case(args, local_rank):
                         "peak_GBps": hbm, "bound": "fp64 latency"},
         "T_max": float(prim[5].max()),
         "gpu_launches": launches,
+        "cpu_baseline": cpu,
     }
     return out, prim
 
@@ -549,6 +575,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-sample", type=int, default=96)
+    ap.add_argument("--cpu-reacting-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--headline-only", action="store_true",

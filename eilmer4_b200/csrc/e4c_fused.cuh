@@ -248,16 +248,26 @@ struct FaceList {
     static constexpr int passes = FULL + (REM > 0 ? 1 : 0);
 };
 
-// Blocks per SM the launch bounds ask for: register budget of two CTAs in FP64.
-template <typename R>
+// Blocks per SM the launch bounds ask for: a resident-warp target per SM
+// (FP64: 16 warps, i.e. 128 registers; FP32: 24 warps) divided by the warps
+// of one CTA of the tile shape.
+#ifndef E4C_FUSED_WARPS64
+#define E4C_FUSED_WARPS64 16
+#endif
+#ifndef E4C_FUSED_WARPS32
+#define E4C_FUSED_WARPS32 24
+#endif
+template <typename R, int TI, int TJ>
 struct FusedMinBlocks {
-    static constexpr int value = sizeof(R) == 8 ? 2 : 3;
+    static constexpr int warps = (sizeof(R) == 8 ? E4C_FUSED_WARPS64 : E4C_FUSED_WARPS32);
+    static constexpr int per_cta = (TI * TJ) / 32;
+    static constexpr int value = warps / per_cta > 0 ? warps / per_cta : 1;
 };
 
 // The fused stage.  stage 1: W=WA -> WB, writes dUdt0; stage 2: W=WB -> WA,
 // writes U0 (the end-of-step state).
 template <typename R, int FLUX, int TI, int TJ>
-__global__ void __launch_bounds__(FusedThreads<TI, TJ>::total, FusedMinBlocks<R>::value)
+__global__ void __launch_bounds__(FusedThreads<TI, TJ>::total, FusedMinBlocks<R, TI, TJ>::value)
 k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems, int kc,
               SimDev* sim, GasConsts gas, FluxOpts o, int stage) {
     if (sim->status != 0 || sim->finished) return;
