@@ -8,12 +8,15 @@
 // (Hendrycks & Gimpel 2016); output 6 values, the normalised transforms
 // asinh(dY_s / sY) (5 species) and asinh(dT / sT).  Weights are kept in FP32
 // (master copy for Adam) and run as BF16 on the tensor cores with FP32
-// accumulation: mma.sync m16n8k16, one warp per 16 samples, the activations
-// of one layer passed to the next in registers (the accumulator fragment of
-// two adjacent 8-column tiles is exactly the A fragment of one 16-column
-// k-tile).  Training runs forward and backward in one kernel per mini-batch
-// of 64-sample tiles, with weight gradients accumulated over the tile by
-// tensor-core products of the stored activations and output gradients.
+// accumulation.  Inference (the chemistry step and e4c_seed_predict) runs on
+// the 5th-generation tensor cores: tcgen05.mma with the accumulators in
+// tensor memory, 128 rows per CTA.  Training runs forward and backward in one
+// kernel per mini-batch of 64-row tiles on mma.sync m16n8k16, one warp per 16
+// rows, the activations of one layer passed to the next in registers (the
+// accumulator fragment of two adjacent 8-column tiles is exactly the A
+// fragment of one 16-column k-tile), with the weight gradients accumulated
+// over the tile by tensor-core products of the stored activations and output
+// gradients.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -446,32 +449,6 @@ struct BlockCells {
     }
 };
 
-// Forward pass of one warp over 16 rows whose normalised features are in
-// xs[16][8]; writes the 6 normalised outputs of each row to os[16][8].
-__device__ __forceinline__ void warp_forward(const uint16_t* sw, const float* sb,
-                                             const float (*xs)[8], float (*os)[8], int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    uint32_t a0[1][4];
-    a0[0][0] = pack_bf16(xs[g][2 * t], xs[g][2 * t + 1]);
-    a0[0][1] = pack_bf16(xs[g + 8][2 * t], xs[g + 8][2 * t + 1]);
-    a0[0][2] = 0u;
-    a0[0][3] = 0u;
-    float acc[8][4];
-    uint32_t a[4][4];
-    dense64<1>(a0, sw + OFF_W1, S16, sb, acc, lane);
-    gelu_to_a(acc, a, nullptr);
-    dense64<4>(a, sw + OFF_W2, S64, sb + 64, acc, lane);
-    gelu_to_a(acc, a, nullptr);
-    dense64<4>(a, sw + OFF_W3, S64, sb + 128, acc, lane);
-    gelu_to_a(acc, a, nullptr);
-    float z4[4];
-    dense_out(a, sw + OFF_W4, sb + 192, z4, lane);
-    os[g][2 * t] = z4[0];
-    os[g][2 * t + 1] = z4[1];
-    os[g + 8][2 * t] = z4[2];
-    os[g + 8][2 * t + 1] = z4[3];
-}
-
 __device__ __forceinline__ void seed_features(double T, double p, const double* Y, double dt,
                                               const double* norm, float* x) {
     double f[8] = {log(T), log(p), Y[0], Y[1], Y[2], Y[3], Y[4], log(dt)};
@@ -479,101 +456,315 @@ __device__ __forceinline__ void seed_features(double T, double p, const double* 
     for (int q = 0; q < 8; ++q) x[q] = float((f[q] - norm[N_MU_IN + q]) / norm[N_SD_IN + q]);
 }
 
-// Guess for the chemistry step of the cells in the work list (interior
-// indices work[0..*nwork)): guess[s * n + q] (s < 5) = predicted end
-// concentration of species s of the q-th listed cell, guess[5 * n + q] =
-// its predicted end temperature (n = interior cells of the block).
-__global__ void __launch_bounds__(128) k_seed_infer(BlockCells b, long long n,
-                                                    const int* __restrict__ work,
-                                                    const int* __restrict__ nwork,
-                                                    const float* __restrict__ params,
-                                                    const uint16_t* __restrict__ packed,
-                                                    const double* __restrict__ norm,
-                                                    const double* __restrict__ dt_p, SeedMolar mol,
-                                                    double* __restrict__ guess) {
-    __shared__ __align__(16) uint16_t sw[PACKED_FWD];
-    __shared__ float sb[NBIAS];
-    __shared__ float xs[4][16][8];
-    __shared__ float os[4][16][8];
-    const long long nw = *nwork;
-    if ((long long)blockIdx.x * 64 >= nw) return;
-    load_weights(sw, sb, packed, params, PACKED_FWD);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const double dt = *dt_p;
-    for (long long base = (long long)blockIdx.x * 64 + warp * 16; base < nw;
-         base += (long long)gridDim.x * 64) {
-        const long long q = base + lane;
-        double rho = 0.0, T = 0.0, Y[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (lane < 16) {
-            float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (q < nw) {
-                const size_t c = b.cell(work[q]);
-                rho = b.W[W_RHO * b.npad + c];
-                T = b.W[W_T * b.npad + c];
-                const double p = b.W[W_P * b.npad + c];
+// Rows of the chemistry step: the cells of the pass-1 work list of a block.
+// Output: guess[s * n + q] (s < 5) = predicted end concentration of species
+// s of the q-th listed cell, guess[5 * n + q] = its predicted end temperature.
+struct WorkRows {
+    BlockCells b;
+    long long n;           // interior cells of the block (stride of guess)
+    const int* work;
+    const int* nwork;
+    const double* dt_p;
+    SeedMolar mol;
+    double* guess;
+    double rho, T, Y[5];
+    __device__ long long count() const { return *nwork; }
+    __device__ void load(long long q, const double* norm, float* x) {
+        const size_t c = b.cell(work[q]);
+        rho = b.W[W_RHO * b.npad + c];
+        T = b.W[W_T * b.npad + c];
+        const double p = b.W[W_P * b.npad + c];
 #pragma unroll
-                for (int s = 0; s < 5; ++s) Y[s] = b.W[(W_NBASE + s) * b.npad + c];
-                seed_features(T, p, Y, dt, norm, x);
-            }
-#pragma unroll
-            for (int f = 0; f < 8; ++f) xs[warp][lane][f] = x[f];
-        }
-        __syncwarp();
-        warp_forward(sw, sb, xs[warp], os[warp], lane);
-        __syncwarp();
-        if (lane < 16 && q < nw) {
-#pragma unroll
-            for (int s = 0; s < 5; ++s) {
-                const double z = double(os[warp][lane][s]) * norm[N_SD_OUT + s] + norm[N_MU_OUT + s];
-                const double y = Y[s] + norm[N_SY] * sinh(z);
-                guess[s * n + q] = fmax(y, 0.0) * rho / mol.M[s];
-            }
-            const double zT = double(os[warp][lane][5]) * norm[N_SD_OUT + 5] + norm[N_MU_OUT + 5];
-            guess[5 * n + q] = T + norm[N_ST] * sinh(zT);
-        }
-        __syncwarp();
+        for (int s = 0; s < 5; ++s) Y[s] = b.W[(W_NBASE + s) * b.npad + c];
+        seed_features(T, p, Y, *dt_p, norm, x);
     }
+    __device__ void store(long long q, const float* z, const double* norm) const {
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const double zz = double(z[s]) * norm[N_SD_OUT + s] + norm[N_MU_OUT + s];
+            const double y = Y[s] + norm[N_SY] * sinh(zz);
+            guess[s * n + q] = fmax(y, 0.0) * rho / mol.M[s];
+        }
+        const double zT = double(z[5]) * norm[N_SD_OUT + 5] + norm[N_MU_OUT + 5];
+        guess[5 * n + q] = T + norm[N_ST] * sinh(zT);
+    }
+};
+
+// Rows given by the host: (T, p, Y[5], dt) -> out[q][6] = predicted dY[5], dT.
+struct HostRows {
+    const double* rows;
+    long long n;
+    double* out;
+    __device__ long long count() const { return n; }
+    __device__ void load(long long q, const double* norm, float* x) {
+        const double* r = rows + q * 8;
+        seed_features(r[0], r[1], r + 2, r[7], norm, x);
+    }
+    __device__ void store(long long q, const float* z, const double* norm) const {
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            const double zz = double(z[s]) * norm[N_SD_OUT + s] + norm[N_MU_OUT + s];
+            out[q * 6 + s] = norm[s < 5 ? N_SY : N_ST] * sinh(zz);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05): 128 rows per CTA
+// tile, M = 128 x N = 64 (N = 16 for the output layer) x K = 16 BF16
+// instructions issued by one thread, FP32 accumulators in tensor memory
+// (64 columns), operands in shared memory in the canonical K-major layout
+// without swizzle: 8-row x 16-byte core matrices, consecutive along the rows
+// (stride 128 B), the K chunks of 8 elements LBO bytes apart.  Each warp
+// reads its 32 rows of the accumulator back with tcgen05.ld, adds the bias,
+// applies GELU and writes the next layer's BF16 operand.
+// ---------------------------------------------------------------------------
+constexpr int TC_W1 = 0;          // W1: 64 rows x 16 (2 chunks), LBO 1024
+constexpr int TC_W2 = 2048;       // W2: 64 x 64 (8 chunks), LBO 1024
+constexpr int TC_W3 = 10240;      // W3
+constexpr int TC_W4 = 18432;      // W4: 16 rows (6 used) x 64, LBO 256
+constexpr int TC_X0 = 20480;      // input rows: 128 x 16, LBO 2048
+constexpr int TC_H = 24576;       // hidden rows: 128 x 64, LBO 2048
+constexpr int TC_BIAS = 40960;    // NBIAS floats
+constexpr int TC_MBAR = 41984;    // mbarrier (8 B)
+constexpr int TC_TSLOT = 41992;   // tensor-memory address written by tcgen05.alloc
+constexpr int TC_FLAG = 41996;    // MMA completion seen by thread 0
+constexpr int TC_SMEM = 42000 + 1024;   // + slack to align the base to 1 KB
+constexpr uint32_t TC_COLS = 64;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Prediction for rows (T, p, Y[5], dt) -> (dY[5], dT), through the same
-// forward pass as k_seed_infer.
-__global__ void __launch_bounds__(128) k_seed_predict(const double* __restrict__ rows, long long n,
-                                                      const float* __restrict__ params,
-                                                      const uint16_t* __restrict__ packed,
-                                                      const double* __restrict__ norm,
-                                                      double* __restrict__ out) {
-    __shared__ __align__(16) uint16_t sw[PACKED_FWD];
-    __shared__ float sb[NBIAS];
-    __shared__ float xs[4][16][8];
-    __shared__ float os[4][16][8];
-    load_weights(sw, sb, packed, params, PACKED_FWD);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (long long base = (long long)blockIdx.x * 64 + warp * 16; base < n;
-         base += (long long)gridDim.x * 64) {
-        const long long q = base + lane;
-        if (lane < 16) {
-            float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            if (q < n) {
-                const double* r = rows + q * 8;
-                seed_features(r[0], r[1], r + 2, r[7], norm, x);
-            }
-#pragma unroll
-            for (int f = 0; f < 8; ++f) xs[warp][lane][f] = x[f];
-        }
-        __syncwarp();
-        warp_forward(sw, sb, xs[warp], os[warp], lane);
-        __syncwarp();
-        if (lane < 16 && q < n) {
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                const double z = double(os[warp][lane][s]) * norm[N_SD_OUT + s] + norm[N_MU_OUT + s];
-                out[q * 6 + s] = norm[s < 5 ? N_SY : N_ST] * sinh(z);
-            }
-        }
-        __syncwarp();
+// Shared-memory matrix descriptor: start, leading (K chunk) and stride
+// (8-row group) byte offsets, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((saddr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulate, BF16 A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t umma_idesc(uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :
+                 : "r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for an mbarrier phase (each try_wait itself suspends for a
+// while): false after ~1e6 tries.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (int it = 0; it < (1 << 20); ++it)
+        if (mbar_try(mbar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void proxy_fence() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 32 lanes x 64 columns of FP32 from TMEM (this warp's lane quarter).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// 32 lanes x 16 columns.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Row r of a K-major canonical operand: chunk c (8 BF16) at
+// (c * groups + r / 8) * 128 + (r % 8) * 16.
+__device__ __forceinline__ uint32_t tc_row_chunk(int r, int c, int groups) {
+    return uint32_t((c * groups + (r >> 3)) * 128 + (r & 7) * 16);
+}
+
+template <class Src>
+__global__ void __launch_bounds__(128) k_seed_infer_tc(Src src, const float* __restrict__ params,
+                                                       const uint16_t* __restrict__ packed,
+                                                       const double* __restrict__ norm,
+                                                       SimDev* sim) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const long long nrows = src.count();
+    if ((long long)blockIdx.x * 128 >= nrows) return;   // before any tensor-memory use
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+    unsigned char* sm = smem_raw + pad;
+    const uint32_t sb = raw + pad;
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    // weights into the canonical layouts, biases
+    const uint4* pk = reinterpret_cast<const uint4*>(packed);
+    const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+    for (int e = tid; e < 128; e += 128) {   // W1: 64 rows x 2 chunks
+        const int r = e >> 1, c = e & 1;
+        *reinterpret_cast<uint4*>(sm + TC_W1 + tc_row_chunk(r, c, 8)) = pk[(OFF_W1 + r * S16 + 8 * c) / 8];
     }
+    for (int e = tid; e < 512; e += 128) {   // W2, W3: 64 rows x 8 chunks
+        const int r = e >> 3, c = e & 7;
+        *reinterpret_cast<uint4*>(sm + TC_W2 + tc_row_chunk(r, c, 8)) = pk[(OFF_W2 + r * S64 + 8 * c) / 8];
+        *reinterpret_cast<uint4*>(sm + TC_W3 + tc_row_chunk(r, c, 8)) = pk[(OFF_W3 + r * S64 + 8 * c) / 8];
+    }
+    for (int e = tid; e < 128; e += 128) {   // W4: 16 rows (8.. zero) x 8 chunks
+        const int r = e >> 3, c = e & 7;
+        *reinterpret_cast<uint4*>(sm + TC_W4 + tc_row_chunk(r, c, 2)) =
+            r < 8 ? pk[(OFF_W4 + r * S64 + 8 * c) / 8] : zero4;
+    }
+    float* bias = reinterpret_cast<float*>(sm + TC_BIAS);
+    for (int q = tid; q < NBIAS; q += 128) {
+        float v = 0.0f;
+        if (q < 64) v = params[P_B1 + q];
+        else if (q < 128) v = params[P_B2 + q - 64];
+        else if (q < 192) v = params[P_B3 + q - 128];
+        else if (q < 198) v = params[P_B4 + q - 192];
+        bias[q] = v;
+    }
+    const uint32_t mbar = sb + TC_MBAR;
+    volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(sm + TC_FLAG);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(sb + TC_TSLOT), "r"(TC_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + TC_TSLOT);
+    const uint32_t tmem_warp = tmem + (uint32_t(32 * warp) << 16);
+    uint32_t phase = 0;
+    bool failed = false;
+
+    for (long long tile = blockIdx.x; tile * 128 < nrows && !failed; tile += gridDim.x) {
+        const long long q = tile * 128 + tid;
+        float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (q < nrows) src.load(q, norm, x);
+        {
+            uint4 v;
+            v.x = pack_bf16(x[0], x[1]);
+            v.y = pack_bf16(x[2], x[3]);
+            v.z = pack_bf16(x[4], x[5]);
+            v.w = pack_bf16(x[6], x[7]);
+            *reinterpret_cast<uint4*>(sm + TC_X0 + tc_row_chunk(tid, 0, 16)) = v;
+            *reinterpret_cast<uint4*>(sm + TC_X0 + tc_row_chunk(tid, 1, 16)) = zero4;
+        }
+        proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        for (int layer = 0; layer < 4; ++layer) {
+            if (tid == 0) {
+                tc_fence_after();
+                if (layer == 0) {
+                    umma_bf16(tmem, umma_desc(sb + TC_X0, 2048, 128), umma_desc(sb + TC_W1, 1024, 128),
+                              umma_idesc(64), 0u);
+                } else {
+                    const uint32_t wb = layer == 1 ? TC_W2 : layer == 2 ? TC_W3 : TC_W4;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint64_t ad = umma_desc(sb + TC_H + 4096 * k, 2048, 128);
+                        const uint64_t bd = layer < 3 ? umma_desc(sb + wb + 2048 * k, 1024, 128)
+                                                      : umma_desc(sb + wb + 512 * k, 256, 128);
+                        umma_bf16(tmem, ad, bd, umma_idesc(layer < 3 ? 64 : 16), k > 0 ? 1u : 0u);
+                    }
+                }
+                umma_commit(mbar);
+                *flag = mbar_wait(mbar, phase) ? 1u : 0u;
+            }
+            __syncthreads();
+            if (*flag == 0u) {
+                failed = true;
+                break;
+            }
+            phase ^= 1u;
+            tc_fence_after();
+            if (layer < 3) {
+                uint32_t r[64];
+                tmem_ld64(tmem_warp, r);
+                const float* bl = bias + 64 * layer;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    float h[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) h[e] = gelu_f(__uint_as_float(r[8 * c + e]) + bl[8 * c + e]);
+                    uint4 v;
+                    v.x = pack_bf16(h[0], h[1]);
+                    v.y = pack_bf16(h[2], h[3]);
+                    v.z = pack_bf16(h[4], h[5]);
+                    v.w = pack_bf16(h[6], h[7]);
+                    *reinterpret_cast<uint4*>(sm + TC_H + tc_row_chunk(tid, c, 16)) = v;
+                }
+                proxy_fence();
+            } else {
+                uint32_t r[16];
+                tmem_ld16(tmem_warp, r);
+                float z[6];
+#pragma unroll
+                for (int e = 0; e < 6; ++e) z[e] = __uint_as_float(r[e]) + bias[192 + e];
+                if (q < nrows) src.store(q, z, norm);
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+    }
+    if (failed) {
+        // the tensor cores did not signal completion: report, give the MMA a
+        // second bounded wait, then release the tensor memory
+        if (tid == 0) {
+            if (sim && atomicCAS(&sim->status, 0, E4C_ERR_TIMEOUT) == 0) sim->status_step = sim->step;
+            (void)mbar_wait(mbar, phase);
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS)
+                     : "memory");
 }
 
 // Sums over the valid samples (first feature finite) of the features, the
@@ -705,11 +896,18 @@ int Ctx::seed_guess_reserve(size_t ncell) {
 }
 
 void Ctx::seed_infer(const BlockView& v, const double* dt, const int* work, const int* nwork) {
-    BlockCells bc{v.W, v.npad, v.ni, v.nj, v.imin, v.jmin, v.kmin, v.nidim, v.njdim};
-    const long long n = (long long)v.ni * v.nj * v.nk;
+    WorkRows rows{};
+    rows.b = BlockCells{v.W, v.npad, v.ni, v.nj, v.imin, v.jmin, v.kmin, v.nidim, v.njdim};
+    rows.n = (long long)v.ni * v.nj * v.nk;
+    rows.work = work;
+    rows.nwork = nwork;
+    rows.dt_p = dt;
+    rows.mol = seed.mol;
+    rows.guess = seed.d_guess;
     // the list length is known only on the device: CTAs past its end return
-    k_seed_infer<<<grid_of(n, 64, 148 * 4), 128, 0, stream>>>(
-        bc, n, work, nwork, seed.d_params, seed.d_packed, seed.d_norm, dt, seed.mol, seed.d_guess);
+    // before touching tensor memory
+    k_seed_infer_tc<WorkRows><<<grid_of(rows.n, 128, 148 * 4), 128, TC_SMEM, stream>>>(
+        rows, seed.d_params, seed.d_packed, seed.d_norm, d_sim);
 }
 
 }  // namespace e4c
@@ -977,9 +1175,9 @@ int e4c_seed_predict(const double* rows, long long n, double* out) {
     double* d = static_cast<double*>(c.dalloc(size_t(n) * 14 * sizeof(double)));
     if (!d) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
     E4C_CUDA(cudaMemcpyAsync(d, rows, size_t(n) * 8 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    k_seed_predict<<<grid_of(n, 64, 148 * 8), 128, 0, c.stream>>>(d, n, c.seed.d_params,
-                                                                  c.seed.d_packed, c.seed.d_norm,
-                                                                  d + n * 8);
+    HostRows hr{d, n, d + n * 8};
+    k_seed_infer_tc<HostRows><<<grid_of(n, 128, 148 * 4), 128, TC_SMEM, c.stream>>>(
+        hr, c.seed.d_params, c.seed.d_packed, c.seed.d_norm, nullptr);
     c.launches += 1;
     E4C_CUDA(cudaGetLastError());
     E4C_CUDA(cudaMemcpyAsync(out, d + n * 8, size_t(n) * 6 * sizeof(double), cudaMemcpyDeviceToHost,
