@@ -27,10 +27,31 @@
 
 namespace e4c {
 
+// Inlining of the CEA curve evaluations and of exp/log.  The thermally perfect
+// kernels are large enough for instruction fetch to matter: calling the CEA
+// evaluations instead of inlining them measured 1.1x (cold channel) to 1.3x
+// (reacting channel) faster.
+#ifndef E4C_CEA_NOINLINE
+#define E4C_CEA_NOINLINE 1
+#endif
+#if E4C_CEA_NOINLINE
+#define E4C_CEA_FN __noinline__
+#else
+#define E4C_CEA_FN __forceinline__
+#endif
+#ifndef E4C_PM_NOINLINE
+#define E4C_PM_NOINLINE 0
+#endif
+#if E4C_PM_NOINLINE
+#define E4C_PM_FN __noinline__
+#else
+#define E4C_PM_FN __forceinline__
+#endif
+
 // ---------------------------------------------------------------------------
 // Portable exp / log / pow
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double pm_log(double x) {
+static __device__ E4C_PM_FN double pm_log(double x) {
     if (!(x > 0.0)) return (x == 0.0) ? -HUGE_VAL : CUDART_NAN;
     if (isinf(x)) return x;
     int k;
@@ -56,7 +77,7 @@ __device__ __forceinline__ double pm_log(double x) {
     return kd * ln2_hi + (2.0 * s * p + kd * ln2_lo);
 }
 
-__device__ __forceinline__ double pm_exp(double x) {
+static __device__ E4C_PM_FN double pm_exp(double x) {
     if (x != x) return x;
     if (x > 709.78) return HUGE_VAL;
     if (x < -745.2) return 0.0;
@@ -97,7 +118,7 @@ __device__ __forceinline__ double pm_pow(double x, double n) {
 // ---------------------------------------------------------------------------
 // CEA thermo curves
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void cea_coefficients(const e4c_thermochem& tc, int isp, double T,
+static __device__ E4C_CEA_FN void cea_coefficients(const e4c_thermochem& tc, int isp, double T,
                                                  double a[9]) {
     const int nseg = tc.nseg[isp];
     const double* tb = tc.T_break[isp];
@@ -127,7 +148,7 @@ __device__ __forceinline__ void cea_coefficients(const e4c_thermochem& tc, int i
     for (int j = 0; j < 9; ++j) a[j] = CUDART_NAN;
 }
 
-__device__ __forceinline__ double cea_Cp(const e4c_thermochem& tc, int isp, double R, double T) {
+static __device__ E4C_CEA_FN double cea_Cp(const e4c_thermochem& tc, int isp, double R, double T) {
     const int nseg = tc.nseg[isp];
     if (T < tc.T_break[isp][0]) T = tc.T_break[isp][0];
     if (T > tc.T_break[isp][nseg]) T = tc.T_break[isp][nseg];
@@ -138,7 +159,7 @@ __device__ __forceinline__ double cea_Cp(const e4c_thermochem& tc, int isp, doub
     return R * Cp_on_R;
 }
 
-__device__ __forceinline__ double cea_h_in_range(const e4c_thermochem& tc, int isp, double R,
+static __device__ E4C_CEA_FN double cea_h_in_range(const e4c_thermochem& tc, int isp, double R,
                                                  double T) {
     double a[9];
     cea_coefficients(tc, isp, T, a);
@@ -147,7 +168,7 @@ __device__ __forceinline__ double cea_h_in_range(const e4c_thermochem& tc, int i
     return R * T * h_on_RT;
 }
 
-__device__ __forceinline__ double cea_h(const e4c_thermochem& tc, int isp, double R, double T) {
+static __device__ E4C_CEA_FN double cea_h(const e4c_thermochem& tc, int isp, double R, double T) {
     const int nseg = tc.nseg[isp];
     if (T < tc.T_break[isp][0]) {
         double T_low = tc.T_break[isp][0];
