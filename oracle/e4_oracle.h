@@ -126,6 +126,11 @@ int e4o_tp_update(const e4o_thermochem* tc, int mode, const double* massf, doubl
 int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double rho,
                   double* T, double* u, double* p, double* massf, double* dt_chem);
 
+/* The chemistry update alone (ChemistryUpdate.opCall with the point-implicit
+ * step) at constant rho and T: new mass fractions, no temperature update. */
+int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, double* massf,
+                    double* dt_chem);
+
 /* Low-level pieces exposed for golden-vector tests. */
 int e4o_ideal_gas_pT(double mol_mass, double gamma, double p, double T,
                      double* rho, double* u, double* a);

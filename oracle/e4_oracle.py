@@ -115,6 +115,7 @@ def lib():
         L.e4o_set_thermochem.argtypes = [vp, P(ThermoChem)]
         L.e4o_tp_update.argtypes = [P(ThermoChem), ip, P(dp), P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
+        L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
         _lib = L
     return _lib
 
@@ -242,3 +243,12 @@ def chem_cell(thermochem, T_frozen, dt, rho, T, u, p, massf, dt_chem=-1.0):
     rc = lib().e4o_chem_cell(ctypes.byref(tc), T_frozen, dt, rho, ctypes.byref(TT),
                              ctypes.byref(uu), ctypes.byref(pp), _dptr(mf), ctypes.byref(dc))
     return rc, {"T": TT.value, "u": uu.value, "p": pp.value, "massf": mf, "dt_chem": dc.value}
+
+
+def chem_update(thermochem, dt, rho, T, massf, dt_chem=-1.0):
+    """The chemistry update alone at constant rho and T (no temperature update)."""
+    tc = thermochem.fill(ThermoChem())
+    mf = np.array(massf, dtype=np.float64)
+    dc = ctypes.c_double(dt_chem)
+    rc = lib().e4o_chem_update(ctypes.byref(tc), dt, rho, T, _dptr(mf), ctypes.byref(dc))
+    return rc, mf

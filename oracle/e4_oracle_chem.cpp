@@ -689,6 +689,17 @@ int e4o_tp_update(const e4o_thermochem* tc, int mode, const double* massf, doubl
     return 0;
 }
 
+int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, double* massf,
+                    double* dt_chem) {
+    GasState Q;
+    Q.rho = rho; Q.T = T; Q.u = 0.0; Q.p = 0.0;
+    for (int i = 0; i < tc->nsp; ++i) Q.massf[i] = massf[i];
+    int rc = chemistry_update(*tc, Q, dt, *dt_chem);
+    if (rc != 0) return rc;
+    for (int i = 0; i < tc->nsp; ++i) massf[i] = Q.massf[i];
+    return 0;
+}
+
 int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double rho, double* T,
                   double* u, double* p, double* massf, double* dt_chem) {
     GasState Q;

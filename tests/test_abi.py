@@ -69,6 +69,17 @@ def test_calls_before_init_are_rejected(e4lib):
     vtx = np.zeros(12)
     bc = (ctypes.c_int * 6)(0, 0, 0, 0, 0, 0)
     assert e4lib.e4c_block_create(2, 2, 1, _lib.dptr(vtx), bc, _lib.dptr(vtx)) == _lib.E4C_ERR_STATE
+    # chemistry and the learned seed refuse as well, without touching a GPU
+    h = (ctypes.c_int * 1)(0)
+    assert e4lib.e4c_chemistry_step(h, 1, 1e-7) == _lib.E4C_ERR_STATE
+    out = (ctypes.c_longlong * 4)()
+    assert e4lib.e4c_chemistry_counters(out, 0) == _lib.E4C_ERR_STATE
+    assert e4lib.e4c_seed_enable(1) == _lib.E4C_ERR_STATE
+    assert e4lib.e4c_seed_train(1, 1024, 1e-3, 1, None) == _lib.E4C_ERR_STATE
+    assert e4lib.e4c_seed_collect(h, 1, 1e-7, 10, 1) == _lib.E4C_ERR_STATE
+    params = np.zeros(_lib.SEED_NPARAM, dtype=np.float32)
+    norm = np.ones(_lib.SEED_NNORM)
+    assert e4lib.e4c_seed_set(_lib.fptr(params), _lib.dptr(norm)) == _lib.E4C_ERR_STATE
 
 
 def test_init_rejects_unsupported_config(e4lib):
