@@ -55,6 +55,15 @@ void Ctx::release() {
     allocations.clear();
     if (host_pinned) cudaFreeHost(host_pinned);
     host_pinned = nullptr;
+    if (h2d_stream) cudaStreamSynchronize(h2d_stream);
+    if (d2h_stream) cudaStreamSynchronize(d2h_stream);
+    for (cudaEvent_t* e : {&ev_in_copied, &ev_in_consumed, &ev_out_ready, &ev_out_copied}) {
+        if (*e) cudaEventDestroy(*e);
+        *e = nullptr;
+    }
+    if (h2d_stream) cudaStreamDestroy(h2d_stream);
+    if (d2h_stream) cudaStreamDestroy(d2h_stream);
+    h2d_stream = d2h_stream = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
     blocks.clear();
@@ -78,6 +87,8 @@ void Ctx::release() {
     dtacc_cap = 0;
     d_staging = nullptr;
     staging_bytes = 0;
+    d_stage_in = d_stage_out = nullptr;
+    stage_io_bytes = 0;
     initialised = false;
 }
 
@@ -276,6 +287,10 @@ int e4c_init(const e4c_config* cfg) {
     c.fopts.local_frame = cfg->interpolate_in_local_frame != 0;
     c.fopts.gas = c.gas;
     E4C_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    E4C_CUDA(cudaStreamCreateWithFlags(&c.h2d_stream, cudaStreamNonBlocking));
+    E4C_CUDA(cudaStreamCreateWithFlags(&c.d2h_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c.ev_in_copied, &c.ev_in_consumed, &c.ev_out_ready, &c.ev_out_copied})
+        E4C_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     c.d_sim = static_cast<SimDev*>(c.dalloc(sizeof(SimDev) + 64));
     c.d_dtacc = nullptr;
     c.dtacc_cap = 0;
@@ -290,6 +305,7 @@ int e4c_init(const e4c_config* cfg) {
     E4C_CUDA(cudaMemcpyAsync(c.d_sim, &s0, sizeof(SimDev), cudaMemcpyHostToDevice, c.stream));
     E4C_CUDA(cudaStreamSynchronize(c.stream));
     c.host_step = 0;
+    c.host_step_valid = false;
     c.have_thermochem = false;
     c.nreac = 0;
     c.initialised = true;
@@ -419,6 +435,88 @@ int e4c_block_download(int h, double* prim, double* cons) {
     return E4C_OK;
 }
 
+int Ctx::ensure_stage_io(size_t bytes) {
+    if (bytes <= stage_io_bytes) return E4C_OK;
+    // the previous buffers may still be in use by queued transfers
+    if (h2d_stream) cudaStreamSynchronize(h2d_stream);
+    if (d2h_stream) cudaStreamSynchronize(d2h_stream);
+    cudaStreamSynchronize(stream);
+    dfree(d_stage_in);
+    dfree(d_stage_out);
+    d_stage_in = static_cast<double*>(dalloc(bytes));
+    d_stage_out = static_cast<double*>(dalloc(bytes));
+    if (!d_stage_in || !d_stage_out) {
+        dfree(d_stage_in);
+        dfree(d_stage_out);
+        d_stage_in = d_stage_out = nullptr;
+        stage_io_bytes = 0;
+        return fail(E4C_ERR_CUDA, "cudaMalloc of the transfer staging buffers failed");
+    }
+    stage_io_bytes = bytes;
+    return E4C_OK;
+}
+
+int e4c_block_upload_async(int h, const double* prim) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size()) || !prim) return fail(E4C_ERR_ARG, "bad handle or pointer");
+    BlockHost& b = c.blocks[h];
+    int rc = c.ensure_stage_io((b.nprim_vars + size_t(b.v.nv)) * b.ncell * sizeof(double));
+    if (rc != E4C_OK) return rc;
+    const size_t bytes = b.nprim_vars * b.ncell * sizeof(double);
+    // the copy waits until the previous upload's conversion has read the buffer
+    E4C_CUDA(cudaStreamWaitEvent(c.h2d_stream, c.ev_in_consumed, 0));
+    E4C_CUDA(cudaMemcpyAsync(c.d_stage_in, prim, bytes, cudaMemcpyHostToDevice, c.h2d_stream));
+    E4C_CUDA(cudaEventRecord(c.ev_in_copied, c.h2d_stream));
+    E4C_CUDA(cudaStreamWaitEvent(c.stream, c.ev_in_copied, 0));
+    if (b.fused) {
+        rc = c.fused_upload(b, c.d_stage_in);
+        if (rc != E4C_OK) return rc;
+    } else {
+        launch_upload(b.v, c.d_stage_in, c.stream);
+    }
+    c.launches += 1;
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaEventRecord(c.ev_in_consumed, c.stream));
+    return E4C_OK;
+}
+
+int e4c_block_download_async(int h, double* prim, double* cons) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad handle");
+    BlockHost& b = c.blocks[h];
+    int rc = c.ensure_stage_io((b.nprim_vars + size_t(b.v.nv)) * b.ncell * sizeof(double));
+    if (rc != E4C_OK) return rc;
+    double* dp = c.d_stage_out;
+    double* dc = c.d_stage_out + b.nprim_vars * b.ncell;
+    // the conversion waits until the previous download has been copied out
+    E4C_CUDA(cudaStreamWaitEvent(c.stream, c.ev_out_copied, 0));
+    if (b.fused) c.fused_download(b, prim ? dp : nullptr, cons ? dc : nullptr);
+    else launch_download(b.v, prim ? dp : nullptr, cons ? dc : nullptr, c.stream);
+    c.launches += 1;
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaEventRecord(c.ev_out_ready, c.stream));
+    E4C_CUDA(cudaStreamWaitEvent(c.d2h_stream, c.ev_out_ready, 0));
+    if (prim)
+        E4C_CUDA(cudaMemcpyAsync(prim, dp, b.nprim_vars * b.ncell * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c.d2h_stream));
+    if (cons)
+        E4C_CUDA(cudaMemcpyAsync(cons, dc, b.v.nv * b.ncell * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c.d2h_stream));
+    E4C_CUDA(cudaEventRecord(c.ev_out_copied, c.d2h_stream));
+    return E4C_OK;
+}
+
+int e4c_transfers_wait(void) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    E4C_CUDA(cudaStreamSynchronize(c.h2d_stream));
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    E4C_CUDA(cudaStreamSynchronize(c.d2h_stream));
+    return E4C_OK;
+}
+
 static int check_handles(const int* h, int nb, std::vector<int>& hs) {
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
@@ -479,6 +577,7 @@ static int status_error(const SimDev& s) {
 }
 
 int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
+    g_ctx.host_step_valid = false;
     std::vector<int> hs;
     int rc = check_handles(h, nb, hs);
     if (rc != E4C_OK) return rc;
@@ -522,6 +621,8 @@ int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
     SimDev s;
     rc = read_sim(s);
     if (rc != E4C_OK) return rc;
+    c.host_step = s.step;
+    c.host_step_valid = true;
     if (info) {
         info->steps_taken = s.step - step_start;
         info->time = s.time;
@@ -531,6 +632,32 @@ int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
         info->bad_cells = s.bad_cells;
     }
     if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
+int e4c_integrate_async(int nsteps, double max_time) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
+    if (nsteps < 0) return fail(E4C_ERR_ARG, "negative step count");
+    std::vector<int> hs = c.all_blocks();
+    int rc = c.prepare_fused();
+    if (rc != E4C_OK) return rc;
+    if (!c.host_step_valid) {
+        SimDev s0;
+        rc = read_sim(s0);
+        if (rc != E4C_OK) return rc;
+        c.host_step = s0.step;
+        c.host_step_valid = true;
+    }
+    launch_begin_run(c.d_sim, max_time, c.stream);
+    for (int q = 0; q < nsteps; ++q) {
+        const bool dt_check = ((c.host_step + q) % c.cfg.cfl_count) == 0;  // simcore.d:1350-1352
+        rc = c.run_step(hs, dt_check);
+        if (rc != E4C_OK) return rc;
+    }
+    c.host_step += nsteps;
+    E4C_CUDA(cudaGetLastError());
     return E4C_OK;
 }
 
@@ -624,6 +751,7 @@ int e4c_get_tile(int* ti, int* tj, int* kc) {
 }
 
 int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step) {
+    g_ctx.host_step_valid = false;
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");

@@ -193,6 +193,7 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     if (need > staging_bytes) {
         double* st = static_cast<double*>(dalloc(need));
         if (!st) return fail(E4C_ERR_CUDA, "cudaMalloc of staging buffer failed");
+        dfree(d_staging);
         d_staging = st;
         staging_bytes = need;
     }

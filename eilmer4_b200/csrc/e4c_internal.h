@@ -67,11 +67,20 @@ struct Ctx {
     double* d_scalars = nullptr;
     double* d_staging = nullptr;
     size_t staging_bytes = 0;
+    // asynchronous transfers: copy streams, staging buffers and ordering events
+    cudaStream_t h2d_stream = nullptr;
+    cudaStream_t d2h_stream = nullptr;
+    double* d_stage_in = nullptr;
+    double* d_stage_out = nullptr;
+    size_t stage_io_bytes = 0;
+    cudaEvent_t ev_in_copied = nullptr, ev_in_consumed = nullptr;
+    cudaEvent_t ev_out_ready = nullptr, ev_out_copied = nullptr;
     void* host_pinned = nullptr;
     std::vector<void*> allocations;
     std::vector<BlockHost> blocks;
     GraphSlot graphs[2];    // [0] plain step, [1] step with dt check
-    int host_step = 0;
+    int host_step = 0;           // device step count as the host last knew it
+    bool host_step_valid = false;
     bool have_thermochem = false;
     int nreac = 0;
     // chemistry counters: reacting cells, Newton iterations, recovered cells
@@ -118,6 +127,7 @@ struct Ctx {
     int seed_guess_reserve(size_t ncell);
     void seed_infer(const BlockView& v, const double* dt, const int* work, const int* nwork);
     int ensure_chem_work(size_t ncell);
+    int ensure_stage_io(size_t bytes);
     void enqueue_dt(const std::vector<int>& hs, const int* d_hl, const double* dt_current,
                     int check_cfl, int step0, SimDev* sim, double* out);
     std::vector<int> all_blocks() const;

@@ -103,6 +103,24 @@ class Simulation:
                                              _lib.dptr(cons) if cons is not None else None))
         return prim, cons
 
+    def upload_async(self, h, prim):
+        """Queue an upload from a contiguous pinned host tensor/array (returns
+        at once; call wait_transfers before reusing the host buffer)."""
+        _lib.check(self.L.e4c_block_upload_async(h, _lib.dptr(prim)))
+
+    def download_async(self, h, prim=None, cons=None):
+        """Queue a download into contiguous pinned host buffers."""
+        _lib.check(self.L.e4c_block_download_async(
+            h, _lib.dptr(prim) if prim is not None else None,
+            _lib.dptr(cons) if cons is not None else None))
+
+    def run_async(self, nsteps, max_time=1.0e300):
+        """Queue nsteps steps without waiting (status: next run())."""
+        _lib.check(self.L.e4c_integrate_async(int(nsteps), float(max_time)))
+
+    def wait_transfers(self):
+        _lib.check(self.L.e4c_transfers_wait())
+
     def run(self, nsteps, max_time=1.0e300) -> RunInfo:
         info = _lib.E4CRunInfo()
         rc = self.L.e4c_integrate(int(nsteps), float(max_time), ctypes.byref(info))

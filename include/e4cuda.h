@@ -229,6 +229,19 @@ int e4c_block_upload(int h, const double* prim);
 /* Download the primitive and/or conserved state (either pointer may be NULL). */
 int e4c_block_download(int h, double* prim, double* cons);
 
+/* Asynchronous forms of e4c_block_upload / e4c_block_download (no
+ * counterpart in the reference, whose host and solver share memory).  The
+ * host-to-device and device-to-host copies run on two copy streams of their
+ * own, ordered by events against the computation, so that one step's
+ * download overlaps the next step's upload.  The host buffers must be
+ * page-locked (cudaHostAlloc / pinned) for the copies to be asynchronous and
+ * must not be touched until e4c_transfers_wait returns.  A download reads the
+ * state left by all work queued before it; an upload is seen by all work
+ * queued after it. */
+int e4c_block_upload_async(int h, const double* prim);
+int e4c_block_download_async(int h, double* prim, double* cons);
+int e4c_transfers_wait(void);
+
 /* Allowable time step over the blocks, as FluidBlock.determine_time_step_size
  * followed by the min/max reduction over blocks (simcore.d:1362-1386);
  * check_cfl corresponds to SimState.step > 0. */
@@ -243,6 +256,13 @@ int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells);
  * dt control every cfl_count steps, dt_init at step 0, x1.5 growth cap and
  * dt_max, then the gas-dynamic step.  The loop stays on the device. */
 int e4c_integrate(int nsteps, double max_time, e4c_run_info* info);
+
+/* e4c_integrate without waiting: the steps are queued on the library stream
+ * and the call returns at once (no counterpart in the reference).  The dt
+ * control cadence follows the host's count of queued steps, so it matches
+ * e4c_integrate as long as every queued step runs (max_time not reached);
+ * errors are reported by the next e4c_integrate (e.g. with nsteps = 0). */
+int e4c_integrate_async(int nsteps, double max_time);
 
 /* Simulation time, dt_global and step counter of the device-side loop. */
 int e4c_sim_state(double* time, double* dt_global, int* step);

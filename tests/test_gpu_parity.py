@@ -260,3 +260,37 @@ def test_autotune_keeps_state_and_parity(oracle, e4lib):
             sim.run(nsteps)
             gp, gc = sim.download(0)
         assert_same(gc, oout[0][1], f"conserved with tile {shape}")
+
+
+def test_async_transfers_match_sync(e4lib):
+    """Upload, steps and download through the asynchronous entry points (two
+    copy streams, event ordering, steps queued without waiting) give the same
+    bits and the same clock as the synchronous ones, call after call."""
+    import torch
+
+    from eilmer4_b200.simcore import Simulation
+    wl = W.inflow_3d(n=32)
+    b = wl.blocks[0]
+    n = b.ncell
+    host_in = torch.from_numpy(b.prim.copy()).pin_memory()
+    outs = []
+    for use_async in (False, True):
+        with Simulation.from_workload(wl) as sim:
+            res = []
+            for _ in range(3):
+                if use_async:
+                    out = torch.empty((8, n), dtype=torch.float64).pin_memory()
+                    sim.upload_async(0, host_in)
+                    sim.run_async(2)
+                    sim.download_async(0, prim=out)
+                    sim.wait_transfers()
+                    res.append(out.numpy().copy())
+                else:
+                    sim.upload(0, b.prim)
+                    sim.run(2)
+                    res.append(sim.download(0, want_cons=False)[0])
+            sim.run(0)
+            res.append(np.array(sim.state()))
+            outs.append(res)
+    for a, c in zip(outs[0], outs[1]):
+        assert np.array_equal(a, c)
