@@ -435,6 +435,34 @@ int e4c_block_download(int h, double* prim, double* cons) {
     return E4C_OK;
 }
 
+static int dt_chem_io(int h, double* host, int to_host) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size()) || !host) return fail(E4C_ERR_ARG, "bad handle or pointer");
+    BlockHost& b = c.blocks[h];
+    if (!b.v.dt_chem) return fail(E4C_ERR_STATE, "the block carries no chemistry step (not reacting)");
+    const size_t bytes = b.ncell * sizeof(double);
+    if (to_host) {
+        launch_dt_chem_copy(b.v, c.d_staging, 1, c.stream);
+        c.launches += 1;
+        E4C_CUDA(cudaGetLastError());
+        E4C_CUDA(cudaMemcpyAsync(host, c.d_staging, bytes, cudaMemcpyDeviceToHost, c.stream));
+    } else {
+        E4C_CUDA(cudaMemcpyAsync(c.d_staging, host, bytes, cudaMemcpyHostToDevice, c.stream));
+        launch_dt_chem_copy(b.v, c.d_staging, 0, c.stream);
+        c.launches += 1;
+        E4C_CUDA(cudaGetLastError());
+    }
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    return E4C_OK;
+}
+
+int e4c_block_get_dt_chem(int h, double* dt_chem) { return dt_chem_io(h, dt_chem, 1); }
+
+int e4c_block_set_dt_chem(int h, const double* dt_chem) {
+    return dt_chem_io(h, const_cast<double*>(dt_chem), 0);
+}
+
 int Ctx::ensure_stage_io(size_t bytes) {
     if (bytes <= stage_io_bytes) return E4C_OK;
     // the previous buffers may still be in use by queued transfers

@@ -531,6 +531,26 @@ void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int st
     else k_update<1, 0><<<grid_for(n, T), T, 0, s>>>(b, sim, gas, stage, final_stage);
 }
 
+// Per-cell chemistry step suggestion of the interior cells (i fastest) to or
+// from a dense array.
+__global__ void k_dt_chem_copy(BlockView b, double* dense, int to_dense) {
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = b.imin + int(t % b.ni);
+        const int j = b.jmin + int((t / b.ni) % b.nj);
+        const int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        if (to_dense) dense[t] = b.dt_chem[c];
+        else b.dt_chem[c] = dense[t];
+    }
+}
+
+void launch_dt_chem_copy(const BlockView& b, double* dense, int to_dense, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_dt_chem_copy<<<grid_for(n, 256), 256, 0, s>>>(b, dense, to_dense);
+}
+
 void launch_dt_reset(unsigned long long* acc, int nb, cudaStream_t s) {
     k_dt_reset<<<(nb + 127) / 128, 128, 0, s>>>(acc, nb);
 }

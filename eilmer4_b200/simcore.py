@@ -40,11 +40,14 @@ class Simulation:
                                use_graphs=use_graphs, gas=gas)
         _lib.check(self.L.e4c_init(self.cfg))
         self.blocks = []   # (ni, nj, nk)
+        self.vertices = []
+        self.species = ["air"]
         self.nsp = 1
         if thermochem is not None:
             self._tc = thermochem.fill(_lib.E4CThermoChem())
             _lib.check(self.L.e4c_set_thermochem(ctypes.byref(self._tc)))
             self.nsp = thermochem.nsp
+            self.species = list(thermochem.species)
 
     @classmethod
     def from_workload(cls, wl, *, precision="fp64", control=None, use_graphs=True, **config):
@@ -77,6 +80,7 @@ class Simulation:
         h = _lib.check(self.L.e4c_block_create(ni, nj, nk, _lib.dptr(vtx), bca, _lib.dptr(inflow)))
         nk_eff = nk if self.cfg.dimensions == 3 else 1
         self.blocks.append((ni, nj, nk_eff))
+        self.vertices.append(vtx)
         return h
 
     def ncell(self, h):
@@ -151,6 +155,36 @@ class Simulation:
         out = (ctypes.c_longlong * 4)()
         _lib.check(self.L.e4c_chemistry_counters(out, int(bool(reset))))
         return tuple(int(x) for x in out)
+
+    # -- flow files (sfluidblock.d:1778-1956) --------------------------------
+    def write_flow(self, h, path, fmt="gziptext", label=""):
+        """Write block h's current state as an Eilmer4 flow file."""
+        from . import flowfile
+        ni, nj, nk = self.blocks[h]
+        dims = self.cfg.dimensions
+        prim, _ = self.download(h, want_cons=False)
+        pos, vol = flowfile.cell_geometry(self.vertices[h], ni, nj, nk, dims)
+        dt_chem = None
+        if self.nsp > 1 and self.cfg.reacting:
+            dt_chem = np.zeros(ni * nj * nk)
+            _lib.check(self.L.e4c_block_get_dt_chem(h, _lib.dptr(dt_chem)))
+        t, _, _ = self.state()
+        flowfile.write_flow(path, prim=prim, pos=pos, volume=vol, dimensions=dims, ni=ni, nj=nj,
+                            nk=nk, species=self.species, sim_time=t, label=label,
+                            dt_chem=dt_chem, fmt=fmt)
+
+    def read_flow(self, h, path, fmt="gziptext"):
+        """Set block h's state from an Eilmer4 flow file; returns its sim_time."""
+        from . import flowfile
+        fl = flowfile.read_flow(path, fmt)
+        if (fl["nicell"], fl["njcell"], fl["nkcell"]) != self.blocks[h]:
+            raise ValueError("the flow file's block size differs from block %d" % h)
+        prim, dt_chem = flowfile.prim_from_flow(fl, self.nsp)
+        self.upload(h, prim)
+        if dt_chem is not None and self.cfg.reacting:
+            dt_chem = np.ascontiguousarray(dt_chem)
+            _lib.check(self.L.e4c_block_set_dt_chem(h, _lib.dptr(dt_chem)))
+        return fl["sim_time"]
 
     # -- learned chemistry seed ---------------------------------------------
     def seed_collect(self, hs, dt, nsamples, seed=1):

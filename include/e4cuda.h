@@ -229,6 +229,13 @@ int e4c_block_upload(int h, const double* prim);
 /* Download the primitive and/or conserved state (either pointer may be NULL). */
 int e4c_block_download(int h, double* prim, double* cons);
 
+/* Per-cell chemistry step suggestion (dt_chem, the reference's
+ * FVCell.dt_chem, fvcell.d:1510-1621) of a reacting block's interior cells,
+ * i fastest: read for a flow file's dt_chem column, written back from one
+ * on restart (sfluidblock.d:1778-1956). */
+int e4c_block_get_dt_chem(int h, double* dt_chem);
+int e4c_block_set_dt_chem(int h, const double* dt_chem);
+
 /* Asynchronous forms of e4c_block_upload / e4c_block_download (no
  * counterpart in the reference, whose host and solver share memory).  The
  * host-to-device and device-to-host copies run on two copy streams of their
