@@ -132,6 +132,7 @@ def load():
         "e4c_transfers_wait": ([], i),
         "e4c_integrate_async": ([i, d], i),
         "e4c_block_get_dt_chem": ([i, dp], i),
+        "e4c_connect_blocks": ([i, i, i, i, i], i),
         "e4c_block_set_dt_chem": ([i, dp], i),
         "e4c_dt_allow": ([ip, i, d, i, dp, dp], i),
         "e4c_gasdynamic_step": ([ip, i, d, ip], i),

@@ -397,6 +397,71 @@ int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* b
     return int(c.blocks.size()) - 1;
 }
 
+int e4c_connect_blocks(int ha, int fa, int hb, int fb, int orientation) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    const int nb = int(c.blocks.size());
+    if (ha < 0 || ha >= nb || hb < 0 || hb >= nb || ha == hb)
+        return fail(E4C_ERR_ARG, "bad block handles");
+    if (fa < 0 || fa > 5 || fb < 0 || fb > 5) return fail(E4C_ERR_ARG, "bad face");
+    if (orientation != 0)
+        return fail(E4C_ERR_UNSUPPORTED, "only orientation 0 is on this path");
+    static const int opposite[6] = {SOUTH, WEST, NORTH, EAST, BOTTOM, TOP};
+    if (opposite[fa] != fb)
+        return fail(E4C_ERR_UNSUPPORTED, "only opposite faces (east-west, north-south, top-bottom) join");
+    BlockHost& A = c.blocks[ha];
+    BlockHost& B = c.blocks[hb];
+    if (c.cfg.dimensions == 2 && fa >= 4) return fail(E4C_ERR_ARG, "no top/bottom faces in 2-D");
+    const BlockView &va = A.v, &vb = B.v;
+    const bool ew = (fa == EAST || fa == WEST), ns = (fa == NORTH || fa == SOUTH);
+    const bool same = ew ? (va.nj == vb.nj && va.nk == vb.nk)
+                     : ns ? (va.ni == vb.ni && va.nk == vb.nk) : (va.ni == vb.ni && va.nj == vb.nj);
+    if (!same) return fail(E4C_ERR_ARG, "the joined faces differ in size");
+    if (A.fused != B.fused)
+        return fail(E4C_ERR_UNSUPPORTED, "a uniform (fused) block joins only another uniform block");
+    if (A.fused) {
+        const FusedDesc &x = A.f, &y = B.f;
+        bool eq = x.vol == y.vol;
+        for (int q = 0; q < 3; ++q) {
+            eq = eq && x.len[q] == y.len[q] && x.area[q] == y.area[q];
+            for (int r = 0; r < 3; ++r)
+                eq = eq && x.fn[q][r] == y.fn[q][r] && x.ft1[q][r] == y.ft1[q][r] &&
+                     x.ft2[q][r] == y.ft2[q][r];
+        }
+        if (!eq) return fail(E4C_ERR_UNSUPPORTED, "joined uniform blocks must have identical cell geometry");
+        A.f.bc[fa] = E4C_BC_EXCHANGE;
+        B.f.bc[fb] = E4C_BC_EXCHANGE;
+    }
+    A.ex_block[fa] = hb;
+    B.ex_block[fb] = ha;
+    A.v.bc[fa] = E4C_BC_EXCHANGE;
+    B.v.bc[fb] = E4C_BC_EXCHANGE;
+    if (!A.fused) {
+        auto src = [](const BlockView& o) {
+            ExchangeSrc e{};
+            e.W = o.W;
+            e.cgeom = o.cgeom;
+            e.npad = o.npad;
+            e.nidim = o.nidim;
+            e.njdim = o.njdim;
+            e.imax = o.imax;
+            e.jmax = o.jmax;
+            e.kmax = o.kmax;
+            return e;
+        };
+        A.v.ex[fa] = src(B.v);
+        B.v.ex[fb] = src(A.v);
+        launch_exchange_geometry(A.v, fa, c.stream);
+        launch_exchange_geometry(B.v, fb, c.stream);
+        c.launches += 2;
+        E4C_CUDA(cudaGetLastError());
+        E4C_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    c.descs_valid = false;
+    c.reset_graphs();
+    return E4C_OK;
+}
+
 int e4c_block_upload(int h, const double* prim) {
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");

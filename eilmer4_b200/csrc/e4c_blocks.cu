@@ -217,10 +217,17 @@ int Ctx::prepare_fused() {
     }
     std::vector<FusedDesc> ds;
     long long items = 0;
+    std::vector<int> desc_of(blocks.size(), -1);
+    {
+        int q = 0;
+        for (size_t h = 0; h < blocks.size(); ++h)
+            if (blocks[h].fused) desc_of[h] = q++;
+    }
     for (size_t h = 0; h < blocks.size(); ++h) {
         BlockHost& b = blocks[h];
         if (!b.fused) continue;
         FusedDesc& f = b.f;
+        for (int w = 0; w < 6; ++w) f.ex[w] = b.ex_block[w] >= 0 ? desc_of[b.ex_block[w]] : -1;
         f.tiles_i = (f.ni + tile_ti - 1) / tile_ti;
         f.tiles_j = (f.nj + tile_tj - 1) / tile_tj;
         f.kchunks = (f.nk + tile_kc - 1) / tile_kc;
@@ -233,6 +240,7 @@ int Ctx::prepare_fused() {
     fused_items = items;
     if (nfused > 0) {
         if (nfused > descs_cap) {
+            dfree(d_descs);
             d_descs = static_cast<FusedDesc*>(dalloc(sizeof(FusedDesc) * std::max(nfused, 64)));
             if (!d_descs) return fail(E4C_ERR_CUDA, "cudaMalloc of block descriptors failed");
             descs_cap = std::max(nfused, 64);

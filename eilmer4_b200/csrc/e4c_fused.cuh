@@ -52,7 +52,8 @@ __device__ __forceinline__ void reflect_normal(R& vx, R& vy, R& vz, const double
 // built from the boundary condition of the face they lie beyond; corner
 // ghosts and cells beyond the second ghost layer are never read and skipped.
 template <typename R, int TI, int TJ>
-__device__ __forceinline__ void load_plane(const FusedDesc& d, const R* __restrict__ W, int use_a0,
+__device__ __forceinline__ void load_plane(const FusedDesc* __restrict__ descs, int stage,
+                                           const FusedDesc& d, const R* __restrict__ W, int use_a0,
                                            const GasConsts& gas, R* plane, int i0, int j0,
                                            int kk) {
     constexpr int PI = TI + 4, PJ = TJ + 4;
@@ -78,7 +79,31 @@ __device__ __forceinline__ void load_plane(const FusedDesc& d, const R* __restri
         if (layer > 1) continue;
         R rho, vx, vy, vz, u, a;
         int type = which >= 0 ? d.bc[which] : -1;
-        if (type == 1) {  // supersonic inflow: both ghost layers hold the inflow state
+        if (type == 3) {
+            // full-face copy (full_face_copy.d, opposite faces, orientation 0):
+            // the partner block's first two cells beyond the joint face
+            const FusedDesc& o = descs[d.ex[which]];
+            int si = gi, sj = gj, sk = gk;
+            switch (which) {
+                case WEST: si = o.ni - 1 - layer; break;
+                case EAST: si = layer; break;
+                case SOUTH: sj = o.nj - 1 - layer; break;
+                case NORTH: sj = layer; break;
+                case BOTTOM: sk = o.nk - 1 - layer; break;
+                default: sk = layer; break;
+            }
+            const size_t onc = size_t(o.ni) * o.nj * o.nk;
+            const size_t c = (size_t(sk) * o.nj + sj) * o.ni + si;
+            const R* OW = static_cast<const R*>(stage == 1 ? o.WA : o.WB);
+            rho = OW[0 * onc + c]; vx = OW[1 * onc + c]; vy = OW[2 * onc + c];
+            vz = OW[3 * onc + c]; u = OW[4 * onc + c];
+            if (stage == 1 && *o.use_a0) {
+                a = R(o.A0[c]);
+            } else {
+                R T = u * R(gas.Cvinv);
+                a = sqrt(R(gas.gamma) * R(gas.Rgas) * T);
+            }
+        } else if (type == 1) {  // supersonic inflow: both ghost layers hold the inflow state
             rho = R(d.inflow[0]); vx = R(d.inflow[1]); vy = R(d.inflow[2]); vz = R(d.inflow[3]);
             u = R(d.inflow[4]); a = R(d.inflow[5]);
         } else {
@@ -306,7 +331,7 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
         // prologue: planes k0-2 .. k0+1
         __syncthreads();
         for (int kk = k0 - 2; kk <= k0 + 1; ++kk)
-            load_plane<R, TI, TJ>(d, Win, use_a0, gas, planes + ((kk + 8) & 3) * S::PLANE, i0, j0, kk);
+            load_plane<R, TI, TJ>(descs, stage, d, Win, use_a0, gas, planes + ((kk + 8) & 3) * S::PLANE, i0, j0, kk);
         __syncthreads();
         R Fbot[5];
         const int coff = (tj + 2) * PI + (ti + 2);
@@ -321,7 +346,8 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
         __syncthreads();  // plane k0-2 is overwritten by the first load below
         for (int k = k0; k < k1; ++k) {
             // plane k+2 replaces plane k-2 (not read since the previous iteration)
-            load_plane<R, TI, TJ>(d, Win, use_a0, gas, planes + ((k + 2 + 8) & 3) * S::PLANE, i0, j0, k + 2);
+            load_plane<R, TI, TJ>(descs, stage, d, Win, use_a0, gas, planes + ((k + 2 + 8) & 3) * S::PLANE, i0, j0,
+                                  k + 2);
             __syncthreads();
             const R* pk = planes + ((k + 8) & 3) * S::PLANE;
             // i-faces, (TI+1) x TJ (face fi is the west face of cell i0+fi), then

@@ -306,7 +306,23 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
     const size_t g2 = pidx(b, i + 2 * di, j + 2 * dj, k + 2 * dk);
     const int nw = W_NBASE + (NSP > 1 ? NSP : 0);
     const int type = b.bc[which];
-    if (type == 1) {  // InFlowBC_Supersonic: both ghosts <- inflow FlowState
+    if (type == 3) {  // full-face copy: the partner's first two cells
+        const ExchangeSrc& o = b.ex[which];
+        const size_t dst[2] = {g1, g2};
+        for (int g = 0; g < 2; ++g) {
+            int si = i, sj = j, sk = k;
+            switch (which) {
+                case NORTH: sj = 2 + g; break;
+                case EAST: si = 2 + g; break;
+                case SOUTH: sj = o.jmax - g; break;
+                case WEST: si = o.imax - g; break;
+                case TOP: sk = 2 + g; break;
+                default: sk = o.kmax - g; break;
+            }
+            const size_t sc = (size_t(sk) * o.njdim + sj) * o.nidim + si;
+            for (int q = 0; q < nw; ++q) b.W[q * b.npad + dst[g]] = o.W[q * o.npad + sc];
+        }
+    } else if (type == 1) {  // InFlowBC_Supersonic: both ghosts <- inflow FlowState
         for (int q = 0; q < nw; ++q) {
             b.W[q * b.npad + g1] = b.inflow[q];
             b.W[q * b.npad + g2] = b.inflow[q];
@@ -345,6 +361,50 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
             b.W[W_VZ * b.npad + dst[g]] = v.z;
         }
     }
+}
+
+// Ghost cells of an exchange boundary take the partner cells' volume and
+// lengths (exchange_geometry, full_face_copy.d:963-1083, CopyDataOption.grid).
+__global__ void k_exchange_geometry(BlockView b, int which) {
+    int n1, n2;
+    if (which == NORTH || which == SOUTH) { n1 = b.ni; n2 = b.nk; }
+    else if (which == EAST || which == WEST) { n1 = b.nj; n2 = b.nk; }
+    else { n1 = b.ni; n2 = b.nj; }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n1 * n2) return;
+    const int a1 = t % n1, a2 = t / n1;
+    int i, j, k, di = 0, dj = 0, dk = 0;
+    switch (which) {
+        case NORTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmax; dj = 1; break;
+        case SOUTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmin; dj = -1; break;
+        case EAST: j = b.jmin + a1; k = b.kmin + a2; i = b.imax; di = 1; break;
+        case WEST: j = b.jmin + a1; k = b.kmin + a2; i = b.imin; di = -1; break;
+        case TOP: i = b.imin + a1; j = b.jmin + a2; k = b.kmax; dk = 1; break;
+        default: i = b.imin + a1; j = b.jmin + a2; k = b.kmin; dk = -1; break;
+    }
+    const ExchangeSrc& o = b.ex[which];
+    for (int g = 0; g < 2; ++g) {
+        int si = i, sj = j, sk = k;
+        switch (which) {
+            case NORTH: sj = 2 + g; break;
+            case EAST: si = 2 + g; break;
+            case SOUTH: sj = o.jmax - g; break;
+            case WEST: si = o.imax - g; break;
+            case TOP: sk = 2 + g; break;
+            default: sk = o.kmax - g; break;
+        }
+        const size_t sc = (size_t(sk) * o.njdim + sj) * o.nidim + si;
+        const size_t gc = pidx(b, i + (g + 1) * di, j + (g + 1) * dj, k + (g + 1) * dk);
+        for (int q = 0; q < 4; ++q) b.cgeom[q * b.npad + gc] = o.cgeom[q * o.npad + sc];
+    }
+}
+
+void launch_exchange_geometry(const BlockView& b, int which, cudaStream_t s) {
+    int n;
+    if (which == NORTH || which == SOUTH) n = b.ni * b.nk;
+    else if (which == EAST || which == WEST) n = b.nj * b.nk;
+    else n = b.ni * b.nj;
+    k_exchange_geometry<<<(n + 127) / 128, 128, 0, s>>>(b, which);
 }
 
 // ---------------------------------------------------------------------------

@@ -18,6 +18,7 @@ struct BlockHost {
     size_t nprim_vars = 8;
     bool fused = false;
     FusedDesc f{};          // fused path: storage and uniform geometry
+    int ex_block[6] = {-1, -1, -1, -1, -1, -1};   // partner handle of an exchange boundary
 };
 
 // The learned chemistry seed (e4c_seed.cu): network, training set, guesses.

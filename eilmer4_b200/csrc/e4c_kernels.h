@@ -41,6 +41,8 @@ void launch_begin_run(SimDev* sim, double max_time, cudaStream_t s);
 void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
 // thermally perfect mixture / mechanism into constant memory; chemistry of one block
 int set_thermochem_constants(const e4c_thermochem& tc);
+// ghost-cell geometry of an exchange boundary from the partner block
+void launch_exchange_geometry(const BlockView& b, int which, cudaStream_t s);
 // per-cell chemistry step suggestions to (to_dense = 1) or from a dense array
 void launch_dt_chem_copy(const BlockView& b, double* dense, int to_dense, cudaStream_t s);
 // thermally perfect face fluxes / cell updates (e4c_tp.cu)

@@ -20,6 +20,18 @@ enum Bnd { NORTH = 0, EAST = 1, SOUTH = 2, WEST = 3, TOP = 4, BOTTOM = 5 };
 // rho, vel.x, vel.y, vel.z, p, T, u, a (then mass fractions).
 enum PrimField { W_RHO = 0, W_VX, W_VY, W_VZ, W_P, W_T, W_U, W_A, W_NBASE };
 
+// The partner of an exchange boundary on the general path (full-face copy,
+// opposite faces, orientation 0): its padded primitive arrays and cell
+// geometry; padded indices start at 2 in every active direction.
+struct ExchangeSrc {
+    const double* W;
+    const double* cgeom;
+    size_t npad;
+    int nidim, njdim;
+    int imax, jmax, kmax;
+    int pad_;
+};
+
 // Device view of one structured block on the general-geometry path.  All
 // arrays use the reference's padded (i,j,k) index with two ghost layers,
 // (k*njdim + j)*nidim + i (src/eilmer/sfluidblock.d:205).
@@ -52,6 +64,7 @@ struct BlockView {
     int block_id;
     int axis_frames;                // every face frame is made of signed unit axes
     double* dt_chem;                // per-cell chemistry step suggestion (reacting blocks)
+    ExchangeSrc ex[6];              // partners of exchange boundaries (bc == 3)
 };
 
 // Device-resident simulation state (one per library context).
@@ -87,6 +100,7 @@ struct FusedDesc {
     double area[3];
     double fn[3][3], ft1[3][3], ft2[3][3];
     double inflow[6];           // rho, vx, vy, vz, u, a
+    int ex[6];                  // descriptor index of the partner of an exchange boundary
 };
 
 // Molar masses of the five species, for the chemistry seed's guesses.

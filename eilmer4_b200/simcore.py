@@ -83,6 +83,11 @@ class Simulation:
         self.vertices.append(vtx)
         return h
 
+    def connect(self, ha, face_a, hb, face_b, orientation=0):
+        """Join two blocks' opposite faces with an exchange boundary."""
+        _lib.check(self.L.e4c_connect_blocks(int(ha), int(face_a), int(hb), int(face_b),
+                                             int(orientation)))
+
     def ncell(self, h):
         ni, nj, nk = self.blocks[h]
         return ni * nj * nk

@@ -289,3 +289,80 @@ def reacting_channel_hot(ni=512, nj=256, nsteps=300):
     wl = reacting_channel(ni, nj, nsteps, T_in=2000.0, p_in=2.0e4)
     wl.name = "reacting_channel_hot_%dx%d" % (ni, nj)
     return wl
+
+
+def split_block(b: BlockSpec, dimensions, parts=(2, 1, 1)):
+    """Cut a block into parts[0] x parts[1] x parts[2] blocks joined by
+    exchange boundaries (the FluidBlockArray split of the reference's prep,
+    src/eilmer/prep.lua).  Returns (blocks, connections), connections as
+    (block a, face a, block b, face b) with orientation 0, blocks numbered
+    i fastest."""
+    pi, pj, pk = parts
+    if dimensions == 2:
+        pk = 1
+    nk1 = b.nk + 1 if dimensions == 3 else 1
+    v = np.asarray(b.vtx).reshape(nk1, b.nj + 1, b.ni + 1, 3)
+    nv = b.prim.shape[0]
+    pr = b.prim.reshape(nv, b.nk, b.nj, b.ni)
+
+    def cuts(n, p):
+        e = [round(n * q / p) for q in range(p + 1)]
+        if any(e[q + 1] - e[q] < 2 for q in range(p)):
+            raise ValueError("a part would have fewer than 2 cells")
+        return e
+
+    ei, ej = cuts(b.ni, pi), cuts(b.nj, pj)
+    ek = cuts(b.nk, pk) if dimensions == 3 else [0, 1]
+    blocks, index = [], {}
+    for ck in range(pk):
+        for cj in range(pj):
+            for ci in range(pi):
+                i0, i1, j0, j1, k0, k1 = ei[ci], ei[ci + 1], ej[cj], ej[cj + 1], ek[ck], ek[ck + 1]
+                kv = slice(k0, k1 + 1) if dimensions == 3 else slice(0, 1)
+                vtx = v[kv, j0:j1 + 1, i0:i1 + 1].reshape(-1, 3).copy()
+                prim = pr[:, k0:k1, j0:j1, i0:i1].reshape(nv, -1).copy()
+                bc = list(b.bc)
+                # faces inside the original block become exchange boundaries
+                if ci > 0: bc[WEST] = BC_SLIP_WALL
+                if ci < pi - 1: bc[EAST] = BC_SLIP_WALL
+                if cj > 0: bc[SOUTH] = BC_SLIP_WALL
+                if cj < pj - 1: bc[NORTH] = BC_SLIP_WALL
+                if ck > 0: bc[BOTTOM] = BC_SLIP_WALL
+                if ck < pk - 1: bc[TOP] = BC_SLIP_WALL
+                index[(ci, cj, ck)] = len(blocks)
+                blocks.append(BlockSpec(i1 - i0, j1 - j0, (k1 - k0) if dimensions == 3 else 1,
+                                        vtx, tuple(bc), b.inflow, prim))
+    conns = []
+    for (ci, cj, ck), a in index.items():
+        if ci + 1 < pi:
+            conns.append((a, EAST, index[(ci + 1, cj, ck)], WEST))
+        if cj + 1 < pj:
+            conns.append((a, NORTH, index[(ci, cj + 1, ck)], SOUTH))
+        if ck + 1 < pk:
+            conns.append((a, TOP, index[(ci, cj, ck + 1)], BOTTOM))
+    return blocks, conns
+
+
+def join_prims(blocks, b_shape, dimensions, parts=(2, 1, 1)):
+    """Reassemble the primitive arrays of split_block's blocks (list of
+    (nv, n) arrays) into the original block's (nv, ni*nj*nk) layout."""
+    ni, nj, nk = b_shape
+    pi, pj, pk = parts
+    if dimensions == 2:
+        pk = 1
+    nv = blocks[0].shape[0]
+    out = np.zeros((nv, nk, nj, ni))
+
+    def cuts(n, p):
+        return [round(n * q / p) for q in range(p + 1)]
+
+    ei, ej = cuts(ni, pi), cuts(nj, pj)
+    ek = cuts(nk, pk) if dimensions == 3 else [0, 1]
+    q = 0
+    for ck in range(pk):
+        for cj in range(pj):
+            for ci in range(pi):
+                i0, i1, j0, j1, k0, k1 = ei[ci], ei[ci + 1], ej[cj], ej[cj + 1], ek[ck], ek[ck + 1]
+                out[:, k0:k1, j0:j1, i0:i1] = blocks[q].reshape(nv, k1 - k0, j1 - j0, i1 - i0)
+                q += 1
+    return out.reshape(nv, -1)

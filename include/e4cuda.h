@@ -64,6 +64,7 @@ extern "C" {
 #define E4C_BC_WALL_WITH_SLIP 0
 #define E4C_BC_INFLOW_SUPERSONIC 1
 #define E4C_BC_OUTFLOW_SIMPLE_EXTRAPOLATE 2
+#define E4C_BC_EXCHANGE 3      /* set by e4c_connect_blocks only */
 
 /* flux_calculator (src/eilmer/fvcore.d:184-228, plus the new "hllc"). */
 #define E4C_FLUX_AUSMDV 0
@@ -222,6 +223,16 @@ int e4c_finalize(void);
  * inflow_prim is one primitive FlowState used by inflow boundaries. */
 int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* bc_type,
                      const double* inflow_prim);
+
+/* Join face face_a of block ha to face face_b of block hb
+ * (GhostCellFullFaceCopy, src/eilmer/bc/ghost_cell_effect/full_face_copy.d,
+ * set up by the reference's FluidBlockArray / connectBlocks in prep):
+ * opposite faces (east-west, north-south, top-bottom), orientation 0, equal
+ * face sizes, both blocks on the same path (both general, or both fused with
+ * identical uniform geometry).  Both faces become exchange boundaries: the
+ * ghost cells take the partner's cell geometry now and its flow state at the
+ * start of every stage.  Call after creating the blocks, before stepping. */
+int e4c_connect_blocks(int ha, int face_a, int hb, int face_b, int orientation);
 
 /* Upload a block's primitive state and encode its conserved quantities. */
 int e4c_block_upload(int h, const double* prim);

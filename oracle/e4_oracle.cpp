@@ -670,7 +670,23 @@ void Sim::apply_bcs(Block& b) {
                 for (int i = i0; i <= i1; ++i) {
                     Cell& g1 = b.cell(i + di, j + dj, k + dk);
                     Cell& g2 = b.cell(i + 2 * di, j + 2 * dj, k + 2 * dk);
-                    if (type == E4O_BC_INFLOW_SUPERSONIC) {
+                    if (type == E4O_BC_EXCHANGE) {
+                        // full_face_copy.d (orientation 0, opposite faces): the
+                        // ghost layers take the partner's first two cells
+                        Block& o = *blocks[b.ex_block[which]];
+                        for (int g = 0; g < 2; ++g) {
+                            int si = i, sj = j, sk = k;
+                            switch (which) {
+                                case 0: sj = o.jmin + g; break;
+                                case 1: si = o.imin + g; break;
+                                case 2: sj = o.jmax - g; break;
+                                case 3: si = o.imax - g; break;
+                                case 4: sk = o.kmin + g; break;
+                                default: sk = o.kmax - g; break;
+                            }
+                            (g == 0 ? g1 : g2).fs = o.cell(si, sj, sk).fs;
+                        }
+                    } else if (type == E4O_BC_INFLOW_SUPERSONIC) {
                         g1.fs = b.inflow;  // flow_state_copy.d:66+
                         g2.fs = b.inflow;
                     } else if (type == E4O_BC_OUTFLOW_EXTRAPOLATE) {
@@ -904,10 +920,10 @@ int Sim::gasdynamic_increment() {
     const int nstages = (cfg.update_scheme == E4O_UPDATE_PC) ? 2 : 1;
     last_bad_cells = 0;
     for (int stage = 1; stage <= nstages; ++stage) {
-        for (Block* b : blocks) {
-            apply_bcs(*b);
-            convective_flux(*b);
-        }
+        // every block's ghost cells first (exchange copies see no flux-loop
+        // state), then every block's fluxes
+        for (Block* b : blocks) apply_bcs(*b);
+        for (Block* b : blocks) convective_flux(*b);
         for (Block* b : blocks) {
             int rc = stage_cells(*b, stage, dt_global);
             if (rc != 0) return rc;
@@ -1003,6 +1019,68 @@ int e4o_add_block(void* sim, int ni, int nj, int nk, const double* vtx, const in
     s->mutate_in_place = s->mutate_in_place || !b->axis_frames;
     s->blocks.push_back(b);
     return int(s->blocks.size()) - 1;
+}
+
+int e4o_connect_blocks(void* sim, int a, int fa, int b, int fb, int orientation) {
+    Sim* s = static_cast<Sim*>(sim);
+    const int nb = int(s->blocks.size());
+    if (a < 0 || a >= nb || b < 0 || b >= nb || a == b) return E4O_ERR_ARG;
+    if (fa < 0 || fa > 5 || fb < 0 || fb > 5 || orientation != 0) return E4O_ERR_ARG;
+    // opposite faces only: north-south, east-west, top-bottom
+    static const int opposite[6] = {2, 3, 0, 1, 5, 4};
+    if (opposite[fa] != fb) return E4O_ERR_ARG;
+    Block& A = *s->blocks[a];
+    Block& B = *s->blocks[b];
+    if (A.dim == 2 && fa >= 4) return E4O_ERR_ARG;
+    const bool ew = (fa == 1 || fa == 3), ns = (fa == 0 || fa == 2);
+    if (ew && (A.nj != B.nj || A.nk != B.nk)) return E4O_ERR_ARG;
+    if (ns && (A.ni != B.ni || A.nk != B.nk)) return E4O_ERR_ARG;
+    if (!ew && !ns && (A.ni != B.ni || A.nj != B.nj)) return E4O_ERR_ARG;
+    A.bc[fa] = E4O_BC_EXCHANGE; A.ex_block[fa] = b;
+    B.bc[fb] = E4O_BC_EXCHANGE; B.ex_block[fb] = a;
+    // exchange_geometry (full_face_copy.d:963-1083, CopyDataOption.grid):
+    // ghost cells take the partner cells' volume and lengths
+    auto copy_geom = [](Block& D, int which, Block& O) {
+        int di = 0, dj = 0, dk = 0;
+        switch (which) {
+            case 0: dj = 1; break;
+            case 1: di = 1; break;
+            case 2: dj = -1; break;
+            case 3: di = -1; break;
+            case 4: dk = 1; break;
+            default: dk = -1; break;
+        }
+        int i0 = D.imin, i1 = D.imax, j0 = D.jmin, j1 = D.jmax, k0 = D.kmin, k1 = D.kmax;
+        if (which == 0) j0 = j1 = D.jmax;
+        if (which == 2) j0 = j1 = D.jmin;
+        if (which == 1) i0 = i1 = D.imax;
+        if (which == 3) i0 = i1 = D.imin;
+        if (which == 4) k0 = k1 = D.kmax;
+        if (which == 5) k0 = k1 = D.kmin;
+        for (int k = k0; k <= k1; ++k)
+            for (int j = j0; j <= j1; ++j)
+                for (int i = i0; i <= i1; ++i)
+                    for (int g = 0; g < 2; ++g) {
+                        int si = i, sj = j, sk = k;
+                        switch (which) {
+                            case 0: sj = O.jmin + g; break;
+                            case 1: si = O.imin + g; break;
+                            case 2: sj = O.jmax - g; break;
+                            case 3: si = O.imax - g; break;
+                            case 4: sk = O.kmin + g; break;
+                            default: sk = O.kmax - g; break;
+                        }
+                        Cell& gc = D.cell(i + (g + 1) * di, j + (g + 1) * dj, k + (g + 1) * dk);
+                        const Cell& sc = O.cell(si, sj, sk);
+                        gc.vol = sc.vol;
+                        gc.iLen = sc.iLen;
+                        gc.jLen = sc.jLen;
+                        gc.kLen = sc.kLen;
+                    }
+    };
+    copy_geom(A, fa, B);
+    copy_geom(B, fb, A);
+    return 0;
 }
 
 int e4o_set_flow(void* sim, int blk, const double* prim) {

@@ -24,7 +24,8 @@
 extern "C" {
 #endif
 
-enum { E4O_BC_SLIP_WALL = 0, E4O_BC_INFLOW_SUPERSONIC = 1, E4O_BC_OUTFLOW_EXTRAPOLATE = 2 };
+enum { E4O_BC_SLIP_WALL = 0, E4O_BC_INFLOW_SUPERSONIC = 1, E4O_BC_OUTFLOW_EXTRAPOLATE = 2,
+       E4O_BC_EXCHANGE = 3 };
 enum { E4O_FLUX_AUSMDV = 0, E4O_FLUX_HLLC = 1 };
 enum { E4O_UPDATE_EULER = 0, E4O_UPDATE_PC = 1 };
 enum { E4O_GAS_IDEAL = 0, E4O_GAS_THERM_PERF_5SP_AIR = 1 };
@@ -87,6 +88,13 @@ void e4o_sim_free(void* sim);
  * Returns the block index, or a negative error code. */
 int e4o_add_block(void* sim, int ni, int nj, int nk, const double* vtx,
                   const int* bc, const double* inflow);
+
+/* Connect face fa of block a to face fb of block b (GhostCellFullFaceCopy,
+ * src/eilmer/bc/ghost_cell_effect/full_face_copy.d): opposite faces
+ * (east-west, north-south, top-bottom), orientation 0, equal face sizes.
+ * Both faces become exchange boundaries; the ghost cells take the partner's
+ * cell geometry now and its flow state at every stage. */
+int e4o_connect_blocks(void* sim, int a, int fa, int b, int fb, int orientation);
 
 /* Set the interior flow state from a primitive SoA array and encode the
  * conserved quantities (src/eilmer/fvcell.d encode_conserved). */

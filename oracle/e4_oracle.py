@@ -20,6 +20,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libe4oracle.so")
 BC_SLIP_WALL = 0
 BC_INFLOW_SUPERSONIC = 1
 BC_OUTFLOW_EXTRAPOLATE = 2
+BC_EXCHANGE = 3
 FLUX_AUSMDV = 0
 FLUX_HLLC = 1
 UPDATE_EULER = 0
@@ -100,6 +101,7 @@ def lib():
         L.e4o_add_block.argtypes = [vp, ip, ip, ip, P(dp), P(ip), P(dp)]
         L.e4o_add_block.restype = ip
         L.e4o_set_flow.argtypes = [vp, ip, P(dp)]
+        L.e4o_connect_blocks.argtypes = [vp, ip, ip, ip, ip, ip]
         L.e4o_get_flow.argtypes = [vp, ip, P(dp), P(dp)]
         L.e4o_get_cell_geometry.argtypes = [vp, ip, P(dp)]
         L.e4o_run.argtypes = [vp, ip, dp]
@@ -160,6 +162,11 @@ class OracleSim:
             raise RuntimeError(f"e4o_add_block failed: {b}")
         self.blocks.append((ni, nj, nk if self.cfg.dimensions == 3 else 1))
         return b
+
+    def connect(self, a, fa, b, fb, orientation=0):
+        rc = lib().e4o_connect_blocks(self._h, a, fa, b, fb, orientation)
+        if rc != 0:
+            raise RuntimeError(f"e4o_connect_blocks failed: {rc}")
 
     def nvar_prim(self):
         return 8 + (self.nsp if self.nsp > 1 else 0)

@@ -64,6 +64,7 @@ struct Block {
     std::vector<Face> ifi, ifj, ifk;
     std::vector<Vec3> vtx;
     int bc[6] = {0, 0, 0, 0, 0, 0};
+    int ex_block[6] = {-1, -1, -1, -1, -1, -1};   // partner block of an exchange boundary
     FlowState inflow;
     bool axis_frames = true;
 

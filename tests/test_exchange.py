@@ -1,0 +1,117 @@
+"""Blocks joined by exchange boundaries (GhostCellFullFaceCopy,
+src/eilmer/bc/ghost_cell_effect/full_face_copy.d, opposite faces,
+orientation 0): a domain cut into blocks advances exactly as the uncut
+block, on the CPU oracle and on the GPU (general and fused paths)."""
+import numpy as np
+import pytest
+
+from eilmer4_b200 import workloads as W
+
+
+def oracle_run(oracle, wl, blocks, conns, nsteps, **cfgkw):
+    cfg = oracle.default_config(dimensions=wl.dimensions, n_threads=0, **cfgkw)
+    sim = oracle.OracleSim(cfg)
+    for b in blocks:
+        h = sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+        sim.set_flow(h, b.prim)
+    for (a, fa, b, fb) in conns:
+        sim.connect(a, fa, b, fb)
+    assert sim.run(nsteps) == 0
+    return [sim.get_flow(h)[0] for h in range(len(blocks))], (sim.time, sim.dt_global, sim.step)
+
+
+@pytest.mark.parametrize("case", ["sod2d_i", "sod2d_j", "inflow3d_ik"])
+def test_split_domain_matches_single_block_on_the_oracle(oracle, case):
+    if case.startswith("sod2d"):
+        wl = W.sod_2d(40, 12)
+        parts = (3, 1, 1) if case == "sod2d_i" else (1, 2, 1)
+        kw = {"flux_calculator": oracle.FLUX_AUSMDV}
+        n = 40
+    else:
+        wl = W.inflow_3d(n=12)
+        parts = (2, 1, 2)
+        kw = {"flux_calculator": oracle.FLUX_HLLC}
+        n = 15
+    b = wl.blocks[0]
+    (single,), st1 = oracle_run(oracle, wl, [b], [], n, **kw)
+    blocks, conns = W.split_block(b, wl.dimensions, parts)
+    prims, st2 = oracle_run(oracle, wl, blocks, conns, n, **kw)
+    joined = W.join_prims(prims, (b.ni, b.nj, b.nk), wl.dimensions, parts)
+    assert st1 == st2
+    assert np.array_equal(joined, single)
+
+
+def test_connect_rejects_bad_pairs(oracle):
+    wl = W.sod_2d(20, 8)
+    blocks, _ = W.split_block(wl.blocks[0], 2, (2, 1, 1))
+    cfg = oracle.default_config(dimensions=2)
+    sim = oracle.OracleSim(cfg)
+    for b in blocks:
+        sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    with pytest.raises(RuntimeError):
+        sim.connect(0, W.EAST, 1, W.NORTH)      # not opposite faces
+    with pytest.raises(RuntimeError):
+        sim.connect(0, W.EAST, 1, W.WEST, 1)    # orientation other than 0
+
+
+def gpu_run(wl, blocks, conns, nsteps, precision="fp64", **cfg):
+    from eilmer4_b200.simcore import Simulation
+    cfgd = {"dimensions": wl.dimensions, "flux_calculator": wl.flux_calculator}
+    cfgd.update(cfg)
+    with Simulation(cfgd, precision=precision) as sim:
+        for b in blocks:
+            h = sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+            sim.upload(h, b.prim)
+        for (a, fa, b, fb) in conns:
+            sim.connect(a, fa, b, fb)
+        sim.run(nsteps)
+        out = [sim.download(h) for h in range(len(blocks))]
+        return out, sim.state()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("parts", [(3, 1, 1), (1, 2, 1), (2, 2, 1)])
+def test_gpu_split_2d_matches_oracle_and_single_block(oracle, e4lib, parts):
+    wl = W.sod_2d(40, 12)
+    b = wl.blocks[0]
+    n = 40
+    blocks, conns = W.split_block(b, 2, parts)
+    (single,), st1 = gpu_run(wl, [b], [], n)
+    split, st2 = gpu_run(wl, blocks, conns, n)
+    oprims, ost = oracle_run(oracle, wl, blocks, conns, n, flux_calculator=oracle.FLUX_AUSMDV)
+    for (gp, gc), op in zip(split, oprims):
+        assert np.array_equal(gp, op)
+    joined = W.join_prims([p for p, _ in split], (b.ni, b.nj, b.nk), 2, parts)
+    assert np.array_equal(joined, single[0])
+    assert st1 == st2 and st2[2] == ost[2] and st2[0] == ost[0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32_flux"])
+def test_gpu_split_3d_fused_matches_single_block(oracle, e4lib, precision):
+    """Uniform blocks stay on the fused path across the joints: the partner's
+    cells are read straight from its stage-input arrays."""
+    from eilmer4_b200.simcore import Simulation
+    wl = W.inflow_3d(n=32)
+    b = wl.blocks[0]
+    parts = (2, 1, 2)
+    blocks, conns = W.split_block(b, 3, parts)
+    n = 12
+    (single,), st1 = gpu_run(wl, [b], [], n, precision)
+    split, st2 = gpu_run(wl, blocks, conns, n, precision)
+    joined = W.join_prims([p for p, _ in split], (b.ni, b.nj, b.nk), 3, parts)
+    assert np.array_equal(joined, single[0]) and st1 == st2
+    if precision == "fp64":
+        oprims, ost = oracle_run(oracle, wl, blocks, conns, n, flux_calculator=oracle.FLUX_HLLC)
+        for (gp, _), op in zip(split, oprims):
+            assert np.array_equal(gp, op)
+    # and the blocks did run on the fused path
+    with Simulation({"dimensions": 3, "flux_calculator": "hllc"}, precision=precision) as sim:
+        for q in blocks:
+            h = sim.add_block(q.ni, q.nj, q.nk, q.vtx, q.bc, q.inflow)
+            sim.upload(h, q.prim)
+        for c in conns:
+            sim.connect(*c)
+        sim.run(1)
+        prof = sim.profile(1)
+        assert prof["stage"][1] > 0 and prof["flux"][1] == 0
