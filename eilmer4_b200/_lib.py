@@ -32,7 +32,7 @@ ERROR_NAMES = {
     E4C_ERR_STATE: "E4C_ERR_STATE",
 }
 
-FLUX = {"ausmdv": 0, "hllc": 1}
+FLUX = {"ausmdv": 0, "hllc": 1, "hanel": 2, "adaptive_hanel_ausmdv": 3, "adaptive": 3}
 UPDATE = {"euler": 0, "pc": 1, "predictor-corrector": 1, "predictor_corrector": 1}
 PRECISION = {"fp64": 0, "fp32_flux": 1}
 GAS = {"ideal": 0, "therm_perf_5sp_air": 1}
@@ -60,6 +60,8 @@ class E4CConfig(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
+        ("shear_tolerance", ctypes.c_double),
+        ("compression_tolerance", ctypes.c_double),
     ]
 
 

@@ -39,6 +39,8 @@ CONFIG_DEFAULTS = {
     "with_super_time_stepping": False,
     "high_order_flux_calculator": False,
     "strang_splitting": "full_T_full_R",          # :456
+    "shear_tolerance": 0.20,                      # :585
+    "compression_tolerance": -0.30,               # :600
 }
 
 CONTROL_DEFAULTS = {
@@ -70,7 +72,8 @@ def make_config(config: dict | None = None, control: dict | None = None, *,
 
     need(c["dimensions"] in (2, 3), "dimensions must be 2 or 3")
     need(c["flux_calculator"] in _lib.FLUX,
-         f"flux_calculator {c['flux_calculator']!r} is not on this path (ausmdv, hllc)")
+         f"flux_calculator {c['flux_calculator']!r} is not on this path "
+         "(ausmdv, hllc, hanel, adaptive_hanel_ausmdv)")
     need(c["interpolation_order"] in (1, 2), "interpolation_order must be 1 or 2")
     need(c["thermo_interpolator"] == "rhou", "thermo_interpolator must be rhou")
     need(c["gasdynamic_update_scheme"] in _lib.UPDATE,
@@ -108,6 +111,8 @@ def make_config(config: dict | None = None, control: dict | None = None, *,
     cfg.precision = _lib.PRECISION[precision]
     cfg.device = int(device)
     cfg.use_graphs = int(bool(use_graphs))
+    cfg.shear_tolerance = float(c["shear_tolerance"])
+    cfg.compression_tolerance = float(c["compression_tolerance"])
     return cfg
 
 

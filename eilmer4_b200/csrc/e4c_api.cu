@@ -125,6 +125,15 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
         const BlockHost& b = blocks[h];
         if (!b.fused) launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc(b.v, d_sim, stream); });
     }
+    // simcore.d:2354-2358: shock points after every block's ghost cells
+    if (cfg.flux_calculator == E4C_FLUX_ADAPTIVE_HANEL_AUSMDV) {
+        for (int h : hs) {
+            const BlockHost& b = blocks[h];
+            if (!b.fused)
+                launch_as(*this, E4C_KCLASS_BC, 1,
+                          [&] { launch_shock(b.v, d_sim, fopts.compression_tol, stream); });
+        }
+    }
     for (int h : hs) {
         const BlockHost& b = blocks[h];
         if (b.fused) continue;
@@ -225,7 +234,7 @@ int e4c_config_default(e4c_config* c) {
     if (!c) return fail(E4C_ERR_ARG, "e4c_config_default: null config");
     std::memset(c, 0, sizeof(*c));
     c->dimensions = 2;
-    c->flux_calculator = E4C_FLUX_AUSMDV;
+    c->flux_calculator = E4C_FLUX_ADAPTIVE_HANEL_AUSMDV;  // globalconfig.d:533
     c->interpolation_order = 2;
     c->apply_limiter = 1;
     c->extrema_clipping = 1;
@@ -244,6 +253,8 @@ int e4c_config_default(e4c_config* c) {
     c->precision = E4C_PREC_FP64;
     c->device = 0;
     c->use_graphs = 1;
+    c->shear_tolerance = 0.20;        // globalconfig.d:585
+    c->compression_tolerance = -0.30; // globalconfig.d:600
     return E4C_OK;
 }
 
@@ -252,8 +263,9 @@ int e4c_init(const e4c_config* cfg) {
     if (g_ctx.initialised) g_ctx.release();
     if (cfg->dimensions != 2 && cfg->dimensions != 3)
         return fail(E4C_ERR_UNSUPPORTED, "dimensions must be 2 or 3");
-    if (cfg->flux_calculator != E4C_FLUX_AUSMDV && cfg->flux_calculator != E4C_FLUX_HLLC)
-        return fail(E4C_ERR_UNSUPPORTED, "flux_calculator must be ausmdv or hllc");
+    if (cfg->flux_calculator < E4C_FLUX_AUSMDV || cfg->flux_calculator > E4C_FLUX_ADAPTIVE_HANEL_AUSMDV)
+        return fail(E4C_ERR_UNSUPPORTED,
+                    "flux_calculator must be ausmdv, hllc, hanel or adaptive_hanel_ausmdv");
     if (cfg->interpolation_order != 1 && cfg->interpolation_order != 2)
         return fail(E4C_ERR_UNSUPPORTED, "interpolation_order must be 1 or 2");
     if (cfg->gasdynamic_update_scheme != E4C_UPDATE_EULER &&
@@ -286,6 +298,8 @@ int e4c_init(const e4c_config* cfg) {
     c.fopts.clip = cfg->extrema_clipping != 0;
     c.fopts.local_frame = cfg->interpolate_in_local_frame != 0;
     c.fopts.gas = c.gas;
+    c.fopts.shear_tol = cfg->shear_tolerance;
+    c.fopts.compression_tol = cfg->compression_tolerance;
     E4C_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     E4C_CUDA(cudaStreamCreateWithFlags(&c.h2d_stream, cudaStreamNonBlocking));
     E4C_CUDA(cudaStreamCreateWithFlags(&c.d2h_stream, cudaStreamNonBlocking));
@@ -441,6 +455,7 @@ int e4c_connect_blocks(int ha, int fa, int hb, int fb, int orientation) {
             ExchangeSrc e{};
             e.W = o.W;
             e.cgeom = o.cgeom;
+            e.S = o.S;
             e.npad = o.npad;
             e.nidim = o.nidim;
             e.njdim = o.njdim;

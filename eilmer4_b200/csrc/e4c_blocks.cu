@@ -106,7 +106,9 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     out.nprim_vars = nw;
     v.axis_frames = (flags[1] == 0) ? 1 : 0;
     const bool uniform = (flags[0] == 0);
-    out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC && v.nsp == 1;
+    // the fused kernel carries the ausmdv and hllc fluxes (no shock flags)
+    out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC && v.nsp == 1 &&
+                cfg.flux_calculator <= E4C_FLUX_HLLC;
     if (cfg.precision == E4C_PREC_FP32_FLUX && !out.fused)
         return fail(E4C_ERR_UNSUPPORTED,
                     "the FP32-flux form needs a 3-D block with uniform geometry and the "
@@ -186,6 +188,10 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
         v.Fj = q; q += v.nv * np;
         v.Fk = q; q += v.nv * np;
         v.dt_chem = cfg.reacting ? q : nullptr;  // zero: no suggestion yet, as dt_chem = -1
+        // shock flags, false at the start (FlowState.S)
+        v.S = static_cast<int*>(dalloc(np * sizeof(int)));
+        if (!v.S) return fail(E4C_ERR_CUDA, "cudaMalloc of shock flags failed");
+        E4C_CUDA(cudaMemsetAsync(v.S, 0, np * sizeof(int), stream));
     }
     out.v = v;
     // staging area for uploads and downloads (primitive + conserved)

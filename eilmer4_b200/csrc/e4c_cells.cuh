@@ -191,8 +191,24 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
         to_local(Lf.vel, fr.n, fr.t1, fr.t2);
         to_local(Rt.vel, fr.n, fr.t1, fr.t2);
         double F[5 + NSPC];
-        if (FLUX == 1) hllc<double, NSP, NSPC>(Lf, Rt, F);
-        else ausmdv<double, NSP, NSPC>(Lf, Rt, F);
+        if (FLUX == 1) {
+            hllc<double, NSP, NSPC>(Lf, Rt, F);
+        } else if (FLUX == 2) {
+            hanel<double, NSP, NSPC>(Lf, Rt, F);
+        } else if (FLUX == 3) {
+            // adaptive_hanel_ausmdv (fluxcalc.d:824-838); the states carry the
+            // shock flags of the cells they were reconstructed from
+            const double sound_speed = 0.5 * (Lf.a + Rt.a);
+            const double shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
+            const double shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
+            const bool shear_is_small = fmax(shear_y, shear_z) <= o.shear_tol;
+            if ((b.S[cL0] == 1 || b.S[cR0] == 1) && shear_is_small)
+                hanel<double, NSP, NSPC>(Lf, Rt, F);
+            else
+                ausmdv<double, NSP, NSPC>(Lf, Rt, F);
+        } else {
+            ausmdv<double, NSP, NSPC>(Lf, Rt, F);
+        }
         V3<double> m{F[1], F[2], F[3]};
         to_global(m, fr.n, fr.t1, fr.t2);
         F[1] = m.x; F[2] = m.y; F[3] = m.z;

@@ -321,19 +321,26 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
             }
             const size_t sc = (size_t(sk) * o.njdim + sj) * o.nidim + si;
             for (int q = 0; q < nw; ++q) b.W[q * b.npad + dst[g]] = o.W[q * o.npad + sc];
+            b.S[dst[g]] = o.S[sc];
         }
     } else if (type == 1) {  // InFlowBC_Supersonic: both ghosts <- inflow FlowState
         for (int q = 0; q < nw; ++q) {
             b.W[q * b.npad + g1] = b.inflow[q];
             b.W[q * b.npad + g2] = b.inflow[q];
         }
+        b.S[g1] = 0;
+        b.S[g2] = 0;
     } else if (type == 2) {  // OutFlowBC_SimpleExtrapolate, x_order 0
         for (int q = 0; q < nw; ++q) {
             double v = b.W[q * b.npad + c0];
             b.W[q * b.npad + g1] = v;
             b.W[q * b.npad + g2] = v;
         }
+        b.S[g1] = b.S[c0];
+        b.S[g2] = b.S[c0];
     } else {  // WallBC_WithSlip: copy then reflect the normal velocity
+        b.S[g1] = b.S[c0];
+        b.S[g2] = b.S[c1];
         size_t f;
         const double* fg;
         switch (which) {
@@ -360,6 +367,46 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
             b.W[W_VY * b.npad + dst[g]] = v.y;
             b.W[W_VZ * b.npad + dst[g]] = v.z;
         }
+    }
+}
+
+// detect_shock_points (fluidblock.d:415-431) with PJ_ShockDetector
+// (shockdetectors.d:20-59): a face flags compression between its two cells,
+// (uR - uL) / min(aL, aR) < tol with u the velocity along the face normal; a
+// cell is a shock point if any of its faces is.  The flags of ghost cells are
+// those copied by the boundary conditions (the previous detection's).
+__device__ __forceinline__ int face_shock(const BlockView& b, const double* fg, size_t f,
+                                          size_t cl, size_t cr, double tol) {
+    const double nx = fg[0 * b.npad + f], ny = fg[1 * b.npad + f], nz = fg[2 * b.npad + f];
+    const double uL = b.W[W_VX * b.npad + cl] * nx + b.W[W_VY * b.npad + cl] * ny +
+                      b.W[W_VZ * b.npad + cl] * nz;
+    const double uR = b.W[W_VX * b.npad + cr] * nx + b.W[W_VY * b.npad + cr] * ny +
+                      b.W[W_VZ * b.npad + cr] * nz;
+    const double aL = b.W[W_A * b.npad + cl], aR = b.W[W_A * b.npad + cr];
+    const double a_min = (aL < aR) ? aL : aR;
+    return ((uR - uL) / a_min) < tol ? 1 : 0;
+}
+
+__global__ void k_shock(BlockView b, const SimDev* sim, double tol) {
+    if (sim->status != 0 || sim->finished) return;
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const size_t si = 1, sj = size_t(b.nidim), sk = size_t(b.nidim) * b.njdim;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = b.imin + int(t % b.ni);
+        const int j = b.jmin + int((t / b.ni) % b.nj);
+        const int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        int S = 0;
+        S |= face_shock(b, b.fgi, c, c - si, c, tol);
+        S |= face_shock(b, b.fgi, c + si, c, c + si, tol);
+        S |= face_shock(b, b.fgj, c, c - sj, c, tol);
+        S |= face_shock(b, b.fgj, c + sj, c, c + sj, tol);
+        if (b.dim == 3) {
+            S |= face_shock(b, b.fgk, c, c - sk, c, tol);
+            S |= face_shock(b, b.fgk, c + sk, c, c + sk, tol);
+        }
+        b.S[c] = S;
     }
 }
 
@@ -570,6 +617,11 @@ void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s) {
     else k_bc<1><<<grid, 128, 0, s>>>(b, sim);
 }
 
+void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_shock<<<grid_for(n, 256), 256, 0, s>>>(b, sim, tol);
+}
+
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
                  cudaStream_t s) {
     long long n = (long long)(b.ni + (dir == 0)) * (b.nj + (dir == 1)) * (b.nk + (dir == 2));
@@ -579,6 +631,8 @@ void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int d
         launch_flux_tp(b, sim, o, dir, g, T, s);
     } else {
         if (o.flux == 1) k_flux<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+        else if (o.flux == 2) k_flux<1, 2, 0><<<g, T, 0, s>>>(b, sim, o, dir);
+        else if (o.flux == 3) k_flux<1, 3, 0><<<g, T, 0, s>>>(b, sim, o, dir);
         else k_flux<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, dir);
     }
 }

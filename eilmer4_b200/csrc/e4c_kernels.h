@@ -9,12 +9,14 @@
 namespace e4c {
 
 struct FluxOpts {
-    int flux;          // 0 ausmdv, 1 hllc
+    int flux;          // 0 ausmdv, 1 hllc, 2 hanel, 3 adaptive_hanel_ausmdv
     int order2;        // interpolation_order > 1
     int limiter;       // apply_limiter
     int clip;          // extrema_clipping
     int local_frame;   // interpolate_in_local_frame
     GasConsts gas;
+    double shear_tol;        // adaptive flux: shear_tolerance
+    double compression_tol;  // shock detector: compression_tolerance
 };
 
 // general-geometry FP64 path (e4c_general.cu)
@@ -22,6 +24,8 @@ void launch_geometry(const BlockView& b, const double* vtx, cudaStream_t s);
 void launch_upload(const BlockView& b, const double* prim, cudaStream_t s);
 void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_t s);
 void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s);
+// shock points (detect_shock_points with the PJ detector)
+void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s);
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, cudaStream_t s);
 void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
                    int final_stage, cudaStream_t s);

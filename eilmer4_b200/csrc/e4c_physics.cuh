@@ -138,6 +138,48 @@ __device__ __forceinline__ bool scale_mass_fractions(R* massf) {
 }
 
 // AUSMDV flux in the face frame: src/eilmer/fluxcalc.d:376-529.
+// Hanel's flux (fluxcalc.d:532-629; Hanel, Schwane & Seider 1987, in the
+// form of Wada & Liou 1997), in the face frame.
+template <typename R, int NSP, int NSPC>
+__device__ __forceinline__ void hanel(const Prim<R, NSP>& Lf, const Prim<R, NSP>& Rt, R* F) {
+    R rL = Lf.rho, pL = Lf.p;
+    R pLrL = pL / rL;
+    R uL = Lf.vel.x, vL = Lf.vel.y, wL = Lf.vel.z;
+    R eL = Lf.u, aL = Lf.a;
+    R keL = R(0.5) * (uL * uL + vL * vL + wL * wL);
+    R HL = eL + pLrL + keL;
+    R rR = Rt.rho, pR = Rt.p;
+    R pRrR = pR / rR;
+    R uR = Rt.vel.x, vR = Rt.vel.y, wR = Rt.vel.z;
+    R eR = Rt.u, aR = Rt.a;
+    R keR = R(0.5) * (uR * uR + vR * vR + wR * wR);
+    R HR = eR + pRrR + keR;
+    R pLplus, uLplus;
+    if (fabs(uL) <= aL) {
+        uLplus = R(1.0) / (R(4.0) * aL) * (uL + aL) * (uL + aL);
+        pLplus = pL * uLplus * (R(1.0) / aL * (R(2.0) - uL / aL));
+    } else {
+        uLplus = R(0.5) * (uL + fabs(uL));
+        pLplus = pL * uLplus * (R(1.0) / uL);
+    }
+    R pRminus, uRminus;
+    if (fabs(uR) <= aR) {
+        uRminus = -R(1.0) / (R(4.0) * aR) * (uR - aR) * (uR - aR);
+        pRminus = pR * uRminus * (R(1.0) / aR * (-R(2.0) - uR / aR));
+    } else {
+        uRminus = R(0.5) * (uR - fabs(uR));
+        pRminus = pR * uRminus * (R(1.0) / uR);
+    }
+    R p_half = pLplus + pRminus;
+    F[0] = uLplus * rL + uRminus * rR;
+    F[1] = uLplus * rL * uL + uRminus * rR * uR + p_half;
+    F[2] = uLplus * rL * vL + uRminus * rR * vR;
+    F[3] = uLplus * rL * wL + uRminus * rR * wR;
+    F[4] = uLplus * rL * HL + uRminus * rR * HR;
+#pragma unroll
+    for (int i = 0; i < NSPC; ++i) F[5 + i] = uLplus * rL * Lf.massf[i] + uRminus * rR * Rt.massf[i];
+}
+
 // F: mass, xmom, ymom, zmom, energy, species (when NSPC > 0).
 template <typename R, int NSP, int NSPC>
 __device__ __forceinline__ void ausmdv(const Prim<R, NSP>& Lf, const Prim<R, NSP>& Rt, R* F) {

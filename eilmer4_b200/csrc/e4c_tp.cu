@@ -91,6 +91,8 @@ static int grid_for(long long n, int threads) {
 void launch_flux_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, int g,
                     int T, cudaStream_t s) {
     if (o.flux == 1) k_flux<5, 1, 1><<<g, T, 0, s>>>(b, sim, o, dir);
+    else if (o.flux == 2) k_flux<5, 2, 1><<<g, T, 0, s>>>(b, sim, o, dir);
+    else if (o.flux == 3) k_flux<5, 3, 1><<<g, T, 0, s>>>(b, sim, o, dir);
     else k_flux<5, 0, 1><<<g, T, 0, s>>>(b, sim, o, dir);
 }
 

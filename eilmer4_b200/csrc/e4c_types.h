@@ -26,6 +26,7 @@ enum PrimField { W_RHO = 0, W_VX, W_VY, W_VZ, W_P, W_T, W_U, W_A, W_NBASE };
 struct ExchangeSrc {
     const double* W;
     const double* cgeom;
+    const int* S;
     size_t npad;
     int nidim, njdim;
     int imax, jmax, kmax;
@@ -65,6 +66,7 @@ struct BlockView {
     int axis_frames;                // every face frame is made of signed unit axes
     double* dt_chem;                // per-cell chemistry step suggestion (reacting blocks)
     ExchangeSrc ex[6];              // partners of exchange boundaries (bc == 3)
+    int* S;                         // shock flag per padded cell (adaptive flux)
 };
 
 // Device-resident simulation state (one per library context).

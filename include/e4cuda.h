@@ -69,6 +69,9 @@ extern "C" {
 /* flux_calculator (src/eilmer/fvcore.d:184-228, plus the new "hllc"). */
 #define E4C_FLUX_AUSMDV 0
 #define E4C_FLUX_HLLC 1
+#define E4C_FLUX_HANEL 2                  /* fluxcalc.d:532-629 */
+#define E4C_FLUX_ADAPTIVE_HANEL_AUSMDV 3  /* fluxcalc.d:824-838, the reference's default;
+                                             turns on the shock detector */
 
 /* gasdynamic_update_scheme (fvcore.d:29-110). */
 #define E4C_UPDATE_EULER 0
@@ -103,6 +106,8 @@ typedef struct e4c_config {
     int precision;                  /* E4C_PREC_* */
     int device;                     /* CUDA device ordinal */
     int use_graphs;                 /* capture e4c_integrate steps in CUDA graphs */
+    double shear_tolerance;         /* "shear_tolerance" (globalconfig.d:585), adaptive flux */
+    double compression_tolerance;   /* "compression_tolerance" (globalconfig.d:600), shock detector */
 } e4c_config;
 
 typedef struct e4c_run_info {

@@ -466,6 +466,77 @@ void Sim::ausmdv(const FlowState& Lft, const FlowState& Rght, double* F) const {
     }
 }
 
+void Sim::hanel(const FlowState& Lft, const FlowState& Rght, double* F) const {
+    // fluxcalc.d:532-629 (Hanel, Schwane & Seider 1987, as in Wada & Liou 1997)
+    double rL = Lft.gas.rho, pL = Lft.gas.p;
+    double pLrL = pL / rL;
+    double uL = Lft.vel.x, vL = Lft.vel.y, wL = Lft.vel.z;
+    double eL = Lft.gas.u;
+    double aL = Lft.gas.a;
+    double keL = 0.5 * (uL * uL + vL * vL + wL * wL);
+    double HL = eL + pLrL + keL;
+    double rR = Rght.gas.rho, pR = Rght.gas.p;
+    double pRrR = pR / rR;
+    double uR = Rght.vel.x, vR = Rght.vel.y, wR = Rght.vel.z;
+    double eR = Rght.gas.u;
+    double aR = Rght.gas.a;
+    double keR = 0.5 * (uR * uR + vR * vR + wR * wR);
+    double HR = eR + pRrR + keR;
+    double pLplus, uLplus;
+    if (std::fabs(uL) <= aL) {
+        uLplus = 1.0 / (4.0 * aL) * (uL + aL) * (uL + aL);
+        pLplus = pL * uLplus * (1.0 / aL * (2.0 - uL / aL));
+    } else {
+        uLplus = 0.5 * (uL + std::fabs(uL));
+        pLplus = pL * uLplus * (1.0 / uL);
+    }
+    double pRminus, uRminus;
+    if (std::fabs(uR) <= aR) {
+        uRminus = -1.0 / (4.0 * aR) * (uR - aR) * (uR - aR);
+        pRminus = pR * uRminus * (1.0 / aR * (-2.0 - uR / aR));
+    } else {
+        uRminus = 0.5 * (uR - std::fabs(uR));
+        pRminus = pR * uRminus * (1.0 / uR);
+    }
+    double p_half = pLplus + pRminus;
+    F[0] = uLplus * rL + uRminus * rR;
+    F[1] = uLplus * rL * uL + uRminus * rR * uR + p_half;
+    F[2] = uLplus * rL * vL + uRminus * rR * vR;
+    F[3] = uLplus * rL * wL + uRminus * rR * wR;
+    F[4] = uLplus * rL * HL + uRminus * rR * HR;
+    for (int i = 0; i < nsp_cons; ++i)
+        F[5 + i] = uLplus * rL * Lft.gas.massf[i] + uRminus * rR * Rght.gas.massf[i];
+}
+
+void Sim::detect_shock_points(Block& b) {
+    // fluidblock.d:415-431 with PJ_ShockDetector (shockdetectors.d:20-59):
+    // every face flags compression between its two cells, every interior
+    // cell is a shock point if any of its faces is.  All boundaries in scope
+    // carry ghost cells, so both cells of a face always exist.
+    const double tol = cfg.compression_tolerance;
+    auto face_S = [&](const Face& f, const Cell& L, const Cell& R) {
+        double uL = L.fs.vel.x * f.n.x + L.fs.vel.y * f.n.y + L.fs.vel.z * f.n.z;
+        double uR = R.fs.vel.x * f.n.x + R.fs.vel.y * f.n.y + R.fs.vel.z * f.n.z;
+        double aL = L.fs.gas.a, aR = R.fs.gas.a;
+        double a_min = (aL < aR) ? aL : aR;
+        return ((uR - uL) / a_min) < tol ? 1 : 0;
+    };
+    for (int k = b.kmin; k <= b.kmax; ++k)
+        for (int j = b.jmin; j <= b.jmax; ++j)
+            for (int i = b.imin; i <= b.imax; ++i) {
+                int S = 0;
+                S |= face_S(b.ifi[b.idx(i, j, k)], b.cell(i - 1, j, k), b.cell(i, j, k));
+                S |= face_S(b.ifi[b.idx(i + 1, j, k)], b.cell(i, j, k), b.cell(i + 1, j, k));
+                S |= face_S(b.ifj[b.idx(i, j, k)], b.cell(i, j - 1, k), b.cell(i, j, k));
+                S |= face_S(b.ifj[b.idx(i, j + 1, k)], b.cell(i, j, k), b.cell(i, j + 1, k));
+                if (b.dim == 3) {
+                    S |= face_S(b.ifk[b.idx(i, j, k)], b.cell(i, j, k - 1), b.cell(i, j, k));
+                    S |= face_S(b.ifk[b.idx(i, j, k + 1)], b.cell(i, j, k), b.cell(i, j, k + 1));
+                }
+                b.cell(i, j, k).fs.S = S;
+            }
+}
+
 void Sim::hllc(const FlowState& Lft, const FlowState& Rght, double* F) const {
     // No reference counterpart: Toro's HLLC (Riemann Solvers and Numerical
     // Methods for Fluid Dynamics, 3rd ed., sec. 10.4-10.6) in the face frame,
@@ -519,8 +590,22 @@ void Sim::interface_flux(FlowState& Lft, FlowState& Rght, Face& f) const {
     // the grid-velocity terms add signed zeros only and are left out.
     to_local(Lft.vel, f.n, f.t1, f.t2);
     to_local(Rght.vel, f.n, f.t1, f.t2);
-    if (cfg.flux_calculator == E4O_FLUX_HLLC) hllc(Lft, Rght, f.F);
-    else ausmdv(Lft, Rght, f.F);
+    if (cfg.flux_calculator == E4O_FLUX_HLLC) {
+        hllc(Lft, Rght, f.F);
+    } else if (cfg.flux_calculator == E4O_FLUX_HANEL) {
+        hanel(Lft, Rght, f.F);
+    } else if (cfg.flux_calculator == E4O_FLUX_ADAPTIVE_HANEL_AUSMDV) {
+        // adaptive_hanel_ausmdv, fluxcalc.d:824-838: Hanel next to shocks
+        // unless the shear across the face is large, AUSMDV elsewhere
+        double sound_speed = 0.5 * (Lft.gas.a + Rght.gas.a);
+        double shear_y = std::fabs(Lft.vel.y - Rght.vel.y) / sound_speed;
+        double shear_z = std::fabs(Lft.vel.z - Rght.vel.z) / sound_speed;
+        bool shear_is_small = std::fmax(shear_y, shear_z) <= cfg.shear_tolerance;
+        if ((Lft.S == 1 || Rght.S == 1) && shear_is_small) hanel(Lft, Rght, f.F);
+        else ausmdv(Lft, Rght, f.F);
+    } else {
+        ausmdv(Lft, Rght, f.F);
+    }
     Vec3 m{f.F[1], f.F[2], f.F[3]};
     to_global(m, f.n, f.t1, f.t2);
     f.F[1] = m.x; f.F[2] = m.y; f.F[3] = m.z;
@@ -923,6 +1008,10 @@ int Sim::gasdynamic_increment() {
         // every block's ghost cells first (exchange copies see no flux-loop
         // state), then every block's fluxes
         for (Block* b : blocks) apply_bcs(*b);
+        // simcore.d:2354-2358, turned on by the adaptive flux calculator
+        // (globalconfig.d:1942-1950)
+        if (cfg.flux_calculator == E4O_FLUX_ADAPTIVE_HANEL_AUSMDV)
+            for (Block* b : blocks) detect_shock_points(*b);
         for (Block* b : blocks) convective_flux(*b);
         for (Block* b : blocks) {
             int rc = stage_cells(*b, stage, dt_global);
@@ -987,6 +1076,8 @@ void e4o_default_config(e4o_config* c) {
     c->reacting = 0;
     c->T_frozen = 300.0;
     c->n_threads = 1;
+    c->shear_tolerance = 0.20;
+    c->compression_tolerance = -0.30;
 }
 
 void* e4o_sim_new(const e4o_config* cfg) {

@@ -26,7 +26,7 @@ extern "C" {
 
 enum { E4O_BC_SLIP_WALL = 0, E4O_BC_INFLOW_SUPERSONIC = 1, E4O_BC_OUTFLOW_EXTRAPOLATE = 2,
        E4O_BC_EXCHANGE = 3 };
-enum { E4O_FLUX_AUSMDV = 0, E4O_FLUX_HLLC = 1 };
+enum { E4O_FLUX_AUSMDV = 0, E4O_FLUX_HLLC = 1, E4O_FLUX_HANEL = 2, E4O_FLUX_ADAPTIVE_HANEL_AUSMDV = 3 };
 enum { E4O_UPDATE_EULER = 0, E4O_UPDATE_PC = 1 };
 enum { E4O_GAS_IDEAL = 0, E4O_GAS_THERM_PERF_5SP_AIR = 1 };
 
@@ -49,6 +49,8 @@ typedef struct e4o_config {
     int reacting;                   /* finite-rate chemistry after each step */
     double T_frozen;
     int n_threads;                  /* OpenMP threads; <=0 means all */
+    double shear_tolerance;         /* adaptive flux: globalconfig.d:585 */
+    double compression_tolerance;   /* shock detector: globalconfig.d:600 */
 } e4o_config;
 
 /* Thermally perfect mixture and reaction mechanism (plain arrays).

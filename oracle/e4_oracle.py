@@ -23,6 +23,8 @@ BC_OUTFLOW_EXTRAPOLATE = 2
 BC_EXCHANGE = 3
 FLUX_AUSMDV = 0
 FLUX_HLLC = 1
+FLUX_HANEL = 2
+FLUX_ADAPTIVE_HANEL_AUSMDV = 3
 UPDATE_EULER = 0
 UPDATE_PC = 1
 GAS_IDEAL = 0
@@ -49,6 +51,8 @@ class Config(ctypes.Structure):
         ("reacting", ctypes.c_int),
         ("T_frozen", ctypes.c_double),
         ("n_threads", ctypes.c_int),
+        ("shear_tolerance", ctypes.c_double),
+        ("compression_tolerance", ctypes.c_double),
     ]
 
 

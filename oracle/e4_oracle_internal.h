@@ -39,6 +39,7 @@ struct GasState {  // src/gas/gas_state.d:18 (single temperature)
 struct FlowState {  // src/eilmer/flowstate.d:30
     GasState gas;
     Vec3 vel;
+    int S = 0;         // shock flag (copied with the state, flowstate.d:177-193)
 };
 
 struct Cell {  // the parts of src/eilmer/fvcell.d used on the hot path
@@ -142,6 +143,8 @@ struct Sim {
     // gas dynamics
     void ausmdv(const FlowState& L, const FlowState& R, double* F) const;
     void hllc(const FlowState& L, const FlowState& R, double* F) const;
+    void hanel(const FlowState& L, const FlowState& R, double* F) const;
+    void detect_shock_points(Block& b);
     void interface_flux(FlowState& L, FlowState& R, Face& f) const;
     bool scale_mass_fractions(double* massf) const;
     void interp_l2r2(Face& f, Cell& cL1, Cell& cL0, Cell& cR0, Cell& cR1, double lenL1,

@@ -47,14 +47,19 @@ def test_config_default_matches_reference_defaults(e4lib):
     assert c.cfl_count == 10 and c.interpolation_order == 2 and c.apply_limiter == 1
     assert c.extrema_clipping == 1 and c.interpolate_in_local_frame == 1
     assert c.gasdynamic_update_scheme == 1 and c.max_invalid_cells == 0
+    assert c.flux_calculator == 3 and c.shear_tolerance == 0.2 and c.compression_tolerance == -0.3
 
 
 def test_config_keys_select_path(e4lib):
     from eilmer4_b200.config import UnsupportedConfig, make_config
     cfg = make_config({"dimensions": 3, "flux_calculator": "hllc"}, {"cfl_value": 0.4})
     assert cfg.flux_calculator == 1 and cfg.cfl_value == 0.4 and cfg.dimensions == 3
+    # the reference's default flux calculator is on the path
+    cfg = make_config({})
+    assert cfg.flux_calculator == 3 and cfg.shear_tolerance == 0.2
+    assert cfg.compression_tolerance == -0.3
     with pytest.raises(UnsupportedConfig):
-        make_config({"flux_calculator": "adaptive_hanel_ausmdv"})
+        make_config({"flux_calculator": "efm"})
     with pytest.raises(UnsupportedConfig):
         make_config({"flux_calculator": "ausmdv", "viscous": True})
     with pytest.raises(UnsupportedConfig):

@@ -11,7 +11,7 @@ from eilmer4_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-FLUX = {"ausmdv": 0, "hllc": 1}
+FLUX = {"ausmdv": 0, "hllc": 1, "hanel": 2, "adaptive_hanel_ausmdv": 3}
 
 
 def run_oracle(oracle, wl, nsteps, max_time=1.0e300, **cfgkw):
@@ -84,6 +84,25 @@ def test_sod_tube_3d_reference_deck(oracle, e4lib):
     # examples/eilmer/3D/sod-shock-tube/sg: run to t = 0.6 ms like the deck
     info = compare(oracle, W.sod_3d_tube(), 600, max_time=0.6e-3)
     assert abs(info.steps_taken - 75) < 3
+
+
+@pytest.mark.parametrize("flux", ["hanel", "adaptive_hanel_ausmdv"])
+def test_sod_2d_hanel_and_adaptive_bitexact(oracle, e4lib, flux):
+    """Hanel's flux and the reference's default adaptive Hanel/AUSMDV
+    switch, with the shock detector run after every stage's ghost cells."""
+    wl = W.sod_2d(64, 16)
+    wl.flux_calculator = flux
+    compare(oracle, wl, 120)
+
+
+def test_adaptive_3d_inflow_and_reference_deck(oracle, e4lib):
+    wl = W.Workload("inflow3d", 3, flux_calculator="adaptive_hanel_ausmdv")
+    wl.blocks.append(W.inflow_3d_block(16, 10, 8, seed=3))
+    compare(oracle, wl, 30)
+    wl = W.sod_3d_tube()
+    wl.flux_calculator = "adaptive_hanel_ausmdv"
+    info = compare(oracle, wl, 600, max_time=0.6e-3)
+    assert abs(info.steps_taken - 75) < 4
 
 
 def test_inflow_3d_ausmdv_bitexact(oracle, e4lib):

@@ -68,6 +68,22 @@ def test_hllc_sod_tube_close_to_ausmdv(oracle):
     assert rel(prim[4, q], 30.2e3) < 1.0e-2
 
 
+@pytest.mark.parametrize("flux", ["hanel", "adaptive_hanel_ausmdv"])
+def test_hanel_and_adaptive_sod_tube_regression(oracle, flux):
+    # The reference's default flux calculator (adaptive_hanel_ausmdv,
+    # globalconfig.d:533) and Hanel's: the Sod deck's regression values hold
+    # within the test's 1 % band.
+    f = oracle.FLUX_HANEL if flux == "hanel" else oracle.FLUX_ADAPTIVE_HANEL_AUSMDV
+    sim, prim, xc = _run_sod3d(oracle, f)
+    assert abs(sim.step - 75) < 4
+    for x, ref in ((0.78, {"rho": 0.2647, "p": 30.2e3, "T": 398.0, "velx": 293.0}),
+                   (0.6, {"rho": 0.4271, "T": 247.0})):
+        q = int(np.argmin(np.abs(xc - x)))
+        got = {"rho": prim[0, q], "velx": prim[1, q], "p": prim[4, q], "T": prim[5, q]}
+        for k, v in ref.items():
+            assert rel(got[k], v) < 1.0e-2, (flux, x, k, got[k], v)
+
+
 def test_uniform_geometry_is_exact(oracle):
     # Dyadic Cartesian grids give bit-identical geometry in every cell and face.
     wl = W.inflow_3d(n=8, nsteps=1)
