@@ -53,10 +53,13 @@ BYTES_PER_CELL_UPDATE = {"fp64": 360.0, "fp32_flux": 280.0}
 # chemistry of one reacting cell: read rho, u, T, massf x5, dt_chem; write
 # massf x5, T, p, u, a, dt_chem and rho*massf x5 (doubles)
 BYTES_PER_REACTING_CELL = 8.0 * (9 + 15)
-# DRAM bytes per launch of the fused stage kernel from ncu captures of the
-# 256^3 workload (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
-# (precision, kernel class); None where no capture exists
-TRAFFIC = {}
+# DRAM bytes per launch of the fused stage kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum, mean of the stage-1 and stage-2 launches) from the
+# ncu capture of the 128^3 block, scaled to 256^3 by the cell count (the
+# kernel's traffic grows with the cells it processes), keyed by (precision,
+# kernel class).  Algorithmic bytes per launch at 256^3: 3020 MB (FP64),
+# 2349 MB (FP32-flux).
+TRAFFIC = {("fp64", "stage"): 2762540032, ("fp32_flux", "stage"): 2058403840}
 
 
 def peaks():
