@@ -115,6 +115,19 @@ __device__ __forceinline__ double pm_pow(double x, double n) {
     return pm_exp(n * pm_log(x));
 }
 
+// pm_pow(x, n) given lx = pm_log(x): the same value, bit for bit
+__device__ __forceinline__ double pm_pow_l(double x, double lx, double n) {
+    if (n == 0.0) return 1.0;
+    if (n == 1.0) return x;
+    if (n == -1.0) return 1.0 / x;
+    if (n == 2.0) return x * x;
+    if (n == 0.5) return sqrt(x);
+    if (n == -0.5) return 1.0 / sqrt(x);
+    if (n == 1.5) return x * sqrt(x);
+    if (n == -1.5) return 1.0 / (x * sqrt(x));
+    return pm_exp(n * lx);
+}
+
 // ---------------------------------------------------------------------------
 // CEA thermo curves
 // ---------------------------------------------------------------------------
@@ -159,30 +172,32 @@ static __device__ E4C_CEA_FN double cea_Cp(const e4c_thermochem& tc, int isp, do
     return R * Cp_on_R;
 }
 
+// lT is pm_log(T), shared by the species of a mixture evaluated at one T
 static __device__ E4C_CEA_FN double cea_h_in_range(const e4c_thermochem& tc, int isp, double R,
-                                                 double T) {
+                                                 double T, double lT) {
     double a[9];
     cea_coefficients(tc, isp, T, a);
-    double h_on_RT = -a[0] / (T * T) + a[1] / T * pm_log(T) + a[2] + a[3] * T / 2.0;
+    double h_on_RT = -a[0] / (T * T) + a[1] / T * lT + a[2] + a[3] * T / 2.0;
     h_on_RT += a[4] * T * T / 3.0 + a[5] * T * T * T / 4.0 + a[6] * T * T * T * T / 5.0 + a[7] / T;
     return R * T * h_on_RT;
 }
 
-static __device__ E4C_CEA_FN double cea_h(const e4c_thermochem& tc, int isp, double R, double T) {
+static __device__ E4C_CEA_FN double cea_h(const e4c_thermochem& tc, int isp, double R, double T,
+                                        double lT) {
     const int nseg = tc.nseg[isp];
     if (T < tc.T_break[isp][0]) {
         double T_low = tc.T_break[isp][0];
-        double h_low = cea_h_in_range(tc, isp, R, T_low);
+        double h_low = cea_h_in_range(tc, isp, R, T_low, pm_log(T_low));
         double Cp_low = cea_Cp(tc, isp, R, T_low);
         return h_low - Cp_low * (T_low - T);
     }
     if (T > tc.T_break[isp][nseg]) {
         double T_high = tc.T_break[isp][nseg];
-        double h_high = cea_h_in_range(tc, isp, R, T_high);
+        double h_high = cea_h_in_range(tc, isp, R, T_high, pm_log(T_high));
         double Cp_high = cea_Cp(tc, isp, R, T_high);
         return h_high + Cp_high * (T - T_high);
     }
-    return cea_h_in_range(tc, isp, R, T);
+    return cea_h_in_range(tc, isp, R, T, lT);
 }
 
 // ---------------------------------------------------------------------------
@@ -211,8 +226,9 @@ struct TPGas {
     __device__ double Rmix(const double* massf) const { return mass_average(massf, R); }
     __device__ double energy(const double* massf, double T) const {
         double e[NSP];
+        const double lT = pm_log(T);
 #pragma unroll
-        for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], T) - R[i] * T;
+        for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], T, lT) - R[i] * T;
         return mass_average(massf, e);
     }
     __device__ double dudT(const double* massf, double T) const {
@@ -315,9 +331,10 @@ struct MechD {
     __device__ void rate_constants(double T) {
         if (T < tc.T_lower) T = tc.T_lower;
         if (T > tc.T_upper) T = tc.T_upper;
+        const double lT = pm_log(T);
         for (int r = 0; r < NR; ++r) {
-            kf[r] = tc.A_f[r] * pm_pow(T, tc.n_f[r]) * pm_exp(-tc.C_f[r] / T);
-            kb[r] = tc.A_b[r] * pm_pow(T, tc.n_b[r]) * pm_exp(-tc.C_b[r] / T);
+            kf[r] = tc.A_f[r] * pm_pow_l(T, lT, tc.n_f[r]) * pm_exp(-tc.C_f[r] / T);
+            kb[r] = tc.A_b[r] * pm_pow_l(T, lT, tc.n_b[r]) * pm_exp(-tc.C_b[r] / T);
         }
     }
     __device__ void rates(int r, const double* c, double& wf, double& wb) const {
