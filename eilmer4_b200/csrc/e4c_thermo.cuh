@@ -39,6 +39,15 @@ namespace e4c {
 #else
 #define E4C_CEA_FN __forceinline__
 #endif
+// The segment/blend selection is inlined into each called evaluation, which
+// keeps the nine coefficients in registers (1.27x on the reacting channel
+// against calling it too).
+#ifndef E4C_COEF_FN
+#define E4C_COEF_FN __forceinline__
+#endif
+#ifndef E4C_SOLVE_FN
+#define E4C_SOLVE_FN
+#endif
 #ifndef E4C_PM_NOINLINE
 #define E4C_PM_NOINLINE 0
 #endif
@@ -131,7 +140,7 @@ __device__ __forceinline__ double pm_pow_l(double x, double lx, double n) {
 // ---------------------------------------------------------------------------
 // CEA thermo curves
 // ---------------------------------------------------------------------------
-static __device__ E4C_CEA_FN void cea_coefficients(const e4c_thermochem& tc, int isp, double T,
+static __device__ E4C_COEF_FN void cea_coefficients(const e4c_thermochem& tc, int isp, double T,
                                                  double a[9]) {
     const int nseg = tc.nseg[isp];
     const double* tb = tc.T_break[isp];
@@ -238,7 +247,7 @@ struct TPGas {
         return -1.0 * mass_average(massf, v);
     }
     // nm/newton.d:40-99, f(T) = e_tgt - u(T); Q.T and Q.u follow every evaluation
-    __device__ bool solve_T(TPState<NSP>& Q, double e_tgt, double x0, double xMin, double xMax,
+    __device__ E4C_SOLVE_FN bool solve_T(TPState<NSP>& Q, double e_tgt, double x0, double xMin, double xMax,
                             double tol, double& root) const {
         const int MAXIT = 30;
         double xL = xMin, xH = xMax;
