@@ -101,11 +101,8 @@ static __device__ void replay_roundtrips(const BlockView& b, int dir, int fpos, 
 // update_thermo_from_rhou of a reconstructed state: ideal gas, or the
 // thermally perfect mixture started from the cell-centre temperature (the
 // state was copied from the cell, onedinterp.d / sfluidblock.d:2199-2208)
-#ifndef E4C_RHOU_FN
-#define E4C_RHOU_FN __forceinline__
-#endif
 template <int NSP, int GAS>
-__device__ E4C_RHOU_FN bool rhou_update(const FluxOpts& o, Prim<double, NSP>& s) {
+__device__ __forceinline__ bool rhou_update(const FluxOpts& o, Prim<double, NSP>& s) {
     if (GAS == 0) {
         double T;
         return ideal_rhou<double>(o.gas, s.rho, s.u, s.p, T);

@@ -45,9 +45,6 @@ namespace e4c {
 #ifndef E4C_COEF_FN
 #define E4C_COEF_FN __forceinline__
 #endif
-#ifndef E4C_SOLVE_FN
-#define E4C_SOLVE_FN
-#endif
 #ifndef E4C_PM_NOINLINE
 #define E4C_PM_NOINLINE 0
 #endif
@@ -247,7 +244,7 @@ struct TPGas {
         return -1.0 * mass_average(massf, v);
     }
     // nm/newton.d:40-99, f(T) = e_tgt - u(T); Q.T and Q.u follow every evaluation
-    __device__ E4C_SOLVE_FN bool solve_T(TPState<NSP>& Q, double e_tgt, double x0, double xMin, double xMax,
+    __device__ bool solve_T(TPState<NSP>& Q, double e_tgt, double x0, double xMin, double xMax,
                             double tol, double& root) const {
         const int MAXIT = 30;
         double xL = xMin, xH = xMax;
