@@ -27,7 +27,9 @@ same line also carries, each timed the same way on its own simulation:
       mass-fraction difference from the plain update.
 --impl reference times the CPU FP64 restatement of the reference algorithm
 (the D solver itself cannot be built: no D compiler) on the host cores, on a
-bounded sample of the same workload.
+bounded sample of the same workload; its line also carries "gpu_chem", the
+reference's own GPU chemistry (GPUChem and its alpha-QSS kernel, built for
+sm_100a) on the high-enthalpy channel's cell states.
 """
 from __future__ import annotations
 
@@ -168,6 +170,87 @@ def cpu_oracle_reacting(wl, steps):
                                        f"({secs:.1f} s), CPU FP64 restatement, OpenMP"}
 
 
+def reference_gpu_chem(ni, nj, steps):
+    """The reference's own GPU chemistry path (GPUChem, cuda_gpu_chem.d:133-168,
+    with its alpha-QSS kernel compiled for sm_100a from the reference's
+    template) on the high-enthalpy channel after `steps` flow steps of the CPU
+    oracle: the host preparation (concentrations, rate constants, step
+    estimate; one cell after another as the D host does), the copies, the
+    kernel (CUDA events) and the host's per-cell finish.  The sub-step loop of
+    every cell is first bounded on the CPU by the kernel's NumPy restatement
+    on the same inputs."""
+    import torch
+
+    from eilmer4_b200 import workloads as W
+    from oracle import e4_oracle as O
+    from oracle import ref_qss as RQ
+    if not os.path.exists(RQ.LIB):
+        return {"unavailable": "the reference kernel was not built (oracle/_ref)"}
+    O.build()
+    wl = W.reacting_channel_hot(ni=ni, nj=nj)
+    tc = wl.thermochem
+    cfg = O.default_config(dimensions=2, flux_calculator=O.FLUX_AUSMDV,
+                           gas_model=O.GAS_THERM_PERF_5SP_AIR, reacting=1, n_threads=0)
+    sim = O.OracleSim(cfg, tc)
+    b = wl.blocks[0]
+    sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    sim.set_flow(0, b.prim)
+    if sim.run(steps) != 0:
+        return {"unavailable": "the oracle run that makes the cell states failed"}
+    prim, _ = sim.get_flow(0)
+    dt = sim.dt_global
+    n = b.ncell
+    rho, T, u, p, y = prim[0], prim[5], prim[6], prim[4], prim[8:13]
+    t0 = time.perf_counter()
+    conc, kf, kb, h = O.gpuchem_prepare(tc, rho, T, y, np.full(n, -1.0))
+    prep_s = time.perf_counter() - t0
+    _, _, passes = RQ.new_qss_numpy(tc, kf, kb, conc, h, dt, max_outer=20000)
+    L = RQ.load()
+    dev = torch.device("cuda:0")
+    host = {"kf": kf, "kb": kb, "Y": conc, "h": h}
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(v).ravel()).pin_memory()
+              for k, v in host.items()}
+    names = ["kf", "kb", "MM", "Y", "Yp", "Yc", "h", "alpha", "q", "p", "qp", "pp", "q_bar",
+             "p_bar", "alpha_bar", "Ypo"]
+    rows = {"kf": tc.nreac, "kb": tc.nreac, "MM": tc.nreac, "h": 1}
+    bufs = {k: torch.zeros(rows.get(k, tc.nsp) * n, dtype=torch.float64, device=dev)
+            for k in names}
+    dbg = torch.zeros(1, dtype=torch.float64, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    Yout = torch.empty(tc.nsp * n, dtype=torch.float64).pin_memory()
+    hout = torch.empty(n, dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    ev[0].record()
+    for k in host:
+        bufs[k].copy_(pinned[k], non_blocking=True)
+    ev[1].record()
+    L.kernel_launcher(*[bufs[k].data_ptr() for k in names], tc.nsp, tc.nreac, n, dt,
+                      dbg.data_ptr(), 1, 1, n, 1)
+    ev[2].record()
+    Yout.copy_(bufs["Y"], non_blocking=True)
+    hout.copy_(bufs["h"], non_blocking=True)
+    ev[3].record()
+    torch.cuda.synchronize()
+    h2d_ms, kern_ms, d2h_ms = (ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]),
+                               ev[2].elapsed_time(ev[3]))
+    t0 = time.perf_counter()
+    rc, _ = O.gpuchem_finish(tc, Yout.numpy().reshape(tc.nsp, n), hout.numpy(), rho, T, u, p)
+    fin_s = time.perf_counter() - t0
+    total_s = prep_s + fin_s + (h2d_ms + kern_ms + d2h_ms) * 1e-3
+    return {
+        "workload": f"reacting_channel_hot {ni}x{nj} after {steps} flow steps of the CPU oracle, "
+                    f"one chemistry step of the flow dt ({dt:.3e} s), every cell",
+        "kernel": "new_qss (alpha_qss_kernel_cuda_tmplt.cu), one cell per one-thread block, "
+                  "nvcc defaults, sm_100a",
+        "cells": n, "finish_rc": rc,
+        "substeps_per_cell_mean": float(passes.mean()), "substeps_per_cell_max": int(passes.max()),
+        "kernel_ms": kern_ms, "kernel_reacting_cells_per_s": n / (kern_ms * 1e-3),
+        "h2d_ms": h2d_ms, "d2h_ms": d2h_ms, "host_prepare_ms": prep_s * 1e3,
+        "host_finish_ms": fin_s * 1e3, "reacting_cells_per_s": n / total_s,
+        "host_threads": 1,
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -191,6 +274,9 @@ def run_reference(args, rank, world):
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu_chem:
+        line["gpu_chem"] = reference_gpu_chem(args.ref_chem_ni, args.ref_chem_nj,
+                                              args.ref_chem_steps)
     print(json.dumps(line), flush=True)
 
 
@@ -583,6 +669,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-sample", type=int, default=96)
     ap.add_argument("--cpu-reacting-steps", type=int, default=5)
+    ap.add_argument("--no-ref-gpu-chem", action="store_true",
+                    help="--impl reference: skip the reference's GPU chemistry kernel")
+    ap.add_argument("--ref-chem-ni", type=int, default=256)
+    ap.add_argument("--ref-chem-nj", type=int, default=128)
+    ap.add_argument("--ref-chem-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--headline-only", action="store_true",

@@ -141,6 +141,16 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
 int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, double* massf,
                     double* dt_chem);
 
+/* The host side of the reference's GPU chemistry (GPUChem, cuda_gpu_chem.d)
+ * around its alpha-QSS kernel, for n cells in SoA arrays (species or reaction
+ * outer): prepare gives the kernel's inputs, finish applies its outputs. */
+int e4o_gpuchem_prepare(const e4o_thermochem* tc, int n, const double* rho, const double* T,
+                        const double* massf, const double* dt_chem, double* conc, double* kf,
+                        double* kb, double* h);
+int e4o_gpuchem_finish(const e4o_thermochem* tc, int n, const double* conc, const double* h,
+                       const double* rho, double* T, double* u, double* p, double* massf,
+                       double* dt_chem);
+
 /* Low-level pieces exposed for golden-vector tests. */
 int e4o_ideal_gas_pT(double mol_mass, double gamma, double p, double T,
                      double* rho, double* u, double* a);

@@ -122,6 +122,8 @@ def lib():
         L.e4o_tp_update.argtypes = [P(ThermoChem), ip, P(dp), P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
+        L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
+        L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
         _lib = L
     return _lib
 
@@ -263,3 +265,42 @@ def chem_update(thermochem, dt, rho, T, massf, dt_chem=-1.0):
     dc = ctypes.c_double(dt_chem)
     rc = lib().e4o_chem_update(ctypes.byref(tc), dt, rho, T, _dptr(mf), ctypes.byref(dc))
     return rc, mf
+
+
+def gpuchem_prepare(thermochem, rho, T, massf, dt_chem):
+    """Inputs of the reference's GPU chemistry kernel for n cells
+    (GPUChem.prepareDataForGPU): conc (nsp, n), kf, kb (nreac, n), h (n,)."""
+    tc = thermochem.fill(ThermoChem())
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    n = rho.size
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    mf = np.ascontiguousarray(massf, dtype=np.float64).reshape(thermochem.nsp, n)
+    dc = np.ascontiguousarray(dt_chem, dtype=np.float64)
+    conc = np.zeros((thermochem.nsp, n))
+    kf = np.zeros((thermochem.nreac, n))
+    kb = np.zeros((thermochem.nreac, n))
+    h = np.zeros(n)
+    rc = lib().e4o_gpuchem_prepare(ctypes.byref(tc), n, _dptr(rho), _dptr(T), _dptr(mf),
+                                   _dptr(dc), _dptr(conc), _dptr(kf), _dptr(kb), _dptr(h))
+    if rc != 0:
+        raise ValueError(f"gpuchem_prepare failed: {rc}")
+    return conc, kf, kb, h
+
+
+def gpuchem_finish(thermochem, conc, h, rho, T, u, p):
+    """The cell loop after the reference's GPU chemistry kernel: massf (nsp, n),
+    T, u, p and dt_chem (n,) as GPUChem.thermochemical_increment leaves them,
+    and the return code (0, or the thermo error if a temperature solve failed)."""
+    tc = thermochem.fill(ThermoChem())
+    conc = np.ascontiguousarray(conc, dtype=np.float64)
+    n = conc.shape[1]
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    T = np.array(T, dtype=np.float64)
+    u = np.array(u, dtype=np.float64)
+    p = np.array(p, dtype=np.float64)
+    mf = np.zeros((thermochem.nsp, n))
+    dc = np.zeros(n)
+    rc = lib().e4o_gpuchem_finish(ctypes.byref(tc), n, _dptr(conc), _dptr(h), _dptr(rho),
+                                  _dptr(T), _dptr(u), _dptr(p), _dptr(mf), _dptr(dc))
+    return rc, {"massf": mf, "T": T, "u": u, "p": p, "dt_chem": dc}

@@ -712,4 +712,56 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
     return 0;
 }
 
+// GPUChem.prepareDataForGPU (src/eilmer/cuda_gpu_chem.d:183-205): per cell,
+// one after another as the D host does, the concentrations (massf2conc,
+// gas_model.d:196-212), the rate constants at the cell's temperature and the
+// starting step h (the cell's dt_chem, else estimateStepSize).  Arrays are
+// by cell, species or reaction outer: conc[s*n+i], kf[r*n+i].
+int e4o_gpuchem_prepare(const e4o_thermochem* tc, int n, const double* rho, const double* T,
+                        const double* massf, const double* dt_chem, double* conc, double* kf,
+                        double* kb, double* h) {
+    const int nsp = tc->nsp;
+    Mech m(*tc);
+    for (int i = 0; i < n; ++i) {
+        if (std::isnan(rho[i]) || rho[i] <= 0.0) return E4O_ERR_CHEM;
+        double c[E4O_MAXSP];
+        for (int s = 0; s < nsp; ++s) {
+            c[s] = massf[size_t(s) * n + i] * rho[i] / tc->M[s];
+            if (c[s] < 1.0e-30) c[s] = 0.0;
+            conc[size_t(s) * n + i] = c[s];
+        }
+        m.eval_rate_constants(T[i]);
+        for (int r = 0; r < tc->nreac; ++r) {
+            kf[size_t(r) * n + i] = m.kf[r];
+            kb[size_t(r) * n + i] = m.kb[r];
+        }
+        h[i] = dt_chem[i] <= 0.0 ? m.estimate_step_size(c) : dt_chem[i];
+    }
+    return 0;
+}
+
+// The cell loop after the kernel (cuda_gpu_chem.d:156-167): conc2massf
+// (gas_model.d:214-230), dt_chem = h, update_thermo_from_rhou (T holds the
+// starting guess; u is left at the energy of the last iterate, p follows).
+int e4o_gpuchem_finish(const e4o_thermochem* tc, int n, const double* conc, const double* h,
+                       const double* rho, double* T, double* u, double* p, double* massf,
+                       double* dt_chem) {
+    const int nsp = tc->nsp;
+    TP tp(*tc);
+    int err = 0;
+    for (int i = 0; i < n; ++i) {
+        GasState Q;
+        Q.rho = rho[i]; Q.T = T[i]; Q.u = u[i]; Q.p = p[i];
+        for (int s = 0; s < nsp; ++s) {
+            Q.massf[s] = conc[size_t(s) * n + i] * tc->M[s] / rho[i];
+            if (Q.massf[s] < 1.0e-30) Q.massf[s] = 0.0;
+        }
+        dt_chem[i] = h[i];
+        if (!tp.update_thermo_from_rhou(Q)) err = E4O_ERR_THERMO;
+        T[i] = Q.T; u[i] = Q.u; p[i] = Q.p;
+        for (int s = 0; s < nsp; ++s) massf[size_t(s) * n + i] = Q.massf[s];
+    }
+    return err;
+}
+
 }  // extern "C"
