@@ -140,6 +140,12 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
         for (int d = 0; d < b.v.dim; ++d)
             launch_as(*this, E4C_KCLASS_FLUX, 1, [&] { launch_flux(b.v, d_sim, fopts, d, stream); });
     }
+    // applyPostConvFluxAction of every block (simcore.d:2373-2377)
+    for (int h : hs) {
+        const BlockHost& b = blocks[h];
+        if (b.fused || !b.simple_flux) continue;
+        launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc_flux(b.v, d_sim, fopts, stream); });
+    }
     for (int h : hs) {
         const BlockHost& b = blocks[h];
         if (b.fused) continue;
@@ -397,7 +403,8 @@ int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* b
     if (ni < 2 || nj < 2 || (dim == 3 && nk < 2))
         return fail(E4C_ERR_ARG, "a block needs at least 2 cells in each active direction");
     for (int q = 0; q < 6; ++q)
-        if (bc_type[q] < 0 || bc_type[q] > 2) return fail(E4C_ERR_UNSUPPORTED, "unknown boundary type");
+        if (bc_type[q] < 0 || bc_type[q] > E4C_BC_OUTFLOW_SIMPLE_FLUX || bc_type[q] == E4C_BC_EXCHANGE)
+            return fail(E4C_ERR_UNSUPPORTED, "unknown boundary type");
     BlockHost b;
     int rc = c.build_block(ni, nj, nk, vtx_xyz, bc_type, inflow_prim, b);
     if (rc != E4C_OK) return rc;

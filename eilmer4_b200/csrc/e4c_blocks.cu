@@ -106,9 +106,12 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     out.nprim_vars = nw;
     v.axis_frames = (flags[1] == 0) ? 1 : 0;
     const bool uniform = (flags[0] == 0);
+    out.simple_flux = false;
+    for (int q = 0; q < 6; ++q) out.simple_flux = out.simple_flux || bc[q] == E4C_BC_OUTFLOW_SIMPLE_FLUX;
     // the fused kernel carries the ausmdv and hllc fluxes (no shock flags)
+    // and the ghost-cell boundaries (no flux computed in a boundary)
     out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC && v.nsp == 1 &&
-                cfg.flux_calculator <= E4C_FLUX_HLLC;
+                cfg.flux_calculator <= E4C_FLUX_HLLC && !out.simple_flux;
     if (cfg.precision == E4C_PREC_FP32_FLUX && !out.fused)
         return fail(E4C_ERR_UNSUPPORTED,
                     "the FP32-flux form needs a 3-D block with uniform geometry and the "

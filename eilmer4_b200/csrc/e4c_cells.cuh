@@ -98,6 +98,23 @@ static __device__ void replay_roundtrips(const BlockView& b, int dir, int fpos, 
     }
 }
 
+// Velocity of an interior cell as the reference holds it after all of a
+// stage's convective-flux loops: the round trips of every face it took part
+// in, i faces, then j, then k, each in loop order.
+static __device__ void replay_all_roundtrips(const BlockView& b, int ci, int cj, int ck,
+                                             V3<double>& v) {
+    const int c[3] = {ci, cj, ck};
+    const int lo[3] = {b.imin, b.jmin, b.kmin}, hi[3] = {b.imax, b.jmax, b.kmax};
+    const double* fgs[3] = {b.fgi, b.fgj, b.fgk};
+    for (int d = 0; d < b.dim; ++d)
+        for (int g = c[d] - 1; g <= c[d] + 2; ++g) {
+            if (g < lo[d] || g > hi[d] + 1) continue;
+            int p[3] = {c[0], c[1], c[2]};
+            p[d] = g;
+            roundtrip(v, fgs[d], b.npad, pidx(b, p[0], p[1], p[2]));
+        }
+}
+
 // update_thermo_from_rhou of a reconstructed state: ideal gas, or the
 // thermally perfect mixture started from the cell-centre temperature (the
 // state was copied from the cell, onedinterp.d / sfluidblock.d:2199-2208)

@@ -330,7 +330,9 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
         }
         b.S[g1] = 0;
         b.S[g2] = 0;
-    } else if (type == 2) {  // OutFlowBC_SimpleExtrapolate, x_order 0
+    } else if (type == 2 || type == 4) {
+        // OutFlowBC_SimpleExtrapolate, x_order 0; also the ghost cells of
+        // OutFlowBC_SimpleFlux (bc.lua:1124-1146)
         for (int q = 0; q < nw; ++q) {
             double v = b.W[q * b.npad + c0];
             b.W[q * b.npad + g1] = v;
@@ -368,6 +370,75 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
             b.W[W_VZ * b.npad + dst[g]] = v.z;
         }
     }
+}
+
+// BFE_SimpleOutflowFlux (bc/boundary_flux_effect.d:367-546), the flux action
+// of OutFlowBC_SimpleFlux, after the convective fluxes of every block
+// (simcore.d:2373-2377): each face of the boundary takes the flux of its
+// interior cell's flow state (fixed grid), or that of a closed face if the
+// state would flow in.  The face fluxes the flux kernels computed there are
+// overwritten, as the reference's flux loops skip those faces (sfluidblock.d:
+// 2227-2228 and alike) after reconstructing them.
+template <int NSP>
+__global__ void k_bc_flux(BlockView b, const SimDev* sim, FluxOpts o) {
+    if (sim->status != 0 || sim->finished) return;
+    const int which = blockIdx.y;
+    if (b.dim == 2 && which >= 4) return;
+    if (b.bc[which] != E4C_BC_OUTFLOW_SIMPLE_FLUX) return;
+    int n1, n2;
+    if (which == NORTH || which == SOUTH) { n1 = b.ni; n2 = b.nk; }
+    else if (which == EAST || which == WEST) { n1 = b.nj; n2 = b.nk; }
+    else { n1 = b.ni; n2 = b.nj; }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n1 * n2) return;
+    const int a1 = t % n1, a2 = t / n1;
+    int i, j, k, fi, fj, fk, outsign;
+    const double* fg;
+    double* Fo;
+    switch (which) {
+        case NORTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmax; fi = i; fj = j + 1; fk = k;
+                    fg = b.fgj; Fo = b.Fj; outsign = 1; break;
+        case SOUTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmin; fi = i; fj = j; fk = k;
+                    fg = b.fgj; Fo = b.Fj; outsign = -1; break;
+        case EAST: j = b.jmin + a1; k = b.kmin + a2; i = b.imax; fi = i + 1; fj = j; fk = k;
+                   fg = b.fgi; Fo = b.Fi; outsign = 1; break;
+        case WEST: j = b.jmin + a1; k = b.kmin + a2; i = b.imin; fi = i; fj = j; fk = k;
+                   fg = b.fgi; Fo = b.Fi; outsign = -1; break;
+        case TOP: i = b.imin + a1; j = b.jmin + a2; k = b.kmax; fi = i; fj = j; fk = k + 1;
+                  fg = b.fgk; Fo = b.Fk; outsign = 1; break;
+        default: i = b.imin + a1; j = b.jmin + a2; k = b.kmin; fi = i; fj = j; fk = k;
+                 fg = b.fgk; Fo = b.Fk; outsign = -1; break;
+    }
+    const size_t c = pidx(b, i, j, k), f = pidx(b, fi, fj, fk);
+    const double rho = b.W[W_RHO * b.npad + c], p = b.W[W_P * b.npad + c];
+    const double u = b.W[W_U * b.npad + c];
+    V3<double> v{b.W[W_VX * b.npad + c], b.W[W_VY * b.npad + c], b.W[W_VZ * b.npad + c]};
+    if (o.order2 && o.local_frame && !b.axis_frames) replay_all_roundtrips(b, i, j, k, v);
+    const double nx = fg[0 * b.npad + f], ny = fg[1 * b.npad + f], nz = fg[2 * b.npad + f];
+    const double vrx = v.x - 0.0, vry = v.y - 0.0, vrz = v.z - 0.0;
+    const double mass_flux = rho * (vrx * nx + vry * ny + vrz * nz);
+    constexpr int NSPC = NSP > 1 ? NSP : 0;
+    double F[5 + NSPC];
+    if ((outsign * mass_flux) > 0.0) {
+        F[0] = mass_flux;
+        F[1] = p * nx + v.x * mass_flux;
+        F[2] = p * ny + v.y * mass_flux;
+        F[3] = p * nz + v.z * mass_flux;
+        const double utot = u + 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z);
+        F[4] = mass_flux * utot + p * (v.x * nx + v.y * ny + v.z * nz);
+#pragma unroll
+        for (int q = 0; q < NSPC; ++q) F[5 + q] = mass_flux * b.W[(W_NBASE + q) * b.npad + c];
+    } else {
+        F[0] = 0.0;
+        F[1] = nx * p;
+        F[2] = ny * p;
+        F[3] = nz * p;
+        F[4] = p * (0.0 * nx + 0.0 * ny + 0.0 * nz);
+#pragma unroll
+        for (int q = 0; q < NSPC; ++q) F[5 + q] = 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 5 + NSPC; ++q) Fo[q * b.npad + f] = F[q];
 }
 
 // detect_shock_points (fluidblock.d:415-431) with PJ_ShockDetector
@@ -615,6 +686,15 @@ void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s) {
     dim3 grid((m + 127) / 128, 6);
     if (b.nsp == 5) k_bc<5><<<grid, 128, 0, s>>>(b, sim);
     else k_bc<1><<<grid, 128, 0, s>>>(b, sim);
+}
+
+void launch_bc_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, cudaStream_t s) {
+    int m = b.ni * b.nk;
+    m = m > b.nj * b.nk ? m : b.nj * b.nk;
+    m = m > b.ni * b.nj ? m : b.ni * b.nj;
+    dim3 grid((m + 127) / 128, 6);
+    if (b.nsp == 5) k_bc_flux<5><<<grid, 128, 0, s>>>(b, sim, o);
+    else k_bc_flux<1><<<grid, 128, 0, s>>>(b, sim, o);
 }
 
 void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s) {

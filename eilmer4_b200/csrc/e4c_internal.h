@@ -17,6 +17,7 @@ struct BlockHost {
     size_t ncell = 0;
     size_t nprim_vars = 8;
     bool fused = false;
+    bool simple_flux = false;   // has an OutFlowBC_SimpleFlux boundary
     FusedDesc f{};          // fused path: storage and uniform geometry
     int ex_block[6] = {-1, -1, -1, -1, -1, -1};   // partner handle of an exchange boundary
 };

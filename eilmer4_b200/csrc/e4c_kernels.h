@@ -27,6 +27,8 @@ void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s);
 // shock points (detect_shock_points with the PJ detector)
 void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s);
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, cudaStream_t s);
+// boundary-face fluxes of OutFlowBC_SimpleFlux boundaries (after launch_flux)
+void launch_bc_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, cudaStream_t s);
 void launch_update(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
                    int final_stage, cudaStream_t s);
 void launch_dt_reset(unsigned long long* acc, int nb, cudaStream_t s);

@@ -34,6 +34,7 @@ NORTH, EAST, SOUTH, WEST, TOP, BOTTOM = range(6)
 BC_SLIP_WALL = 0
 BC_INFLOW_SUPERSONIC = 1
 BC_OUTFLOW_EXTRAPOLATE = 2
+BC_OUTFLOW_SIMPLE_FLUX = 4   # OutFlowBC_SimpleFlux (bc.lua:1124-1146)
 
 DEFAULT_SEED = 20261203
 

@@ -65,6 +65,9 @@ extern "C" {
 #define E4C_BC_INFLOW_SUPERSONIC 1
 #define E4C_BC_OUTFLOW_SIMPLE_EXTRAPOLATE 2
 #define E4C_BC_EXCHANGE 3      /* set by e4c_connect_blocks only */
+/* OutFlowBC_SimpleFlux (bc.lua:1124-1146): extrapolated ghost cells and the
+ * boundary-face flux from the interior cell (boundary_flux_effect.d:367-546) */
+#define E4C_BC_OUTFLOW_SIMPLE_FLUX 4
 
 /* flux_calculator (src/eilmer/fvcore.d:184-228, plus the new "hllc"). */
 #define E4C_FLUX_AUSMDV 0

@@ -693,6 +693,66 @@ void Sim::face_flux(Block& b, Face& f, Cell& cL1, Cell& cL0, Cell& cR0, Cell& cR
     interface_flux(Lft, Rght, f);
 }
 
+// BFE_SimpleOutflowFlux (bc/boundary_flux_effect.d:367-546), the flux action
+// of OutFlowBC_SimpleFlux: every face of the boundary takes the flux of the
+// interior cell's flow state (fixed grid: v_rel = v), or that of a closed
+// face if that state would flow in.  The convective-flux loops skip these
+// faces (sfluidblock.d:2227-2228 and alike), after reconstructing them; the
+// face flux computed there is overwritten here, which is the same.
+void Sim::simple_outflow_flux(Block& b) {
+    const int nb = (b.dim == 3) ? 6 : 4;
+    const int nsp = gm.nsp;
+    for (int which = 0; which < nb; ++which) {
+        if (b.bc[which] != E4O_BC_OUTFLOW_SIMPLE_FLUX) continue;
+        int i0 = b.imin, i1 = b.imax, j0 = b.jmin, j1 = b.jmax, k0 = b.kmin, k1 = b.kmax;
+        if (which == 0) j0 = j1 = b.jmax;
+        if (which == 2) j0 = j1 = b.jmin;
+        if (which == 1) i0 = i1 = b.imax;
+        if (which == 3) i0 = i1 = b.imin;
+        if (which == 4) k0 = k1 = b.kmax;
+        if (which == 5) k0 = k1 = b.kmin;
+        const int outsign = (which == 0 || which == 1 || which == 4) ? 1 : -1;
+        for (int k = k0; k <= k1; ++k)
+            for (int j = j0; j <= j1; ++j)
+                for (int i = i0; i <= i1; ++i) {
+                    Face* f;
+                    switch (which) {
+                        case 0: f = &b.ifj[b.idx(i, j + 1, k)]; break;
+                        case 1: f = &b.ifi[b.idx(i + 1, j, k)]; break;
+                        case 2: f = &b.ifj[b.idx(i, j, k)]; break;
+                        case 3: f = &b.ifi[b.idx(i, j, k)]; break;
+                        case 4: f = &b.ifk[b.idx(i, j, k + 1)]; break;
+                        default: f = &b.ifk[b.idx(i, j, k)]; break;
+                    }
+                    const FlowState& fs = b.cell(i, j, k).fs;
+                    const Vec3 v_rel{fs.vel.x - 0.0, fs.vel.y - 0.0, fs.vel.z - 0.0};
+                    const double mass_flux =
+                        fs.gas.rho * (v_rel.x * f->n.x + v_rel.y * f->n.y + v_rel.z * f->n.z);
+                    if ((outsign * mass_flux) > 0.0) {
+                        f->F[0] = mass_flux;
+                        f->F[1] = fs.gas.p * f->n.x + fs.vel.x * mass_flux;
+                        f->F[2] = fs.gas.p * f->n.y + fs.vel.y * mass_flux;
+                        f->F[3] = fs.gas.p * f->n.z + fs.vel.z * mass_flux;
+                        const double utot =
+                            fs.gas.u + 0.5 * (fs.vel.x * fs.vel.x + fs.vel.y * fs.vel.y +
+                                              fs.vel.z * fs.vel.z);
+                        f->F[4] = mass_flux * utot +
+                                  fs.gas.p * (fs.vel.x * f->n.x + fs.vel.y * f->n.y + fs.vel.z * f->n.z);
+                        if (nsp > 1)
+                            for (int s = 0; s < nsp; ++s) f->F[5 + s] = mass_flux * fs.gas.massf[s];
+                    } else {
+                        f->F[0] = 0.0;
+                        f->F[1] = f->n.x * fs.gas.p;
+                        f->F[2] = f->n.y * fs.gas.p;
+                        f->F[3] = f->n.z * fs.gas.p;
+                        f->F[4] = fs.gas.p * (0.0 * f->n.x + 0.0 * f->n.y + 0.0 * f->n.z);
+                        if (nsp > 1)
+                            for (int s = 0; s < nsp; ++s) f->F[5 + s] = 0.0;
+                    }
+                }
+    }
+}
+
 void Sim::convective_flux(Block& b) {
     const bool par = !mutate_in_place;
     // i-faces (east-facing), loops k, j, i.
@@ -774,8 +834,11 @@ void Sim::apply_bcs(Block& b) {
                     } else if (type == E4O_BC_INFLOW_SUPERSONIC) {
                         g1.fs = b.inflow;  // flow_state_copy.d:66+
                         g2.fs = b.inflow;
-                    } else if (type == E4O_BC_OUTFLOW_EXTRAPOLATE) {
-                        const Cell& src = b.cell(i, j, k);  // extrapolate_copy.d:82+, x_order 0
+                    } else if (type == E4O_BC_OUTFLOW_EXTRAPOLATE ||
+                               type == E4O_BC_OUTFLOW_SIMPLE_FLUX) {
+                        // extrapolate_copy.d:82+, x_order 0 (also the ghost
+                        // cells of OutFlowBC_SimpleFlux, bc.lua:1124-1146)
+                        const Cell& src = b.cell(i, j, k);
                         g1.fs = src.fs;
                         g2.fs = src.fs;
                     } else {
@@ -1013,6 +1076,8 @@ int Sim::gasdynamic_increment() {
         if (cfg.flux_calculator == E4O_FLUX_ADAPTIVE_HANEL_AUSMDV)
             for (Block* b : blocks) detect_shock_points(*b);
         for (Block* b : blocks) convective_flux(*b);
+        // applyPostConvFluxAction of every block (simcore.d:2373-2377)
+        for (Block* b : blocks) simple_outflow_flux(*b);
         for (Block* b : blocks) {
             int rc = stage_cells(*b, stage, dt_global);
             if (rc != 0) return rc;

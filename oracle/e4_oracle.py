@@ -21,6 +21,7 @@ BC_SLIP_WALL = 0
 BC_INFLOW_SUPERSONIC = 1
 BC_OUTFLOW_EXTRAPOLATE = 2
 BC_EXCHANGE = 3
+BC_OUTFLOW_SIMPLE_FLUX = 4
 FLUX_AUSMDV = 0
 FLUX_HLLC = 1
 FLUX_HANEL = 2

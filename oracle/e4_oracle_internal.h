@@ -152,6 +152,7 @@ struct Sim {
                      FlowState& Rght) const;
     void face_flux(Block& b, Face& f, Cell& cL1, Cell& cL0, Cell& cR0, Cell& cR1, int dir) const;
     void convective_flux(Block& b);
+    void simple_outflow_flux(Block& b);
     void apply_bcs(Block& b);
     void encode_conserved(Cell& c, int ftl) const;
     int decode_conserved(Cell& c, int ftl) const;
