@@ -838,7 +838,7 @@ int e4c_profile_steps(int nsteps, double* ms, int* launches) {
 static int read_sim(SimDev& s);
 
 static bool tile_available(int ti, int tj) {
-    const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}};
+    const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}, {32, 16}};
     for (auto& t : tiles)
         if (t[0] == ti && t[1] == tj) return true;
     return false;
@@ -911,7 +911,7 @@ int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step) {
             cudaMemcpyAsync(const_cast<void*>(x.src), x.dst, x.bytes, cudaMemcpyDeviceToDevice,
                             c.stream);
     };
-    const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}};
+    const int tiles[][2] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}, {32, 16}};
     const int kcs[] = {16, 32, 64, 128};
     int best_ti = c.tile_ti, best_tj = c.tile_tj, best_kc = c.tile_kc;
     double best = 1.0e300;

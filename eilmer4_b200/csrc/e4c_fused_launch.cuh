@@ -43,7 +43,7 @@ static int occupancy_one() {
 }
 
 // Tile shapes available to the autotuner: (TI, TJ).
-#define E4C_TILES(X) X(32, 8) X(32, 4) X(16, 8) X(64, 4) X(16, 16)
+#define E4C_TILES(X) X(32, 8) X(32, 4) X(16, 8) X(64, 4) X(16, 16) X(32, 16)
 
 int fused_stage(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o,
                 int stage, cudaStream_t s) {
