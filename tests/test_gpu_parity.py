@@ -225,6 +225,39 @@ def test_fused_multiblock(oracle, e4lib):
     compare(oracle, wl, 20)
 
 
+@pytest.mark.parametrize("kc", [3, 5, 64])
+def test_fused_one_cta_tile_bitexact(oracle, e4lib, kc):
+    """The 32x16 tile (one 16-warp CTA per SM): with partial tiles in i and j,
+    k chunks with remainders, slip walls on every face and blocks joined by
+    exchange boundaries, the state stays bit for bit the oracle's."""
+    from eilmer4_b200.simcore import Simulation
+    b = uniform_block(70, 37, 23, 41, all_walls=True, swirl=True)
+    nsteps = 12
+    blocks, conns = W.split_block(b, 3, (2, 1, 1))
+    cfg = oracle.default_config(dimensions=3, n_threads=0, flux_calculator=oracle.FLUX_HLLC)
+    osim = oracle.OracleSim(cfg)
+    for q in blocks:
+        h = osim.add_block(q.ni, q.nj, q.nk, q.vtx, q.bc, q.inflow)
+        osim.set_flow(h, q.prim)
+    for (a, fa, bb, fb) in conns:
+        osim.connect(a, fa, bb, fb)
+    assert osim.run(nsteps) == 0
+    with Simulation({"dimensions": 3, "flux_calculator": "hllc"}) as sim:
+        for q in blocks:
+            h = sim.add_block(q.ni, q.nj, q.nk, q.vtx, q.bc, q.inflow)
+            sim.upload(h, q.prim)
+        for (a, fa, bb, fb) in conns:
+            sim.connect(a, fa, bb, fb)
+        sim.set_tile(32, 16, kc)
+        sim.run(nsteps)
+        for h in range(len(blocks)):
+            gp, gc = sim.download(h)
+            op, oc = osim.get_flow(h)
+            assert_same(gc, oc, f"conserved, block {h}")
+            assert_same(gp, op, f"primitive, block {h}")
+        assert sim.state()[2] == osim.step
+
+
 def test_fused_dt_allow_and_step_calls(oracle, e4lib):
     from eilmer4_b200.simcore import Simulation
     wl = W.Workload("u", 3, flux_calculator="hllc")
@@ -266,14 +299,14 @@ def test_autotune_keeps_state_and_parity(oracle, e4lib):
     _, ost, otime, odt, oout = run_oracle(oracle, wl, nsteps)
     with Simulation.from_workload(wl) as sim:
         (ti, tj, kc), ms = sim.autotune(2)
-        assert ms > 0.0 and (ti, tj) in ((32, 8), (32, 4), (16, 8), (64, 4), (16, 16))
+        assert ms > 0.0 and (ti, tj) in ((32, 8), (32, 4), (16, 8), (64, 4), (16, 16), (32, 16))
         t, dt, st = sim.state()
         assert st == 0 and t == 0.0
         sim.run(nsteps)
         gp, gc = sim.download(0)
         assert sim.state()[2] == ost
     assert_same(gc, oout[0][1], "conserved after autotune + run")
-    for shape in ((16, 16, 16), (64, 4, 128), (32, 4, 7)):
+    for shape in ((16, 16, 16), (64, 4, 128), (32, 4, 7), (32, 16, 5), (32, 16, 64)):
         with Simulation.from_workload(wl) as sim:
             sim.set_tile(*shape)
             sim.run(nsteps)
