@@ -49,8 +49,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s (256^3 Euler)"
 UNIT = "cell-updates/s"
-# Algorithmic bytes per cell-update (both stages): FP64 W (5) + U (5) per
-# stage read/write as laid out in DESIGN.md: 45 doubles; FP32-flux form 280 B.
+# Algorithmic bytes per cell-update (both stages), ideal gas, FP64: stage 1
+# reads W0 (5) and U0 (5), writes U1 (5) and W1 (5); stage 2 reads W1, U0 and
+# U1, writes U2 and W2: 45 doubles = 360 B.  FP32-flux form (W in FP32): 280 B.
 BYTES_PER_CELL_UPDATE = {"fp64": 360.0, "fp32_flux": 280.0}
 # chemistry of one reacting cell: read rho, u, T, massf x5, dt_chem; write
 # massf x5, T, p, u, a, dt_chem and rho*massf x5 (doubles)
@@ -61,7 +62,7 @@ BYTES_PER_REACTING_CELL = 8.0 * (9 + 15)
 # kernel's traffic grows with the cells it processes), keyed by (precision,
 # kernel class).  Algorithmic bytes per launch at 256^3: 3020 MB (FP64),
 # 2349 MB (FP32-flux).
-TRAFFIC = {("fp64", "stage"): 2762540032, ("fp32_flux", "stage"): 2058403840}
+TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2058403840}
 
 
 def peaks():
@@ -353,7 +354,10 @@ def euler_case(args, precision, local_rank, dist, world, headline):
     sim = Simulation.from_workload(wl, precision=precision, device=local_rank)
     ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
     tile = sim.get_tile()
-    if not args.no_autotune:
+    if args.tile:
+        tile = tuple(int(x) for x in args.tile.split(","))
+        sim.set_tile(*tile)
+    elif not args.no_autotune:
         # project autotuner: fastest fused tile shape; the state is restored
         tile, _ = sim.autotune(3)
     for _ in range(args.warmup):
@@ -372,7 +376,8 @@ def euler_case(args, precision, local_rank, dist, world, headline):
     res = {
         "value": value, "unit": UNIT, "ms_per_step": ms_per_step, "steps": args.steps,
         "dtype": "f64" if precision == "fp64" else "f32-flux/f64-accum",
-        "tile": {"ti": tile[0], "tj": tile[1], "kc": tile[2], "autotuned": not args.no_autotune},
+        "tile": {"ti": tile[0], "tj": tile[1], "kc": tile[2],
+                 "autotuned": not (args.no_autotune or args.tile)},
         "roofline": {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                      "traffic": TRAFFIC.get((precision, cls)),
@@ -676,6 +681,8 @@ def main():
     ap.add_argument("--ref-chem-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--tile", default="",
+                    help="TI,TJ,KC: fixed fused tile shape for the 256^3 block (no autotuning)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the --precision 256^3 line, no FP32/batched/reacting parts")
     ap.add_argument("--batched-steps", type=int, default=20)
