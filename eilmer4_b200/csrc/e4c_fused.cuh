@@ -30,9 +30,13 @@ template <typename R, int TI, int TJ>
 struct FusedSmem {
     static constexpr int PI = TI + 4, PJ = TJ + 4;
     static constexpr int PLANE = NF * PI * PJ;
-    static constexpr size_t bytes() {
+    // per-cell van Albada values of a plane for its i-faces ([5][TJ][TI+2],
+    // cells -1..TI of each row) and j-faces ([5][TJ+2][TI])
+    static constexpr int NVI = TJ * (TI + 2), NVJ = (TJ + 2) * TI;
+    static constexpr size_t base() {
         return sizeof(R) * (size_t(4) * PLANE + 5 * TJ * (TI + 1) + 5 * (TJ + 1) * TI);
     }
+    static constexpr size_t va_bytes() { return sizeof(R) * 5 * size_t(NVI + NVJ); }
 };
 
 template <typename R>
@@ -184,10 +188,15 @@ __device__ __forceinline__ void cell_pressure(Prim<R, 1>& s, const GasConsts& ga
 // Reconstruction + flux of one face from four cells (general-path semantics,
 // sfluidblock.d:2190-2344 with onedinterp.d:435-585 and fluxcalc.d:26-128),
 // with the face frame of direction DIR applied as a permutation.
+//
+// vaL, vaR (optional, with the limiter on): the van Albada values of the
+// cells L0 and R0 for this direction, at stride vs, in the order rho, vx, vy,
+// vz, u of the global frame (L2R2::va).
 template <typename R, int FLUX, int DIR>
 __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R, 1> sR0,
                                           Prim<R, 1> sR1, const L2R2<R>& w, const FluxOpts& o,
-                                          R* F) {
+                                          R* F, const R* vaL = nullptr, const R* vaR = nullptr,
+                                          int vs = 0) {
     Prim<R, 1> Lf = sL0, Rt = sR0;
     if (o.order2) {
         if (o.local_frame) {
@@ -197,13 +206,30 @@ __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R
             axis_to_local<DIR>(sR1.vel);
         }
         const bool lim = o.limiter, clip = o.clip;
-        w.scalar(lim, clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
-        w.scalar(lim, clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
-        w.scalar(lim, clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
+        if (vaL) {
+            // local x, y, z are the global components DIR, DIR+1, DIR+2 (mod 3)
+            const int cx = o.local_frame ? DIR : 0;
+            const int c0 = 1 + cx, c1 = 1 + (cx + 1) % 3, c2 = 1 + (cx + 2) % 3;
+            w.scalar_with(vaL[c0 * vs], vaR[c0 * vs], clip, sL1.vel.x, sL0.vel.x, sR0.vel.x,
+                          sR1.vel.x, Lf.vel.x, Rt.vel.x);
+            w.scalar_with(vaL[c1 * vs], vaR[c1 * vs], clip, sL1.vel.y, sL0.vel.y, sR0.vel.y,
+                          sR1.vel.y, Lf.vel.y, Rt.vel.y);
+            w.scalar_with(vaL[c2 * vs], vaR[c2 * vs], clip, sL1.vel.z, sL0.vel.z, sR0.vel.z,
+                          sR1.vel.z, Lf.vel.z, Rt.vel.z);
+        } else {
+            w.scalar(lim, clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
+            w.scalar(lim, clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
+            w.scalar(lim, clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
+        }
         Lf.massf[0] = R(1.0);
         Rt.massf[0] = R(1.0);
-        w.scalar(lim, clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
-        w.scalar(lim, clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
+        if (vaL) {
+            w.scalar_with(vaL[0], vaR[0], clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
+            w.scalar_with(vaL[4 * vs], vaR[4 * vs], clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
+        } else {
+            w.scalar(lim, clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
+            w.scalar(lim, clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
+        }
         R T;
         if (!ideal_rhou<R>(o.gas, Lf.rho, Lf.u, Lf.p, T)) { Lf = sL0; cell_pressure(Lf, o.gas); }
         if (!ideal_rhou<R>(o.gas, Rt.rho, Rt.u, Rt.p, T)) { Rt = sR0; cell_pressure(Rt, o.gas); }
@@ -289,6 +315,21 @@ struct FusedMinBlocks {
     static constexpr int value = warps / per_cta > 0 ? warps / per_cta : 1;
 };
 
+// The per-cell limiter values take shared memory of their own and a barrier
+// per plane; they halve the FP64 divisions of the limiter (measured 3 % on the
+// 256^3 block with the 32x16 tile), while in FP32 (approximate division) the
+// barrier costs more than they save.  A tile shape keeps them where they fit
+// beside the CTAs per SM its launch bounds ask for (228 KB per SM, 1 KB
+// reserved per CTA, 227 KB per CTA).
+template <typename R, int TI, int TJ>
+struct FusedShareVA {
+    using S = FusedSmem<R, TI, TJ>;
+    static constexpr size_t with = S::base() + S::va_bytes();
+    static constexpr bool value = sizeof(R) == 8 && with <= 227 * 1024 &&
+                                  FusedMinBlocks<R, TI, TJ>::value * (with + 1024) <= 228 * 1024;
+    static constexpr size_t bytes() { return value ? with : S::base(); }
+};
+
 // The fused stage.  stage 1: W=WA -> WB, writes dUdt0; stage 2: W=WB -> WA,
 // writes U0 (the end-of-step state).
 template <typename R, int FLUX, int TI, int TJ>
@@ -302,6 +343,9 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
     R* planes = reinterpret_cast<R*>(smem_raw);
     R* Fi = planes + 4 * S::PLANE;              // [5][TJ][TI+1]
     R* Fj = Fi + 5 * TJ * (TI + 1);             // [5][TJ+1][TI]
+    R* VAi = Fj + 5 * (TJ + 1) * TI;            // [5][TJ][TI+2] (FusedShareVA)
+    R* VAj = VAi + 5 * S::NVI;                  // [5][TJ+2][TI]
+    const bool share_va = FusedShareVA<R, TI, TJ>::value && o.order2 && o.limiter;
     const bool cell_thread = threadIdx.x < FusedThreads<TI, TJ>::cells;
     const int ti = threadIdx.x % TI, tj = threadIdx.x / TI;
     const double dt = sim->dt_global;
@@ -350,6 +394,33 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                                   k + 2);
             __syncthreads();
             const R* pk = planes + ((k + 8) & 3) * S::PLANE;
+            if (share_va) {
+                // van Albada values of the cells of this plane that the i- and
+                // j-faces below use (cells -1..n of each direction)
+                for (int e = threadIdx.x; e < S::NVI + S::NVJ; e += blockDim.x) {
+                    int off, step, dir;
+                    R* dst;
+                    int vs;
+                    if (e < S::NVI) {
+                        const int ci = e % (TI + 2), cj = e / (TI + 2);
+                        if (i0 + ci - 1 > d.ni || j0 + cj >= d.nj) continue;
+                        off = (cj + 2) * PI + (ci + 1);
+                        step = 1; dir = 0; dst = VAi + e; vs = S::NVI;
+                    } else {
+                        const int g = e - S::NVI;
+                        const int ci = g % TI, cj = g / TI;
+                        if (i0 + ci >= d.ni || j0 + cj - 1 > d.nj) continue;
+                        off = (cj + 1) * PI + (ci + 2);
+                        step = PI; dir = 1; dst = VAj + g; vs = S::NVJ;
+                    }
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        const R* q = pk + f * FS + off;
+                        dst[f * vs] = w[dir].va(q[-step], q[0], q[step]);
+                    }
+                }
+                __syncthreads();
+            }
             // i-faces, (TI+1) x TJ (face fi is the west face of cell i0+fi), then
             // j-faces, TI x (TJ+1) (face fj is the south face of cell j0+fj), as
             // one list over all the CTA's threads
@@ -367,7 +438,12 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                     get_cell(pk, off + 2, FS, gas, a2);
                     get_cell(pk, off + 3, FS, gas, a3);
                     R F[5];
-                    face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F);
+                    if (share_va) {
+                        const R* v = VAi + fj * (TI + 2) + fi;
+                        face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F, v, v + 1, S::NVI);
+                    } else {
+                        face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F);
+                    }
 #pragma unroll
                     for (int v = 0; v < 5; ++v) Fi[(v * TJ + fj) * (TI + 1) + fi] = F[v];
                 } else {
@@ -381,7 +457,12 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                     get_cell(pk, off + 2 * PI, FS, gas, a2);
                     get_cell(pk, off + 3 * PI, FS, gas, a3);
                     R F[5];
-                    face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F);
+                    if (share_va) {
+                        const R* v = VAj + fj * TI + fi;
+                        face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F, v, v + TI, S::NVJ);
+                    } else {
+                        face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F);
+                    }
 #pragma unroll
                     for (int v = 0; v < 5; ++v) Fj[(v * (TJ + 1) + fj) * TI + fi] = F[v];
                 }

@@ -18,7 +18,7 @@ using RT = E4C_FUSED_R;
 template <int FLUX, int TI, int TJ>
 static int launch_one(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o,
                       int stage, cudaStream_t s) {
-    constexpr size_t smem = FusedSmem<RT, TI, TJ>::bytes();
+    constexpr size_t smem = FusedShareVA<RT, TI, TJ>::bytes();
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_fused_stage<RT, FLUX, TI, TJ>,
@@ -32,7 +32,7 @@ static int launch_one(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, c
 
 template <int FLUX, int TI, int TJ>
 static int occupancy_one() {
-    constexpr size_t smem = FusedSmem<RT, TI, TJ>::bytes();
+    constexpr size_t smem = FusedShareVA<RT, TI, TJ>::bytes();
     cudaFuncSetAttribute(k_fused_stage<RT, FLUX, TI, TJ>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     int n = 0;

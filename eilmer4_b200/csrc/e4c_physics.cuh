@@ -103,6 +103,28 @@ struct L2R2 {
             qR = clip_to_limits(qR, qL0, qR0);
         }
     }
+    // With uniform cell lengths (tw_L0L1 == tw_R0L0 == tw_R1R0) the sL of a
+    // face and the sR of the face before it are one van Albada value of their
+    // shared cell, bit for bit: va() gives it from the cell and its two
+    // neighbours, scalar_with() interpolates a face from the two values.
+    __device__ __forceinline__ R va(R qm, R q0, R qp) const {
+        const R eps = R(1.0e-12);
+        R a = (q0 - qm) * tw_L0L1;
+        R b = (qp - q0) * tw_R0L0;
+        return (a * b + fabs(a * b) + eps) / (a * a + b * b + eps);
+    }
+    __device__ __forceinline__ void scalar_with(R sL, R sR, bool clip, R qL1, R qL0, R qR0, R qR1,
+                                                R& qL, R& qR) const {
+        R delLminus = (qL0 - qL1) * tw_L0L1;
+        R del = (qR0 - qL0) * tw_R0L0;
+        R delRplus = (qR1 - qR0) * tw_R1R0;
+        qL = qL0 + sL * aL0 * (del * two_L0_L1 + delLminus * lenR0);
+        qR = qR0 - sR * aR0 * (delRplus * lenL0 + del * two_R0_R1);
+        if (clip) {
+            qL = clip_to_limits(qL, qL0, qR0);
+            qR = clip_to_limits(qR, qL0, qR0);
+        }
+    }
 };
 
 // IdealGas.update_thermo_from_rhou, src/gas/ideal_gas.d:98-106
