@@ -134,11 +134,11 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
                           [&] { launch_shock(b.v, d_sim, fopts.compression_tol, stream); });
         }
     }
+    // every face direction of a block in one launch
     for (int h : hs) {
         const BlockHost& b = blocks[h];
         if (b.fused) continue;
-        for (int d = 0; d < b.v.dim; ++d)
-            launch_as(*this, E4C_KCLASS_FLUX, 1, [&] { launch_flux(b.v, d_sim, fopts, d, stream); });
+        launch_as(*this, E4C_KCLASS_FLUX, 1, [&] { launch_flux(b.v, d_sim, fopts, -1, stream); });
     }
     // applyPostConvFluxAction of every block (simcore.d:2373-2377)
     for (int h : hs) {

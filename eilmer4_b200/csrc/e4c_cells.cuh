@@ -134,17 +134,30 @@ __device__ __forceinline__ bool rhou_update(const FluxOpts& o, Prim<double, NSP>
     return true;
 }
 
+// Faces of direction dir, or of every direction of the block in one launch
+// (dir < 0: i faces, then j, then k, one index space).
 template <int NSP, int FLUX, int GAS>
-__global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir) {
+__global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) {
     if (sim->status != 0 || sim->finished) return;
-    const int ni = b.ni + (dir == 0), nj = b.nj + (dir == 1), nk = b.nk + (dir == 2);
-    const long long n = (long long)ni * nj * nk;
-    const size_t stride = dir == 0 ? 1 : (dir == 1 ? size_t(b.nidim) : size_t(b.nidim) * b.njdim);
-    const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
-    double* Fo = dir == 0 ? b.Fi : (dir == 1 ? b.Fj : b.Fk);
+    long long nd[3];
+    for (int d = 0; d < 3; ++d)
+        nd[d] = (long long)(b.ni + (d == 0)) * (b.nj + (d == 1)) * (b.nk + (d == 2));
+    if (b.dim == 2) nd[2] = 0;
+    const long long n = dir_arg >= 0 ? nd[dir_arg] : nd[0] + nd[1] + nd[2];
     constexpr int NSPC = NSP > 1 ? NSP : 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
+    for (long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x; tt < n;
+         tt += (long long)gridDim.x * blockDim.x) {
+        int dir = dir_arg;
+        long long t = tt;
+        if (dir < 0) {
+            dir = 0;
+            if (t >= nd[0]) { t -= nd[0]; dir = 1; }
+            if (dir == 1 && t >= nd[1]) { t -= nd[1]; dir = 2; }
+        }
+        const int ni = b.ni + (dir == 0), nj = b.nj + (dir == 1);
+        const size_t stride = dir == 0 ? 1 : (dir == 1 ? size_t(b.nidim) : size_t(b.nidim) * b.njdim);
+        const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
+        double* Fo = dir == 0 ? b.Fi : (dir == 1 ? b.Fj : b.Fk);
         int i = b.imin + int(t % ni);
         int j = b.jmin + int((t / ni) % nj);
         int k = b.kmin + int(t / ((long long)ni * nj));

@@ -704,7 +704,10 @@ void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_
 
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
                  cudaStream_t s) {
-    long long n = (long long)(b.ni + (dir == 0)) * (b.nj + (dir == 1)) * (b.nk + (dir == 2));
+    long long n = 0;
+    for (int d = 0; d < b.dim; ++d)
+        if (dir < 0 || d == dir)
+            n += (long long)(b.ni + (d == 0)) * (b.nj + (d == 1)) * (b.nk + (d == 2));
     const int T = 128;
     const int g = grid_for(n, T);
     if (b.nsp == 5) {

@@ -26,6 +26,7 @@ void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_
 void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s);
 // shock points (detect_shock_points with the PJ detector)
 void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s);
+// face fluxes of direction dir, or of every direction when dir < 0
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, cudaStream_t s);
 // boundary-face fluxes of OutFlowBC_SimpleFlux boundaries (after launch_flux)
 void launch_bc_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, cudaStream_t s);
