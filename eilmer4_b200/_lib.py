@@ -130,6 +130,8 @@ def load():
         "e4c_block_upload": ([i, dp], i),
         "e4c_block_download": ([i, dp, dp], i),
         "e4c_block_upload_async": ([i, dp], i),
+        "e4c_block_upload_cons": ([i, dp], i),
+        "e4c_block_upload_cons_async": ([i, dp], i),
         "e4c_block_download_async": ([i, dp, dp], i),
         "e4c_transfers_wait": ([], i),
         "e4c_integrate_async": ([i, d], i),

@@ -502,6 +502,25 @@ int e4c_block_upload(int h, const double* prim) {
     return E4C_OK;
 }
 
+int e4c_block_upload_cons(int h, const double* cons) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size()) || !cons) return fail(E4C_ERR_ARG, "bad handle or pointer");
+    BlockHost& b = c.blocks[h];
+    if (b.v.nsp != 1) return c.upload_cons(b, nullptr);
+    const size_t bytes = 5 * b.ncell * sizeof(double);
+    E4C_CUDA(cudaMemcpyAsync(c.d_staging, cons, bytes, cudaMemcpyHostToDevice, c.stream));
+    int rc = c.upload_cons(b, c.d_staging);
+    if (rc != E4C_OK) return rc;
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaStreamSynchronize(c.stream));
+    SimDev st;
+    rc = read_sim(st);
+    if (rc != E4C_OK) return rc;
+    if (st.status != 0) return status_error(st);
+    return E4C_OK;
+}
+
 int e4c_block_download(int h, double* prim, double* cons) {
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
@@ -590,6 +609,27 @@ int e4c_block_upload_async(int h, const double* prim) {
     } else {
         launch_upload(b.v, c.d_stage_in, c.stream);
     }
+    c.launches += 1;
+    E4C_CUDA(cudaGetLastError());
+    E4C_CUDA(cudaEventRecord(c.ev_in_consumed, c.stream));
+    return E4C_OK;
+}
+
+int e4c_block_upload_cons_async(int h, const double* cons) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (h < 0 || h >= int(c.blocks.size()) || !cons) return fail(E4C_ERR_ARG, "bad handle or pointer");
+    BlockHost& b = c.blocks[h];
+    if (b.v.nsp != 1) return c.upload_cons(b, nullptr);
+    int rc = c.ensure_stage_io((b.nprim_vars + size_t(b.v.nv)) * b.ncell * sizeof(double));
+    if (rc != E4C_OK) return rc;
+    const size_t bytes = 5 * b.ncell * sizeof(double);
+    E4C_CUDA(cudaStreamWaitEvent(c.h2d_stream, c.ev_in_consumed, 0));
+    E4C_CUDA(cudaMemcpyAsync(c.d_stage_in, cons, bytes, cudaMemcpyHostToDevice, c.h2d_stream));
+    E4C_CUDA(cudaEventRecord(c.ev_in_copied, c.h2d_stream));
+    E4C_CUDA(cudaStreamWaitEvent(c.stream, c.ev_in_copied, 0));
+    rc = c.upload_cons(b, c.d_stage_in);
+    if (rc != E4C_OK) return rc;
     c.launches += 1;
     E4C_CUDA(cudaGetLastError());
     E4C_CUDA(cudaEventRecord(c.ev_in_consumed, c.stream));

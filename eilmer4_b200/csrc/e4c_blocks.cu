@@ -296,6 +296,27 @@ int Ctx::fused_upload(BlockHost& b, const double* prim) {
     return E4C_OK;
 }
 
+int Ctx::fused_upload_cons(BlockHost& b, const double* cons) {
+    FusedDesc& f = b.f;
+    if (cfg.precision == E4C_PREC_FP32_FLUX) f32::fused_upload_cons(cons, b.ncell, f.WA, f.U0, d_sim, gas, stream);
+    else f64::fused_upload_cons(cons, b.ncell, f.WA, f.U0, d_sim, gas, stream);
+    const int zero = 0;
+    E4C_CUDA(cudaMemcpyAsync(f.use_a0, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+    return E4C_OK;
+}
+
+// Conserved state already on the device (dense, v * ncell + cell) -> the
+// block's state, decoded on the device.
+int Ctx::upload_cons(BlockHost& b, const double* dev_cons) {
+    if (b.v.nsp != 1)
+        return fail(E4C_ERR_UNSUPPORTED,
+                    "a conserved-state upload decodes the ideal gas only (the mixture's "
+                    "temperature iteration needs a starting temperature)");
+    if (b.fused) return fused_upload_cons(b, dev_cons);
+    launch_upload_cons(b.v, dev_cons, d_sim, gas, stream);
+    return E4C_OK;
+}
+
 void Ctx::fused_download(const BlockHost& b, double* prim, double* cons) {
     const FusedDesc& f = b.f;
     if (cfg.precision == E4C_PREC_FP32_FLUX)

@@ -92,6 +92,24 @@ __global__ void k_fused_upload(const double* prim, size_t nc, RT* W, double* A0,
     }
 }
 
+// U (dense) -> U0 and the decoded W (R) of a fused block (decode_ideal, the
+// operations of the stage's decode); the sound speed then comes from W
+__global__ void k_fused_upload_cons(const double* cons, size_t nc, RT* W, double* U0, SimDev* sim,
+                                    GasConsts gas) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < nc;
+         c += size_t(gridDim.x) * blockDim.x) {
+        double Un[5];
+        for (int v = 0; v < 5; ++v) Un[v] = cons[v * nc + c];
+        double rho, vx, vy, vz, u, p, T, a;
+        if (!decode_ideal(gas, Un, rho, vx, vy, vz, u, p, T, a)) {
+            if (atomicCAS(&sim->status, 0, -5) == 0) sim->status_step = sim->step;
+        }
+        W[0 * nc + c] = RT(rho); W[1 * nc + c] = RT(vx); W[2 * nc + c] = RT(vy);
+        W[3 * nc + c] = RT(vz); W[4 * nc + c] = RT(u);
+        for (int v = 0; v < 5; ++v) U0[v * nc + c] = Un[v];
+    }
+}
+
 // W (R) -> prim with p, T, a from update_thermo_from_rhou + update_sound_speed
 __global__ void k_fused_download(const RT* W, const double* A0, const int* use_a0,
                                  const double* U0, size_t nc, GasConsts gas, double* prim,
@@ -120,6 +138,13 @@ void fused_upload(const double* prim, size_t nc, void* W, double* A0, double* U0
     int g = int((nc + 255) / 256);
     if (g > 148 * 32) g = 148 * 32;
     k_fused_upload<<<g, 256, 0, s>>>(prim, nc, static_cast<RT*>(W), A0, U0);
+}
+
+void fused_upload_cons(const double* cons, size_t nc, void* W, double* U0, SimDev* sim,
+                       const GasConsts& gas, cudaStream_t s) {
+    int g = int((nc + 255) / 256);
+    if (g > 148 * 32) g = 148 * 32;
+    k_fused_upload_cons<<<g, 256, 0, s>>>(cons, nc, static_cast<RT*>(W), U0, sim, gas);
 }
 
 void fused_download(const void* W, const double* A0, const int* use_a0, const double* U0,

@@ -258,6 +258,29 @@ __global__ void k_upload(BlockView b, const double* prim) {
     }
 }
 
+// Conserved state (dense, v * n + t) -> U0 and the decoded primitive state of
+// the interior cells, ideal gas (decode_ideal).
+__global__ void k_upload_cons(BlockView b, const double* cons, SimDev* sim, GasConsts gas) {
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = b.imin + int(t % b.ni);
+        int j = b.jmin + int((t / b.ni) % b.nj);
+        int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        size_t c = pidx(b, i, j, k);
+        double Un[5];
+        for (int v = 0; v < 5; ++v) Un[v] = cons[v * n + t];
+        double rho, vx, vy, vz, u, p, T, a;
+        if (!decode_ideal(gas, Un, rho, vx, vy, vz, u, p, T, a)) set_status(sim, -5);
+        double* W = b.W;
+        W[W_RHO * b.npad + c] = rho;
+        W[W_VX * b.npad + c] = vx; W[W_VY * b.npad + c] = vy; W[W_VZ * b.npad + c] = vz;
+        W[W_P * b.npad + c] = p; W[W_T * b.npad + c] = T;
+        W[W_U * b.npad + c] = u; W[W_A * b.npad + c] = a;
+        for (int v = 0; v < 5; ++v) b.U0[v * b.npad + c] = Un[v];
+    }
+}
+
 __global__ void k_download(BlockView b, double* prim, double* cons) {
     const long long n = (long long)b.ni * b.nj * b.nk;
     const int nw = W_NBASE + (b.nsp > 1 ? b.nsp : 0);
@@ -672,6 +695,12 @@ void launch_geometry(const BlockView& b, const double* vtx, cudaStream_t s) {
 void launch_upload(const BlockView& b, const double* prim, cudaStream_t s) {
     long long n = (long long)b.ni * b.nj * b.nk;
     k_upload<<<grid_for(n, 256), 256, 0, s>>>(b, prim);
+}
+
+void launch_upload_cons(const BlockView& b, const double* cons, SimDev* sim, const GasConsts& gas,
+                        cudaStream_t s) {
+    long long n = (long long)b.ni * b.nj * b.nk;
+    k_upload_cons<<<grid_for(n, 256), 256, 0, s>>>(b, cons, sim, gas);
 }
 
 void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_t s) {

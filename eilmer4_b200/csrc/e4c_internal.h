@@ -137,6 +137,8 @@ struct Ctx {
     void fused_stage_all(int stage);
     void fused_dt_all(SimDev* sim, const double* dt_current);
     int fused_upload(BlockHost& b, const double* prim);
+    int fused_upload_cons(BlockHost& b, const double* cons);
+    int upload_cons(BlockHost& b, const double* dev_cons);
     void fused_download(const BlockHost& b, double* prim, double* cons);
 };
 

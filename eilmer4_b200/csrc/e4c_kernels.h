@@ -23,6 +23,9 @@ struct FluxOpts {
 void launch_geometry(const BlockView& b, const double* vtx, cudaStream_t s);
 void launch_upload(const BlockView& b, const double* prim, cudaStream_t s);
 void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_t s);
+// conserved state of the interior cells (ideal gas) -> U0 and the decoded W
+void launch_upload_cons(const BlockView& b, const double* cons, SimDev* sim, const GasConsts& gas,
+                        cudaStream_t s);
 void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s);
 // shock points (detect_shock_points with the PJ detector)
 void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s);
@@ -91,6 +94,8 @@ struct FusedLaunch {
                   double cfl_value, const double* dt_current, cudaStream_t s);              \
     void fused_upload(const double* prim, size_t nc, void* W, double* A0, double* U0,        \
                       cudaStream_t s);                                                       \
+    void fused_upload_cons(const double* cons, size_t nc, void* W, double* U0, SimDev* sim,  \
+                           const GasConsts& gas, cudaStream_t s);                            \
     void fused_download(const void* W, const double* A0, const int* use_a0, const double* U0, \
                         size_t nc, const GasConsts& gas, double* prim, double* cons,        \
                         cudaStream_t s);                                                     \

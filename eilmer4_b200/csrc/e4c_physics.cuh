@@ -142,6 +142,35 @@ __device__ __forceinline__ R ideal_sound_speed(const GasConsts& g, R T) {
     return sqrt(R(g.gamma) * R(g.Rgas) * T);
 }
 
+// decode_conserved (fvcell.d:563-732) of one ideal-gas cell with the
+// reference's defaults (adjust_invalid_cell_data = false,
+// ignore_low_T_thermo_update_failure = true, suggested_low_T_value = 200 K):
+// the primitive state from U, and U re-encoded where the low-temperature
+// fallback applies.  The same operations as the stage kernels' decode.
+// Returns false for a non-positive density (the state is then left zero).
+__device__ __forceinline__ bool decode_ideal(const GasConsts& gas, double* Un, double& rho,
+                                             double& vx, double& vy, double& vz, double& u,
+                                             double& p, double& T, double& a) {
+    rho = Un[0]; vx = 0.0; vy = 0.0; vz = 0.0; u = 0.0; p = 0.0; T = 0.0; a = 0.0;
+    if (!(Un[0] > 0.0)) return false;
+    const double dinv = 1.0 / rho;
+    vx = Un[1] * dinv; vy = Un[2] * dinv; vz = Un[3] * dinv;
+    u = Un[4] * dinv;
+    const double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
+    u -= ke;
+    if (!ideal_rhou<double>(gas, rho, u, p, T)) {
+        T = 200.0;
+        p = rho * gas.Rgas * T;
+        u = gas.Cv * T;
+        Un[0] = rho;
+        Un[1] = rho * vx; Un[2] = rho * vy; Un[3] = rho * vz;
+        const double ke2 = 0.5 * (vx * vx + vy * vy + vz * vz);
+        Un[4] = rho * (u + ke2);
+    }
+    a = ideal_sound_speed<double>(gas, T);
+    return true;
+}
+
 // gas_model.d:295-327 scale_mass_fractions (tolerance 0.0, assert tolerance 0.1)
 template <typename R, int NSP>
 __device__ __forceinline__ bool scale_mass_fractions(R* massf) {

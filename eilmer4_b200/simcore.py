@@ -99,6 +99,14 @@ class Simulation:
             assert prim.shape[-1] == self.ncell(h)
         _lib.check(self.L.e4c_block_upload(h, _lib.dptr(prim)))
 
+    def upload_cons(self, h, cons):
+        """cons: (5, ncell) conserved state (ideal gas), decoded on the device as
+        the end of a stage decodes it, so a run continues bit for bit."""
+        if not hasattr(cons, "data_ptr"):
+            cons = np.ascontiguousarray(cons, dtype=np.float64)
+            assert cons.shape == (5, self.ncell(h))
+        _lib.check(self.L.e4c_block_upload_cons(h, _lib.dptr(cons)))
+
     def download(self, h, prim=None, cons=None, want_cons=True):
         """Primitive (8, ncell) and conserved (5, ncell) state; the outputs may be
         given (numpy arrays or contiguous pinned torch tensors)."""
@@ -116,6 +124,11 @@ class Simulation:
         """Queue an upload from a contiguous pinned host tensor/array (returns
         at once; call wait_transfers before reusing the host buffer)."""
         _lib.check(self.L.e4c_block_upload_async(h, _lib.dptr(prim)))
+
+    def upload_cons_async(self, h, cons):
+        """Queue a conserved-state upload (see upload_cons) from a contiguous
+        pinned host tensor/array."""
+        _lib.check(self.L.e4c_block_upload_cons_async(h, _lib.dptr(cons)))
 
     def download_async(self, h, prim=None, cons=None):
         """Queue a download into contiguous pinned host buffers."""

@@ -245,6 +245,15 @@ int e4c_connect_blocks(int ha, int face_a, int hb, int face_b, int orientation);
 /* Upload a block's primitive state and encode its conserved quantities. */
 int e4c_block_upload(int h, const double* prim);
 
+/* Upload a block's conserved state (rho, rho*v, E as SoA, ideal gas) and
+ * decode it on the device as the end of a stage does (decode_conserved,
+ * fvcell.d:563-732): a host that hands the conserved state back and forth
+ * between steps continues bit for bit as an uninterrupted run (a primitive
+ * upload re-encodes U).  The mixture returns E4C_ERR_UNSUPPORTED (its
+ * temperature iteration needs a starting temperature).  A non-positive
+ * density returns E4C_ERR_BAD_MASS and leaves the simulation in that error. */
+int e4c_block_upload_cons(int h, const double* cons);
+
 /* Download the primitive and/or conserved state (either pointer may be NULL). */
 int e4c_block_download(int h, double* prim, double* cons);
 
@@ -265,6 +274,7 @@ int e4c_block_set_dt_chem(int h, const double* dt_chem);
  * state left by all work queued before it; an upload is seen by all work
  * queued after it. */
 int e4c_block_upload_async(int h, const double* prim);
+int e4c_block_upload_cons_async(int h, const double* cons);
 int e4c_block_download_async(int h, double* prim, double* cons);
 int e4c_transfers_wait(void);
 

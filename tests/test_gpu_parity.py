@@ -346,3 +346,58 @@ def test_async_transfers_match_sync(e4lib):
             outs.append(res)
     for a, c in zip(outs[0], outs[1]):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("case", ["fused3d", "fused3d_fp32", "general2d"])
+def test_conserved_handoff_continues_bit_for_bit(e4lib, case):
+    """A host that takes the conserved state off the device between steps and
+    hands it back (e4c_block_upload_cons, decoded on the device as a stage's
+    end decodes it) continues exactly as the uninterrupted run: the decoded
+    primitive state and U are the run's own, and the next steps give the
+    same bits (fused 3-D FP64 and FP32-flux, general 2-D)."""
+    from eilmer4_b200.simcore import Simulation
+    if case.startswith("fused3d"):
+        wl = W.Workload("u", 3, flux_calculator="hllc")
+        wl.blocks.append(uniform_block(40, 24, 20, 7))
+    else:
+        wl = W.sod_2d(48, 16)
+    prec = "fp32_flux" if case.endswith("fp32") else "fp64"
+    with Simulation.from_workload(wl, precision=prec) as a:
+        dt = 1.0e-3
+        for q in range(6):
+            dta, _ = a.dt_allow([0], dt, q > 0)
+            dt = min(dta, 1.0e-3)
+            assert a.gasdynamic_step([0], dt) == 0
+        pA, cA = a.download(0)
+        dt_more = 0.5 * a.dt_allow([0], dt, True)[0]
+        for q in range(4):
+            assert a.gasdynamic_step([0], dt_more) == 0
+        pA2, cA2 = a.download(0)
+    with Simulation.from_workload(wl, precision=prec) as b:
+        b.upload_cons(0, cA)
+        pB, cB = b.download(0)
+        assert_same(cB, cA, "conserved after the upload")
+        assert_same(pB, pA, "decoded primitive state")
+        for q in range(4):
+            assert b.gasdynamic_step([0], dt_more) == 0
+        pB2, cB2 = b.download(0)
+    assert_same(cB2, cA2, "conserved after four more steps")
+    assert_same(pB2, pA2, "primitive after four more steps")
+
+
+def test_conserved_upload_rejects_bad_mass_and_the_mixture(e4lib):
+    from eilmer4_b200 import _lib
+    from eilmer4_b200.simcore import Simulation
+    wl = W.sod_2d(16, 8)
+    with Simulation.from_workload(wl) as sim:
+        _, c = sim.download(0)
+        c = c.copy()
+        c[0, 5] = -1.0
+        with pytest.raises(_lib.E4CError) as err:
+            sim.upload_cons(0, c)
+        assert err.value.code == _lib.E4C_ERR_BAD_MASS
+    with Simulation.from_workload(W.reacting_channel(ni=16, nj=8), reacting=True) as sim:
+        _, c = sim.download(0)
+        with pytest.raises(_lib.E4CError) as err:
+            sim.upload_cons(0, c[:5].copy())
+        assert err.value.code == _lib.E4C_ERR_UNSUPPORTED
