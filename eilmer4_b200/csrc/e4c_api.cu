@@ -70,6 +70,8 @@ void Ctx::release() {
     // every device pointer above is now dangling: forget them all
     d_descs = nullptr;
     descs_cap = 0;
+    d_item_order = nullptr;
+    item_order_cap = 0;
     nfused = 0;
     fused_items = 0;
     descs_valid = false;

@@ -256,6 +256,37 @@ int Ctx::prepare_fused() {
         }
         E4C_CUDA(cudaMemcpyAsync(d_descs, ds.data(), sizeof(FusedDesc) * nfused,
                                  cudaMemcpyHostToDevice, stream));
+        // work items ordered by cost, costliest first (longest-processing-time
+        // order for the CTAs that take them from a counter): the cells a tile
+        // updates times its k-chunk length plus the four prologue planes
+        std::vector<std::pair<long long, int>> cost;
+        cost.reserve(size_t(items));
+        for (const FusedDesc& f : ds) {
+            for (int tj = 0; tj < f.tiles_j; ++tj)
+                for (int ti = 0; ti < f.tiles_i; ++ti)
+                    for (int kc = 0; kc < f.kchunks; ++kc) {
+                        const long long ci = std::min(tile_ti, f.ni - ti * tile_ti);
+                        const long long cj = std::min(tile_tj, f.nj - tj * tile_tj);
+                        const long long ck = std::min(tile_kc, f.nk - kc * tile_kc);
+                        const long long item =
+                            f.item0 + (long long)(tj * f.tiles_i + ti) * f.kchunks + kc;
+                        cost.push_back({-(ci * cj * (ck + 4)), int(item)});
+                    }
+        }
+        std::stable_sort(cost.begin(), cost.end());
+        if (items > item_order_cap) {
+            dfree(d_item_order);
+            d_item_order = static_cast<int*>(dalloc(sizeof(int) * size_t(items)));
+            if (!d_item_order) {
+                item_order_cap = 0;
+                return fail(E4C_ERR_CUDA, "cudaMalloc of the work-item order failed");
+            }
+            item_order_cap = items;
+        }
+        std::vector<int> order(cost.size());
+        for (size_t q = 0; q < cost.size(); ++q) order[q] = cost[q].second;
+        E4C_CUDA(cudaMemcpyAsync(d_item_order, order.data(), sizeof(int) * order.size(),
+                                 cudaMemcpyHostToDevice, stream));
         E4C_CUDA(cudaStreamSynchronize(stream));
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg.device);
@@ -272,7 +303,7 @@ int Ctx::prepare_fused() {
 }
 
 void Ctx::fused_stage_all(int stage) {
-    FusedLaunch L{d_descs, nfused, fused_items, tile_kc, tile_ti, tile_tj, fused_grid};
+    FusedLaunch L{d_descs, nfused, fused_items, tile_kc, tile_ti, tile_tj, fused_grid, d_item_order};
     if (cfg.precision == E4C_PREC_FP32_FLUX) f32::fused_stage(L, d_sim, gas, fopts, stage, stream);
     else f64::fused_stage(L, d_sim, gas, fopts, stage, stream);
 }

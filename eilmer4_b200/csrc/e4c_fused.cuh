@@ -335,8 +335,12 @@ struct FusedShareVA {
 template <typename R, int FLUX, int TI, int TJ>
 __global__ void __launch_bounds__(FusedThreads<TI, TJ>::total, FusedMinBlocks<R, TI, TJ>::value)
 k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems, int kc,
-              SimDev* sim, GasConsts gas, FluxOpts o, int stage) {
+              SimDev* sim, GasConsts gas, FluxOpts o, int stage, const int* __restrict__ order) {
     if (sim->status != 0 || sim->finished) return;
+    // CTAs take work items from a counter, costliest first; the other stage's
+    // counter is reset for its next launch (it is not in use now)
+    if (blockIdx.x == 0 && threadIdx.x == 0) sim->item_next[stage == 1 ? 1 : 0] = 0u;
+    __shared__ unsigned int s_item;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using S = FusedSmem<R, TI, TJ>;
     constexpr int PI = S::PI, PJ = S::PJ, FS = PI * PJ;
@@ -351,7 +355,12 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
     const double dt = sim->dt_global;
     int bad = 0;
 
-    for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
+    for (;;) {
+        __syncthreads();  // s_item of the previous item has been read by all
+        if (threadIdx.x == 0) s_item = atomicAdd(&sim->item_next[stage == 1 ? 0 : 1], 1u);
+        __syncthreads();
+        if (s_item >= (unsigned long long)nitems) break;
+        const long long item = order[s_item];
         const int b = find_block(descs, nblocks, item);
         const FusedDesc& d = descs[b];
         long long local = item - d.item0;

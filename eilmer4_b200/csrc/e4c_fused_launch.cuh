@@ -26,7 +26,8 @@ static int launch_one(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, c
         attr_set = true;
     }
     k_fused_stage<RT, FLUX, TI, TJ><<<L.grid, FusedThreads<TI, TJ>::total, smem, s>>>(
-        static_cast<const FusedDesc*>(L.descs), L.nblocks, L.nitems, L.kc, sim, gas, o, stage);
+        static_cast<const FusedDesc*>(L.descs), L.nblocks, L.nitems, L.kc, sim, gas, o, stage,
+        L.order);
     return 0;
 }
 

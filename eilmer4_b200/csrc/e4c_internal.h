@@ -95,6 +95,8 @@ struct Ctx {
     // fused path: descriptors of every fused block, rebuilt when blocks change
     FusedDesc* d_descs = nullptr;
     int descs_cap = 0;
+    int* d_item_order = nullptr;    // fused work items, costliest first
+    long long item_order_cap = 0;
     int nfused = 0;
     long long fused_items = 0;
     bool descs_valid = false;

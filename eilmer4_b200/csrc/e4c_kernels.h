@@ -83,6 +83,7 @@ struct FusedLaunch {
     int kc;                 // k-chunk length
     int ti, tj;             // tile shape
     int grid;               // persistent CTAs
+    const int* order;       // work items, costliest first (device array of nitems)
 };
 
 #define E4C_DECLARE_FUSED(NS)                                                                \

@@ -80,6 +80,8 @@ struct SimDev {
     int bad_cells;                  // invalid cells counted in the last stage
     int finished;                   // set when time >= max_time
     int pad_;
+    unsigned int item_next[2];      // work-item counters of the fused stages 1 and 2
+    unsigned int pad2_[2];
 };
 
 // Per-block descriptor of the fused uniform path (device array, one entry per
