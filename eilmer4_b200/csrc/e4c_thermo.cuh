@@ -206,6 +206,26 @@ static __device__ E4C_CEA_FN double cea_h(const e4c_thermochem& tc, int isp, dou
     return cea_h_in_range(tc, isp, R, T, lT);
 }
 
+// cea_h and cea_Cp of one species at one temperature with one coefficient
+// selection (the same operations as the two functions)
+static __device__ E4C_CEA_FN void cea_h_Cp(const e4c_thermochem& tc, int isp, double R, double T,
+                                          double lT, double& h, double& Cp) {
+    const int nseg = tc.nseg[isp];
+    if (T < tc.T_break[isp][0] || T > tc.T_break[isp][nseg]) {
+        h = cea_h(tc, isp, R, T, lT);
+        Cp = cea_Cp(tc, isp, R, T);
+        return;
+    }
+    double a[9];
+    cea_coefficients(tc, isp, T, a);
+    double Cp_on_R = a[0] / (T * T) + a[1] / T + a[2] + a[3] * T;
+    Cp_on_R += a[4] * T * T + a[5] * T * T * T + a[6] * T * T * T * T;
+    Cp = R * Cp_on_R;
+    double h_on_RT = -a[0] / (T * T) + a[1] / T * lT + a[2] + a[3] * T / 2.0;
+    h_on_RT += a[4] * T * T / 3.0 + a[5] * T * T * T / 4.0 + a[6] * T * T * T * T / 5.0 + a[7] / T;
+    h = R * T * h_on_RT;
+}
+
 // ---------------------------------------------------------------------------
 // Thermally perfect mixture
 // ---------------------------------------------------------------------------
@@ -237,6 +257,20 @@ struct TPGas {
         for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], T, lT) - R[i] * T;
         return mass_average(massf, e);
     }
+    // energy(massf, T) and dudT(massf, T) together
+    __device__ void energy_dudT(const double* massf, double T, double& u, double& du) const {
+        double e[NSP], v[NSP];
+        const double lT = pm_log(T);
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) {
+            double h, cp;
+            cea_h_Cp(tc, i, R[i], T, lT, h, cp);
+            e[i] = h - R[i] * T;
+            v[i] = cp - R[i];
+        }
+        u = mass_average(massf, e);
+        du = -1.0 * mass_average(massf, v);
+    }
     __device__ double dudT(const double* massf, double T) const {
         double v[NSP];
 #pragma unroll
@@ -260,9 +294,9 @@ struct TPGas {
         double rts = x0;
         double dxold = (xMax - xMin);
         double dx = dxold;
-        Q.T = rts; Q.u = energy(Q.massf, Q.T);
+        double df0;
+        Q.T = rts; energy_dudT(Q.massf, Q.T, Q.u, df0);
         double f0 = e_tgt - Q.u;
-        double df0 = dudT(Q.massf, rts);
         for (int j = 0; j < MAXIT; ++j) {
             if ((((rts - xH) * df0 - f0) * ((rts - xL) * df0 - f0) > 0.0) ||
                 (fabs(2.0 * f0) > fabs(dxold * df0))) {
@@ -278,9 +312,8 @@ struct TPGas {
                 if (tmp == rts) { root = rts; return true; }
             }
             if (fabs(dx) < tol) { root = rts; return true; }
-            Q.T = rts; Q.u = energy(Q.massf, Q.T);
+            Q.T = rts; energy_dudT(Q.massf, Q.T, Q.u, df0);
             f0 = e_tgt - Q.u;
-            df0 = dudT(Q.massf, rts);
             if (f0 < 0.0) xL = rts;
             else xH = rts;
         }
