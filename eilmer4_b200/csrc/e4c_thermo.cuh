@@ -235,6 +235,13 @@ struct TPState {
     double massf[NSP];
 };
 
+// kappa of the bracket-sign shortcut of TPGas::solve_T, 0 when off: the
+// installed curves raise each species' energy e(T) = h(T) - R T by at least
+// 2 kappa Cv(x0) per kelvin anywhere within 1000 K of x0, for brackets up to
+// 101,000 K (checked on the host when they are installed,
+// set_thermochem_constants)
+static __constant__ double c_bracket_kappa = 0.0;
+
 template <int NSP>
 struct TPGas {
     const e4c_thermochem& tc;
@@ -278,14 +285,38 @@ struct TPGas {
         return -1.0 * mass_average(massf, v);
     }
     // nm/newton.d:40-99, f(T) = e_tgt - u(T); Q.T and Q.u follow every evaluation
+    //
+    // shortcut: the energies at the bracket ends serve only for their signs
+    // (and zero tests).  With e = e_tgt - u(x0) and Cv = Cv(x0), the mixture's
+    // u rises at no less than 2 kappa Cv per kelvin within the bracket, so
+    // 0 <= e < kappa Cv (xMax - x0) gives e_tgt - u(xMin) > 0 > e_tgt - u(xMax)
+    // (and likewise for e < 0), by margins of at least kappa Cv K that no
+    // rounding reaches: those two evaluations are then skipped, with the same
+    // outcome as when they are made.
     __device__ bool solve_T(TPState<NSP>& Q, double e_tgt, double x0, double xMin, double xMax,
-                            double tol, double& root) const {
+                            double tol, double& root, bool shortcut = false) const {
         const int MAXIT = 30;
         double xL = xMin, xH = xMax;
-        Q.T = xL; Q.u = energy(Q.massf, Q.T);
-        double fL = e_tgt - Q.u;
-        Q.T = xH; Q.u = energy(Q.massf, Q.T);
-        double fH = e_tgt - Q.u;
+        double fL = 0.0, fH = 0.0, u0 = 0.0, df0 = 0.0;
+        bool have0 = false, signs = false;
+        const double kappa = c_bracket_kappa;
+        if (shortcut && kappa > 0.0 && x0 - xMin >= 1.0 && xMax - x0 >= 1.0 && xMax <= 101000.0) {
+            energy_dudT(Q.massf, x0, u0, df0);
+            have0 = true;
+            const double e = e_tgt - u0, cv = -df0;
+            if (cv > 0.0 && ((e >= 0.0 && e < kappa * cv * (xMax - x0)) ||
+                             (e < 0.0 && -e < kappa * cv * (x0 - xMin)))) {
+                fL = 1.0;
+                fH = -1.0;
+                signs = true;
+            }
+        }
+        if (!signs) {
+            Q.T = xL; Q.u = energy(Q.massf, Q.T);
+            fL = e_tgt - Q.u;
+            Q.T = xH; Q.u = energy(Q.massf, Q.T);
+            fH = e_tgt - Q.u;
+        }
         if ((fL > 0.0 && fH > 0.0) || (fL < 0.0 && fH < 0.0)) return false;
         if (fL == 0.0) { root = xMin; return true; }
         if (fH == 0.0) { root = xMax; return true; }
@@ -294,8 +325,8 @@ struct TPGas {
         double rts = x0;
         double dxold = (xMax - xMin);
         double dx = dxold;
-        double df0;
-        Q.T = rts; energy_dudT(Q.massf, Q.T, Q.u, df0);
+        if (!have0) energy_dudT(Q.massf, rts, u0, df0);
+        Q.T = rts; Q.u = u0;
         double f0 = e_tgt - Q.u;
         for (int j = 0; j < MAXIT; ++j) {
             if ((((rts - xH) * df0 - f0) * ((rts - xL) * df0 - f0) > 0.0) ||
@@ -326,7 +357,7 @@ struct TPGas {
         double T1 = fmax(Q.T - 0.5 * 1000.0, 20.0);
         double T2 = T1 + 1000.0;
         double root;
-        if (solve_T(Q, e_tgt, Tsave, T1, T2, 1.0e-6, root)) { Q.T = root; return true; }
+        if (solve_T(Q, e_tgt, Tsave, T1, T2, 1.0e-6, root, true)) { Q.T = root; return true; }
         if (solve_T(Q, e_tgt, Tsave, 20.0, 100000.0, 1.0e-6, root)) { Q.T = root; return true; }
         Q.T = Tsave;
         Q.u = energy(Q.massf, Q.T);

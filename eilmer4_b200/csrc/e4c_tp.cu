@@ -5,12 +5,101 @@
 //
 // Compiled with -fmad=false, as e4c_general.cu: the results match the CPU
 // FP64 oracle bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "e4c_cells.cuh"
 
 namespace e4c {
 
+// Host check for the bracket-sign shortcut of TPGas::solve_T: the least
+// slope of each species' energy e(T) = h(T) - R T, as the device evaluates h
+// (blended segments, linear continuation beyond the curves), over any window
+// of +-1000 K around x0, divided by Cv(x0) (Cp clamped to the curves, minus R);
+// on a 0.25 K grid from 20 K to 101,500 K, slopes taken as the minimum over
+// 100 K blocks that meet the window (a lower bound of the window minimum).
+// Returns the smallest ratio over the species, or 0 if a Cv is not positive.
+namespace {
+void host_coeffs(const e4c_thermochem& tc, int s, double T, double a[9]) {
+    const int ns = tc.nseg[s];
+    const double* tb = tc.T_break[s];
+    const double* bl = tc.T_blend[s];
+    if (T < tb[1] - 0.5 * bl[0]) { for (int j = 0; j < 9; ++j) a[j] = tc.coeffs[s][0][j]; return; }
+    if (T > tb[ns - 1] + 0.5 * bl[ns - 2]) {
+        for (int j = 0; j < 9; ++j) a[j] = tc.coeffs[s][ns - 1][j];
+        return;
+    }
+    for (int i = 1; i < ns; ++i) {
+        const double lo = tb[i] - 0.5 * bl[i - 1], hi = tb[i] + 0.5 * bl[i - 1];
+        if (T >= lo && T <= hi) {
+            const double wB = (T - lo) / bl[i - 1];
+            for (int j = 0; j < 9; ++j) a[j] = (1.0 - wB) * tc.coeffs[s][i - 1][j] + wB * tc.coeffs[s][i][j];
+            return;
+        }
+        if (T > hi && T < tb[i + 1] - 0.5 * bl[i]) {
+            for (int j = 0; j < 9; ++j) a[j] = tc.coeffs[s][i][j];
+            return;
+        }
+    }
+    for (int j = 0; j < 9; ++j) a[j] = 0.0;
+}
+double host_cp(const e4c_thermochem& tc, int s, double R, double T) {
+    T = std::min(std::max(T, tc.T_break[s][0]), tc.T_break[s][tc.nseg[s]]);
+    double a[9];
+    host_coeffs(tc, s, T, a);
+    return R * (a[0] / (T * T) + a[1] / T + a[2] + a[3] * T + a[4] * T * T + a[5] * T * T * T +
+                a[6] * T * T * T * T);
+}
+double host_h_in(const e4c_thermochem& tc, int s, double R, double T) {
+    double a[9];
+    host_coeffs(tc, s, T, a);
+    const double hrt = -a[0] / (T * T) + a[1] / T * std::log(T) + a[2] + a[3] * T / 2.0 +
+                       a[4] * T * T / 3.0 + a[5] * T * T * T / 4.0 +
+                       a[6] * T * T * T * T / 5.0 + a[7] / T;
+    return R * T * hrt;
+}
+double host_h(const e4c_thermochem& tc, int s, double R, double T) {
+    const double lo = tc.T_break[s][0], hi = tc.T_break[s][tc.nseg[s]];
+    if (T < lo) return host_h_in(tc, s, R, lo) - host_cp(tc, s, R, lo) * (lo - T);
+    if (T > hi) return host_h_in(tc, s, R, hi) + host_cp(tc, s, R, hi) * (T - hi);
+    return host_h_in(tc, s, R, T);
+}
+double bracket_slope_ratio(const e4c_thermochem& tc) {
+    const double T0 = 20.0, step = 0.25, Tend = 101500.0;
+    const int n = int((Tend - T0) / step) + 1;
+    const int per_block = 400, nblk = (n - 1 + per_block - 1) / per_block;
+    const int W = int(1000.0 / step);
+    double worst = 1.0e300;
+    std::vector<double> e(n), cv(n), bmin(nblk);
+    for (int s = 0; s < tc.nsp; ++s) {
+        const double R = 8.31451 / tc.M[s];
+        for (int k = 0; k < n; ++k) {
+            const double T = T0 + step * k;
+            e[k] = host_h(tc, s, R, T) - R * T;
+            cv[k] = host_cp(tc, s, R, T) - R;
+            if (!(cv[k] > 0.0)) return 0.0;
+        }
+        for (int b = 0; b < nblk; ++b) bmin[b] = 1.0e300;
+        for (int k = 0; k + 1 < n; ++k)
+            bmin[k / per_block] = std::min(bmin[k / per_block], (e[k + 1] - e[k]) / step);
+        for (int k = 0; k < n; ++k) {
+            const int b0 = std::max(0, k - W) / per_block;
+            const int b1 = std::min(n - 2, k + W) / per_block;
+            double m = 1.0e300;
+            for (int b = b0; b <= b1; ++b) m = std::min(m, bmin[b]);
+            worst = std::min(worst, m / cv[k]);
+        }
+    }
+    return worst;
+}
+}  // namespace
+
 int set_thermochem_constants(const e4c_thermochem& tc) {
-    return cudaMemcpyToSymbol(c_tc, &tc, sizeof(tc)) == cudaSuccess ? 0 : -1;
+    if (cudaMemcpyToSymbol(c_tc, &tc, sizeof(tc)) != cudaSuccess) return -1;
+    // the shortcut with kappa = 1/4 needs a slope ratio of at least 1/2
+    const double kappa = bracket_slope_ratio(tc) >= 0.5 ? 0.25 : 0.0;
+    return cudaMemcpyToSymbol(c_bracket_kappa, &kappa, sizeof(kappa)) == cudaSuccess ? 0 : -1;
 }
 
 // ---------------------------------------------------------------------------
