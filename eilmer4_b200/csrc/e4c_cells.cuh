@@ -115,6 +115,12 @@ static __device__ void replay_all_roundtrips(const BlockView& b, int ci, int cj,
         }
 }
 
+__device__ __forceinline__ void load_frame(const double* fg, size_t npad, size_t f, Frame<double>& fr) {
+    fr.n = {fg[0 * npad + f], fg[1 * npad + f], fg[2 * npad + f]};
+    fr.t1 = {fg[3 * npad + f], fg[4 * npad + f], fg[5 * npad + f]};
+    fr.t2 = {fg[6 * npad + f], fg[7 * npad + f], fg[8 * npad + f]};
+}
+
 // update_thermo_from_rhou of a reconstructed state: ideal gas, or the
 // thermally perfect mixture started from the cell-centre temperature (the
 // state was copied from the cell, onedinterp.d / sfluidblock.d:2199-2208)
@@ -163,55 +169,63 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
         int k = b.kmin + int(t / ((long long)ni * nj));
         const size_t f = pidx(b, i, j, k);
         const size_t cR0 = f, cL0 = f - stride, cL1 = f - 2 * stride, cR1 = f + stride;
+        const int fpos = dir == 0 ? i : (dir == 1 ? j : k);
+        const int di = dir == 0, dj = dir == 1, dk = dir == 2;
+        const bool replay = o.local_frame && !b.axis_frames;
         Frame<double> fr;
-        fr.n = {fg[0 * b.npad + f], fg[1 * b.npad + f], fg[2 * b.npad + f]};
-        fr.t1 = {fg[3 * b.npad + f], fg[4 * b.npad + f], fg[5 * b.npad + f]};
-        fr.t2 = {fg[6 * b.npad + f], fg[7 * b.npad + f], fg[8 * b.npad + f]};
-        Prim<double, NSP> sL1, sL0, sR0, sR1;
-        load_prim<NSP>(b, cL0, sL0);
-        load_prim<NSP>(b, cR0, sR0);
-        Prim<double, NSP> Lf = sL0, Rt = sR0;
+        load_frame(fg, b.npad, f, fr);
+        // a stencil cell's state as the reconstruction holds it: velocity after
+        // the earlier faces' round trips and in this face's frame
+        auto cell_state = [&](size_t c, int ci, int cj, int ck, Prim<double, NSP>& s) {
+            load_prim<NSP>(b, c, s);
+            if (o.order2) {
+                if (replay) replay_roundtrips(b, dir, fpos, ci, cj, ck, s.vel);
+                if (o.local_frame) to_local(s.vel, fr.n, fr.t1, fr.t2);
+            }
+        };
+        Prim<double, NSP> Lf, Rt;
+        cell_state(cL0, i - di, j - dj, k - dk, Lf);
+        cell_state(cR0, i, j, k, Rt);
         if (o.order2) {
-            load_prim<NSP>(b, cL1, sL1);
-            load_prim<NSP>(b, cR1, sR1);
-            if (o.local_frame && !b.axis_frames) {
-                const int fpos = dir == 0 ? i : (dir == 1 ? j : k);
-                const int di = dir == 0, dj = dir == 1, dk = dir == 2;
-                replay_roundtrips(b, dir, fpos, i - 2 * di, j - 2 * dj, k - 2 * dk, sL1.vel);
-                replay_roundtrips(b, dir, fpos, i - di, j - dj, k - dk, sL0.vel);
-                replay_roundtrips(b, dir, fpos, i, j, k, sR0.vel);
-                replay_roundtrips(b, dir, fpos, i + di, j + dj, k + dk, sR1.vel);
-            }
-            const double* len = b.cgeom + size_t(1 + dir) * b.npad;
-            if (o.local_frame) {
-                to_local(sL1.vel, fr.n, fr.t1, fr.t2);
-                to_local(sL0.vel, fr.n, fr.t1, fr.t2);
-                to_local(sR0.vel, fr.n, fr.t1, fr.t2);
-                to_local(sR1.vel, fr.n, fr.t1, fr.t2);
-            }
-            L2R2<double> r;
-            r.prepare(len[cL1], len[cL0], len[cR0], len[cR1]);
-            r.scalar(o.limiter, o.clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
-            r.scalar(o.limiter, o.clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
-            r.scalar(o.limiter, o.clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
-            if (NSP > 1) {
+            {
+                // the outer cells live only for the reconstruction; the inner
+                // ones are reloaded where the reference falls back on them
+                Prim<double, NSP> sL1, sL0 = Lf, sR0 = Rt, sR1;
+                cell_state(cL1, i - 2 * di, j - 2 * dj, k - 2 * dk, sL1);
+                cell_state(cR1, i + di, j + dj, k + dk, sR1);
+                const double* len = b.cgeom + size_t(1 + dir) * b.npad;
+                L2R2<double> r;
+                r.prepare(len[cL1], len[cL0], len[cR0], len[cR1]);
+                r.scalar(o.limiter, o.clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
+                r.scalar(o.limiter, o.clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
+                r.scalar(o.limiter, o.clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
+                if (NSP > 1) {
 #pragma unroll
-                for (int q = 0; q < NSP; ++q)
-                    r.scalar(o.limiter, o.clip, sL1.massf[q], sL0.massf[q], sR0.massf[q],
-                             sR1.massf[q], Lf.massf[q], Rt.massf[q]);
-                if (!scale_mass_fractions<double, NSP>(Lf.massf))
-                    for (int q = 0; q < NSP; ++q) Lf.massf[q] = sL0.massf[q];
-                if (!scale_mass_fractions<double, NSP>(Rt.massf))
-                    for (int q = 0; q < NSP; ++q) Rt.massf[q] = sR0.massf[q];
-            } else {
-                Lf.massf[0] = 1.0;
-                Rt.massf[0] = 1.0;
+                    for (int q = 0; q < NSP; ++q)
+                        r.scalar(o.limiter, o.clip, sL1.massf[q], sL0.massf[q], sR0.massf[q],
+                                 sR1.massf[q], Lf.massf[q], Rt.massf[q]);
+                    if (!scale_mass_fractions<double, NSP>(Lf.massf))
+                        for (int q = 0; q < NSP; ++q) Lf.massf[q] = sL0.massf[q];
+                    if (!scale_mass_fractions<double, NSP>(Rt.massf))
+                        for (int q = 0; q < NSP; ++q) Rt.massf[q] = sR0.massf[q];
+                } else {
+                    Lf.massf[0] = 1.0;
+                    Rt.massf[0] = 1.0;
+                }
+                r.scalar(o.limiter, o.clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
+                r.scalar(o.limiter, o.clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
             }
-            r.scalar(o.limiter, o.clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
-            r.scalar(o.limiter, o.clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
-            // codeForThermoUpdateBoth("rhou"), onedinterp.d:1039-1068
-            if (!rhou_update<NSP, GAS>(o, Lf)) Lf = sL0;
-            if (!rhou_update<NSP, GAS>(o, Rt)) Rt = sR0;
+            // codeForThermoUpdateBoth("rhou"), onedinterp.d:1039-1068: on failure
+            // the cell-centre state (its velocity as above) is taken
+            if (!rhou_update<NSP, GAS>(o, Lf)) {
+                load_frame(fg, b.npad, f, fr);
+                cell_state(cL0, i - di, j - dj, k - dk, Lf);
+            }
+            if (!rhou_update<NSP, GAS>(o, Rt)) {
+                load_frame(fg, b.npad, f, fr);
+                cell_state(cR0, i, j, k, Rt);
+            }
+            load_frame(fg, b.npad, f, fr);
             if (o.local_frame) {
                 to_global(Lf.vel, fr.n, fr.t1, fr.t2);
                 to_global(Rt.vel, fr.n, fr.t1, fr.t2);
