@@ -141,6 +141,10 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
 int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, double* massf,
                     double* dt_chem);
 
+/* Production and loss rates (mol/m^3/s) of every species at temperature T and
+ * concentrations c (mol/m^3). */
+int e4o_rates(const e4o_thermochem* tc, double T, const double* c, double* q, double* L);
+
 /* The host side of the reference's GPU chemistry (GPUChem, cuda_gpu_chem.d)
  * around its alpha-QSS kernel, for n cells in SoA arrays (species or reaction
  * outer): prepare gives the kernel's inputs, finish applies its outputs. */

@@ -83,9 +83,11 @@ class ThermoChem(ctypes.Structure):
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (g++, no GPU needed)."""
-    if force or not os.path.exists(_LIB_PATH):
-        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile the oracle with its Makefile (g++, no GPU needed; make rebuilds
+    only when a source is newer than the library)."""
+    if force and os.path.exists(_LIB_PATH):
+        os.remove(_LIB_PATH)
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
 
@@ -123,6 +125,7 @@ def lib():
         L.e4o_tp_update.argtypes = [P(ThermoChem), ip, P(dp), P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
+        L.e4o_rates.argtypes = [P(ThermoChem), dp, P(dp), P(dp), P(dp)]
         L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
         L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
         _lib = L
@@ -305,3 +308,13 @@ def gpuchem_finish(thermochem, conc, h, rho, T, u, p):
     rc = lib().e4o_gpuchem_finish(ctypes.byref(tc), n, _dptr(conc), _dptr(h), _dptr(rho),
                                   _dptr(T), _dptr(u), _dptr(p), _dptr(mf), _dptr(dc))
     return rc, {"massf": mf, "T": T, "u": u, "p": p, "dt_chem": dc}
+
+
+def rates(thermochem, T, conc):
+    """Production and loss rates (q, L) of every species at T and conc."""
+    tc = thermochem.fill(ThermoChem())
+    c = np.ascontiguousarray(conc, dtype=np.float64)
+    q = np.zeros(thermochem.nsp)
+    L = np.zeros(thermochem.nsp)
+    lib().e4o_rates(ctypes.byref(tc), float(T), _dptr(c), _dptr(q), _dptr(L))
+    return q, L

@@ -712,6 +712,16 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
     return 0;
 }
 
+// Production and loss rates of every species at temperature T and
+// concentrations c (eval_rate_constants then eval_split_rates,
+// reaction_mechanism.d:47-82): golden-vector tests of the rate machinery.
+int e4o_rates(const e4o_thermochem* tc, double T, const double* c, double* q, double* L) {
+    Mech m(*tc);
+    m.eval_rate_constants(T);
+    m.split_rates(c, q, L);
+    return 0;
+}
+
 // GPUChem.prepareDataForGPU (src/eilmer/cuda_gpu_chem.d:183-205): per cell,
 // one after another as the D host does, the concentrations (massf2conc,
 // gas_model.d:196-212), the rate constants at the cell's temperature and the

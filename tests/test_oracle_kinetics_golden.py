@@ -1,0 +1,64 @@
+"""The oracle's rate machinery against the reference's own kinetics tests on
+the hydrogen-iodide system (src/kinetics/sample-input/H2-I2-HI.lua,
+H2-I2-inp.lua):
+
+* reaction.d:475-493 -- H2 + I2 -> 2 HI with k = 1.94e14 exp(-20620/T) both
+  ways at 700 K and concentrations (4.54, 4.54, 0): HI produced at
+  1287.8606, H2 and I2 lost at 643.9303 mol/m^3/s (relative 1e-6);
+* chemistry_update.d:659-733 -- the same system with the mechanism's rate
+  constants from 4.54 mol/m^3 each of H2 and I2 at 700 K: the analytic HI
+  concentration after 60,000 s is 7.1420197868416215 mol/m^3.  The oracle's
+  point-implicit update, repeated over shorter intervals, converges to it at
+  first order (it is one backward-Euler step per interval)."""
+import numpy as np
+import pytest
+
+M = np.array([0.00201588, 0.25380894, 0.12791241])   # H2, I2, HI (kg/mol)
+
+
+def h2_i2(A_f, C_f, A_b, C_b):
+    from eilmer4_b200.thermochem import ThermoChem
+    nsp, maxseg = 3, 4
+    T_break = np.zeros((nsp, maxseg + 1))
+    T_break[:, 0], T_break[:, 1] = 200.0, 20000.0
+    coeffs = np.zeros((nsp, maxseg, 9))
+    coeffs[:, 0, 2] = 3.5          # Cp/R = 3.5 (not used by the rate tests)
+    return ThermoChem(
+        species=["H2", "I2", "HI"], M=M.copy(), nseg=np.ones(nsp, dtype=np.int32),
+        T_break=T_break, T_blend=np.zeros((nsp, maxseg)), coeffs=coeffs,
+        A_f=np.array([A_f]), n_f=np.array([0.0]), C_f=np.array([C_f]),
+        A_b=np.array([A_b]), n_b=np.array([0.0]), C_b=np.array([C_b]),
+        nu_r=np.array([[1, 1, 0]], dtype=np.int32), nu_p=np.array([[0, 0, 2]], dtype=np.int32),
+        third_body=np.array([0], dtype=np.int32), eff=np.zeros((1, nsp)),
+        T_lower=300.0, T_upper=50000.0)
+
+
+def test_elementary_reaction_rates_golden(oracle):
+    tc = h2_i2(1.94e14, 20620.0, 1.94e14, 20620.0)
+    q, L = oracle.rates(tc, 700.0, [4.54, 4.54, 0.0])
+    assert q[0] == 0.0 and q[1] == 0.0 and L[2] == 0.0
+    assert q[2] == pytest.approx(1287.8606, rel=1e-6)
+    assert L[0] == pytest.approx(643.9303, rel=1e-6)
+    assert L[1] == pytest.approx(643.9303, rel=1e-6)
+
+
+def test_hydrogen_iodide_update_converges_to_the_analytic_value(oracle):
+    tc = h2_i2(1.93e8, 20620.0, 5.470705805110e-07, 0.0)
+    T, c0, t_end = 700.0, 4.54, 60000.0
+    analytic = 7.1420197868416215
+    conc0 = np.array([c0, c0, 0.0])
+    rho = float(conc0 @ M)
+    errs = []
+    for n in (200, 400, 800):
+        y = conc0 * M / rho
+        dtc = -1.0
+        for _ in range(n):
+            rc, y = oracle.chem_update(tc, t_end / n, rho, T, y, dtc)
+            assert rc == 0
+        c_hi = y[2] * rho / M[2]
+        errs.append(c_hi - analytic)
+    # first order: the error halves with the interval
+    assert 1.8 < errs[0] / errs[1] < 2.2 and 1.8 < errs[1] / errs[2] < 2.2, errs
+    assert abs(errs[2]) < 1e-3 * analytic, errs
+    # Richardson extrapolation of the two finest runs lands on the analytic value
+    assert abs((2.0 * (errs[2] + analytic) - (errs[1] + analytic)) - analytic) < 1e-5 * analytic
