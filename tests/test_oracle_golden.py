@@ -175,3 +175,59 @@ def test_reacting_channel_oracle_runs(oracle):
     prim, cons = sim.get_flow(0)
     assert np.all(np.isfinite(prim)) and prim[5].max() > 300.0
     assert np.allclose(prim[8:].sum(axis=0), 1.0, atol=1e-12)
+
+
+def _thermo_only(species):
+    """A ThermoChem with the given species' curves and no reactions."""
+    from eilmer4_b200.thermochem import ThermoChem
+    nsp, maxseg = len(species), 4
+    T_break = np.zeros((nsp, maxseg + 1))
+    T_blend = np.zeros((nsp, maxseg))
+    coeffs = np.zeros((nsp, maxseg, 9))
+    for i, s in enumerate(species):
+        n = len(s["coeffs"])
+        T_break[i, :n + 1] = s["T_break"]
+        T_blend[i, :n - 1] = s["T_blend"]
+        coeffs[i, :n] = s["coeffs"]
+    return ThermoChem(
+        species=[s["name"] for s in species], M=np.array([s["M"] for s in species]),
+        nseg=np.array([len(s["coeffs"]) for s in species], dtype=np.int32),
+        T_break=T_break, T_blend=T_blend, coeffs=coeffs,
+        A_f=np.zeros(0), n_f=np.zeros(0), C_f=np.zeros(0), A_b=np.zeros(0), n_b=np.zeros(0),
+        C_b=np.zeros(0), nu_r=np.zeros((0, nsp), dtype=np.int32),
+        nu_p=np.zeros((0, nsp), dtype=np.int32), third_body=np.zeros(0, dtype=np.int32),
+        eff=np.zeros((0, nsp)), T_lower=300.0, T_upper=50000.0)
+
+
+def test_cea_curve_of_atomic_oxygen_golden(oracle):
+    """cea_thermo_curves.d:173-189 (sample-data/O-thermo.lua, the same curves as
+    the air data's O): Cp(500 K) = 1328.627 J/kg/K, h(3700 K) = 20030794.683 J/kg.
+    The oracle's pure-O mixture gives h = u + R T and Cp from its frozen sound
+    speed, a^2 = gamma R T."""
+    from eilmer4_b200.thermochem import load_air5
+    tc = load_air5()
+    y = np.zeros(tc.nsp)
+    y[tc.species.index("O")] = 1.0
+    R = 8.31451 / 0.0159994
+    s = oracle.tp_update(tc, 2, y, rho=0.1, T=3700.0)
+    assert s["u"] + R * 3700.0 == pytest.approx(20030794.683, rel=1e-6)
+    s = oracle.tp_update(tc, 2, y, rho=0.1, T=500.0)
+    gamma = s["a"] ** 2 / (R * 500.0)
+    assert gamma * R / (gamma - 1.0) == pytest.approx(1328.627, rel=1e-6)
+
+
+def test_mixture_eos_golden(oracle):
+    """therm_perf_gas_mix_eos.d:179-200 (sample-data/O2-N2-H2.lua, extracted to
+    tests/golden/o2_n2_h2_thermo.json by tests/golden/make_o2_n2_h2.py): mass
+    fractions 0.2, 0.7, 0.1 at 1000 K give u = 1031849.875 J/kg, and the
+    temperature iteration started from 1500 K returns 1000 K."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "o2_n2_h2_thermo.json")
+    with open(path) as f:
+        tc = _thermo_only(json.load(f)["species"])
+    y = [0.2, 0.7, 0.1]
+    s = oracle.tp_update(tc, 2, y, rho=1.0, T=1000.0)
+    assert s["u"] == pytest.approx(1031849.875, rel=1e-6)
+    s2 = oracle.tp_update(tc, 1, y, rho=1.0, u=s["u"], T=1500.0)
+    assert s2["T"] == pytest.approx(1000.0, rel=1e-6)
