@@ -141,6 +141,9 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
 int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, double* massf,
                     double* dt_chem);
 
+/* The reference's Newton-solver unit-test problems (which = 0 or 1). */
+int e4o_newton_test(int which, double* root);
+
 /* Production and loss rates (mol/m^3/s) of every species at temperature T and
  * concentrations c (mol/m^3). */
 int e4o_rates(const e4o_thermochem* tc, double T, const double* c, double* q, double* L);

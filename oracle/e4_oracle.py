@@ -126,6 +126,7 @@ def lib():
         L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
         L.e4o_rates.argtypes = [P(ThermoChem), dp, P(dp), P(dp), P(dp)]
+        L.e4o_newton_test.argtypes = [ip, P(dp)]
         L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
         L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
         _lib = L
@@ -318,3 +319,10 @@ def rates(thermochem, T, conc):
     L = np.zeros(thermochem.nsp)
     lib().e4o_rates(ctypes.byref(tc), float(T), _dptr(c), _dptr(q), _dptr(L))
     return q, L
+
+
+def newton_test(which):
+    """Root of the reference's Newton unit-test problem `which` (0 or 1)."""
+    r = ctypes.c_double()
+    rc = lib().e4o_newton_test(int(which), ctypes.byref(r))
+    return rc, r.value

@@ -172,6 +172,49 @@ static double eval_h(const e4o_thermochem& tc, int isp, double R, double T) {
 // ---------------------------------------------------------------------------
 // Thermally perfect mixture (therm_perf_gas.d and the mixture EOS files)
 // ---------------------------------------------------------------------------
+// nm/newton.d:40-99 (rtsafe after Numerical Recipes): Newton's method
+// safeguarded by bisection within a bracket; returns false where the reference
+// throws (no bracket, no convergence in 30 iterations).
+template <class F, class DF>
+static bool rtsafe(F&& f, DF&& dfdx, double x0, double xMin, double xMax, double tol,
+                   double& root) {
+    const int MAXIT = 30;
+    double xL = xMin, xH = xMax;
+    double fL = f(xL);
+    double fH = f(xH);
+    if ((fL > 0.0 && fH > 0.0) || (fL < 0.0 && fH < 0.0)) return false;
+    if (fL == 0.0) { root = xMin; return true; }
+    if (fH == 0.0) { root = xMax; return true; }
+    if (fL < 0.0) { xL = xMin; xH = xMax; }
+    else { xH = xMin; xL = xMax; }
+    double rts = x0;
+    double dxold = (xMax - xMin);
+    double dx = dxold;
+    double f0 = f(rts);
+    double df0 = dfdx(rts);
+    for (int j = 0; j < MAXIT; ++j) {
+        if ((((rts - xH) * df0 - f0) * ((rts - xL) * df0 - f0) > 0.0) ||
+            (std::fabs(2.0 * f0) > std::fabs(dxold * df0))) {
+            dxold = dx;
+            dx = 0.5 * (xH - xL);
+            rts = xL + dx;
+            if (xL == rts) { root = rts; return true; }
+        } else {
+            dxold = dx;
+            dx = f0 / df0;
+            double tmp = rts;
+            rts -= dx;
+            if (tmp == rts) { root = rts; return true; }
+        }
+        if (std::fabs(dx) < tol) { root = rts; return true; }
+        f0 = f(rts);
+        df0 = dfdx(rts);
+        if (f0 < 0.0) xL = rts;
+        else xH = rts;
+    }
+    return false;
+}
+
 struct TP {
     const e4o_thermochem& tc;
     double R[E4O_MAXSP];
@@ -212,41 +255,7 @@ struct TP {
             for (int i = 0; i < tc.nsp; ++i) v[i] = eval_Cp(tc, i, R[i], T) - R[i];
             return -1.0 * mass_average(Q, v);
         };
-        const int MAXIT = 30;
-        double xL = xMin, xH = xMax;
-        double fL = f(xL);
-        double fH = f(xH);
-        if ((fL > 0.0 && fH > 0.0) || (fL < 0.0 && fH < 0.0)) return false;
-        if (fL == 0.0) { root = xMin; return true; }
-        if (fH == 0.0) { root = xMax; return true; }
-        if (fL < 0.0) { xL = xMin; xH = xMax; }
-        else { xH = xMin; xL = xMax; }
-        double rts = x0;
-        double dxold = (xMax - xMin);
-        double dx = dxold;
-        double f0 = f(rts);
-        double df0 = dfdx(rts);
-        for (int j = 0; j < MAXIT; ++j) {
-            if ((((rts - xH) * df0 - f0) * ((rts - xL) * df0 - f0) > 0.0) ||
-                (std::fabs(2.0 * f0) > std::fabs(dxold * df0))) {
-                dxold = dx;
-                dx = 0.5 * (xH - xL);
-                rts = xL + dx;
-                if (xL == rts) { root = rts; return true; }
-            } else {
-                dxold = dx;
-                dx = f0 / df0;
-                double tmp = rts;
-                rts -= dx;
-                if (tmp == rts) { root = rts; return true; }
-            }
-            if (std::fabs(dx) < tol) { root = rts; return true; }
-            f0 = f(rts);
-            df0 = dfdx(rts);
-            if (f0 < 0.0) xL = rts;
-            else xH = rts;
-        }
-        return false;
+        return rtsafe(f, dfdx, x0, xMin, xMax, tol, root);
     }
     // ThermallyPerfectGasMixEOS.update_temperature (therm_perf_gas_mix_eos.d:70-150)
     bool update_temperature(GasState& Q) const {
@@ -710,6 +719,25 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
     *T = Q.T; *u = Q.u; *p = Q.p;
     for (int i = 0; i < tc->nsp; ++i) massf[i] = Q.massf[i];
     return 0;
+}
+
+// The two problems of the reference's Newton-solver unit test
+// (nm/newton.d:109-135), solved by the same rtsafe the temperature iteration
+// uses: x^3 + x^2 - 3x - 3 on [-5, 5] from 1, and 3x + sin(x) - exp(x) on
+// [0, 1] from 0.2, with the solver's default tolerance 1e-9.
+int e4o_newton_test(int which, double* root) {
+    bool ok;
+    if (which == 0) {
+        ok = rtsafe([](double x) { return x * x * x + x * x - 3.0 * x - 3.0; },
+                    [](double x) { return 3.0 * x * x + 2.0 * x - 3.0; }, 1.0, -5.0, 5.0, 1.0e-9,
+                    *root);
+    } else {
+        const double a = 3.0;
+        ok = rtsafe([&](double x) { return a * x + std::sin(x) - std::exp(x); },
+                    [&](double x) { return a + std::cos(x) - std::exp(x); }, 0.2, 0.0, 1.0, 1.0e-9,
+                    *root);
+    }
+    return ok ? 0 : E4O_ERR_THERMO;
 }
 
 // Production and loss rates of every species at temperature T and

@@ -62,3 +62,12 @@ def test_hydrogen_iodide_update_converges_to_the_analytic_value(oracle):
     assert abs(errs[2]) < 1e-3 * analytic, errs
     # Richardson extrapolation of the two finest runs lands on the analytic value
     assert abs((2.0 * (errs[2] + analytic) - (errs[1] + analytic)) - analytic) < 1e-5 * analytic
+
+
+def test_newton_solver_golden(oracle):
+    """nm/newton.d:109-135: the safeguarded Newton method (the one the
+    mixture's temperature iteration uses) finds 1.732051 and 0.3604217."""
+    rc, r = oracle.newton_test(0)
+    assert rc == 0 and abs(r - 1.732051) < 1e-5
+    rc, r = oracle.newton_test(1)
+    assert rc == 0 and abs(r - 0.3604217) < 1e-5
