@@ -62,6 +62,7 @@ class E4CConfig(ctypes.Structure):
         ("use_graphs", ctypes.c_int),
         ("shear_tolerance", ctypes.c_double),
         ("compression_tolerance", ctypes.c_double),
+        ("chem_newton_iterations", ctypes.c_int),
     ]
 
 

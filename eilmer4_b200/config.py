@@ -41,6 +41,7 @@ CONFIG_DEFAULTS = {
     "strang_splitting": "full_T_full_R",          # :456
     "shear_tolerance": 0.20,                      # :585
     "compression_tolerance": -0.30,               # :600
+    "chem_newton_iterations": 12,                 # whole-interval point-implicit step
 }
 
 CONTROL_DEFAULTS = {
@@ -113,6 +114,7 @@ def make_config(config: dict | None = None, control: dict | None = None, *,
     cfg.use_graphs = int(bool(use_graphs))
     cfg.shear_tolerance = float(c["shear_tolerance"])
     cfg.compression_tolerance = float(c["compression_tolerance"])
+    cfg.chem_newton_iterations = int(c["chem_newton_iterations"])
     return cfg
 
 

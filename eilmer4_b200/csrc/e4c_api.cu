@@ -4,6 +4,7 @@
 // loop of integrate_in_time (src/eilmer/simcore.d:791-1110) recorded as CUDA
 // graphs, and the error conventions of src/gas/gas_cwrap.d (int handles,
 // 0 / negative return codes, never throwing across the ABI).
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -263,6 +264,7 @@ int e4c_config_default(e4c_config* c) {
     c->use_graphs = 1;
     c->shear_tolerance = 0.20;        // globalconfig.d:585
     c->compression_tolerance = -0.30; // globalconfig.d:600
+    c->chem_newton_iterations = 12;
     return E4C_OK;
 }
 
@@ -288,6 +290,8 @@ int e4c_init(const e4c_config* cfg) {
     if (cfg->gas_model != E4C_GAS_IDEAL && cfg->precision != E4C_PREC_FP64)
         return fail(E4C_ERR_UNSUPPORTED, "the FP32-flux form is for the ideal gas");
     if (cfg->cfl_count < 1) return fail(E4C_ERR_ARG, "cfl_count must be >= 1");
+    if (cfg->chem_newton_iterations < 0 || cfg->chem_newton_iterations > 100)
+        return fail(E4C_ERR_ARG, "chem_newton_iterations must be in 0..100");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return fail(E4C_ERR_CUDA, "no CUDA device available");
@@ -352,6 +356,8 @@ int e4c_set_thermochem(const e4c_thermochem* tc) {
             return fail(E4C_ERR_ARG, "bad species thermo data");
     if (!c.blocks.empty()) return fail(E4C_ERR_STATE, "set the mixture before creating blocks");
     if (set_thermochem_constants(*tc) != 0) return fail(E4C_ERR_CUDA, "copy of the mixture failed");
+    if (set_chem_newton_iterations(c.cfg.chem_newton_iterations) != 0)
+        return fail(E4C_ERR_CUDA, "copy of the chemistry settings failed");
     c.have_thermochem = true;
     c.nreac = tc->nreac;
     for (int i = 0; i < 5; ++i) c.seed.mol.M[i] = tc->M[i];
@@ -363,6 +369,7 @@ int e4c_chemistry_step(const int* h, int nb, double dt) {
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (!c.cfg.reacting || !c.have_thermochem) return fail(E4C_ERR_STATE, "not a reacting configuration");
     if (!h || nb <= 0) return fail(E4C_ERR_ARG, "no blocks given");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(E4C_ERR_ARG, "dt must be positive and finite");
     std::vector<int> hs(h, h + nb);
     for (int x : hs)
         if (x < 0 || x >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad block handle");
@@ -738,6 +745,7 @@ int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
     std::vector<int> hs;
     int rc = check_handles(h, nb, hs);
     if (rc != E4C_OK) return rc;
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(E4C_ERR_ARG, "dt must be positive and finite");
     Ctx& c = g_ctx;
     // The host owns dt: write it as SimState.dt_global, clear a stale finish flag.
     launch_begin_run(c.d_sim, 1.0e300, c.stream);

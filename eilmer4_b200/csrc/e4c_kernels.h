@@ -51,6 +51,7 @@ void launch_begin_run(SimDev* sim, double max_time, cudaStream_t s);
 void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
 // thermally perfect mixture / mechanism into constant memory; chemistry of one block
 int set_thermochem_constants(const e4c_thermochem& tc);
+int set_chem_newton_iterations(int n);
 // ghost-cell geometry of an exchange boundary from the partner block
 void launch_exchange_geometry(const BlockView& b, int which, cudaStream_t s);
 // per-cell chemistry step suggestions to (to_dense = 1) or from a dense array

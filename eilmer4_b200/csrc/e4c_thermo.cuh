@@ -557,12 +557,17 @@ __device__ bool point_implicit_step(const MechD<NSP, NR>& m, const double* c0, c
     if (!converged) return false;
     double q0[NSP], L0[NSP];
     m.split_rates(c0, q0, L0);
+    // the distance from the explicit Euler prediction, measured as RKFStep
+    // measures its error (chemistry_update.d:418-427): atol = rtol = errTol,
+    // root mean square over the species
     double err = 0.0;
     for (int i = 0; i < NSP; ++i) {
         double xe = c0[i] + h * (q0[i] - L0[i]);
-        double sc = 1.0e-12 * cscale + 1.0e-3 * fmax(fabs(x[i]), fabs(c0[i]));
-        err = fmax(err, fabs(x[i] - xe) / sc);
+        double sk = 1.0e-3 + 1.0e-3 * fmax(fabs(c0[i]), fabs(x[i]));
+        double e = (x[i] - xe) / sk;
+        err += e * e;
     }
+    err = sqrt(err / NSP);
     double fac = (err > 0.0) ? 0.9 / sqrt(err) : 5.0;
     fac = fmin(5.0, fmax(0.2, fac));
     h_suggest = h * fac;
@@ -586,6 +591,9 @@ constexpr int CHEM_NEEDS_WORK = 1;
 // unless every entry is finite and non-negative) it starts from whichever of
 // c0 and the guess has the smaller residual.  Without a guess the operations are exactly the
 // CPU oracle's.
+// Newton iterations of the whole-interval step (e4c_config.chem_newton_iterations)
+static __constant__ int c_chem_newton_iterations = 12;
+
 template <int NSP, int NR>
 __device__ int point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
                                     const double* guess, double h, double* cOut, int& iters,
@@ -596,7 +604,8 @@ __device__ int point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
     if (!(cscale > 0.0)) return probe ? PI_MORE : PI_FAILED;
     double x[NSP];
     for (int i = 0; i < NSP; ++i) x[i] = c0[i];
-    for (int it = 0; it <= 12; ++it) {
+    const int maxit = c_chem_newton_iterations;
+    for (int it = 0; it <= maxit; ++it) {
         double q[NSP], L[NSP], F[NSP];
         m.split_rates(x, q, L);
         double res = 0.0;
@@ -627,7 +636,7 @@ __device__ int point_implicit_whole(const MechD<NSP, NR>& m, const double* c0,
             for (int i = 0; i < NSP; ++i) cOut[i] = x[i];
             return PI_CONVERGED;
         }
-        if (it == 12) break;
+        if (it == maxit) break;
         double J[NSP][NSP], A[NSP][NSP];
         m.jacobian(x, J);
         for (int i = 0; i < NSP; ++i)

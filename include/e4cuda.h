@@ -111,6 +111,10 @@ typedef struct e4c_config {
     int use_graphs;                 /* capture e4c_integrate steps in CUDA graphs */
     double shear_tolerance;         /* "shear_tolerance" (globalconfig.d:585), adaptive flux */
     double compression_tolerance;   /* "compression_tolerance" (globalconfig.d:600), shock detector */
+    int chem_newton_iterations;     /* Newton iterations of the whole-interval point-implicit
+                                       chemistry step before opCall's sub-cycling takes over
+                                       (default 12; 0 sends every cell that needs Newton work
+                                       to the sub-cycling) */
 } e4c_config;
 
 typedef struct e4c_run_info {
@@ -168,7 +172,8 @@ int e4c_set_thermochem(const e4c_thermochem* tc);
  * step over dt, solved by Newton iteration with the analytic Jacobian; when
  * that iteration does not converge, ChemistryUpdate.opCall's sub-cycling
  * (src/kinetics/chemistry_update.d:119-307) with error-controlled
- * point-implicit sub-steps takes over for that cell. */
+ * point-implicit sub-steps takes over for that cell.  dt must be positive and
+ * finite (E4C_ERR_ARG otherwise). */
 int e4c_chemistry_step(const int* h, int nb, double dt);
 
 /* Chemistry counters accumulated since e4c_init or the last reset: out[0]
@@ -285,7 +290,8 @@ int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double*
                  double* cfl_max);
 
 /* One explicit gas-dynamic step of size dt over the blocks; returns the
- * invalid-cell count of the last stage in *bad_cells. */
+ * invalid-cell count of the last stage in *bad_cells.  dt must be positive and
+ * finite (E4C_ERR_ARG otherwise; nothing is queued). */
 int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells);
 
 /* Run the time loop over all blocks for nsteps steps or until max_time:

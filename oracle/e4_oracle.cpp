@@ -1143,6 +1143,7 @@ void e4o_default_config(e4o_config* c) {
     c->n_threads = 1;
     c->shear_tolerance = 0.20;
     c->compression_tolerance = -0.30;
+    c->chem_newton_iterations = 12;
 }
 
 void* e4o_sim_new(const e4o_config* cfg) {

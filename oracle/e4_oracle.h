@@ -51,6 +51,7 @@ typedef struct e4o_config {
     int n_threads;                  /* OpenMP threads; <=0 means all */
     double shear_tolerance;         /* adaptive flux: globalconfig.d:585 */
     double compression_tolerance;   /* shock detector: globalconfig.d:600 */
+    int chem_newton_iterations;     /* whole-interval point-implicit step (default 12) */
 } e4o_config;
 
 /* Thermally perfect mixture and reaction mechanism (plain arrays).
@@ -135,6 +136,11 @@ int e4o_tp_update(const e4o_thermochem* tc, int mode, const double* massf, doubl
  * fractions, T, u, p and the suggested chemistry step in *dt_chem. */
 int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double rho,
                   double* T, double* u, double* p, double* massf, double* dt_chem);
+
+/* Newton iterations of the whole-interval point-implicit step used by the
+ * single-cell entry points above (default 12; a simulation uses its own
+ * configuration's value). */
+int e4o_set_chem_newton_iterations(int n);
 
 /* The chemistry update alone (ChemistryUpdate.opCall with the point-implicit
  * step) at constant rho and T: new mass fractions, no temperature update. */

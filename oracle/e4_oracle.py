@@ -54,6 +54,7 @@ class Config(ctypes.Structure):
         ("n_threads", ctypes.c_int),
         ("shear_tolerance", ctypes.c_double),
         ("compression_tolerance", ctypes.c_double),
+        ("chem_newton_iterations", ctypes.c_int),
     ]
 
 
@@ -126,6 +127,7 @@ def lib():
         L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
         L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
         L.e4o_rates.argtypes = [P(ThermoChem), dp, P(dp), P(dp), P(dp)]
+        L.e4o_set_chem_newton_iterations.argtypes = [ip]
         L.e4o_newton_test.argtypes = [ip, P(dp)]
         L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
         L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
@@ -326,3 +328,8 @@ def newton_test(which):
     r = ctypes.c_double()
     rc = lib().e4o_newton_test(int(which), ctypes.byref(r))
     return rc, r.value
+
+
+def set_chem_newton_iterations(n):
+    """Newton iterations of the whole-interval step for chem_cell / chem_update."""
+    lib().e4o_set_chem_newton_iterations(int(n))

@@ -486,15 +486,19 @@ static bool point_implicit_step(const Mech& m, const double* c0, double h, doubl
         ++iters;
     }
     if (!converged) return false;
-    // error estimate: distance from the explicit Euler prediction
+    // error estimate: the distance from the explicit Euler prediction,
+    // measured as RKFStep measures its error (chemistry_update.d:418-427):
+    // atol = rtol = errTol, root mean square over the species
     double q0[E4O_MAXSP], L0[E4O_MAXSP];
     m.split_rates(c0, q0, L0);
     double err = 0.0;
     for (int i = 0; i < n; ++i) {
         double xe = c0[i] + h * (q0[i] - L0[i]);
-        double sc = 1.0e-12 * cscale + PI_ERR_TOL * std::fmax(std::fabs(x[i]), std::fabs(c0[i]));
-        err = std::fmax(err, std::fabs(x[i] - xe) / sc);
+        double sk = PI_ERR_TOL + PI_ERR_TOL * std::fmax(std::fabs(c0[i]), std::fabs(x[i]));
+        double e = (x[i] - xe) / sk;
+        err += e * e;
     }
+    err = std::sqrt(err / n);
     double fac = (err > 0.0) ? 0.9 / std::sqrt(err) : 5.0;
     fac = std::fmin(5.0, std::fmax(0.2, fac));
     h_suggest = h * fac;
@@ -503,14 +507,13 @@ static bool point_implicit_step(const Mech& m, const double* c0, double h, doubl
 }
 
 // One backward-Euler step over the whole interval h, x = c0 + h w(x), by
-// Newton iteration from the start x = c0 (at most PI_WHOLE_MAXIT iterations,
+// Newton iteration from the start x = c0 (at most maxit iterations, 12 unless
+// configured otherwise,
 // same convergence test as point_implicit_step, no error control).  This is
 // the point-implicit update proper; the sub-cycled recovery below runs only
 // when it does not converge.
-static const int PI_WHOLE_MAXIT = 12;
-
 static bool point_implicit_whole(const Mech& m, const double* c0, double h, double* cOut,
-                                 int& iters) {
+                                 int& iters, int maxit) {
     const int n = m.tc.nsp;
     double cscale = 0.0;
     for (int i = 0; i < n; ++i) cscale += c0[i];
@@ -518,7 +521,7 @@ static bool point_implicit_whole(const Mech& m, const double* c0, double h, doub
     if (!(cscale > 0.0)) return false;
     double x[E4O_MAXSP];
     for (int i = 0; i < n; ++i) x[i] = c0[i];
-    for (int it = 0; it <= PI_WHOLE_MAXIT; ++it) {
+    for (int it = 0; it <= maxit; ++it) {
         double q[E4O_MAXSP], L[E4O_MAXSP], F[E4O_MAXSP];
         m.split_rates(x, q, L);
         double res = 0.0;
@@ -530,7 +533,7 @@ static bool point_implicit_whole(const Mech& m, const double* c0, double h, doub
             for (int i = 0; i < n; ++i) cOut[i] = x[i];
             return true;
         }
-        if (it == PI_WHOLE_MAXIT) break;
+        if (it == maxit) break;
         double J[E4O_MAXSP][E4O_MAXSP], A[E4O_MAXSP][E4O_MAXSP];
         m.jacobian(x, J);
         for (int i = 0; i < n; ++i)
@@ -554,7 +557,7 @@ static bool point_implicit_whole(const Mech& m, const double* c0, double h, doub
 // over, with error-controlled point-implicit sub-steps and the per-cell
 // dt_chem warm start.
 static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInterval,
-                            double& dtChemSuggest) {
+                            double& dtChemSuggest, int maxit) {
     const int n = tc.nsp;
     GasState Qinit = Q;
     double conc0[E4O_MAXSP], concOut[E4O_MAXSP];
@@ -568,7 +571,7 @@ static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInter
     m.eval_rate_constants(Q.T);
     {
         int iters;
-        if (point_implicit_whole(m, conc0, tInterval, concOut, iters)) {
+        if (point_implicit_whole(m, conc0, tInterval, concOut, iters, maxit)) {
             double total = 0.0;
             for (int i = 0; i < n; ++i) {
                 Q.massf[i] = concOut[i] * tc.M[i] / Q.rho;
@@ -637,12 +640,12 @@ static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInter
 
 // FVCell.thermochemical_increment (fvcell.d:1510-1621)
 static int thermochemical_increment(const e4o_thermochem& tc, double T_frozen, GasState& Q,
-                                    double dt, double& dt_chem) {
+                                    double dt, double& dt_chem, int maxit) {
     if (Q.T <= T_frozen) return 0;
-    int rc = chemistry_update(tc, Q, dt, dt_chem);
+    int rc = chemistry_update(tc, Q, dt, dt_chem, maxit);
     if (rc != 0) {
         dt_chem = -1.0;
-        rc = chemistry_update(tc, Q, dt, dt_chem);
+        rc = chemistry_update(tc, Q, dt, dt_chem, maxit);
         if (rc != 0) return rc;
     }
     TP tp(tc);
@@ -662,7 +665,8 @@ int Sim::chemistry_step(double dt) {
                     Cell& c = b->cell(i, j, k);
                     // fvcell.d:1514: frozen cells return before U.massf is touched
                     if (c.fs.gas.T <= cfg.T_frozen) continue;
-                    int rc = thermochemical_increment(gm.tc, cfg.T_frozen, c.fs.gas, dt, c.dt_chem);
+                    int rc = thermochemical_increment(gm.tc, cfg.T_frozen, c.fs.gas, dt, c.dt_chem,
+                                                      cfg.chem_newton_iterations);
                     if (rc != 0) { err = std::min(err, rc); continue; }
                     for (int s = 0; s < nsp_cons; ++s) c.U[0][5 + s] = c.fs.gas.rho * c.fs.gas.massf[s];
                 }
@@ -674,7 +678,16 @@ int Sim::chemistry_step(double dt) {
 
 using namespace e4o;
 
+// Newton iterations of the whole-interval step for the single-cell entry
+// points (a simulation uses its configuration's value).
+static int g_chem_newton_iterations = 12;
+
 extern "C" {
+
+int e4o_set_chem_newton_iterations(int n) {
+    g_chem_newton_iterations = n;
+    return 0;
+}
 
 int e4o_set_thermochem(void* sim, const e4o_thermochem* tc) {
     Sim* s = static_cast<Sim*>(sim);
@@ -703,7 +716,7 @@ int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, d
     GasState Q;
     Q.rho = rho; Q.T = T; Q.u = 0.0; Q.p = 0.0;
     for (int i = 0; i < tc->nsp; ++i) Q.massf[i] = massf[i];
-    int rc = chemistry_update(*tc, Q, dt, *dt_chem);
+    int rc = chemistry_update(*tc, Q, dt, *dt_chem, g_chem_newton_iterations);
     if (rc != 0) return rc;
     for (int i = 0; i < tc->nsp; ++i) massf[i] = Q.massf[i];
     return 0;
@@ -714,7 +727,7 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
     GasState Q;
     Q.rho = rho; Q.T = *T; Q.u = *u; Q.p = *p;
     for (int i = 0; i < tc->nsp; ++i) Q.massf[i] = massf[i];
-    int rc = thermochemical_increment(*tc, T_frozen, Q, dt, *dt_chem);
+    int rc = thermochemical_increment(*tc, T_frozen, Q, dt, *dt_chem, g_chem_newton_iterations);
     if (rc != 0) return rc;
     *T = Q.T; *u = Q.u; *p = Q.p;
     for (int i = 0; i < tc->nsp; ++i) massf[i] = Q.massf[i];
