@@ -365,6 +365,7 @@ int e4c_set_thermochem(const e4c_thermochem* tc) {
 }
 
 int e4c_chemistry_step(const int* h, int nb, double dt) {
+    NvtxRange nvtx_range("e4c_chemistry_step");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (!c.cfg.reacting || !c.have_thermochem) return fail(E4C_ERR_STATE, "not a reacting configuration");
@@ -402,6 +403,7 @@ int e4c_chemistry_counters(long long* out, int reset) {
 
 int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* bc_type,
                      const double* inflow_prim) {
+    NvtxRange nvtx_range("e4c_block_create");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "e4c_block_create before e4c_init");
     if (c.cfg.gas_model == E4C_GAS_THERM_PERF_5SP_AIR && !c.have_thermochem)
@@ -494,6 +496,7 @@ int e4c_connect_blocks(int ha, int fa, int hb, int fb, int orientation) {
 }
 
 int e4c_block_upload(int h, const double* prim) {
+    NvtxRange nvtx_range("e4c_block_upload");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (h < 0 || h >= int(c.blocks.size()) || !prim) return fail(E4C_ERR_ARG, "bad handle or pointer");
@@ -512,6 +515,7 @@ int e4c_block_upload(int h, const double* prim) {
 }
 
 int e4c_block_upload_cons(int h, const double* cons) {
+    NvtxRange nvtx_range("e4c_block_upload_cons");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (h < 0 || h >= int(c.blocks.size()) || !cons) return fail(E4C_ERR_ARG, "bad handle or pointer");
@@ -531,6 +535,7 @@ int e4c_block_upload_cons(int h, const double* cons) {
 }
 
 int e4c_block_download(int h, double* prim, double* cons) {
+    NvtxRange nvtx_range("e4c_block_download");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (h < 0 || h >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad handle");
@@ -600,6 +605,7 @@ int Ctx::ensure_stage_io(size_t bytes) {
 }
 
 int e4c_block_upload_async(int h, const double* prim) {
+    NvtxRange nvtx_range("e4c_block_upload_async");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (h < 0 || h >= int(c.blocks.size()) || !prim) return fail(E4C_ERR_ARG, "bad handle or pointer");
@@ -625,6 +631,7 @@ int e4c_block_upload_async(int h, const double* prim) {
 }
 
 int e4c_block_upload_cons_async(int h, const double* cons) {
+    NvtxRange nvtx_range("e4c_block_upload_cons_async");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (h < 0 || h >= int(c.blocks.size()) || !cons) return fail(E4C_ERR_ARG, "bad handle or pointer");
@@ -646,6 +653,7 @@ int e4c_block_upload_cons_async(int h, const double* cons) {
 }
 
 int e4c_block_download_async(int h, double* prim, double* cons) {
+    NvtxRange nvtx_range("e4c_block_download_async");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (h < 0 || h >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad handle");
@@ -698,6 +706,7 @@ static int check_handles(const int* h, int nb, std::vector<int>& hs) {
 
 int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double* dt_allow,
                  double* cfl_max) {
+    NvtxRange nvtx_range("e4c_dt_allow");
     std::vector<int> hs;
     int rc = check_handles(h, nb, hs);
     if (rc != E4C_OK) return rc;
@@ -741,6 +750,7 @@ static int status_error(const SimDev& s) {
 }
 
 int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
+    NvtxRange nvtx_range("e4c_gasdynamic_step");
     g_ctx.host_step_valid = false;
     std::vector<int> hs;
     int rc = check_handles(h, nb, hs);
@@ -764,6 +774,7 @@ int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
 }
 
 int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
+    NvtxRange nvtx_range("e4c_integrate");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
@@ -801,6 +812,7 @@ int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
 }
 
 int e4c_integrate_async(int nsteps, double max_time) {
+    NvtxRange nvtx_range("e4c_integrate_async");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
@@ -848,6 +860,7 @@ void* e4c_stream(void) { return g_ctx.initialised ? static_cast<void*>(g_ctx.str
 long long e4c_kernel_launches(void) { return g_ctx.launches; }
 
 int e4c_profile_steps(int nsteps, double* ms, int* launches) {
+    NvtxRange nvtx_range("e4c_profile_steps");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
@@ -916,6 +929,7 @@ int e4c_get_tile(int* ti, int* tj, int* kc) {
 }
 
 int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step) {
+    NvtxRange nvtx_range("e4c_autotune");
     g_ctx.host_step_valid = false;
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");

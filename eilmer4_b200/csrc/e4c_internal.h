@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 #include <vector>
@@ -11,6 +12,15 @@
 #include "e4c_types.h"
 
 namespace e4c {
+
+// A named NVTX range for the duration of a C-ABI call (seen by Nsight
+// Systems and other NVTX tools; a no-op when none is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct BlockHost {
     BlockView v{};          // general path (device arrays unset on the fused path)

@@ -917,6 +917,7 @@ using namespace e4c;
 extern "C" {
 
 int e4c_seed_collect(const int* h, int nb, double dt, long long nsamples, unsigned long long rng_seed) {
+    NvtxRange nvtx_range("e4c_seed_collect");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (!c.cfg.reacting || !c.have_thermochem) return fail(E4C_ERR_STATE, "not a reacting configuration");
@@ -984,6 +985,7 @@ int e4c_seed_clear(void) {
 }
 
 int e4c_seed_train(int epochs, int batch, double lr, unsigned long long rng_seed, double* report) {
+    NvtxRange nvtx_range("e4c_seed_train");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (epochs < 1 || batch < 64 || !(lr > 0.0)) return fail(E4C_ERR_ARG, "bad training arguments");
