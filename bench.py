@@ -675,10 +675,11 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--flux", default="hllc", choices=["hllc", "ausmdv"])
     ap.add_argument("--profile-steps", type=int, default=4)
-    ap.add_argument("--cpu-sample", type=int, default=64)
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    # CPU baseline samples: about 10 s of oracle work each on a 16-core host
+    ap.add_argument("--cpu-sample", type=int, default=128)
+    ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--ref-sample", type=int, default=96)
-    ap.add_argument("--cpu-reacting-steps", type=int, default=5)
+    ap.add_argument("--cpu-reacting-steps", type=int, default=25)
     ap.add_argument("--no-ref-gpu-chem", action="store_true",
                     help="--impl reference: skip the reference's GPU chemistry kernel")
     ap.add_argument("--ref-chem-ni", type=int, default=256)
