@@ -62,7 +62,7 @@ BYTES_PER_REACTING_CELL = 8.0 * (9 + 15)
 # kernel's traffic grows with the cells it processes), keyed by (precision,
 # kernel class).  Algorithmic bytes per launch at 256^3: 3020 MB (FP64),
 # 2349 MB (FP32-flux).
-TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2058403840}
+TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2063725568}
 
 
 def peaks():
