@@ -231,6 +231,57 @@ def inflow_3d_block(ni, nj, nk, seed, spacing=None, mach=3.0, p_in=1.0e5, T_in=3
     return BlockSpec(ni, nj, nk, vtx, tuple(bc), inflow, prim)
 
 
+def skewed_box_3d(ni=12, nj=10, nk=8, flux="ausmdv", amp=0.04, seed=DEFAULT_SEED,
+                  reacting=False) -> Workload:
+    """A curvilinear 3-D block: the unit box with every vertex displaced by
+    smooth sines (amplitude amp in each direction), so no face frame is an
+    axis permutation and cell volumes and lengths vary.  Mach-3 inflow at
+    i-min, extrapolate outflow at i-max, slip walls elsewhere; the density
+    perturbed as in inflow_3d.  reacting: 5-species air at the reacting
+    channel's inflow state (Mach 10, 2000 K, 20 kPa) instead of ideal air,
+    the density perturbed at constant pressure."""
+    vtx = box_vertices(ni, nj, nk, 1.0, 1.0, 1.0, 3)
+    x, y, z = vtx[:, 0].copy(), vtx[:, 1].copy(), vtx[:, 2].copy()
+    tp = 2.0 * math.pi
+    vtx[:, 0] = x + amp * np.sin(tp * y) * np.sin(tp * z)
+    vtx[:, 1] = y + amp * np.sin(tp * z) * np.sin(tp * x)
+    vtx[:, 2] = z + amp * np.sin(tp * x) * np.sin(tp * y)
+    centres = cell_centres(vtx, ni, nj, nk, 3)
+    bc = [BC_SLIP_WALL] * 6
+    bc[WEST] = BC_INFLOW_SUPERSONIC
+    bc[EAST] = BC_OUTFLOW_EXTRAPOLATE
+    wl = Workload("skewed_box_3d_%dx%dx%d" % (ni, nj, nk), 3, flux_calculator=flux, nsteps=50)
+    if not reacting:
+        gas = IdealGas()
+        rho_in, u_in, a_in = gas.from_pT(1.0e5, 300.0)
+        vx = 3.0 * float(a_in)
+        inflow = np.array([float(rho_in), vx, 0.0, 0.0, 1.0e5, 300.0, float(u_in), float(a_in)])
+        rho = float(rho_in) * (1.0 + 0.05 * _perturbation(centres, seed))
+        p = np.full_like(rho, 1.0e5)
+        T, u, a = gas.from_rhop(rho, p)
+        z0 = np.zeros_like(rho)
+        prim = prim_from(rho, np.full_like(rho, vx), z0, z0, p, T, u, a)
+        wl.gas = gas
+    else:
+        from .thermochem import load_air5
+        tc = load_air5()
+        massf = (0.767, 0.233, 0.0, 0.0, 0.0)
+        rho_in, u_in, a_in = tc.state_pT(2.0e4, 2000.0, massf)
+        inflow = np.array([rho_in, 10.0 * a_in, 0.0, 0.0, 2.0e4, 2000.0, u_in, a_in] + list(massf))
+        # the stream with the density perturbed at constant pressure (an
+        # entropy wave it carries through the block)
+        n = ni * nj * nk
+        prim = np.repeat(inflow[:, None], n, axis=1).copy()
+        pert = 1.0 + 0.05 * _perturbation(centres, seed)
+        for q in range(n):
+            T = 2000.0 / pert[q]
+            rho, u, a = tc.state_pT(2.0e4, T, massf)
+            prim[0, q], prim[5, q], prim[6, q], prim[7, q] = rho, T, u, a
+        wl.thermochem = tc
+    wl.blocks.append(BlockSpec(ni, nj, nk, vtx, tuple(bc), inflow, prim))
+    return wl
+
+
 def inflow_3d(n=256, seed=DEFAULT_SEED, flux="hllc", nsteps=500) -> Workload:
     wl = Workload("inflow_3d_%d^3" % n, 3, flux_calculator=flux, nsteps=nsteps)
     wl.blocks.append(inflow_3d_block(n, n, n, seed))
