@@ -317,20 +317,26 @@ __device__ __forceinline__ void hllc(const Prim<R, NSP>& Lf, const Prim<R, NSP>&
     R ER = rR * (Rt.u + R(0.5) * (uR * uR + vR * vR + wR * wR));
     R SL = fmin(uL - aL, uR - aR);
     R SR = fmax(uL + aL, uR + aR);
-    R mL = rL * (SL - uL);
-    R mR = rR * (SR - uR);
-    R Sstar = (pR - pL + mL * uL - mR * uR) / (mL - mR);
     if (SL >= R(0.0)) {
         R m = rL * uL;
         F[0] = m; F[1] = m * uL + pL; F[2] = m * vL; F[3] = m * wL; F[4] = uL * (EL + pL);
 #pragma unroll
         for (int i = 0; i < NSPC; ++i) F[5 + i] = m * Lf.massf[i];
-    } else if (SR <= R(0.0)) {
+        return;
+    }
+    if (SR <= R(0.0)) {
         R m = rR * uR;
         F[0] = m; F[1] = m * uR + pR; F[2] = m * vR; F[3] = m * wR; F[4] = uR * (ER + pR);
 #pragma unroll
         for (int i = 0; i < NSPC; ++i) F[5 + i] = m * Rt.massf[i];
-    } else if (Sstar >= R(0.0)) {
+        return;
+    }
+    // subsonic: the contact speed (computed only here; the supersonic faces
+    // above do not use it)
+    R mL = rL * (SL - uL);
+    R mR = rR * (SR - uR);
+    R Sstar = (pR - pL + mL * uL - mR * uR) / (mL - mR);
+    if (Sstar >= R(0.0)) {
         R m = rL * uL;
         R coef = mL / (SL - Sstar);
         R Estar = coef * (EL / rL + (Sstar - uL) * (Sstar + pL / mL));
