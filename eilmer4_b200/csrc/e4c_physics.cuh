@@ -312,9 +312,11 @@ __device__ __forceinline__ void ausmdv(const Prim<R, NSP>& Lf, const Prim<R, NSP
 template <typename R, int NSP, int NSPC>
 __device__ __forceinline__ void hllc(const Prim<R, NSP>& Lf, const Prim<R, NSP>& Rt, R* F) {
     R rL = Lf.rho, pL = Lf.p, uL = Lf.vel.x, vL = Lf.vel.y, wL = Lf.vel.z, aL = Lf.a;
-    R EL = rL * (Lf.u + R(0.5) * (uL * uL + vL * vL + wL * wL));
+    R eL = Lf.u + R(0.5) * (uL * uL + vL * vL + wL * wL);  // total energy per mass
+    R EL = rL * eL;
     R rR = Rt.rho, pR = Rt.p, uR = Rt.vel.x, vR = Rt.vel.y, wR = Rt.vel.z, aR = Rt.a;
-    R ER = rR * (Rt.u + R(0.5) * (uR * uR + vR * vR + wR * wR));
+    R eR = Rt.u + R(0.5) * (uR * uR + vR * vR + wR * wR);
+    R ER = rR * eR;
     R SL = fmin(uL - aL, uR - aR);
     R SR = fmax(uL + aL, uR + aR);
     if (SL >= R(0.0)) {
@@ -339,7 +341,7 @@ __device__ __forceinline__ void hllc(const Prim<R, NSP>& Lf, const Prim<R, NSP>&
     if (Sstar >= R(0.0)) {
         R m = rL * uL;
         R coef = mL / (SL - Sstar);
-        R Estar = coef * (EL / rL + (Sstar - uL) * (Sstar + pL / mL));
+        R Estar = coef * (eL + (Sstar - uL) * (Sstar + pL / mL));
         F[0] = m + SL * (coef - rL);
         F[1] = (m * uL + pL) + SL * (coef * Sstar - m);
         F[2] = m * vL + SL * (coef * vL - rL * vL);
@@ -350,7 +352,7 @@ __device__ __forceinline__ void hllc(const Prim<R, NSP>& Lf, const Prim<R, NSP>&
     } else {
         R m = rR * uR;
         R coef = mR / (SR - Sstar);
-        R Estar = coef * (ER / rR + (Sstar - uR) * (Sstar + pR / mR));
+        R Estar = coef * (eR + (Sstar - uR) * (Sstar + pR / mR));
         F[0] = m + SR * (coef - rR);
         F[1] = (m * uR + pR) + SR * (coef * Sstar - m);
         F[2] = m * vR + SR * (coef * vR - rR * vR);

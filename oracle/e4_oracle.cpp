@@ -545,10 +545,12 @@ void Sim::hllc(const FlowState& Lft, const FlowState& Rght, double* F) const {
     // mass flux of the upwind star state.
     double rL = Lft.gas.rho, pL = Lft.gas.p, uL = Lft.vel.x, vL = Lft.vel.y, wL = Lft.vel.z;
     double aL = Lft.gas.a;
-    double EL = rL * (Lft.gas.u + 0.5 * (uL * uL + vL * vL + wL * wL));
+    double eL = Lft.gas.u + 0.5 * (uL * uL + vL * vL + wL * wL);  // total energy per mass
+    double EL = rL * eL;
     double rR = Rght.gas.rho, pR = Rght.gas.p, uR = Rght.vel.x, vR = Rght.vel.y, wR = Rght.vel.z;
     double aR = Rght.gas.a;
-    double ER = rR * (Rght.gas.u + 0.5 * (uR * uR + vR * vR + wR * wR));
+    double eR = Rght.gas.u + 0.5 * (uR * uR + vR * vR + wR * wR);
+    double ER = rR * eR;
     double SL = std::fmin(uL - aL, uR - aR);
     double SR = std::fmax(uL + aL, uR + aR);
     double mL = rL * (SL - uL);
@@ -565,7 +567,7 @@ void Sim::hllc(const FlowState& Lft, const FlowState& Rght, double* F) const {
     } else if (Sstar >= 0.0) {
         double m = rL * uL;
         double coef = mL / (SL - Sstar);  // rho*L
-        double Estar = coef * (EL / rL + (Sstar - uL) * (Sstar + pL / mL));
+        double Estar = coef * (eL + (Sstar - uL) * (Sstar + pL / mL));
         F[0] = m + SL * (coef - rL);
         F[1] = (m * uL + pL) + SL * (coef * Sstar - m);
         F[2] = m * vL + SL * (coef * vL - rL * vL);
@@ -575,7 +577,7 @@ void Sim::hllc(const FlowState& Lft, const FlowState& Rght, double* F) const {
     } else {
         double m = rR * uR;
         double coef = mR / (SR - Sstar);
-        double Estar = coef * (ER / rR + (Sstar - uR) * (Sstar + pR / mR));
+        double Estar = coef * (eR + (Sstar - uR) * (Sstar + pR / mR));
         F[0] = m + SR * (coef - rR);
         F[1] = (m * uR + pR) + SR * (coef * Sstar - m);
         F[2] = m * vR + SR * (coef * vR - rR * vR);
