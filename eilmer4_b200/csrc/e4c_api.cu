@@ -141,6 +141,8 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
     for (int h : hs) {
         const BlockHost& b = blocks[h];
         if (b.fused) continue;
+        if (b.v.Vrt && fopts.order2 && fopts.local_frame)
+            launch_as(*this, E4C_KCLASS_FLUX, 1, [&] { launch_replay_base(b.v, d_sim, stream); });
         launch_as(*this, E4C_KCLASS_FLUX, 1, [&] { launch_flux(b.v, d_sim, fopts, -1, stream); });
     }
     // applyPostConvFluxAction of every block (simcore.d:2373-2377)

@@ -195,6 +195,11 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
         v.S = static_cast<int*>(dalloc(np * sizeof(int)));
         if (!v.S) return fail(E4C_ERR_CUDA, "cudaMalloc of shock flags failed");
         E4C_CUDA(cudaMemsetAsync(v.S, 0, np * sizeof(int), stream));
+        if (!v.axis_frames) {
+            v.Vrt = static_cast<double*>(dalloc(6 * np * sizeof(double)));
+            if (!v.Vrt) return fail(E4C_ERR_CUDA, "cudaMalloc of round-trip velocities failed");
+            E4C_CUDA(cudaMemsetAsync(v.Vrt, 0, 6 * np * sizeof(double), stream));
+        }
     }
     out.v = v;
     // staging area for uploads and downloads (primitive + conserved)

@@ -73,28 +73,26 @@ __device__ __forceinline__ void roundtrip(V3<double>& v, const double* fg, size_
 }
 
 // Velocity of stencil cell (ci,cj,ck) as the reference holds it when it
-// reaches the face of direction dir at index fpos along dir.
-static __device__ void replay_roundtrips(const BlockView& b, int dir, int fpos, int ci, int cj, int ck,
-                                  V3<double>& v) {
-    const int c[3] = {ci, cj, ck};
-    const int lo[3] = {b.imin, b.jmin, b.kmin}, hi[3] = {b.imax, b.jmax, b.kmax};
-    const double* fgs[3] = {b.fgi, b.fgj, b.fgk};
-    // faces of the earlier directions (their loops cover interior rows only)
-    if (c[dir] >= lo[dir] && c[dir] <= hi[dir]) {
-        for (int d = 0; d < dir; ++d)
-            for (int g = c[d] - 1; g <= c[d] + 2; ++g) {
-                if (g < lo[d] || g > hi[d] + 1) continue;
-                int p[3] = {c[0], c[1], c[2]};
-                p[d] = g;
-                roundtrip(v, fgs[d], b.npad, pidx(b, p[0], p[1], p[2]));
-            }
+// reaches the face of direction dir at index fpos along dir.  The round trips
+// of the earlier directions' faces (their loops cover interior rows only, so
+// only cells interior along dir took part) come precomputed per cell in
+// b.Vrt (k_replay_base); this applies the earlier faces of direction dir in
+// the same row, in loop order.
+__device__ __forceinline__ void replay_roundtrips(const BlockView& b, int dir, int fpos, int ci,
+                                                  int cj, int ck, size_t c, V3<double>& v) {
+    const int cd = dir == 0 ? ci : (dir == 1 ? cj : ck);
+    const int lo = dir == 0 ? b.imin : (dir == 1 ? b.jmin : b.kmin);
+    const int hi = dir == 0 ? b.imax : (dir == 1 ? b.jmax : b.kmax);
+    if (dir > 0 && cd >= lo && cd <= hi) {
+        const double* V = b.Vrt + size_t(3 * (dir - 1)) * b.npad;
+        v = {V[c], V[b.npad + c], V[2 * b.npad + c]};
     }
-    // earlier faces of this direction in the same row
-    for (int g = c[dir] - 1; g <= c[dir] + 2 && g < fpos; ++g) {
-        if (g < lo[dir] || g > hi[dir] + 1) continue;
-        int p[3] = {c[0], c[1], c[2]};
+    const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
+    for (int g = cd - 1; g <= cd + 2 && g < fpos; ++g) {
+        if (g < lo || g > hi + 1) continue;
+        int p[3] = {ci, cj, ck};
         p[dir] = g;
-        roundtrip(v, fgs[dir], b.npad, pidx(b, p[0], p[1], p[2]));
+        roundtrip(v, fg, b.npad, pidx(b, p[0], p[1], p[2]));
     }
 }
 
@@ -179,7 +177,7 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
         auto cell_state = [&](size_t c, int ci, int cj, int ck, Prim<double, NSP>& s) {
             load_prim<NSP>(b, c, s);
             if (o.order2) {
-                if (replay) replay_roundtrips(b, dir, fpos, ci, cj, ck, s.vel);
+                if (replay) replay_roundtrips(b, dir, fpos, ci, cj, ck, c, s.vel);
                 if (o.local_frame) to_local(s.vel, fr.n, fr.t1, fr.t2);
             }
         };

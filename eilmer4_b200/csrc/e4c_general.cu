@@ -731,6 +731,47 @@ void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_
     k_shock<<<grid_for(n, 256), 256, 0, s>>>(b, sim, tol);
 }
 
+// The velocity each interior cell of a block with general face frames holds
+// when its j faces (V1) and its k faces (V2) begin: interp_l2r2 turns the
+// velocities of its four stencil cells into the face frame and back in place
+// (onedinterp.d:445-454, 576-584), so after the i-face loop of
+// sfluidblock.d:2190-2344 a cell carries the round-off of the (up to) four i
+// faces it took part in, in loop order, and after the j-face loop that of its
+// j faces too.  Each cell depends only on its own velocity and the frames of
+// its faces, so one thread per cell replays them once per stage for every
+// face that reads the cell.
+__global__ void k_replay_base(BlockView b, const SimDev* sim) {
+    if (sim->status != 0 || sim->finished) return;
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = b.imin + int(t % b.ni);
+        const int j = b.jmin + int((t / b.ni) % b.nj);
+        const int k = b.kmin + int(t / ((long long)b.ni * b.nj));
+        const size_t c = pidx(b, i, j, k);
+        V3<double> v{b.W[W_VX * b.npad + c], b.W[W_VY * b.npad + c], b.W[W_VZ * b.npad + c]};
+        for (int g = i - 1; g <= i + 2; ++g) {
+            if (g < b.imin || g > b.imax + 1) continue;
+            roundtrip(v, b.fgi, b.npad, pidx(b, g, j, k));
+        }
+        b.Vrt[c] = v.x; b.Vrt[b.npad + c] = v.y; b.Vrt[2 * b.npad + c] = v.z;
+        if (b.dim == 3) {
+            for (int g = j - 1; g <= j + 2; ++g) {
+                if (g < b.jmin || g > b.jmax + 1) continue;
+                roundtrip(v, b.fgj, b.npad, pidx(b, i, g, k));
+            }
+            b.Vrt[3 * b.npad + c] = v.x; b.Vrt[4 * b.npad + c] = v.y;
+            b.Vrt[5 * b.npad + c] = v.z;
+        }
+    }
+}
+
+void launch_replay_base(const BlockView& b, const SimDev* sim, cudaStream_t s) {
+    const long long n = (long long)b.ni * b.nj * b.nk;
+    const int T = 128;
+    k_replay_base<<<grid_for(n, T), T, 0, s>>>(b, sim);
+}
+
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
                  cudaStream_t s) {
     long long n = 0;

@@ -29,6 +29,9 @@ void launch_upload_cons(const BlockView& b, const double* cons, SimDev* sim, con
 void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s);
 // shock points (detect_shock_points with the PJ detector)
 void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s);
+// velocities of the interior cells after their i (and j) face round trips
+// (blocks with general face frames, before the flux launch)
+void launch_replay_base(const BlockView& b, const SimDev* sim, cudaStream_t s);
 // face fluxes of direction dir, or of every direction when dir < 0
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, cudaStream_t s);
 // boundary-face fluxes of OutFlowBC_SimpleFlux boundaries (after launch_flux)

@@ -67,6 +67,10 @@ struct BlockView {
     double* dt_chem;                // per-cell chemistry step suggestion (reacting blocks)
     ExchangeSrc ex[6];              // partners of exchange boundaries (bc == 3)
     int* S;                         // shock flag per padded cell (adaptive flux)
+    // blocks with general face frames: velocity (x, y, z) of each interior
+    // cell after the in-place round trips of its i faces, then of its i and j
+    // faces (6 x npad; null for blocks whose frames are signed unit axes)
+    double* Vrt;
 };
 
 // Device-resident simulation state (one per library context).
