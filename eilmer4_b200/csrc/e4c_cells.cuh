@@ -259,6 +259,166 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
     }
 }
 
+// Faces of a block with general face frames (second order, reconstruction in
+// the face frame), a run of consecutive faces of one row per thread.  The
+// reference's in-place round trips (onedinterp.d:445-454, 576-584) are taken
+// literally: the thread holds its four stencil cells with their velocities as
+// the reference holds them, turns them into the face frame for the
+// reconstruction and back afterwards, and moves on to the next face of the
+// row, as the loops of sfluidblock.d:2190-2344 do.  The first face of a run
+// starts from the replayed velocities (replay_roundtrips).  Runs of the
+// i faces are interleaved across threads (neighbouring threads take
+// neighbouring runs of a row); j and k faces are taken with i fastest.
+// runs[d]: runs per row of direction d.
+template <int NSP, int FLUX, int GAS>
+__global__ void k_flux_rows(BlockView b, const SimDev* sim, FluxOpts o, int3 runs) {
+    if (sim->status != 0 || sim->finished) return;
+    const int nrun[3] = {runs.x, runs.y, runs.z};
+    const int next[3] = {b.ni, b.nj, b.nk};
+    long long nd[3];
+    for (int d = 0; d < 3; ++d) {
+        const long long rows = d == 0 ? (long long)b.nj * b.nk
+                                      : (d == 1 ? (long long)b.ni * b.nk : (long long)b.ni * b.nj);
+        nd[d] = (d < b.dim) ? rows * nrun[d] : 0;
+    }
+    const long long n = nd[0] + nd[1] + nd[2];
+    constexpr int NSPC = NSP > 1 ? NSP : 0;
+    for (long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x; tt < n;
+         tt += (long long)gridDim.x * blockDim.x) {
+        int dir = 0;
+        long long t = tt;
+        if (t >= nd[0]) { t -= nd[0]; dir = 1; }
+        if (dir == 1 && t >= nd[1]) { t -= nd[1]; dir = 2; }
+        int run, a1, a2;  // run index; the row's coordinates (i, j, k without dir)
+        if (dir == 0) {
+            run = int(t % nrun[0]);
+            a1 = b.jmin + int((t / nrun[0]) % b.nj);
+            a2 = b.kmin + int(t / ((long long)nrun[0] * b.nj));
+        } else if (dir == 1) {
+            a1 = b.imin + int(t % b.ni);
+            run = int((t / b.ni) % nrun[1]);
+            a2 = b.kmin + int(t / ((long long)b.ni * nrun[1]));
+        } else {
+            a1 = b.imin + int(t % b.ni);
+            a2 = b.jmin + int((t / b.ni) % b.nj);
+            run = int(t / ((long long)b.ni * b.nj));
+        }
+        const int lo = dir == 0 ? b.imin : (dir == 1 ? b.jmin : b.kmin);
+        const int nf = next[dir] + 1;  // faces lo .. lo + nf - 1 of the row
+        const int g0 = lo + int((long long)run * nf / nrun[dir]);
+        const int g1 = lo + int((long long)(run + 1) * nf / nrun[dir]);
+        const size_t stride = dir == 0 ? 1 : (dir == 1 ? size_t(b.nidim) : size_t(b.nidim) * b.njdim);
+        const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
+        double* Fo = dir == 0 ? b.Fi : (dir == 1 ? b.Fj : b.Fk);
+        const double* len = b.cgeom + size_t(1 + dir) * b.npad;
+        auto coords = [&](int x, int& ci, int& cj, int& ck) {
+            if (dir == 0) { ci = x; cj = a1; ck = a2; }
+            else if (dir == 1) { ci = a1; cj = x; ck = a2; }
+            else { ci = a1; cj = a2; ck = x; }
+        };
+        // stencil window: cells g-2, g-1, g, g+1 of face g, velocities as held
+        Prim<double, NSP> w[4];
+        double wl[4];
+        {
+            int ci, cj, ck;
+            coords(g0, ci, cj, ck);
+            const size_t f0 = pidx(b, ci, cj, ck);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int x = g0 - 2 + q;
+                coords(x, ci, cj, ck);
+                const size_t c = f0 + (q - 2) * (long long)stride;
+                load_prim<NSP>(b, c, w[q]);
+                replay_roundtrips(b, dir, g0, ci, cj, ck, c, w[q].vel);
+                wl[q] = len[c];
+            }
+        }
+        for (int g = g0; g < g1; ++g) {
+            int ci, cj, ck;
+            coords(g, ci, cj, ck);
+            const size_t f = pidx(b, ci, cj, ck);
+            if (g > g0) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) { w[q] = w[q + 1]; wl[q] = wl[q + 1]; }
+                const size_t c = f + stride;
+                load_prim<NSP>(b, c, w[3]);
+                wl[3] = len[c];
+                int ni_, nj_, nk_;
+                coords(g + 1, ni_, nj_, nk_);
+                // a cell entering the window has met no face of this row yet
+                replay_roundtrips(b, dir, g, ni_, nj_, nk_, c, w[3].vel);
+            }
+            Frame<double> fr;
+            load_frame(fg, b.npad, f, fr);
+            Prim<double, NSP> sL1 = w[0], sL0 = w[1], sR0 = w[2], sR1 = w[3];
+            to_local(sL1.vel, fr.n, fr.t1, fr.t2);
+            to_local(sL0.vel, fr.n, fr.t1, fr.t2);
+            to_local(sR0.vel, fr.n, fr.t1, fr.t2);
+            to_local(sR1.vel, fr.n, fr.t1, fr.t2);
+            Prim<double, NSP> Lf = sL0, Rt = sR0;
+            {
+                L2R2<double> r;
+                r.prepare(wl[0], wl[1], wl[2], wl[3]);
+                r.scalar(o.limiter, o.clip, sL1.vel.x, sL0.vel.x, sR0.vel.x, sR1.vel.x, Lf.vel.x, Rt.vel.x);
+                r.scalar(o.limiter, o.clip, sL1.vel.y, sL0.vel.y, sR0.vel.y, sR1.vel.y, Lf.vel.y, Rt.vel.y);
+                r.scalar(o.limiter, o.clip, sL1.vel.z, sL0.vel.z, sR0.vel.z, sR1.vel.z, Lf.vel.z, Rt.vel.z);
+                if (NSP > 1) {
+#pragma unroll
+                    for (int q = 0; q < NSP; ++q)
+                        r.scalar(o.limiter, o.clip, sL1.massf[q], sL0.massf[q], sR0.massf[q],
+                                 sR1.massf[q], Lf.massf[q], Rt.massf[q]);
+                    if (!scale_mass_fractions<double, NSP>(Lf.massf))
+                        for (int q = 0; q < NSP; ++q) Lf.massf[q] = sL0.massf[q];
+                    if (!scale_mass_fractions<double, NSP>(Rt.massf))
+                        for (int q = 0; q < NSP; ++q) Rt.massf[q] = sR0.massf[q];
+                } else {
+                    Lf.massf[0] = 1.0;
+                    Rt.massf[0] = 1.0;
+                }
+                r.scalar(o.limiter, o.clip, sL1.rho, sL0.rho, sR0.rho, sR1.rho, Lf.rho, Rt.rho);
+                r.scalar(o.limiter, o.clip, sL1.u, sL0.u, sR0.u, sR1.u, Lf.u, Rt.u);
+            }
+            // codeForThermoUpdateBoth("rhou"), onedinterp.d:1039-1068: on failure
+            // the cell-centre state (its velocity in the face frame) is taken
+            if (!rhou_update<NSP, GAS>(o, Lf)) Lf = sL0;
+            if (!rhou_update<NSP, GAS>(o, Rt)) Rt = sR0;
+            to_global(Lf.vel, fr.n, fr.t1, fr.t2);
+            to_global(Rt.vel, fr.n, fr.t1, fr.t2);
+            // the stencil cells back to the global frame in place; cell g-2
+            // leaves the window and is not needed again
+            to_global(sL0.vel, fr.n, fr.t1, fr.t2);
+            to_global(sR0.vel, fr.n, fr.t1, fr.t2);
+            to_global(sR1.vel, fr.n, fr.t1, fr.t2);
+            w[1].vel = sL0.vel; w[2].vel = sR0.vel; w[3].vel = sR1.vel;
+            // compute_interface_flux, fluxcalc.d:26-128 (fixed grid)
+            to_local(Lf.vel, fr.n, fr.t1, fr.t2);
+            to_local(Rt.vel, fr.n, fr.t1, fr.t2);
+            double F[5 + NSPC];
+            if (FLUX == 1) {
+                hllc<double, NSP, NSPC>(Lf, Rt, F);
+            } else if (FLUX == 2) {
+                hanel<double, NSP, NSPC>(Lf, Rt, F);
+            } else if (FLUX == 3) {
+                const double sound_speed = 0.5 * (Lf.a + Rt.a);
+                const double shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
+                const double shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
+                const bool shear_is_small = fmax(shear_y, shear_z) <= o.shear_tol;
+                if ((b.S[f - stride] == 1 || b.S[f] == 1) && shear_is_small)
+                    hanel<double, NSP, NSPC>(Lf, Rt, F);
+                else
+                    ausmdv<double, NSP, NSPC>(Lf, Rt, F);
+            } else {
+                ausmdv<double, NSP, NSPC>(Lf, Rt, F);
+            }
+            V3<double> m{F[1], F[2], F[3]};
+            to_global(m, fr.n, fr.t1, fr.t2);
+            F[1] = m.x; F[2] = m.y; F[3] = m.z;
+#pragma unroll
+            for (int q = 0; q < 5 + NSPC; ++q) Fo[q * b.npad + f] = F[q];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Cell update: time_derivatives + stage update + decode + validity check
 // (fvcell.d:735-875, 1153-1311, 563-732; fluidblock.d:433-499)

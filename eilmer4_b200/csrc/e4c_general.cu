@@ -772,8 +772,45 @@ void launch_replay_base(const BlockView& b, const SimDev* sim, cudaStream_t s) {
     k_replay_base<<<grid_for(n, T), T, 0, s>>>(b, sim);
 }
 
+// Faces per run of the row-walking flux kernel: i faces (runs of neighbouring
+// threads interleave along the row) and j, k faces (threads along i).
+#ifndef E4C_ROW_RUN_I
+#define E4C_ROW_RUN_I 8
+#endif
+#ifndef E4C_ROW_RUN_JK
+#define E4C_ROW_RUN_JK 32
+#endif
+
+int3 flux_row_runs(const BlockView& b) {
+    const int nf[3] = {b.ni + 1, b.nj + 1, b.nk + 1};
+    int r[3];
+    for (int d = 0; d < 3; ++d) {
+        const int len = d == 0 ? E4C_ROW_RUN_I : E4C_ROW_RUN_JK;
+        r[d] = (nf[d] + len - 1) / len;
+        if (r[d] < 1) r[d] = 1;
+    }
+    return make_int3(r[0], r[1], r[2]);
+}
+
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
                  cudaStream_t s) {
+    if (dir < 0 && b.Vrt && o.order2 && o.local_frame) {
+        // general face frames: every direction's rows in one launch
+        const int3 runs = flux_row_runs(b);
+        long long n = (long long)b.nj * b.nk * runs.x + (long long)b.ni * b.nk * runs.y;
+        if (b.dim == 3) n += (long long)b.ni * b.nj * runs.z;
+        const int T = 128;
+        const int g = grid_for(n, T);
+        if (b.nsp == 5) {
+            launch_flux_rows_tp(b, sim, o, runs, g, T, s);
+        } else {
+            if (o.flux == 1) k_flux_rows<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+            else if (o.flux == 2) k_flux_rows<1, 2, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+            else if (o.flux == 3) k_flux_rows<1, 3, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+            else k_flux_rows<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+        }
+        return;
+    }
     long long n = 0;
     for (int d = 0; d < b.dim; ++d)
         if (dir < 0 || d == dir)
