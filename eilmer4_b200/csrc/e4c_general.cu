@@ -773,7 +773,10 @@ void launch_replay_base(const BlockView& b, const SimDev* sim, cudaStream_t s) {
 }
 
 // Faces per run of the row-walking flux kernel: i faces (runs of neighbouring
-// threads interleave along the row) and j, k faces (threads along i).
+// threads interleave along the row) and j, k faces (threads along i).  Long
+// runs share the stencil replay of a run's first face over more faces; small
+// blocks halve them until the launch has about half an SM-full of threads on
+// every SM.
 #ifndef E4C_ROW_RUN_I
 #define E4C_ROW_RUN_I 8
 #endif
@@ -781,34 +784,45 @@ void launch_replay_base(const BlockView& b, const SimDev* sim, cudaStream_t s) {
 #define E4C_ROW_RUN_JK 32
 #endif
 
+static long long row_threads(const BlockView& b, const int r[3]) {
+    long long n = (long long)b.nj * b.nk * r[0] + (long long)b.ni * b.nk * r[1];
+    if (b.dim == 3) n += (long long)b.ni * b.nj * r[2];
+    return n;
+}
+
 int3 flux_row_runs(const BlockView& b) {
     const int nf[3] = {b.ni + 1, b.nj + 1, b.nk + 1};
+    const long long want = 148LL * 1024;
     int r[3];
-    for (int d = 0; d < 3; ++d) {
-        const int len = d == 0 ? E4C_ROW_RUN_I : E4C_ROW_RUN_JK;
-        r[d] = (nf[d] + len - 1) / len;
-        if (r[d] < 1) r[d] = 1;
+    for (int shift = 0;; ++shift) {
+        bool all_single = true;
+        for (int d = 0; d < 3; ++d) {
+            int len = (d == 0 ? E4C_ROW_RUN_I : E4C_ROW_RUN_JK) >> shift;
+            if (len < 1) len = 1;
+            all_single = all_single && len == 1;
+            r[d] = (nf[d] + len - 1) / len;
+        }
+        if (all_single || row_threads(b, r) >= want) break;
     }
     return make_int3(r[0], r[1], r[2]);
 }
 
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
                  cudaStream_t s) {
-    if (dir < 0 && b.Vrt && o.order2 && o.local_frame) {
-        // general face frames: every direction's rows in one launch
+    if (dir < 0 && b.Vrt && o.order2 && o.local_frame && b.dim == 3 && b.nsp == 1) {
+        // general face frames of a 3-D ideal-gas block: every direction's rows
+        // in one launch.  (The 5-species form of the row kernel would spill
+        // under its register cap, and 2-D rows are too few to run long: those
+        // blocks keep one thread per face, starting from k_replay_base.)
         const int3 runs = flux_row_runs(b);
-        long long n = (long long)b.nj * b.nk * runs.x + (long long)b.ni * b.nk * runs.y;
-        if (b.dim == 3) n += (long long)b.ni * b.nj * runs.z;
+        const int r[3] = {runs.x, runs.y, runs.z};
+        const long long n = row_threads(b, r);
         const int T = 128;
         const int g = grid_for(n, T);
-        if (b.nsp == 5) {
-            launch_flux_rows_tp(b, sim, o, runs, g, T, s);
-        } else {
-            if (o.flux == 1) k_flux_rows<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-            else if (o.flux == 2) k_flux_rows<1, 2, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-            else if (o.flux == 3) k_flux_rows<1, 3, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-            else k_flux_rows<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-        }
+        if (o.flux == 1) k_flux_rows<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+        else if (o.flux == 2) k_flux_rows<1, 2, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+        else if (o.flux == 3) k_flux_rows<1, 3, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+        else k_flux_rows<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, runs);
         return;
     }
     long long n = 0;

@@ -62,8 +62,6 @@ void launch_dt_chem_copy(const BlockView& b, double* dense, int to_dense, cudaSt
 // thermally perfect face fluxes / cell updates (e4c_tp.cu)
 void launch_flux_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir, int g,
                     int T, cudaStream_t s);
-void launch_flux_rows_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, int3 runs,
-                         int g, int T, cudaStream_t s);
 void launch_update_tp(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
                       int final_stage, int g, int T, cudaStream_t s);
 // training pairs of the chemistry seed: list of the cells needing Newton work

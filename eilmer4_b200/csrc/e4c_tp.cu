@@ -189,14 +189,6 @@ void launch_flux_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, in
     else k_flux<5, 0, 1><<<g, T, 0, s>>>(b, sim, o, dir);
 }
 
-void launch_flux_rows_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, int3 runs,
-                         int g, int T, cudaStream_t s) {
-    if (o.flux == 1) k_flux_rows<5, 1, 1><<<g, T, 0, s>>>(b, sim, o, runs);
-    else if (o.flux == 2) k_flux_rows<5, 2, 1><<<g, T, 0, s>>>(b, sim, o, runs);
-    else if (o.flux == 3) k_flux_rows<5, 3, 1><<<g, T, 0, s>>>(b, sim, o, runs);
-    else k_flux_rows<5, 0, 1><<<g, T, 0, s>>>(b, sim, o, runs);
-}
-
 void launch_update_tp(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
                       int final_stage, int g, int T, cudaStream_t s) {
     k_update<5, 1><<<g, T, 0, s>>>(b, sim, gas, stage, final_stage);
