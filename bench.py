@@ -17,6 +17,9 @@ same line also carries, each timed the same way on its own simulation:
       FP64 run after the same steps;
   "batched": 64 uneven blocks (edges log-uniform in [16, 96]) in one
       persistent launch per stage inside a CUDA graph, autotuned tiles;
+  "curvilinear": a 128^3 curvilinear block (the unit box with every vertex
+      displaced by smooth sines) on the general path, with per-kernel-class
+      times and the CPU oracle on a 96^3 block of the same grid;
   "reacting": the 512x256 5-species reacting ramp channel, 300 steps, with
       reacting cells/s, Newton iterations per reacting cell and the chemistry
       share of the step;
@@ -449,6 +452,67 @@ def batched_case(args, local_rank):
     }
 
 
+def cpu_oracle_curvilinear(n, steps, flux):
+    """Cell-updates/s of the CPU FP64 oracle (OpenMP, all cores) on an n^3
+    curvilinear block (workloads.skewed_box_3d)."""
+    from eilmer4_b200 import workloads as W
+    from oracle import e4_oracle as O
+    O.build()
+    wl = W.skewed_box_3d(ni=n, nj=n, nk=n, flux=flux)
+    b = wl.blocks[0]
+    cfg = O.default_config(dimensions=3, flux_calculator=O.FLUX_HLLC if flux == "hllc"
+                           else O.FLUX_AUSMDV, n_threads=0)
+    sim = O.OracleSim(cfg)
+    sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    sim.set_flow(0, b.prim)
+    sim.run(1)
+    t0 = time.perf_counter()
+    rc = sim.run(steps)
+    dt = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(f"oracle failed: {rc}")
+    return n ** 3 * steps / dt, os.cpu_count() or 1, dt
+
+
+def curvilinear_case(args, local_rank):
+    """A curvilinear 3-D block (every vertex of the unit box displaced by
+    smooth sines): the general path, whose face frames are no axis
+    permutations, so the reference's in-place frame round trips are carried
+    through every face."""
+    import torch
+
+    from eilmer4_b200 import workloads as W
+    from eilmer4_b200.simcore import Simulation
+
+    n = args.curv_n
+    wl = W.skewed_box_3d(ni=n, nj=n, nk=n, flux=args.flux)
+    ncell = wl.ncell
+    sim = Simulation.from_workload(wl, device=local_rank)
+    ext = torch.cuda.ExternalStream(sim.stream_handle(), device=local_rank)
+    for _ in range(args.warmup):
+        sim.run(1)
+    sim.synchronize()
+    ms, launches = _timed_steps(sim, ext, args.curv_steps)
+    prof = sim.profile(args.profile_steps)
+    sim.close()
+    res = {
+        "workload": f"skewed_box_3d {n}^3 (curvilinear, amplitude 0.04), {args.flux}, "
+                    "MUSCL/vanAlbada in the face frame, PC, CFL 0.5, fp64, general path",
+        "cells": ncell, "steps": args.curv_steps,
+        "value": ncell * args.curv_steps / (ms * 1e-3), "unit": UNIT,
+        "ms_per_step": ms / args.curv_steps,
+        "kernel_ms_per_step": {k: v[0] / args.profile_steps for k, v in prof.items() if v[1]},
+        "gpu_launches": launches,
+        "cpu_baseline": None,
+    }
+    if not args.no_cpu_baseline:
+        rate, cores, secs = cpu_oracle_curvilinear(args.curv_cpu_n, args.curv_cpu_steps, args.flux)
+        res["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"{args.curv_cpu_n}^3 block of the same grid, "
+                                         f"{args.curv_cpu_steps} steps, {secs:.1f} s"}
+    return res
+
+
 def reacting_case(args, local_rank):
     """512x256 5-species reacting ramp channel: gas dynamics + point-implicit
     chemistry every step."""
@@ -614,7 +678,8 @@ def run_ours(args, rank, world, local_rank):
         # one part alone (profiling runs): its own JSON line
         fn = {"reacting": lambda: reacting_case(args, local_rank)[0],
               "learned": lambda: learned_case(args, local_rank),
-              "batched": lambda: batched_case(args, local_rank)}[args.part]
+              "batched": lambda: batched_case(args, local_rank),
+              "curvilinear": lambda: curvilinear_case(args, local_rank)}[args.part]
         if rank == 0:
             print(json.dumps({"part": args.part, **fn()}), flush=True)
         return
@@ -629,6 +694,7 @@ def run_ours(args, rank, world, local_rank):
                                   else head["value"] / res["value"])
         extra["fp32_flux" if other == "fp32_flux" else "plain_fp64"] = res
         extra["batched"] = batched_case(args, local_rank)
+        extra["curvilinear"] = curvilinear_case(args, local_rank)
         extra["reacting"], _ = reacting_case(args, local_rank)
         if not args.no_learned:
             extra["learned"] = learned_case(args, local_rank)
@@ -692,9 +758,15 @@ def main():
     ap.add_argument("--headline-only", action="store_true",
                     help="only the --precision 256^3 line, no FP32/batched/reacting parts")
     ap.add_argument("--batched-steps", type=int, default=20)
+    ap.add_argument("--curv-n", type=int, default=128,
+                    help="edge of the curvilinear general-path block")
+    ap.add_argument("--curv-steps", type=int, default=40)
+    ap.add_argument("--curv-cpu-n", type=int, default=96)
+    ap.add_argument("--curv-cpu-steps", type=int, default=5)
     ap.add_argument("--reacting-steps", type=int, default=300)
     ap.add_argument("--no-learned", action="store_true")
-    ap.add_argument("--part", default="all", choices=["all", "reacting", "learned", "batched"],
+    ap.add_argument("--part", default="all",
+                    choices=["all", "reacting", "learned", "batched", "curvilinear"],
                     help="run one sub-part alone (for profiling)")
     ap.add_argument("--seed-pairs", type=int, default=10_000_000)
     ap.add_argument("--seed-epochs", type=int, default=8)

@@ -37,5 +37,5 @@ def test_bench_options_parse():
                          capture_output=True, text=True, timeout=300, cwd=ROOT)
     assert out.returncode == 0
     for opt in ("--gpus", "--steps", "--warmup", "--impl", "--precision", "--tile", "--part",
-                "--headline-only", "--no-ref-gpu-chem"):
+                "--headline-only", "--no-ref-gpu-chem", "--curv-n"):
         assert opt in out.stdout, opt
