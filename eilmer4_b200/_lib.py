@@ -150,6 +150,7 @@ def load():
         "e4c_profile_steps": ([i, dp, ip], i),
         "e4c_set_tile": ([i, i, i], i),
         "e4c_get_tile": ([ip, ip, ip], i),
+        "e4c_set_flux_runs": ([i, i], i),
         "e4c_autotune": ([i, ip, ip, ip, dp], i),
         "e4c_dt_allow_noalloc": ([ip, i, d, i, dp, dp], i),
         "e4c_set_thermochem": ([P(E4CThermoChem)], i),

@@ -314,6 +314,8 @@ int e4c_init(const e4c_config* cfg) {
     c.fopts.gas = c.gas;
     c.fopts.shear_tol = cfg->shear_tolerance;
     c.fopts.compression_tol = cfg->compression_tolerance;
+    c.fopts.row_run_i = 0;
+    c.fopts.row_run_jk = 0;
     E4C_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     E4C_CUDA(cudaStreamCreateWithFlags(&c.h2d_stream, cudaStreamNonBlocking));
     E4C_CUDA(cudaStreamCreateWithFlags(&c.d2h_stream, cudaStreamNonBlocking));
@@ -917,6 +919,18 @@ int e4c_set_tile(int ti, int tj, int kc) {
     c.tile_tj = tj;
     c.tile_kc = kc;
     c.descs_valid = false;
+    c.reset_graphs();
+    return E4C_OK;
+}
+
+int e4c_set_flux_runs(int i_faces, int jk_faces) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (i_faces < 0 || jk_faces < 0 || (i_faces == 0) != (jk_faces == 0) || i_faces > 4096 ||
+        jk_faces > 4096)
+        return fail(E4C_ERR_ARG, "flux run lengths: both 0, or both in 1..4096");
+    c.fopts.row_run_i = i_faces;
+    c.fopts.row_run_jk = jk_faces;
     c.reset_graphs();
     return E4C_OK;
 }

@@ -776,7 +776,7 @@ void launch_replay_base(const BlockView& b, const SimDev* sim, cudaStream_t s) {
 // threads interleave along the row) and j, k faces (threads along i).  Long
 // runs share the stencil replay of a run's first face over more faces; small
 // blocks halve them until the launch has about half an SM-full of threads on
-// every SM.
+// every SM.  e4c_set_flux_runs fixes both lengths.
 #ifndef E4C_ROW_RUN_I
 #define E4C_ROW_RUN_I 8
 #endif
@@ -790,14 +790,17 @@ static long long row_threads(const BlockView& b, const int r[3]) {
     return n;
 }
 
-int3 flux_row_runs(const BlockView& b) {
+int3 flux_row_runs(const BlockView& b, const FluxOpts& o) {
     const int nf[3] = {b.ni + 1, b.nj + 1, b.nk + 1};
-    const long long want = 148LL * 1024;
+    const bool fixed = o.row_run_i > 0 && o.row_run_jk > 0;
+    const long long want = fixed ? 0 : 148LL * 1024;
+    const int base_i = fixed ? o.row_run_i : E4C_ROW_RUN_I;
+    const int base_jk = fixed ? o.row_run_jk : E4C_ROW_RUN_JK;
     int r[3];
     for (int shift = 0;; ++shift) {
         bool all_single = true;
         for (int d = 0; d < 3; ++d) {
-            int len = (d == 0 ? E4C_ROW_RUN_I : E4C_ROW_RUN_JK) >> shift;
+            int len = (d == 0 ? base_i : base_jk) >> shift;
             if (len < 1) len = 1;
             all_single = all_single && len == 1;
             r[d] = (nf[d] + len - 1) / len;
@@ -814,7 +817,7 @@ void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int d
         // in one launch.  (The 5-species form of the row kernel would spill
         // under its register cap, and 2-D rows are too few to run long: those
         // blocks keep one thread per face, starting from k_replay_base.)
-        const int3 runs = flux_row_runs(b);
+        const int3 runs = flux_row_runs(b, o);
         const int r[3] = {runs.x, runs.y, runs.z};
         const long long n = row_threads(b, r);
         const int T = 128;

@@ -17,6 +17,7 @@ struct FluxOpts {
     GasConsts gas;
     double shear_tol;        // adaptive flux: shear_tolerance
     double compression_tol;  // shock detector: compression_tolerance
+    int row_run_i, row_run_jk;  // faces per run of k_flux_rows (0: chosen per block)
 };
 
 // general-geometry FP64 path (e4c_general.cu)

@@ -283,6 +283,11 @@ class Simulation:
     def set_tile(self, ti, tj, kc):
         _lib.check(self.L.e4c_set_tile(int(ti), int(tj), int(kc)))
 
+    def set_flux_runs(self, i_faces, jk_faces):
+        """Faces per thread of the row-walking flux kernel (curvilinear 3-D
+        ideal-gas blocks); (0, 0) restores the per-block choice."""
+        _lib.check(self.L.e4c_set_flux_runs(int(i_faces), int(jk_faces)))
+
     def get_tile(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _lib.check(self.L.e4c_get_tile(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))

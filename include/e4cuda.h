@@ -337,9 +337,17 @@ int e4c_profile_steps(int nsteps, double* ms, int* launches);
 
 /* Tile shape of the fused stage kernel used for blocks with uniform
  * Cartesian geometry: ti x tj cells per CTA in the i-j plane, marching kc
- * planes in k.  Available (ti, tj): (32,8), (32,4), (16,8), (64,4), (16,16). */
+ * planes in k.  Available (ti, tj): (32,8), (32,4), (16,8), (64,4), (16,16),
+ * (32,16). */
 int e4c_set_tile(int ti, int tj, int kc);
 int e4c_get_tile(int* ti, int* tj, int* kc);
+
+/* Faces per thread of the row-walking flux kernel that 3-D ideal-gas blocks
+ * with general (curvilinear) face frames use: i_faces consecutive i faces,
+ * jk_faces consecutive j or k faces.  Both 0 (the default): 8 and 32, halved
+ * on small blocks until the launch fills the GPU.  Results do not depend on
+ * the lengths (every length gives the same bits); they only set the speed. */
+int e4c_set_flux_runs(int i_faces, int jk_faces);
 
 /* Autotuner: time nsteps steps with every available tile shape and k-chunk
  * length on the current blocks, keep the fastest, and restore the flow state

@@ -62,3 +62,40 @@ def test_skewed_box_reacting_bitexact(oracle, e4lib):
     assert (t, dt, st) == (osim.time, osim.dt_global, osim.step)
     assert_same(gc, oc, "conserved")
     assert_same(gp, op, "primitive")
+
+
+@pytest.fixture(scope="module")
+def skewed_mid_oracle(oracle):
+    """A 40x36x34 curvilinear block after 8 steps of the oracle, per flux."""
+    out = {}
+    for flux, fl in (("hllc", oracle.FLUX_HLLC),
+                     ("adaptive_hanel_ausmdv", oracle.FLUX_ADAPTIVE_HANEL_AUSMDV)):
+        wl = W.skewed_box_3d(ni=40, nj=36, nk=34, flux=flux)
+        cfg = oracle.default_config(dimensions=3, n_threads=0, flux_calculator=fl)
+        osim = oracle.OracleSim(cfg)
+        b = wl.blocks[0]
+        osim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+        osim.set_flow(0, b.prim)
+        assert osim.run(8) == 0
+        out[flux] = (wl, osim.get_flow(0), (osim.time, osim.dt_global, osim.step))
+    return out
+
+
+@pytest.mark.parametrize("flux,runs", [("hllc", (8, 32)), ("hllc", (3, 5)), ("hllc", (1, 1)),
+                                       ("hllc", (64, 64)),
+                                       ("adaptive_hanel_ausmdv", (8, 32))])
+def test_row_walk_any_run_length_bitexact(skewed_mid_oracle, e4lib, flux, runs):
+    """The row-walking flux kernel carries the reference's in-place frame
+    round trips along runs of faces (sfluidblock.d:2190-2344 loop order,
+    onedinterp.d:445-454, 576-584).  Long runs, uneven runs (3 i-faces, 5 j/k
+    faces per thread on rows of 41, 37 and 35 faces), one face per run, and
+    runs longer than a row all give the oracle's bits."""
+    from eilmer4_b200.simcore import Simulation
+    wl, (op, oc), state = skewed_mid_oracle[flux]
+    with Simulation.from_workload(wl) as sim:
+        sim.set_flux_runs(*runs)
+        sim.run(8)
+        gp, gc = sim.download(0)
+        assert tuple(sim.state()) == state
+    assert_same(gc, oc, "conserved")
+    assert_same(gp, op, "primitive")
