@@ -259,6 +259,25 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
     }
 }
 
+// 8-byte asynchronous global -> shared copies of one thread (cp.async; the
+// thread waits for its own copies only).
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Values a run fetches ahead for its next face: the entering cell's rho,
+// velocity (its replayed base where it has one), p, u, a, T and length along
+// the row, and the face frame n, t1, t2.
+constexpr int kRowPrefetch = 18;
+constexpr int kRowThreads = 128;
+
 // Faces of a block with general face frames (second order, reconstruction in
 // the face frame), a run of consecutive faces of one row per thread.  The
 // reference's in-place round trips (onedinterp.d:445-454, 576-584) are taken
@@ -270,11 +289,17 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
 // i faces are interleaved across threads (neighbouring threads take
 // neighbouring runs of a row); j and k faces are taken with i fastest.
 // runs[d]: runs per row of direction d.
+// The next face's loads are issued into shared memory (two slots, by face
+// parity) before the current face is computed, so their latency hides behind
+// its arithmetic.  Launched with kRowThreads threads per block.
 template <int NSP, int FLUX, int GAS>
-__global__ void k_flux_rows(BlockView b, const SimDev* sim, FluxOpts o, int3 runs) {
+__global__ void __launch_bounds__(kRowThreads) k_flux_rows(BlockView b, const SimDev* sim,
+                                                          FluxOpts o, int3 runs) {
+    static_assert(NSP == 1, "the row walk serves ideal-gas blocks");
+    __shared__ double s_pf[2][kRowPrefetch][kRowThreads];
+    const int tid = threadIdx.x;
     if (sim->status != 0 || sim->finished) return;
     const int nrun[3] = {runs.x, runs.y, runs.z};
-    const int next[3] = {b.ni, b.nj, b.nk};
     long long nd[3];
     for (int d = 0; d < 3; ++d) {
         const long long rows = d == 0 ? (long long)b.nj * b.nk
@@ -304,9 +329,11 @@ __global__ void k_flux_rows(BlockView b, const SimDev* sim, FluxOpts o, int3 run
             run = int(t / ((long long)b.ni * b.nj));
         }
         const int lo = dir == 0 ? b.imin : (dir == 1 ? b.jmin : b.kmin);
-        const int nf = next[dir] + 1;  // faces lo .. lo + nf - 1 of the row
-        const int g0 = lo + int((long long)run * nf / nrun[dir]);
-        const int g1 = lo + int((long long)(run + 1) * nf / nrun[dir]);
+        // faces lo .. lo + nf - 1 of the row, in nr runs
+        const int nf = (dir == 0 ? b.ni : (dir == 1 ? b.nj : b.nk)) + 1;
+        const int nr = dir == 0 ? runs.x : (dir == 1 ? runs.y : runs.z);
+        const int g0 = lo + int((long long)run * nf / nr);
+        const int g1 = lo + int((long long)(run + 1) * nf / nr);
         const size_t stride = dir == 0 ? 1 : (dir == 1 ? size_t(b.nidim) : size_t(b.nidim) * b.njdim);
         const double* fg = dir == 0 ? b.fgi : (dir == 1 ? b.fgj : b.fgk);
         double* Fo = dir == 0 ? b.Fi : (dir == 1 ? b.Fj : b.Fk);
@@ -333,23 +360,58 @@ __global__ void k_flux_rows(BlockView b, const SimDev* sim, FluxOpts o, int3 run
                 wl[q] = len[c];
             }
         }
-        for (int g = g0; g < g1; ++g) {
+        const int hi = dir == 0 ? b.imax : (dir == 1 ? b.jmax : b.kmax);
+        size_t f;
+        {
             int ci, cj, ck;
-            coords(g, ci, cj, ck);
-            const size_t f = pidx(b, ci, cj, ck);
+            coords(g0, ci, cj, ck);
+            f = pidx(b, ci, cj, ck);
+        }
+        for (int g = g0; g < g1; ++g, f += stride) {
+            Frame<double> fr;
             if (g > g0) {
+                // the entering cell g+1 (it has met no face of this row yet:
+                // its velocity is its base) and the frame of face g
+                cp_async_wait_all();
+                const int sl = g & 1;
 #pragma unroll
                 for (int q = 0; q < 3; ++q) { w[q] = w[q + 1]; wl[q] = wl[q + 1]; }
-                const size_t c = f + stride;
-                load_prim<NSP>(b, c, w[3]);
-                wl[3] = len[c];
-                int ni_, nj_, nk_;
-                coords(g + 1, ni_, nj_, nk_);
-                // a cell entering the window has met no face of this row yet
-                replay_roundtrips(b, dir, g, ni_, nj_, nk_, c, w[3].vel);
+                w[3].rho = s_pf[sl][0][tid];
+                w[3].vel = {s_pf[sl][1][tid], s_pf[sl][2][tid], s_pf[sl][3][tid]};
+                w[3].p = s_pf[sl][4][tid];
+                w[3].u = s_pf[sl][5][tid];
+                w[3].a = s_pf[sl][6][tid];
+                w[3].T = s_pf[sl][7][tid];
+                w[3].massf[0] = 1.0;
+                wl[3] = s_pf[sl][8][tid];
+                fr.n = {s_pf[sl][9][tid], s_pf[sl][10][tid], s_pf[sl][11][tid]};
+                fr.t1 = {s_pf[sl][12][tid], s_pf[sl][13][tid], s_pf[sl][14][tid]};
+                fr.t2 = {s_pf[sl][15][tid], s_pf[sl][16][tid], s_pf[sl][17][tid]};
+            } else {
+                load_frame(fg, b.npad, f, fr);
             }
-            Frame<double> fr;
-            load_frame(fg, b.npad, f, fr);
+            if (g + 1 < g1) {
+                // face g+1: its entering cell g+2 (within the two ghost layers)
+                // and its frame
+                const int sl = (g + 1) & 1;
+                const size_t fn = f + stride, c = fn + stride;
+                const int x = g + 2;
+                const double* V = (dir > 0 && x >= lo && x <= hi)
+                                      ? b.Vrt + size_t(3 * (dir - 1)) * b.npad
+                                      : b.W + size_t(W_VX) * b.npad;
+                cp_async8(&s_pf[sl][0][tid], b.W + size_t(W_RHO) * b.npad + c);
+                cp_async8(&s_pf[sl][1][tid], V + c);
+                cp_async8(&s_pf[sl][2][tid], V + b.npad + c);
+                cp_async8(&s_pf[sl][3][tid], V + 2 * b.npad + c);
+                cp_async8(&s_pf[sl][4][tid], b.W + size_t(W_P) * b.npad + c);
+                cp_async8(&s_pf[sl][5][tid], b.W + size_t(W_U) * b.npad + c);
+                cp_async8(&s_pf[sl][6][tid], b.W + size_t(W_A) * b.npad + c);
+                cp_async8(&s_pf[sl][7][tid], b.W + size_t(W_T) * b.npad + c);
+                cp_async8(&s_pf[sl][8][tid], len + c);
+#pragma unroll
+                for (int q = 0; q < 9; ++q) cp_async8(&s_pf[sl][9 + q][tid], fg + q * b.npad + fn);
+                cp_async_commit();
+            }
             Prim<double, NSP> sL1 = w[0], sL0 = w[1], sR0 = w[2], sR1 = w[3];
             to_local(sL1.vel, fr.n, fr.t1, fr.t2);
             to_local(sL0.vel, fr.n, fr.t1, fr.t2);

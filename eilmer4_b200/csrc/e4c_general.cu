@@ -820,7 +820,7 @@ void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int d
         const int3 runs = flux_row_runs(b, o);
         const int r[3] = {runs.x, runs.y, runs.z};
         const long long n = row_threads(b, r);
-        const int T = 128;
+        const int T = kRowThreads;
         const int g = grid_for(n, T);
         if (o.flux == 1) k_flux_rows<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, runs);
         else if (o.flux == 2) k_flux_rows<1, 2, 0><<<g, T, 0, s>>>(b, sim, o, runs);
