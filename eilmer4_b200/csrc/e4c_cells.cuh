@@ -278,8 +278,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 constexpr int kRowPrefetch = 18;
 constexpr int kRowThreads = 128;
 
-// Faces of a block with general face frames (second order, reconstruction in
-// the face frame), a run of consecutive faces of one row per thread.  The
+// Faces of a 3-D ideal-gas block (second order, reconstruction in the face
+// frame), a run of consecutive faces of one row per thread.  The
 // reference's in-place round trips (onedinterp.d:445-454, 576-584) are taken
 // literally: the thread holds its four stencil cells with their velocities as
 // the reference holds them, turns them into the face frame for the
@@ -292,13 +292,19 @@ constexpr int kRowThreads = 128;
 // The next face's loads are issued into shared memory (two slots, by face
 // parity) before the current face is computed, so their latency hides behind
 // its arithmetic.  Launched with kRowThreads threads per block.
-template <int NSP, int FLUX, int GAS>
+// MUTATE: the block's frames are general (b.Vrt holds the replayed bases).
+template <int NSP, int FLUX, int GAS, bool MUTATE>
 __global__ void __launch_bounds__(kRowThreads) k_flux_rows(BlockView b, const SimDev* sim,
                                                           FluxOpts o, int3 runs) {
     static_assert(NSP == 1, "the row walk serves ideal-gas blocks");
     __shared__ double s_pf[2][kRowPrefetch][kRowThreads];
     const int tid = threadIdx.x;
     if (sim->status != 0 || sim->finished) return;
+    // blocks whose frames are all signed unit axes: the round trips are exact
+    // (up to the sign of a zero) and the reference copies instead of
+    // mutating (its in-place form only serves general frames), so the cells
+    // keep their velocities
+    constexpr bool mutate = MUTATE;
     const int nrun[3] = {runs.x, runs.y, runs.z};
     long long nd[3];
     for (int d = 0; d < 3; ++d) {
@@ -356,7 +362,7 @@ __global__ void __launch_bounds__(kRowThreads) k_flux_rows(BlockView b, const Si
                 coords(x, ci, cj, ck);
                 const size_t c = f0 + (q - 2) * (long long)stride;
                 load_prim<NSP>(b, c, w[q]);
-                replay_roundtrips(b, dir, g0, ci, cj, ck, c, w[q].vel);
+                if (mutate) replay_roundtrips(b, dir, g0, ci, cj, ck, c, w[q].vel);
                 wl[q] = len[c];
             }
         }
@@ -396,7 +402,7 @@ __global__ void __launch_bounds__(kRowThreads) k_flux_rows(BlockView b, const Si
                 const int sl = (g + 1) & 1;
                 const size_t fn = f + stride, c = fn + stride;
                 const int x = g + 2;
-                const double* V = (dir > 0 && x >= lo && x <= hi)
+                const double* V = (mutate && dir > 0 && x >= lo && x <= hi)
                                       ? b.Vrt + size_t(3 * (dir - 1)) * b.npad
                                       : b.W + size_t(W_VX) * b.npad;
                 cp_async8(&s_pf[sl][0][tid], b.W + size_t(W_RHO) * b.npad + c);
@@ -448,10 +454,12 @@ __global__ void __launch_bounds__(kRowThreads) k_flux_rows(BlockView b, const Si
             to_global(Rt.vel, fr.n, fr.t1, fr.t2);
             // the stencil cells back to the global frame in place; cell g-2
             // leaves the window and is not needed again
-            to_global(sL0.vel, fr.n, fr.t1, fr.t2);
-            to_global(sR0.vel, fr.n, fr.t1, fr.t2);
-            to_global(sR1.vel, fr.n, fr.t1, fr.t2);
-            w[1].vel = sL0.vel; w[2].vel = sR0.vel; w[3].vel = sR1.vel;
+            if (mutate) {
+                to_global(sL0.vel, fr.n, fr.t1, fr.t2);
+                to_global(sR0.vel, fr.n, fr.t1, fr.t2);
+                to_global(sR1.vel, fr.n, fr.t1, fr.t2);
+                w[1].vel = sL0.vel; w[2].vel = sR0.vel; w[3].vel = sR1.vel;
+            }
             // compute_interface_flux, fluxcalc.d:26-128 (fixed grid)
             to_local(Lf.vel, fr.n, fr.t1, fr.t2);
             to_local(Rt.vel, fr.n, fr.t1, fr.t2);

@@ -812,20 +812,28 @@ int3 flux_row_runs(const BlockView& b, const FluxOpts& o) {
 
 void launch_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, int dir,
                  cudaStream_t s) {
-    if (dir < 0 && b.Vrt && o.order2 && o.local_frame && b.dim == 3 && b.nsp == 1) {
-        // general face frames of a 3-D ideal-gas block: every direction's rows
-        // in one launch.  (The 5-species form of the row kernel would spill
-        // under its register cap, and 2-D rows are too few to run long: those
-        // blocks keep one thread per face, starting from k_replay_base.)
+    if (dir < 0 && o.order2 && o.local_frame && b.dim == 3 && b.nsp == 1) {
+        // a 3-D ideal-gas block: every direction's rows in one launch, each
+        // stencil cell loaded once per run.  (The 5-species form of the row
+        // kernel would spill under its register cap, and 2-D rows are too few
+        // to run long: those blocks keep one thread per face, starting from
+        // k_replay_base where their frames are general.)
         const int3 runs = flux_row_runs(b, o);
         const int r[3] = {runs.x, runs.y, runs.z};
         const long long n = row_threads(b, r);
         const int T = kRowThreads;
         const int g = grid_for(n, T);
-        if (o.flux == 1) k_flux_rows<1, 1, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-        else if (o.flux == 2) k_flux_rows<1, 2, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-        else if (o.flux == 3) k_flux_rows<1, 3, 0><<<g, T, 0, s>>>(b, sim, o, runs);
-        else k_flux_rows<1, 0, 0><<<g, T, 0, s>>>(b, sim, o, runs);
+        if (b.Vrt) {
+            if (o.flux == 1) k_flux_rows<1, 1, 0, true><<<g, T, 0, s>>>(b, sim, o, runs);
+            else if (o.flux == 2) k_flux_rows<1, 2, 0, true><<<g, T, 0, s>>>(b, sim, o, runs);
+            else if (o.flux == 3) k_flux_rows<1, 3, 0, true><<<g, T, 0, s>>>(b, sim, o, runs);
+            else k_flux_rows<1, 0, 0, true><<<g, T, 0, s>>>(b, sim, o, runs);
+        } else {
+            if (o.flux == 1) k_flux_rows<1, 1, 0, false><<<g, T, 0, s>>>(b, sim, o, runs);
+            else if (o.flux == 2) k_flux_rows<1, 2, 0, false><<<g, T, 0, s>>>(b, sim, o, runs);
+            else if (o.flux == 3) k_flux_rows<1, 3, 0, false><<<g, T, 0, s>>>(b, sim, o, runs);
+            else k_flux_rows<1, 0, 0, false><<<g, T, 0, s>>>(b, sim, o, runs);
+        }
         return;
     }
     long long n = 0;
