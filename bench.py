@@ -400,7 +400,9 @@ def euler_case(args, precision, local_rank, dist, world, headline):
         _, cons0 = sim.download(0)
         host_in = torch.from_numpy(cons0).pin_memory()
         host_out = torch.empty((5, ncell), dtype=torch.float64).pin_memory()
-        e2e_steps = max(2, min(args.steps, 10))
+        # enough steps that the pipeline's fill (the first upload) and drain
+        # (the last download) do not dominate
+        e2e_steps = max(2, min(args.steps, 30))
         sim.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
