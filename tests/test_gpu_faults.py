@@ -95,3 +95,19 @@ def test_chemistry_recovery_path_bitexact(oracle, e4lib):
             assert dtc[q] == out["dt_chem"], q
     finally:
         oracle.set_chem_newton_iterations(12)
+
+
+def test_bad_flux_run_lengths_are_refused(e4lib):
+    """e4c_set_flux_runs takes both lengths 0 (the per-block choice) or both
+    in 1..4096; anything else is refused with E4C_ERR_ARG and changes
+    nothing."""
+    from eilmer4_b200 import _lib
+    from eilmer4_b200.simcore import Simulation
+    with Simulation.from_workload(W.skewed_box_3d(ni=12, nj=10, nk=8)) as sim:
+        for bad in ((0, 4), (4, 0), (-1, 8), (8, -1), (5000, 8), (8, 5000)):
+            with pytest.raises(_lib.E4CError) as ei:
+                sim.set_flux_runs(*bad)
+            assert ei.value.code == _lib.E4C_ERR_ARG, bad
+        sim.set_flux_runs(2, 3)
+        sim.set_flux_runs(0, 0)
+        assert sim.run(2).status == 0
