@@ -66,6 +66,13 @@ BYTES_PER_REACTING_CELL = 8.0 * (9 + 15)
 # kernel class).  Algorithmic bytes per launch at 256^3: 3020 MB (FP64),
 # 2349 MB (FP32-flux).
 TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2063725568}
+# FP64 arithmetic per cell-update of the fused stage kernel (both stages),
+# keyed by (precision, flux): DADD + DMUL + 2 x DFMA thread instructions per
+# cycle times cycles, from the ncu capture of the 128^3 block with the 32x16
+# tile (the count per cell does not depend on the block size for a tile
+# shape).  Compiled without FMA contraction, the kernel's ceiling is half the
+# FP64 peak (64 DFMA per SM per cycle, 2 FLOP each).
+FP64_FLOP_PER_CELL_UPDATE = {("fp64", "hllc"): 2430.0}
 
 
 def peaks():
@@ -389,6 +396,18 @@ def euler_case(args, precision, local_rank, dist, world, headline):
         "profile_ms": {k: round(v[0] / args.profile_steps, 4) for k, v in prof.items()},
         "gpu_launches": launches,
     }
+    fpc = FP64_FLOP_PER_CELL_UPDATE.get((precision, args.flux))
+    if fpc is not None and cls == "stage":
+        # the second bound: FP64 FLOP/s of the same launches (same time base as
+        # `roofline.achieved`) against the FP64 peak at the sampled SM clock
+        mhz = (clk or {}).get("sm_mhz") or 1965.0
+        nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        peak_tf = nsm * 64 * 2 * mhz * 1e6 / 1e12
+        ach_tf = achieved * fpc / bpc / 1e3
+        res["fp64_roofline"] = {"bound": "fp64", "kernel": cls, "achieved": ach_tf,
+                                "peak": peak_tf, "unit": "TFLOP/s", "frac": ach_tf / peak_tf,
+                                "flop_per_cell_update": fpc, "no_fma_ceiling_frac": 0.5,
+                                "peak_kind": "64 DFMA per SM per cycle at the sampled SM clock"}
     if clk is not None:
         res["clocks"] = clk
     if headline:
@@ -721,6 +740,7 @@ def run_ours(args, rank, world, local_rank):
                        "parallelism": f"replicas x{world}" if world > 1 else "single"},
             "tile": head["tile"],
             "roofline": head["roofline"],
+            "fp64_roofline": head.get("fp64_roofline"),
             "profile_ms": head["profile_ms"],
             "gpu_launches": head["gpu_launches"],
             "clocks": head.get("clocks"),
