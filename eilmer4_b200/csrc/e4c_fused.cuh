@@ -400,7 +400,6 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
             // plane k+2 replaces plane k-2 (not read since the previous iteration)
             load_plane<R, TI, TJ>(descs, stage, d, Win, use_a0, gas, planes + ((k + 2 + 8) & 3) * S::PLANE, i0, j0,
                                   k + 2);
-            __syncthreads();
             const R* pk = planes + ((k + 8) & 3) * S::PLANE;
             if (share_va) {
                 // van Albada values of the cells of this plane that the i- and
@@ -427,8 +426,11 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                         dst[f * vs] = w[dir].va(q[-step], q[0], q[step]);
                     }
                 }
-                __syncthreads();
             }
+            // plane k+2 and the limiter values of plane k are in place (plane k
+            // was loaded two iterations ago: the values need no barrier of
+            // their own, and the loads overlap their divisions)
+            __syncthreads();
             // i-faces, (TI+1) x TJ (face fi is the west face of cell i0+fi), then
             // j-faces, TI x (TJ+1) (face fj is the south face of cell j0+fj), as
             // one list over all the CTA's threads
@@ -558,7 +560,9 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
 #pragma unroll
                 for (int v = 0; v < 5; ++v) Fbot[v] = Ftop[v];
             }
-            __syncthreads();
+            // no barrier here: the update reads only Fi/Fj (rewritten after the
+            // next plane's load barrier) and its own registers; the next load
+            // overwrites plane k-1, last read by this plane's k-faces
         }
     }
     if (stage == 2 && blockIdx.x == 0 && threadIdx.x == 0) {
