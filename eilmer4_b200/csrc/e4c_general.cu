@@ -708,20 +708,25 @@ void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_
     k_download<<<grid_for(n, 256), 256, 0, s>>>(b, prim, cons);
 }
 
-void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s) {
+// Cells of the largest boundary face layer of the block (a 2-D block has no
+// top or bottom face: its grid would otherwise be sized by the whole plane).
+static int boundary_extent(const BlockView& b) {
     int m = b.ni * b.nk;
     m = m > b.nj * b.nk ? m : b.nj * b.nk;
-    m = m > b.ni * b.nj ? m : b.ni * b.nj;
-    dim3 grid((m + 127) / 128, 6);
+    if (b.dim == 3) m = m > b.ni * b.nj ? m : b.ni * b.nj;
+    return m;
+}
+
+void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s) {
+    const int m = boundary_extent(b);
+    dim3 grid((m + 127) / 128, b.dim == 3 ? 6 : 4);
     if (b.nsp == 5) k_bc<5><<<grid, 128, 0, s>>>(b, sim);
     else k_bc<1><<<grid, 128, 0, s>>>(b, sim);
 }
 
 void launch_bc_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, cudaStream_t s) {
-    int m = b.ni * b.nk;
-    m = m > b.nj * b.nk ? m : b.nj * b.nk;
-    m = m > b.ni * b.nj ? m : b.ni * b.nj;
-    dim3 grid((m + 127) / 128, 6);
+    const int m = boundary_extent(b);
+    dim3 grid((m + 127) / 128, b.dim == 3 ? 6 : 4);
     if (b.nsp == 5) k_bc_flux<5><<<grid, 128, 0, s>>>(b, sim, o);
     else k_bc_flux<1><<<grid, 128, 0, s>>>(b, sim, o);
 }
