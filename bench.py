@@ -29,10 +29,11 @@ same line also carries, each timed the same way on its own simulation:
       plain and seeded, Newton iterations, chemistry speed-up and the
       mass-fraction difference from the plain update.
 --impl reference times the CPU FP64 restatement of the reference algorithm
-(the D solver itself cannot be built: no D compiler) on the host cores, on a
-bounded sample of the same workload; its line also carries "gpu_chem", the
-reference's own GPU chemistry (GPUChem and its alpha-QSS kernel, built for
-sm_100a) on the high-enthalpy channel's cell states.
+(the D solver itself cannot be built: no D compiler) on the host cores, on the
+bench's own 256^3 block (W warm-up steps, then K steps each timed alone; its
+ms_per_step is the median measured step); its line also carries "gpu_chem",
+the reference's own GPU chemistry (GPUChem and its alpha-QSS kernel, built
+for sm_100a) on the high-enthalpy channel's cell states.
 """
 from __future__ import annotations
 
@@ -264,24 +265,49 @@ def reference_gpu_chem(ni, nj, steps):
 
 
 def run_reference(args, rank, world):
+    """--impl reference: the CPU FP64 restatement of the reference's update
+    (the D solver cannot be built here) on the bench's own block -- the same
+    256^3 workload, flux and initial state -- with OpenMP on every host core.
+    W untimed steps, then K steps each timed alone; ms_per_step is the median
+    measured step.  Rank 0 alone runs it."""
     if rank != 0:
         return
-    n = args.ref_sample
-    rates = []
+    from eilmer4_b200 import workloads as W
+    from oracle import e4_oracle as O
+    O.build()
+    n = args.ref_sample or args.n
+    b = W.inflow_3d_block(n, n, n, W.DEFAULT_SEED)
+    cfg = O.default_config(dimensions=3, flux_calculator=O.FLUX_HLLC if args.flux == "hllc"
+                           else O.FLUX_AUSMDV, n_threads=0)
+    sim = O.OracleSim(cfg)
+    sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    sim.set_flow(0, b.prim)
+    del b
     for _ in range(args.warmup):
-        cpu_oracle_rate(n, 1, args.flux)
+        if sim.run(1) != 0:
+            raise RuntimeError("oracle failed in warm-up")
+    secs = []
     for _ in range(args.steps):
-        r, cores, _ = cpu_oracle_rate(n, 1, args.flux)
-        rates.append(r)
-    value = statistics.median(rates)
-    sample = f"{n}^3 sub-block of the {args.n}^3 workload, 1 time step per bench step"
+        t0 = time.perf_counter()
+        rc = sim.run(1)
+        secs.append(time.perf_counter() - t0)
+        if rc != 0:
+            raise RuntimeError(f"oracle failed: {rc}")
+    del sim
+    step_s = statistics.median(secs)
+    value = n ** 3 / step_s
+    cores = os.cpu_count() or 1
+    workload = (f"inflow_3d {n}^3 ideal air, {args.flux}, MUSCL/vanAlbada, PC, CFL 0.5, "
+                "fp64")
+    sample = (f"the whole {n}^3 block, {args.steps} steps after {args.warmup} warm-up steps, "
+              f"each timed alone (median {step_s:.2f} s, total {sum(secs):.1f} s)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * args.n ** 3 / value, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * step_s, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"inflow_3d {args.n}^3 {args.flux} MUSCL/vanAlbada PC CFL0.5",
-                   "sample": sample, "parallelism": "cpu-openmp"},
+        "config": {"workload": workload, "cells": n ** 3, "sample": sample,
+                   "parallelism": "cpu-openmp", "same_config_as_ours": n == args.n},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -351,15 +377,17 @@ def _roofline_stage(sim, ncell, bpc, profile_steps):
     return cls, achieved, prof
 
 
-def euler_case(args, precision, local_rank, dist, world, headline):
-    """256^3 (or --n) Mach-3 inflow block; returns a result dict and the
-    downloaded density after warm-up + timed steps."""
+def euler_case(args, precision, local_rank, dist, world, headline, flux=None):
+    """256^3 (or --n) Mach-3 inflow block with the --flux calculator (or
+    `flux`); returns a result dict and the downloaded density after warm-up +
+    timed steps."""
     import torch
 
     from eilmer4_b200 import workloads as W
     from eilmer4_b200.simcore import Simulation
 
-    wl = W.inflow_3d(n=args.n, flux=args.flux)
+    flux = flux or args.flux
+    wl = W.inflow_3d(n=args.n, flux=flux)
     blk = wl.blocks[0]
     ncell = blk.ncell
     sim = Simulation.from_workload(wl, precision=precision, device=local_rank)
@@ -386,7 +414,7 @@ def euler_case(args, precision, local_rank, dist, world, headline):
     step_achieved = bpc * ncell / (ms_per_step * 1e-3) / 1e9
     res = {
         "value": value, "unit": UNIT, "ms_per_step": ms_per_step, "steps": args.steps,
-        "dtype": "f64" if precision == "fp64" else "f32-flux/f64-accum",
+        "flux": flux, "dtype": "f64" if precision == "fp64" else "f32-flux/f64-accum",
         "tile": {"ti": tile[0], "tj": tile[1], "kc": tile[2],
                  "autotuned": not (args.no_autotune or args.tile)},
         "roofline": {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": hbm,
@@ -397,7 +425,7 @@ def euler_case(args, precision, local_rank, dist, world, headline):
         "profile_ms": {k: round(v[0] / args.profile_steps, 4) for k, v in prof.items()},
         "gpu_launches": launches,
     }
-    fpc = FP64_FLOP_PER_CELL_UPDATE.get((precision, args.flux))
+    fpc = FP64_FLOP_PER_CELL_UPDATE.get((precision, flux))
     if fpc is not None and cls == "stage":
         # the second bound: FP64 FLOP/s of the same launches (same time base as
         # `roofline.achieved`) against the FP64 peak at the sampled SM clock
@@ -715,6 +743,12 @@ def run_ours(args, rank, world, local_rank):
         res["speedup_vs_fp64"] = (res["value"] / head["value"] if other == "fp32_flux"
                                   else head["value"] / res["value"])
         extra["fp32_flux" if other == "fp32_flux" else "plain_fp64"] = res
+        # the reference's own flux calculator (AUSMDV, fluxcalc.d:376-529) on
+        # the same block in the plain FP64 form
+        other_flux = "ausmdv" if args.flux == "hllc" else "hllc"
+        res, _ = euler_case(args, "fp64", local_rank, dist, world, headline=False,
+                            flux=other_flux)
+        extra[f"{other_flux}_fp64"] = res
         extra["batched"] = batched_case(args, local_rank)
         extra["curvilinear"] = curvilinear_case(args, local_rank)
         extra["reacting"], _ = reacting_case(args, local_rank)
@@ -767,7 +801,9 @@ def main():
     # CPU baseline samples: about 10 s of oracle work each on a 16-core host
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--cpu-steps", type=int, default=20)
-    ap.add_argument("--ref-sample", type=int, default=96)
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="--impl reference: edge of the timed block (default: --n, the "
+                         "bench's own block)")
     ap.add_argument("--cpu-reacting-steps", type=int, default=25)
     ap.add_argument("--no-ref-gpu-chem", action="store_true",
                     help="--impl reference: skip the reference's GPU chemistry kernel")

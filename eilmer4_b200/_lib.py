@@ -153,6 +153,7 @@ def load():
         "e4c_set_flux_runs": ([i, i], i),
         "e4c_autotune": ([i, ip, ip, ip, dp], i),
         "e4c_dt_allow_noalloc": ([ip, i, d, i, dp, dp], i),
+        "e4c_seed_set_wait_limit": ([i], i),
         "e4c_set_thermochem": ([P(E4CThermoChem)], i),
         "e4c_chemistry_step": ([ip, i, d], i),
         "e4c_chemistry_counters": ([P(ctypes.c_longlong), i], i),

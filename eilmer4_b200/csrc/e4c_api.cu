@@ -88,6 +88,7 @@ void Ctx::release() {
     seed = SeedNet{};
     d_dtacc = nullptr;
     dtacc_cap = 0;
+    noalloc_scratch = nullptr;
     d_staging = nullptr;
     staging_bytes = 0;
     d_stage_in = d_stage_out = nullptr;
@@ -301,6 +302,11 @@ int e4c_init(const e4c_config* cfg) {
     E4C_CUDA(cudaSetDevice(cfg->device));
     Ctx& c = g_ctx;
     c.cfg = *cfg;
+    {
+        // the allocation-free dt control's scratch array, on this device
+        int rc = noalloc_setup(&c.noalloc_scratch);
+        if (rc != E4C_OK) return rc;
+    }
     c.gas.Rgas = 8.31451 / cfg->ideal_mol_mass;  // ideal_gas.d:66-69
     c.gas.gamma = cfg->ideal_gamma;
     c.gas.Cv = c.gas.Rgas / (c.gas.gamma - 1.0);

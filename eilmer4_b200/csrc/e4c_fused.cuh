@@ -572,26 +572,26 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
     if (bad) atomicAdd(&sim->bad_cells, bad);
 }
 
-// signal_frequency + block min/max for the fused layout (fvcell.d:1624-1705,
-// fluidblock.d:776-862).  One launch over all fused blocks: blockIdx.y picks
-// the block, a warp reduction precedes one atomic per warp.
+// signal_frequency + block min/max of one fused block (fvcell.d:1624-1705,
+// fluidblock.d:776-862): the cells this thread strides over, a warp
+// reduction, one atomic per warp into acc[0] (min dt) and acc[1] (max CFL);
+// the last cell's signal goes to acc[2].
 template <typename R>
-__global__ void k_fused_dt(const FusedDesc* __restrict__ descs, SimDev* sim, GasConsts gas,
-                           double cfl_value, const double* dt_current_p) {
-    if (sim && (sim->status != 0 || sim->finished)) return;
-    const FusedDesc& d = descs[blockIdx.y];
-    const double dt_current = *dt_current_p;
+__device__ __forceinline__ void fused_dt_cells(const FusedDesc& d, const GasConsts& gas,
+                                               double cfl_value, double dt_current,
+                                               unsigned long long* acc) {
     const long long nc = (long long)d.ni * d.nj * d.nk;
     const R* W = static_cast<const R*>(d.WA);
     const V3<double> nN{d.fn[1][0], d.fn[1][1], d.fn[1][2]};
     const V3<double> nE{d.fn[0][0], d.fn[0][1], d.fn[0][2]};
     const V3<double> nT{d.fn[2][0], d.fn[2][1], d.fn[2][2]};
+    const int use_a0 = *d.use_a0;
     double dmin = DBL_MAX, cmax = 0.0;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
          c += (long long)gridDim.x * blockDim.x) {
         V3<double> v{double(W[1 * nc + c]), double(W[2 * nc + c]), double(W[3 * nc + c])};
         double a;
-        if (*d.use_a0) {
+        if (use_a0) {
             a = d.A0[c];
         } else {
             double T = double(W[4 * nc + c]) * gas.Cvinv;
@@ -606,15 +606,34 @@ __global__ void k_fused_dt(const FusedDesc* __restrict__ descs, SimDev* sim, Gas
         signal = fmax(signal, (un_T + a) / d.len[2]);
         dmin = fmin(dmin, cfl_value / signal);
         cmax = fmax(cmax, dt_current * signal);
-        if (c == nc - 1) d.acc[2] = dbits(signal);
+        if (c == nc - 1) acc[2] = dbits(signal);
     }
     for (int off = 16; off > 0; off >>= 1) {
         dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
         cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
     }
     if ((threadIdx.x & 31) == 0) {
-        atomicMin(&d.acc[0], dbits(dmin));
-        atomicMax(&d.acc[1], dbits(cmax));
+        atomicMin(&acc[0], dbits(dmin));
+        atomicMax(&acc[1], dbits(cmax));
+    }
+}
+
+// The dt reduction for the fused layout.  With a descriptor table, one launch
+// covers all fused blocks (blockIdx.y picks the block, accumulators from the
+// descriptor).  Without one (descs == nullptr), the launch covers the single
+// block `one` passed by value, into the accumulators `one_acc`: the
+// allocation-free dt control uses this form, so both give the same bits.
+template <typename R>
+__global__ void k_fused_dt(const FusedDesc* __restrict__ descs, FusedDesc one,
+                           unsigned long long* one_acc, SimDev* sim, GasConsts gas,
+                           double cfl_value, const double* dt_current_p) {
+    if (sim && (sim->status != 0 || sim->finished)) return;
+    const double dt_current = *dt_current_p;
+    if (descs) {
+        const FusedDesc& d = descs[blockIdx.y];
+        fused_dt_cells<R>(d, gas, cfl_value, dt_current, d.acc);
+    } else {
+        fused_dt_cells<R>(one, gas, cfl_value, dt_current, one_acc);
     }
 }
 

@@ -70,8 +70,15 @@ int fused_occupancy(int flux, int ti, int tj) {
 
 void fused_dt(const void* descs, int nfused, int gx, SimDev* sim, const GasConsts& gas,
               double cfl_value, const double* dt_current, cudaStream_t s) {
-    k_fused_dt<RT><<<dim3(gx, nfused), 256, 0, s>>>(static_cast<const FusedDesc*>(descs), sim, gas,
-                                                   cfl_value, dt_current);
+    k_fused_dt<RT><<<dim3(gx, nfused), 256, 0, s>>>(static_cast<const FusedDesc*>(descs),
+                                                   FusedDesc{}, nullptr, sim, gas, cfl_value,
+                                                   dt_current);
+}
+
+void fused_dt_one(const FusedDesc& d, unsigned long long* acc, int gx, const GasConsts& gas,
+                  double cfl_value, const double* dt_current, cudaStream_t s) {
+    k_fused_dt<RT><<<dim3(gx, 1), 256, 0, s>>>(nullptr, d, acc, nullptr, gas, cfl_value,
+                                              dt_current);
 }
 
 // prim (rho, vx, vy, vz, p, T, u, a) -> W (R), A0 and the encoded U0

@@ -51,6 +51,9 @@ struct SeedNet {
     double* d_guess = nullptr;     // per-cell guesses of the chemistry step [6][ncell]
     size_t guess_cap = 0;
     SeedMolar mol{};
+    // tries of the inference kernel's first wait for the tensor cores (the
+    // second wait after a time-out always takes the full count)
+    int first_wait_tries = 1 << 20;
 };
 
 struct GraphSlot {
@@ -117,6 +120,9 @@ struct Ctx {
     int* d_hlist = nullptr;
     int hlist_cap = 0;
     long long launches = 0;   // kernels enqueued (graph replays add their node count)
+    // device address of the allocation-free dt control's scratch array on
+    // this context's device (resolved by e4c_init)
+    void* noalloc_scratch = nullptr;
     Profiler prof;
     std::string last_error;
 
@@ -155,6 +161,8 @@ struct Ctx {
 };
 
 extern Ctx g_ctx;
+// e4c_noalloc.cu: the scratch array's device address on the current device
+int noalloc_setup(void** out);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 

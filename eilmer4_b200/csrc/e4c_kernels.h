@@ -98,6 +98,9 @@ struct FusedLaunch {
     int fused_occupancy(int flux, int ti, int tj);                                           \
     void fused_dt(const void* descs, int nfused, int gx, SimDev* sim, const GasConsts& gas,  \
                   double cfl_value, const double* dt_current, cudaStream_t s);              \
+    void fused_dt_one(const FusedDesc& d, unsigned long long* acc, int gx,                   \
+                      const GasConsts& gas, double cfl_value, const double* dt_current,      \
+                      cudaStream_t s);                                                       \
     void fused_upload(const double* prim, size_t nc, void* W, double* A0, double* U0,        \
                       cudaStream_t s);                                                       \
     void fused_upload_cons(const double* cons, size_t nc, void* W, double* U0, SimDev* sim,  \

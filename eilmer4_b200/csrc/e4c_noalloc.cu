@@ -8,7 +8,9 @@
 // use; this variant never does.  Its scratch (per-block accumulators, the
 // block list, dt_current and the two results) is one file-scope device array
 // of fixed size, so at most E4C_NOALLOC_MAX_BLOCKS blocks can be reduced in
-// one call.
+// one call.  The kernels are the ones e4c_dt_allow launches (the fused
+// blocks' dt kernel in its single-descriptor form, the general path's dt
+// kernel and the finalising kernel), so the results are the same bits.
 //
 // The array is shared by every call and keeps the last call's contents; each
 // call resets the accumulators it uses before the reduction.  Calls that
@@ -17,9 +19,11 @@
 // single stream and is documented as single-threaded.
 //
 // In host code the name e4c_noalloc_scratch is only a host-side stand-in, not
-// a device address.  The device address is obtained once per device with
-// cudaGetSymbolAddress (with that device current) the first time the entry
-// point runs on it; make that first call before any stream capture.
+// a device address.  e4c_init resolves the device address with
+// cudaGetSymbolAddress, with the library's device current, and keeps it in
+// the library context (cleared by e4c_finalize, resolved again by the next
+// e4c_init).  Resolving it also loads this file's device code, so the array
+// is reserved at e4c_init rather than on the first call inside a time loop.
 #include <cfloat>
 #include <cstring>
 
@@ -38,67 +42,15 @@ constexpr int kScratchWords = kAccWords + kListWords + kScalarWords;
 
 static __device__ __align__(256) unsigned long long e4c_noalloc_scratch[kScratchWords];
 
-// Per-device address of the scratch array (set up once per device).
-static unsigned long long* g_scratch_addr[64] = {nullptr};
-
-static int scratch_for_current_device(unsigned long long** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= 64) return fail(E4C_ERR_ARG, "device ordinal out of range");
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, e4c_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(e4c_noalloc_scratch)");
-        g_scratch_addr[dev] = static_cast<unsigned long long*>(p);
-    }
-    *out = g_scratch_addr[dev];
+// Device address of the scratch array on the current device (called by
+// e4c_init with the library's device current).
+int noalloc_setup(void** out) {
+    *out = nullptr;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, e4c_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(e4c_noalloc_scratch)");
+    *out = p;
     return E4C_OK;
-}
-
-// signal_frequency + min/max for one fused (uniform) block, accumulating into
-// an explicit accumulator triple: the fused dt kernel with its accumulators
-// taken from the caller instead of the block descriptor.
-template <typename R>
-__global__ void k_fused_dt_explicit(FusedDesc d, GasConsts gas, double cfl_value,
-                                    const double* dt_current_p, unsigned long long* acc) {
-    const double dt_current = *dt_current_p;
-    const long long nc = (long long)d.ni * d.nj * d.nk;
-    const R* W = static_cast<const R*>(d.WA);
-    const V3<double> nN{d.fn[1][0], d.fn[1][1], d.fn[1][2]};
-    const V3<double> nE{d.fn[0][0], d.fn[0][1], d.fn[0][2]};
-    const V3<double> nT{d.fn[2][0], d.fn[2][1], d.fn[2][2]};
-    const int use_a0 = *d.use_a0;
-    double dmin = DBL_MAX, cmax = 0.0;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
-         c += (long long)gridDim.x * blockDim.x) {
-        V3<double> v{double(W[1 * nc + c]), double(W[2 * nc + c]), double(W[3 * nc + c])};
-        double a;
-        if (use_a0) {
-            a = d.A0[c];
-        } else {
-            double T = double(W[4 * nc + c]) * gas.Cvinv;
-            a = sqrt(gas.gamma * gas.Rgas * T);
-        }
-        const double un_N = fabs(dot3(v, nN));
-        const double un_E = fabs(dot3(v, nE));
-        const double un_T = fabs(dot3(v, nT));
-        double signal = 0.0;
-        signal = fmax(signal, (un_N + a) / d.len[1]);
-        signal = fmax(signal, (un_E + a) / d.len[0]);
-        signal = fmax(signal, (un_T + a) / d.len[2]);
-        dmin = fmin(dmin, cfl_value / signal);
-        cmax = fmax(cmax, dt_current * signal);
-        if (c == nc - 1) acc[2] = dbits(signal);
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-        dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
-        cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMin(&acc[0], dbits(dmin));
-        atomicMax(&acc[1], dbits(cmax));
-    }
 }
 
 }  // namespace e4c
@@ -108,16 +60,22 @@ using namespace e4c;
 extern "C" int e4c_dt_allow_noalloc(const int* h, int nb, double dt_current, int check_cfl,
                                     double* dt_allow, double* cfl_max) {
     Ctx& c = g_ctx;
-    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.initialised || !c.noalloc_scratch) return fail(E4C_ERR_STATE, "not initialised");
     if (!h || nb <= 0 || !dt_allow || !cfl_max) return fail(E4C_ERR_ARG, "bad arguments");
     if (nb > kNoallocMaxBlocks)
         return fail(E4C_ERR_ARG, "e4c_dt_allow_noalloc reduces over at most "
                                  "E4C_NOALLOC_MAX_BLOCKS (1024) blocks per call");
     for (int q = 0; q < nb; ++q)
         if (h[q] < 0 || h[q] >= int(c.blocks.size())) return fail(E4C_ERR_ARG, "bad block handle");
-    unsigned long long* scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
-    if (rc != E4C_OK) return rc;
+    // the scratch address and the library stream belong to the device that
+    // e4c_init selected
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev != c.cfg.device)
+        return fail(E4C_ERR_STATE, "e4c_dt_allow_noalloc called with another device current "
+                                   "than the one e4c_init selected");
+    unsigned long long* scratch = static_cast<unsigned long long*>(c.noalloc_scratch);
     unsigned long long* acc = scratch;
     int* list = reinterpret_cast<int*>(scratch + kAccWords);
     double* scal = reinterpret_cast<double*>(scratch + kAccWords + kListWords);
@@ -125,8 +83,7 @@ extern "C" int e4c_dt_allow_noalloc(const int* h, int nb, double dt_current, int
     // accumulators are indexed by position in the call's block list)
     int ident[kNoallocMaxBlocks];
     for (int q = 0; q < nb; ++q) ident[q] = q;
-    cudaError_t e = cudaMemcpyAsync(list, ident, size_t(nb) * sizeof(int), cudaMemcpyHostToDevice,
-                                    c.stream);
+    e = cudaMemcpyAsync(list, ident, size_t(nb) * sizeof(int), cudaMemcpyHostToDevice, c.stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(scal, &dt_current, sizeof(double), cudaMemcpyHostToDevice, c.stream);
     if (e != cudaSuccess) return cuda_fail(e, "e4c_dt_allow_noalloc inputs");
@@ -140,9 +97,9 @@ extern "C" int e4c_dt_allow_noalloc(const int* h, int nb, double dt_current, int
             if (g > 148 * 8) g = 148 * 8;
             if (g < 1) g = 1;
             if (c.cfg.precision == E4C_PREC_FP32_FLUX)
-                k_fused_dt_explicit<float><<<g, 256, 0, c.stream>>>(b.f, c.gas, c.cfg.cfl_value, scal, a);
+                f32::fused_dt_one(b.f, a, g, c.gas, c.cfg.cfl_value, scal, c.stream);
             else
-                k_fused_dt_explicit<double><<<g, 256, 0, c.stream>>>(b.f, c.gas, c.cfg.cfl_value, scal, a);
+                f64::fused_dt_one(b.f, a, g, c.gas, c.cfg.cfl_value, scal, c.stream);
         } else {
             launch_dt(b.v, nullptr, c.cfg.cfl_value, scal, a, c.stream);
         }

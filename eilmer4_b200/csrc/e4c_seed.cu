@@ -580,9 +580,10 @@ __device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
 }
 
 // Bounded wait for an mbarrier phase (each try_wait itself suspends for a
-// while): false after ~1e6 tries.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int it = 0; it < (1 << 20); ++it)
+// while): false after `tries` tries (~1e6 by default).
+constexpr int kMbarTries = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int tries = kMbarTries) {
+    for (int it = 0; it < tries; ++it)
         if (mbar_try(mbar, parity)) return true;
     return false;
 }
@@ -623,7 +624,7 @@ template <class Src>
 __global__ void __launch_bounds__(128) k_seed_infer_tc(Src src, const float* __restrict__ params,
                                                        const uint16_t* __restrict__ packed,
                                                        const double* __restrict__ norm,
-                                                       SimDev* sim) {
+                                                       SimDev* sim, int first_wait_tries) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const long long nrows = src.count();
     if ((long long)blockIdx.x * 128 >= nrows) return;   // before any tensor-memory use
@@ -712,7 +713,7 @@ __global__ void __launch_bounds__(128) k_seed_infer_tc(Src src, const float* __r
                     }
                 }
                 umma_commit(mbar);
-                *flag = mbar_wait(mbar, phase) ? 1u : 0u;
+                *flag = mbar_wait(mbar, phase, first_wait_tries) ? 1u : 0u;
             }
             __syncthreads();
             if (*flag == 0u) {
@@ -752,7 +753,8 @@ __global__ void __launch_bounds__(128) k_seed_infer_tc(Src src, const float* __r
     }
     if (failed) {
         // the tensor cores did not signal completion: report, give the MMA a
-        // second bounded wait, then release the tensor memory
+        // second bounded wait (the full count of tries), then release the
+        // tensor memory
         if (tid == 0) {
             if (sim && atomicCAS(&sim->status, 0, E4C_ERR_TIMEOUT) == 0) sim->status_step = sim->step;
             (void)mbar_wait(mbar, phase);
@@ -907,7 +909,7 @@ void Ctx::seed_infer(const BlockView& v, const double* dt, const int* work, cons
     // the list length is known only on the device: CTAs past its end return
     // before touching tensor memory
     k_seed_infer_tc<WorkRows><<<grid_of(rows.n, 128, 148 * 4), 128, TC_SMEM, stream>>>(
-        rows, seed.d_params, seed.d_packed, seed.d_norm, d_sim);
+        rows, seed.d_params, seed.d_packed, seed.d_norm, d_sim, seed.first_wait_tries);
 }
 
 }  // namespace e4c
@@ -1174,18 +1176,33 @@ int e4c_seed_predict(const double* rows, long long n, double* out) {
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
     if (!c.seed.have_weights) return fail(E4C_ERR_STATE, "no trained or installed network");
     if (!rows || !out || n <= 0) return fail(E4C_ERR_ARG, "bad arguments");
-    double* d = static_cast<double*>(c.dalloc(size_t(n) * 14 * sizeof(double)));
+    // rows in, predictions out, and a status word of this call's own (a
+    // time-out here does not touch the simulation's status)
+    double* d = static_cast<double*>(c.dalloc(size_t(n) * 14 * sizeof(double) + sizeof(SimDev)));
     if (!d) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
+    SimDev* st = reinterpret_cast<SimDev*>(d + size_t(n) * 14);
+    E4C_CUDA(cudaMemsetAsync(st, 0, sizeof(SimDev), c.stream));
     E4C_CUDA(cudaMemcpyAsync(d, rows, size_t(n) * 8 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     HostRows hr{d, n, d + n * 8};
     k_seed_infer_tc<HostRows><<<grid_of(n, 128, 148 * 4), 128, TC_SMEM, c.stream>>>(
-        hr, c.seed.d_params, c.seed.d_packed, c.seed.d_norm, nullptr);
+        hr, c.seed.d_params, c.seed.d_packed, c.seed.d_norm, st, c.seed.first_wait_tries);
     c.launches += 1;
     E4C_CUDA(cudaGetLastError());
     E4C_CUDA(cudaMemcpyAsync(out, d + n * 8, size_t(n) * 6 * sizeof(double), cudaMemcpyDeviceToHost,
                              c.stream));
+    int status = 0;
+    E4C_CUDA(cudaMemcpyAsync(&status, &st->status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     E4C_CUDA(cudaStreamSynchronize(c.stream));
     c.dfree(d);
+    if (status != 0) return fail(status, "seed inference: the tensor cores did not signal "
+                                         "completion within the wait limit");
+    return E4C_OK;
+}
+
+int e4c_seed_set_wait_limit(int first_wait_tries) {
+    Ctx& c = g_ctx;
+    if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    c.seed.first_wait_tries = first_wait_tries < 0 ? kMbarTries : first_wait_tries;
     return E4C_OK;
 }
 

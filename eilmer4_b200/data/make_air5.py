@@ -8,7 +8,7 @@ GuptaEtAl-air-reactions.lua), keeping reactions r1, r2, r4, r5, r6, and
 writes air5_gas_model.json next to this script.  Run once where the
 reference is available:
 
-    python eilmer4_b200/data/make_air5.py /root/reference
+    python eilmer4_b200/data/make_air5.py <reference-root>
 """
 import json
 import os
@@ -94,4 +94,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python eilmer4_b200/data/make_air5.py <reference-root>")
+    main(sys.argv[1])

@@ -228,6 +228,14 @@ int e4c_seed_predict(const double* rows, long long n, double* out);
  * targets y[n][6]: loss = mean of the squared errors, grad[E4C_SEED_NPARAM]. */
 int e4c_seed_loss_grad(const float* x, const float* y, int n, double* loss, float* grad);
 
+/* Failure-detection hook (no counterpart in the reference): the number of
+ * tries of the seed inference kernel's first bounded wait for the tensor
+ * cores (negative: the default, about one million).  With 0 the first wait
+ * gives up at once, so the kernel takes its time-out path -- report
+ * E4C_ERR_TIMEOUT, wait again with the full count for the multiply it
+ * issued, release its tensor memory -- on a healthy device. */
+int e4c_seed_set_wait_limit(int first_wait_tries);
+
 /* Free every device buffer and graph; the context may be re-initialised. */
 int e4c_finalize(void);
 
@@ -367,10 +375,13 @@ int e4c_autotune(int nsteps, int* ti, int* tj, int* kc, double* ms_per_step);
  * and results, about 28 KB) in one fixed-size device array that lives in the
  * library for as long as it is loaded, so it reduces over at most
  * E4C_NOALLOC_MAX_BLOCKS blocks per call and returns E4C_ERR_ARG beyond that.
- * Same inputs, outputs and results as e4c_dt_allow.  The first call on a
- * device looks up the array's device address; make that first call before any
- * stream capture.  The array is shared by all calls: calls that overlap on
- * the GPU race (the library is single-threaded and uses one stream). */
+ * Same inputs, outputs and results as e4c_dt_allow (it runs the same
+ * kernels).  e4c_init looks up the array's device address on the library's
+ * device, which also reserves the array there, so no call does either later;
+ * the call returns E4C_ERR_STATE if another device is current.  The array is
+ * shared by all calls and keeps the last call's contents (each call resets
+ * the accumulators it uses): calls that overlap on the GPU race (the library
+ * is single-threaded and uses one stream). */
 int e4c_dt_allow_noalloc(const int* h, int nb, double dt_current, int check_cfl,
                          double* dt_allow, double* cfl_max);
 

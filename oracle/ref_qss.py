@@ -35,7 +35,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libcudakernel.so")
 SRC = os.path.join(OUT, "alpha_qss_kernel.cu")
-TEMPLATE = "/root/reference/src/eilmer/utils/alpha_qss_kernel_cuda_tmplt.cu"
+# the kernel template, relative to the root of the reference tree (the
+# caller names the root: the build step, or E4_REFERENCE_ROOT)
+TEMPLATE_REL = os.path.join("src", "eilmer", "utils", "alpha_qss_kernel_cuda_tmplt.cu")
+
+
+def template_path(reference_root: str) -> str:
+    return os.path.join(reference_root, TEMPLATE_REL)
 MARK = "// <insert-source-terms-here>"
 
 
@@ -92,8 +98,9 @@ def source_terms(tc) -> str:
     return "\n".join(lines) + "\n"
 
 
-def build(tc, force: bool = False, template: str = TEMPLATE) -> str:
-    """Generate and compile the reference kernel for tc's mechanism."""
+def build(tc, template: str, force: bool = False) -> str:
+    """Generate and compile the reference kernel for tc's mechanism from the
+    template file `template` (template_path of the reference tree)."""
     if os.path.exists(LIB) and not force:
         return LIB
     with open(template) as f:

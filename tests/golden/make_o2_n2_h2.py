@@ -4,7 +4,7 @@ src/gas/thermo/therm_perf_gas_mix_eos.d:179-200): molar masses and the
 9-coefficient CEA thermo curves, written as o2_n2_h2_thermo.json next to this
 script.  Run where the reference tree is available:
 
-    python tests/golden/make_o2_n2_h2.py /root/reference
+    python tests/golden/make_o2_n2_h2.py <reference-root>
 """
 import json
 import os
@@ -54,4 +54,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_o2_n2_h2.py <reference-root>")
+    main(sys.argv[1])

@@ -107,3 +107,15 @@ def test_init_without_gpu_fails_cleanly(e4lib):
     e4lib.e4c_config_default(c)
     assert e4lib.e4c_init(c) == _lib.E4C_ERR_CUDA
     assert "CUDA" in _lib.last_error() or "device" in _lib.last_error()
+
+
+def test_noalloc_source_allocates_nothing():
+    """The allocation-free dt control's translation unit calls no allocating
+    routine: its only device memory is the file-scope scratch array."""
+    src = open(os.path.join(ROOT, "eilmer4_b200", "csrc", "e4c_noalloc.cu")).read()
+    code = "\n".join(line.split("//")[0] for line in src.splitlines())
+    for banned in ("cudaMalloc", "cudaFree", "dalloc", "dfree", "malloc(", "new ",
+                   "cudaMallocAsync", "ensure_"):
+        assert banned not in code, banned
+    assert "static __device__ __align__(256)" in code
+    assert "cudaGetSymbolAddress" in code

@@ -30,6 +30,11 @@ def test_reference_arm_line_has_the_contract_keys():
     assert e2e["value"] == line["value"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
     assert "workload" in line["config"]
+    # the line describes what it timed: a 12^3 block, whose measured step time
+    # gives the value
+    assert line["config"]["cells"] == 12 ** 3
+    assert line["config"]["same_config_as_ours"] is False
+    assert abs(line["ms_per_step"] * 1e-3 * line["value"] / 12 ** 3 - 1.0) < 1e-9
 
 
 def test_bench_options_parse():

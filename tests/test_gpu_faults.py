@@ -111,3 +111,39 @@ def test_bad_flux_run_lengths_are_refused(e4lib):
         sim.set_flux_runs(2, 3)
         sim.set_flux_runs(0, 0)
         assert sim.run(2).status == 0
+
+
+def test_seed_inference_wait_runs_out_and_recovers(e4lib):
+    """The seed inference kernel's bounded wait for the tensor cores, made to
+    run out on a healthy device (first wait limited to 0 tries): the call
+    reports E4C_ERR_TIMEOUT, the kernel's second, full wait lets the multiply
+    it issued finish before it releases its tensor memory, and the next calls
+    succeed and give the prediction of a call that never timed out."""
+    from eilmer4_b200 import _lib
+    from eilmer4_b200.simcore import Simulation
+    from oracle import e4_seed_oracle as SO
+    rng = np.random.default_rng(9)
+    params = SO.init_params(3)
+    norm = np.zeros(SO.NNORM)
+    norm[8:16] = 1.0
+    norm[22:28] = 1.0
+    norm[28] = 1.0e-9
+    norm[29] = 1.0e-3
+    n = 1000
+    y = np.array([0.74, 0.2, 0.02, 0.01, 0.03]) + 0.01 * rng.random((n, 5))
+    rows = np.column_stack([2500.0 + 5000.0 * rng.random(n), 1e4 + 1e5 * rng.random(n), y,
+                            1e-7 * (1.0 + rng.random(n))])
+    with Simulation.from_workload(W.sod_2d(16, 4)) as sim:
+        sim.seed_set(params, norm)
+        before = sim.seed_predict(rows)
+        _lib.check(sim.L.e4c_seed_set_wait_limit(0))
+        with pytest.raises(_lib.E4CError) as ei:
+            sim.seed_predict(rows)
+        assert ei.value.code == _lib.E4C_ERR_TIMEOUT
+        _lib.check(sim.L.e4c_seed_set_wait_limit(-1))
+        for _ in range(2):
+            after = sim.seed_predict(rows)
+            assert np.array_equal(after, before)
+        # the simulation itself is untouched: it still steps
+        info = sim.run(3)
+        assert info.steps_taken == 3

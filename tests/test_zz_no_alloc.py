@@ -3,8 +3,10 @@
 Some hosts cannot let a library call cudaMalloc inside their time loop (the
 GPU's memory belongs to the host's own pool, or a fixed budget); this entry
 point keeps its scratch in a fixed device array inside the library.  It must
-give exactly what e4c_dt_allow gives, call after call.  This file is collected
-last so that, should it fail, every other test has already run.
+give exactly what e4c_dt_allow gives, call after call, in both arithmetic
+forms, and a warmed-up call must leave the device's free memory unchanged.
+This file is collected last so that, should it fail, every other test has
+already run.
 """
 import ctypes
 
@@ -26,13 +28,18 @@ def noalloc(L, hs, dt_current, check_cfl):
     return d.value, c.value
 
 
-def test_noalloc_dt_matches_dt_allow(e4lib):
-    from eilmer4_b200.simcore import Simulation
+def mixed_workload():
     wl = W.Workload("mixed", 3, flux_calculator="hllc")
     # one block on the fused uniform path, one on the general path
     wl.blocks.append(W.inflow_3d_block(40, 24, 20, 5, spacing=1.0 / 64.0))
     wl.blocks.append(W.inflow_3d_block(20, 12, 10, 7))
-    with Simulation.from_workload(wl) as sim:
+    return wl
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_flux"])
+def test_noalloc_dt_matches_dt_allow(e4lib, precision):
+    from eilmer4_b200.simcore import Simulation
+    with Simulation.from_workload(mixed_workload(), precision=precision) as sim:
         hs = [0, 1]
         # two calls in a row, on the uploaded state
         for dt_current, check in ((1.0e-3, 0), (2.0e-7, 1)):
@@ -47,6 +54,22 @@ def test_noalloc_dt_matches_dt_allow(e4lib):
                 got = noalloc(sim.L, sub, 3.0e-7, 1)
                 assert got == ref, (sub, call, got, ref)
         assert np.isfinite(got[0]) and got[0] > 0.0
+
+
+def test_noalloc_calls_leave_free_memory_unchanged(e4lib):
+    import torch
+
+    from eilmer4_b200.simcore import Simulation
+    with Simulation.from_workload(mixed_workload()) as sim:
+        sim.run(3)
+        first = noalloc(sim.L, [0, 1], 2.0e-7, 1)
+        torch.cuda.mem_get_info(0)       # the runtime's own set-up, outside the window
+        sim.synchronize()
+        free0, _ = torch.cuda.mem_get_info(0)
+        outs = [noalloc(sim.L, [0, 1], 2.0e-7, 1) for _ in range(5)]
+        free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+    assert all(o == first for o in outs)
 
 
 def test_noalloc_rejects_too_many_blocks(e4lib):
