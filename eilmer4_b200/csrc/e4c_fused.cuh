@@ -335,7 +335,12 @@ template <typename R, int FLUX, int TI, int TJ>
 __global__ void __launch_bounds__(FusedThreads<TI, TJ>::total, FusedMinBlocks<R, TI, TJ>::value)
 k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems, int kc,
               SimDev* sim, GasConsts gas, FluxOpts o, int stage, const int* __restrict__ order) {
-    if (sim->status != 0 || sim->finished) return;
+    // one decision per CTA (another CTA may set the status while this one
+    // starts): every thread leaves, or none
+    __shared__ int s_stop;
+    if (threadIdx.x == 0) s_stop = (sim->status != 0 || sim->finished) ? 1 : 0;
+    __syncthreads();
+    if (s_stop) return;
     // CTAs take work items from a counter, costliest first; the other stage's
     // counter is reset for its next launch (it is not in use now)
     if (blockIdx.x == 0 && threadIdx.x == 0) sim->item_next[stage == 1 ? 1 : 0] = 0u;
