@@ -5,4 +5,6 @@
 // against the FP64 oracle with a tolerance.
 #define E4C_FUSED_R float
 #define E4C_FUSED_NS f32
+// 32-wide tiles take the kernel with edge warps and per-cell reconstruction
+#define E4C_FUSED_WS 1
 #include "e4c_fused_launch.cuh"

@@ -5,6 +5,9 @@
 #pragma once
 
 #include "e4c_fused.cuh"
+#if E4C_FUSED_WS
+#include "e4c_fused_ws.cuh"
+#endif
 
 #ifndef E4C_FUSED_R
 #error "define E4C_FUSED_R (double or float) before including this file"
@@ -43,11 +46,56 @@ static int occupancy_one() {
     return n;
 }
 
+#if E4C_FUSED_WS
+// 32-wide tiles of the FP32-flux form: the kernel with edge warps and per-cell
+// reconstruction (second-order reconstruction only)
+template <int FLUX, int TJ>
+static int launch_ws(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o,
+                     int stage, cudaStream_t s) {
+    constexpr size_t smem = ws::Lay<TJ>::bytes;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(ws::k_fused_stage_ws<FLUX, TJ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        attr_set = true;
+    }
+    ws::k_fused_stage_ws<FLUX, TJ><<<L.grid, ws::Lay<TJ>::threads, smem, s>>>(
+        static_cast<const FusedDesc*>(L.descs), L.nblocks, L.nitems, L.kc, sim, gas, o, stage,
+        L.order);
+    return 0;
+}
+
+template <int FLUX, int TJ>
+static int occupancy_ws() {
+    constexpr size_t smem = ws::Lay<TJ>::bytes;
+    cudaFuncSetAttribute(ws::k_fused_stage_ws<FLUX, TJ>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ws::k_fused_stage_ws<FLUX, TJ>,
+                                                      ws::Lay<TJ>::threads, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+#define E4C_WS_TILES(X) X(4) X(8) X(16)
+#endif
+
 // Tile shapes available to the autotuner: (TI, TJ).
 #define E4C_TILES(X) X(32, 8) X(32, 4) X(16, 8) X(64, 4) X(16, 16) X(32, 16)
 
 int fused_stage(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const FluxOpts& o,
                 int stage, cudaStream_t s) {
+#if E4C_FUSED_WS
+    if (L.ti == 32 && o.order2) {
+#define E4C_WS_CASE(TJ_)                                                            \
+        if (L.tj == TJ_) {                                                          \
+            if (o.flux == 1) return launch_ws<1, TJ_>(L, sim, gas, o, stage, s);    \
+            return launch_ws<0, TJ_>(L, sim, gas, o, stage, s);                     \
+        }
+        E4C_WS_TILES(E4C_WS_CASE)
+#undef E4C_WS_CASE
+    }
+#endif
 #define E4C_CASE(TI_, TJ_)                                                        \
     if (L.ti == TI_ && L.tj == TJ_) {                                            \
         if (o.flux == 1) return launch_one<1, TI_, TJ_>(L, sim, gas, o, stage, s); \
@@ -59,6 +107,14 @@ int fused_stage(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const F
 }
 
 int fused_occupancy(int flux, int ti, int tj) {
+#if E4C_FUSED_WS
+    if (ti == 32) {
+#define E4C_WS_CASE(TJ_)                                                            \
+        if (tj == TJ_) return flux == 1 ? occupancy_ws<1, TJ_>() : occupancy_ws<0, TJ_>();
+        E4C_WS_TILES(E4C_WS_CASE)
+#undef E4C_WS_CASE
+    }
+#endif
 #define E4C_CASE(TI_, TJ_)                                          \
     if (ti == TI_ && tj == TJ_) {                                  \
         return flux == 1 ? occupancy_one<1, TI_, TJ_>() : occupancy_one<0, TI_, TJ_>(); \

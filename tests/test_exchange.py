@@ -90,7 +90,8 @@ def test_gpu_split_2d_matches_oracle_and_single_block(oracle, e4lib, parts):
 @pytest.mark.parametrize("precision", ["fp64", "fp32_flux"])
 def test_gpu_split_3d_fused_matches_single_block(oracle, e4lib, precision):
     """Uniform blocks stay on the fused path across the joints: the partner's
-    cells are read straight from its stage-input arrays."""
+    cells are read straight from its stage-input arrays.  The FP64 form gives
+    the uncut block's bits; the FP32-flux form agrees to FP32 rounding."""
     from eilmer4_b200.simcore import Simulation
     wl = W.inflow_3d(n=32)
     b = wl.blocks[0]
@@ -100,7 +101,22 @@ def test_gpu_split_3d_fused_matches_single_block(oracle, e4lib, precision):
     (single,), st1 = gpu_run(wl, [b], [], n, precision)
     split, st2 = gpu_run(wl, blocks, conns, n, precision)
     joined = W.join_prims([p for p, _ in split], (b.ni, b.nj, b.nk), 3, parts)
-    assert np.array_equal(joined, single[0]) and st1 == st2
+    if precision == "fp64":
+        assert np.array_equal(joined, single[0]) and st1 == st2
+    else:
+        # the FP32-flux form rounds each face in whichever warp computes it
+        # (a face on a tile edge in one decomposition is an interior face in
+        # the other, and the compiler may contract their FP32 arithmetic
+        # differently): the split domain agrees with the uncut block to
+        # rounding, and steps in step with it
+        # (per field, against the field's scale; for a velocity component,
+        # against the speed: the transverse components start at zero)
+        speed = np.abs(single[0][1:4]).max()
+        for q in range(joined.shape[0]):
+            scale = speed if q in (1, 2, 3) else np.abs(single[0][q]).max()
+            err = np.abs(joined[q] - single[0][q]).max() / scale
+            assert err < 1e-6, (q, err)
+        assert st1[2] == st2[2] and abs(st1[0] - st2[0]) <= 1e-9 * st1[0]
     if precision == "fp64":
         oprims, ost = oracle_run(oracle, wl, blocks, conns, n, flux_calculator=oracle.FLUX_HLLC)
         for (gp, _), op in zip(split, oprims):
