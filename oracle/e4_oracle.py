@@ -93,46 +93,57 @@ def build(force: bool = False) -> str:
 
 
 _lib = None
+_lib_libm = None
 
 
-def lib():
-    global _lib
+def lib(libm: bool = False):
+    """The oracle library; libm=True: its build with the C library's exp, log
+    and pow in place of the portable restatements the GPU shares."""
+    global _lib, _lib_libm
+    if libm:
+        if _lib_libm is None:
+            build()
+            _lib_libm = _declare(ctypes.CDLL(os.path.join(_HERE, "_build", "libe4oracle_libm.so")))
+        return _lib_libm
     if _lib is None:
-        path = build()
-        L = ctypes.CDLL(path)
-        vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
-        P = ctypes.POINTER
-        L.e4o_default_config.argtypes = [P(Config)]
-        L.e4o_sim_new.argtypes = [P(Config)]
-        L.e4o_sim_new.restype = vp
-        L.e4o_sim_free.argtypes = [vp]
-        L.e4o_add_block.argtypes = [vp, ip, ip, ip, P(dp), P(ip), P(dp)]
-        L.e4o_add_block.restype = ip
-        L.e4o_set_flow.argtypes = [vp, ip, P(dp)]
-        L.e4o_connect_blocks.argtypes = [vp, ip, ip, ip, ip, ip]
-        L.e4o_get_flow.argtypes = [vp, ip, P(dp), P(dp)]
-        L.e4o_get_cell_geometry.argtypes = [vp, ip, P(dp)]
-        L.e4o_run.argtypes = [vp, ip, dp]
-        L.e4o_time.argtypes = [vp]
-        L.e4o_time.restype = dp
-        L.e4o_dt_global.argtypes = [vp]
-        L.e4o_dt_global.restype = dp
-        L.e4o_step_count.argtypes = [vp]
-        L.e4o_last_bad_cells.argtypes = [vp]
-        L.e4o_last_error.argtypes = [vp]
-        L.e4o_last_error.restype = ctypes.c_char_p
-        L.e4o_ideal_gas_pT.argtypes = [dp, dp, dp, dp, P(dp), P(dp), P(dp)]
-        L.e4o_set_thermochem.argtypes = [vp, P(ThermoChem)]
-        L.e4o_tp_update.argtypes = [P(ThermoChem), ip, P(dp), P(dp), P(dp), P(dp), P(dp), P(dp)]
-        L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
-        L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
-        L.e4o_rates.argtypes = [P(ThermoChem), dp, P(dp), P(dp), P(dp)]
-        L.e4o_set_chem_newton_iterations.argtypes = [ip]
-        L.e4o_newton_test.argtypes = [ip, P(dp)]
-        L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
-        L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
-        _lib = L
+        _lib = _declare(ctypes.CDLL(build()))
     return _lib
+
+
+def _declare(L):
+    """Argument and result types of the oracle's C functions."""
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    P = ctypes.POINTER
+    L.e4o_default_config.argtypes = [P(Config)]
+    L.e4o_sim_new.argtypes = [P(Config)]
+    L.e4o_sim_new.restype = vp
+    L.e4o_sim_free.argtypes = [vp]
+    L.e4o_add_block.argtypes = [vp, ip, ip, ip, P(dp), P(ip), P(dp)]
+    L.e4o_add_block.restype = ip
+    L.e4o_set_flow.argtypes = [vp, ip, P(dp)]
+    L.e4o_connect_blocks.argtypes = [vp, ip, ip, ip, ip, ip]
+    L.e4o_get_flow.argtypes = [vp, ip, P(dp), P(dp)]
+    L.e4o_get_cell_geometry.argtypes = [vp, ip, P(dp)]
+    L.e4o_run.argtypes = [vp, ip, dp]
+    L.e4o_time.argtypes = [vp]
+    L.e4o_time.restype = dp
+    L.e4o_dt_global.argtypes = [vp]
+    L.e4o_dt_global.restype = dp
+    L.e4o_step_count.argtypes = [vp]
+    L.e4o_last_bad_cells.argtypes = [vp]
+    L.e4o_last_error.argtypes = [vp]
+    L.e4o_last_error.restype = ctypes.c_char_p
+    L.e4o_ideal_gas_pT.argtypes = [dp, dp, dp, dp, P(dp), P(dp), P(dp)]
+    L.e4o_set_thermochem.argtypes = [vp, P(ThermoChem)]
+    L.e4o_tp_update.argtypes = [P(ThermoChem), ip, P(dp), P(dp), P(dp), P(dp), P(dp), P(dp)]
+    L.e4o_chem_cell.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp), P(dp), P(dp), P(dp)]
+    L.e4o_chem_update.argtypes = [P(ThermoChem), dp, dp, dp, P(dp), P(dp)]
+    L.e4o_rates.argtypes = [P(ThermoChem), dp, P(dp), P(dp), P(dp)]
+    L.e4o_set_chem_newton_iterations.argtypes = [ip]
+    L.e4o_newton_test.argtypes = [ip, P(dp)]
+    L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
+    L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
+    return L
 
 
 def _dptr(a: np.ndarray):
@@ -151,33 +162,34 @@ def default_config(**kw) -> Config:
 class OracleSim:
     """One simulation (a set of blocks sharing dt_global), as simcore.d runs it."""
 
-    def __init__(self, cfg: Config, thermochem=None):
+    def __init__(self, cfg: Config, thermochem=None, libm: bool = False):
         self.cfg = cfg
-        self._h = lib().e4o_sim_new(ctypes.byref(cfg))
+        self._L = lib(libm)
+        self._h = self._L.e4o_sim_new(ctypes.byref(cfg))
         self.blocks = []
         self.nsp = 5 if cfg.gas_model == GAS_THERM_PERF_5SP_AIR else 1
         if thermochem is not None:
             self._tc = thermochem.fill(ThermoChem())
-            lib().e4o_set_thermochem(self._h, ctypes.byref(self._tc))
+            self._L.e4o_set_thermochem(self._h, ctypes.byref(self._tc))
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().e4o_sim_free(h)
+            self._L.e4o_sim_free(h)
             self._h = None
 
     def add_block(self, ni, nj, nk, vtx, bc, inflow):
         vtx = np.ascontiguousarray(vtx, dtype=np.float64)
         inflow = np.ascontiguousarray(inflow, dtype=np.float64)
         bca = (ctypes.c_int * 6)(*bc)
-        b = lib().e4o_add_block(self._h, ni, nj, nk, _dptr(vtx), bca, _dptr(inflow))
+        b = self._L.e4o_add_block(self._h, ni, nj, nk, _dptr(vtx), bca, _dptr(inflow))
         if b < 0:
             raise RuntimeError(f"e4o_add_block failed: {b}")
         self.blocks.append((ni, nj, nk if self.cfg.dimensions == 3 else 1))
         return b
 
     def connect(self, a, fa, b, fb, orientation=0):
-        rc = lib().e4o_connect_blocks(self._h, a, fa, b, fb, orientation)
+        rc = self._L.e4o_connect_blocks(self._h, a, fa, b, fb, orientation)
         if rc != 0:
             raise RuntimeError(f"e4o_connect_blocks failed: {rc}")
 
@@ -189,7 +201,7 @@ class OracleSim:
 
     def set_flow(self, b, prim):
         prim = np.ascontiguousarray(prim, dtype=np.float64)
-        rc = lib().e4o_set_flow(self._h, b, _dptr(prim))
+        rc = self._L.e4o_set_flow(self._h, b, _dptr(prim))
         if rc != 0:
             raise RuntimeError(f"e4o_set_flow failed: {rc}")
 
@@ -198,7 +210,7 @@ class OracleSim:
         n = ni * nj * nk
         prim = np.zeros((self.nvar_prim(), n))
         cons = np.zeros((self.nvar_cons(), n))
-        lib().e4o_get_flow(self._h, b, _dptr(prim), _dptr(cons))
+        self._L.e4o_get_flow(self._h, b, _dptr(prim), _dptr(cons))
         return prim, cons
 
     def geometry(self, b):
@@ -208,28 +220,28 @@ class OracleSim:
         if self.cfg.dimensions == 3:
             nf += ni * nj * (nk + 1)
         out = np.zeros(4 * n + 10 * nf)
-        lib().e4o_get_cell_geometry(self._h, b, _dptr(out))
+        self._L.e4o_get_cell_geometry(self._h, b, _dptr(out))
         return out[: 4 * n].reshape(4, n), out[4 * n:].reshape(nf, 10)
 
     def run(self, nsteps, max_time=1.0e300):
-        rc = lib().e4o_run(self._h, nsteps, max_time)
+        rc = self._L.e4o_run(self._h, nsteps, max_time)
         return rc
 
     @property
     def time(self):
-        return lib().e4o_time(self._h)
+        return self._L.e4o_time(self._h)
 
     @property
     def dt_global(self):
-        return lib().e4o_dt_global(self._h)
+        return self._L.e4o_dt_global(self._h)
 
     @property
     def step(self):
-        return lib().e4o_step_count(self._h)
+        return self._L.e4o_step_count(self._h)
 
     @property
     def last_bad_cells(self):
-        return lib().e4o_last_bad_cells(self._h)
+        return self._L.e4o_last_bad_cells(self._h)
 
 
 def ideal_gas_pT(mol_mass, gamma, p, T):

@@ -37,6 +37,16 @@ namespace e4o {
 // ---------------------------------------------------------------------------
 // Portable exp / log / pow
 // ---------------------------------------------------------------------------
+#ifdef E4O_LIBM
+// The second build of the oracle (libe4oracle_libm.so): the C library's exp,
+// log and pow in place of the portable restatements below, as the reference
+// calls them (rate_constant.d:71-75, cea_thermo_curves.d:49-127).  It bounds
+// how far the GPU's reacting path, which uses the portable forms, sits from
+// the reference's arithmetic.
+double pm_log(double x) { return std::log(x); }
+double pm_exp(double x) { return std::exp(x); }
+double pm_pow(double x, double n) { return std::pow(x, n); }
+#else
 double pm_log(double x) {
     // log(x) = k ln2 + 2 atanh(s), s = (m-1)/(m+1), x = m 2^k, m in [sqrt(1/2), sqrt(2))
     if (!(x > 0.0)) return (x == 0.0) ? -HUGE_VAL : NAN;
@@ -104,6 +114,7 @@ double pm_pow(double x, double n) {
     if (n == -1.5) return 1.0 / (x * std::sqrt(x));
     return pm_exp(n * pm_log(x));
 }
+#endif  // E4O_LIBM
 
 // ---------------------------------------------------------------------------
 // CEA thermo curves (cea_thermo_curves.d)

@@ -122,3 +122,39 @@ def test_c3_reacting_channel_512x256(oracle, e4lib, hot):
         # the chemistry did Newton work on dissociating cells
         assert counters[1] > 0 and counters[3] > 0, counters
         assert np.max(gp[12]) > 1.0e-4  # atomic oxygen behind the ramp shock
+
+
+@pytest.mark.parametrize("hot", [False, True])
+def test_c3_channel_against_the_libm_oracle(oracle, e4lib, hot):
+    """How far the GPU's reacting path sits from the reference's arithmetic:
+    the GPU (portable exp/log/pow, bit for bit the oracle's) against the
+    oracle built on the C library's exp, log and pow, on the full 512x256
+    channel after 30 steps.  The largest difference of each field, relative
+    to the field's scale (the speed for a velocity component), is printed and
+    bounded by 1e-8."""
+    from eilmer4_b200.simcore import Simulation
+    wl = W.reacting_channel_hot() if hot else W.reacting_channel()
+    nsteps = 30
+    cfg = oracle.default_config(dimensions=2, flux_calculator=oracle.FLUX_AUSMDV,
+                                gas_model=oracle.GAS_THERM_PERF_5SP_AIR, reacting=1,
+                                n_threads=0)
+    osim = oracle.OracleSim(cfg, wl.thermochem, libm=True)
+    b = wl.blocks[0]
+    osim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    osim.set_flow(0, b.prim)
+    assert osim.run(nsteps) == 0
+    op, _ = osim.get_flow(0)
+    with Simulation.from_workload(wl, reacting=True) as sim:
+        sim.run(nsteps)
+        gp, _ = sim.download(0)
+        assert sim.state()[2] == osim.step
+    names = ["rho", "vx", "vy", "vz", "p", "T", "u", "a", "N2", "O2", "NO", "N", "O"]
+    speed = np.abs(op[1:3]).max()
+    diffs = {}
+    for q, name in enumerate(names):
+        scale = speed if q in (1, 2, 3) else np.abs(op[q]).max()
+        if scale > 0.0:
+            diffs[name] = float(np.abs(gp[q] - op[q]).max() / scale)
+    print(f"\nGPU vs libm oracle, {'hot' if hot else 'cold'} channel 512x256, {nsteps} steps:",
+          {k: f"{v:.2e}" for k, v in diffs.items()})
+    assert max(diffs.values()) <= 1e-8, diffs
