@@ -154,6 +154,11 @@ def load():
         "e4c_autotune": ([i, ip, ip, ip, dp], i),
         "e4c_dt_allow_noalloc": ([ip, i, d, i, dp, dp], i),
         "e4c_seed_set_wait_limit": ([i], i),
+        "e4c_stage": ([ip, i, i, d, ip], i),
+        "e4c_connect_remote": ([i, i], i),
+        "e4c_face_slab_bytes": ([i, i, P(ctypes.c_longlong)], i),
+        "e4c_pack_face": ([i, i, i, ctypes.c_void_p], i),
+        "e4c_unpack_face": ([i, i, ctypes.c_void_p], i),
         "e4c_set_thermochem": ([P(E4CThermoChem)], i),
         "e4c_chemistry_step": ([ip, i, d], i),
         "e4c_chemistry_counters": ([P(ctypes.c_longlong), i], i),

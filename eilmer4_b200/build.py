@@ -37,6 +37,7 @@ UNITS = [
     ("e4c_blocks.cu", ["-fmad=false"]),
     ("e4c_api.cu", ["-fmad=false"]),
     ("e4c_noalloc.cu", ["-fmad=false"]),
+    ("e4c_remote.cu", ["-fmad=false"]),
     # learned chemistry seed: BF16 tensor-core MLP, FP32 arithmetic
     ("e4c_seed.cu", []),
 ]

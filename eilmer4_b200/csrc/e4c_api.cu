@@ -89,6 +89,7 @@ void Ctx::release() {
     d_dtacc = nullptr;
     dtacc_cap = 0;
     noalloc_scratch = nullptr;
+    remote.clear();
     d_staging = nullptr;
     staging_bytes = 0;
     d_stage_in = d_stage_out = nullptr;
@@ -767,6 +768,9 @@ int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
     if (rc != E4C_OK) return rc;
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(E4C_ERR_ARG, "dt must be positive and finite");
     Ctx& c = g_ctx;
+    if (!c.remote.empty())
+        return fail(E4C_ERR_STATE, "blocks joined to other ranks advance one stage at a time "
+                                   "(e4c_stage, with the face exchange between stages)");
     // The host owns dt: write it as SimState.dt_global, clear a stale finish flag.
     launch_begin_run(c.d_sim, 1.0e300, c.stream);
     double* hp = static_cast<double*>(c.host_pinned);
@@ -783,10 +787,48 @@ int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells) {
     return E4C_OK;
 }
 
+int e4c_stage(const int* h, int nb, int stage, double dt, int* bad_cells) {
+    NvtxRange nvtx_range("e4c_stage");
+    g_ctx.host_step_valid = false;
+    std::vector<int> hs;
+    int rc = check_handles(h, nb, hs);
+    if (rc != E4C_OK) return rc;
+    Ctx& c = g_ctx;
+    const int nstages = (c.cfg.gasdynamic_update_scheme == E4C_UPDATE_PC) ? 2 : 1;
+    if (stage < 1 || stage > nstages) return fail(E4C_ERR_ARG, "no such stage in this scheme");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(E4C_ERR_ARG, "dt must be positive and finite");
+    if (stage == 1) {
+        // the host owns dt: SimState.dt_global for the whole step
+        launch_begin_run(c.d_sim, 1.0e300, c.stream);
+        double* hp = static_cast<double*>(c.host_pinned);
+        hp[8] = dt;
+        E4C_CUDA(cudaMemcpyAsync(&c.d_sim->dt_global, hp + 8, sizeof(double),
+                                 cudaMemcpyHostToDevice, c.stream));
+    }
+    c.enqueue_stage(hs, stage, stage == nstages);
+    if (stage == nstages) {
+        // chemistry_step(dt_global) after the gas-dynamic increment, then the
+        // step's end (as e4c_gasdynamic_step)
+        if (c.cfg.reacting) c.enqueue_chemistry(hs, &c.d_sim->dt_global);
+        launch_end_step(c.d_sim, c.stream);
+        c.launches += 1;
+    }
+    E4C_CUDA(cudaGetLastError());
+    SimDev s;
+    rc = read_sim(s);
+    if (rc != E4C_OK) return rc;
+    if (bad_cells) *bad_cells = s.bad_cells;
+    if (s.status != 0) return status_error(s);
+    return E4C_OK;
+}
+
 int e4c_integrate(int nsteps, double max_time, e4c_run_info* info) {
     NvtxRange nvtx_range("e4c_integrate");
     Ctx& c = g_ctx;
     if (!c.initialised) return fail(E4C_ERR_STATE, "not initialised");
+    if (!c.remote.empty())
+        return fail(E4C_ERR_STATE, "blocks joined to other ranks advance one stage at a time "
+                                   "(e4c_stage, with the face exchange between stages)");
     if (c.blocks.empty()) return fail(E4C_ERR_STATE, "no blocks");
     if (nsteps < 0) return fail(E4C_ERR_ARG, "negative step count");
     std::vector<int> hs = c.all_blocks();

@@ -232,16 +232,19 @@ int Ctx::prepare_fused() {
     std::vector<FusedDesc> ds;
     long long items = 0;
     std::vector<int> desc_of(blocks.size(), -1);
-    {
-        int q = 0;
-        for (size_t h = 0; h < blocks.size(); ++h)
-            if (blocks[h].fused) desc_of[h] = q++;
-    }
+    int nreal = 0;
+    for (size_t h = 0; h < blocks.size(); ++h)
+        if (blocks[h].fused) desc_of[h] = nreal++;
     for (size_t h = 0; h < blocks.size(); ++h) {
         BlockHost& b = blocks[h];
         if (!b.fused) continue;
         FusedDesc& f = b.f;
-        for (int w = 0; w < 6; ++w) f.ex[w] = b.ex_block[w] >= 0 ? desc_of[b.ex_block[w]] : -1;
+        for (int w = 0; w < 6; ++w) {
+            f.ex[w] = b.ex_block[w] >= 0 ? desc_of[b.ex_block[w]] : -1;
+            // a partner on another rank: its shadow descriptor, after the
+            // real ones (e4c_remote.cu)
+            if (b.remote[w] >= 0) f.ex[w] = nreal + b.remote[w];
+        }
         f.tiles_i = (f.ni + tile_ti - 1) / tile_ti;
         f.tiles_j = (f.nj + tile_tj - 1) / tile_tj;
         f.kchunks = (f.nk + tile_kc - 1) / tile_kc;
@@ -252,14 +255,22 @@ int Ctx::prepare_fused() {
     }
     nfused = int(ds.size());
     fused_items = items;
+    // shadows of remote partners: no work items (item0 past the last item, so
+    // no CTA finds them), only read across the joints
+    for (const RemoteFace& r : remote) {
+        FusedDesc sd = r.d;
+        sd.item0 = items;
+        ds.push_back(sd);
+    }
+    const int ndesc = int(ds.size());
     if (nfused > 0) {
-        if (nfused > descs_cap) {
+        if (ndesc > descs_cap) {
             dfree(d_descs);
-            d_descs = static_cast<FusedDesc*>(dalloc(sizeof(FusedDesc) * std::max(nfused, 64)));
+            d_descs = static_cast<FusedDesc*>(dalloc(sizeof(FusedDesc) * std::max(ndesc, 64)));
             if (!d_descs) return fail(E4C_ERR_CUDA, "cudaMalloc of block descriptors failed");
-            descs_cap = std::max(nfused, 64);
+            descs_cap = std::max(ndesc, 64);
         }
-        E4C_CUDA(cudaMemcpyAsync(d_descs, ds.data(), sizeof(FusedDesc) * nfused,
+        E4C_CUDA(cudaMemcpyAsync(d_descs, ds.data(), sizeof(FusedDesc) * ndesc,
                                  cudaMemcpyHostToDevice, stream));
         // work items ordered by cost, costliest first (longest-processing-time
         // order for the CTAs that take them from a counter): the cells a tile

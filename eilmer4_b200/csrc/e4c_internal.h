@@ -30,6 +30,19 @@ struct BlockHost {
     bool simple_flux = false;   // has an OutFlowBC_SimpleFlux boundary
     FusedDesc f{};          // fused path: storage and uniform geometry
     int ex_block[6] = {-1, -1, -1, -1, -1, -1};   // partner handle of an exchange boundary
+    int remote[6] = {-1, -1, -1, -1, -1, -1};     // shadow of a partner on another rank
+};
+
+// A face of a fused block joined to a block on another rank (e4c_remote.cu):
+// the partner's two cell layers next to the joint, as a two-cell-thick
+// block the fused loader reads across the joint like a local partner.  Its
+// storage (`buf`) is the packed layout e4c_pack_face writes:
+// [5 x n primitive values, precision-typed][n doubles: A0][8 bytes: use_a0].
+struct RemoteFace {
+    int h = -1, face = -1;
+    FusedDesc d{};
+    void* buf = nullptr;
+    size_t bytes = 0;
 };
 
 // The learned chemistry seed (e4c_seed.cu): network, training set, guesses.
@@ -120,6 +133,8 @@ struct Ctx {
     int* d_hlist = nullptr;
     int hlist_cap = 0;
     long long launches = 0;   // kernels enqueued (graph replays add their node count)
+    // faces joined to blocks on other ranks (their shadow descriptors)
+    std::vector<RemoteFace> remote;
     // device address of the allocation-free dt control's scratch array on
     // this context's device (resolved by e4c_init)
     void* noalloc_scratch = nullptr;

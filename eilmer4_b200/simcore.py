@@ -163,6 +163,29 @@ class Simulation:
         _lib.check(self.L.e4c_gasdynamic_step(arr, len(hs), float(dt), ctypes.byref(bad)))
         return bad.value
 
+    def stage(self, hs, stage, dt):
+        """One stage of the gas-dynamic step (the last one ends the step);
+        returns the stage's invalid-cell count."""
+        arr = (ctypes.c_int * len(hs))(*hs)
+        bad = ctypes.c_int()
+        _lib.check(self.L.e4c_stage(arr, len(hs), int(stage), float(dt), ctypes.byref(bad)))
+        return bad.value
+
+    # -- faces joined to blocks on other ranks (sharding.py) -----------------
+    def connect_remote(self, h, face):
+        _lib.check(self.L.e4c_connect_remote(int(h), int(face)))
+
+    def face_slab_bytes(self, h, face):
+        n = ctypes.c_longlong()
+        _lib.check(self.L.e4c_face_slab_bytes(int(h), int(face), ctypes.byref(n)))
+        return n.value
+
+    def pack_face(self, h, face, stage, dev_ptr):
+        _lib.check(self.L.e4c_pack_face(int(h), int(face), int(stage), ctypes.c_void_p(dev_ptr)))
+
+    def unpack_face(self, h, face, dev_ptr):
+        _lib.check(self.L.e4c_unpack_face(int(h), int(face), ctypes.c_void_p(dev_ptr)))
+
     def chemistry_step(self, hs, dt):
         arr = (ctypes.c_int * len(hs))(*hs)
         _lib.check(self.L.e4c_chemistry_step(arr, len(hs), float(dt)))

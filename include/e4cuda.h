@@ -302,6 +302,31 @@ int e4c_dt_allow(const int* h, int nb, double dt_current, int check_cfl, double*
  * finite (E4C_ERR_ARG otherwise; nothing is queued). */
 int e4c_gasdynamic_step(const int* h, int nb, double dt, int* bad_cells);
 
+/* One stage of the explicit gas-dynamic step (stage 1 or 2 of the
+ * predictor-corrector scheme, 1 of Euler) over the blocks, with dt given on
+ * stage 1; the last stage also runs the chemistry (reacting flow) and ends the
+ * step.  Two calls give what e4c_gasdynamic_step gives.  For blocks joined to
+ * other ranks, whose ghost cells must be exchanged before each stage
+ * (simcore.d:2303-2952 calls exchange_ghost_cell_boundary_data before each
+ * stage's fluxes, simcore.d:1599). */
+int e4c_stage(const int* h, int nb, int stage, double dt, int* bad_cells);
+
+/* Blocks on several ranks, one rank per GPU (the reference's MPI runs: the
+ * full-face exchange of full_face_copy.d:1134-1255 between ranks, the dt MIN
+ * and bad-cell MAX reductions of simcore.d:1399-1401, 2489 left to the host).
+ * e4c_connect_remote joins face `face` of block h (fused uniform 3-D blocks
+ * only) to a block on another rank: an opposite face of the same tangential
+ * extents and cell geometry, orientation 0.  Before each stage the host calls
+ * e4c_pack_face on the partner's rank (the partner's two cell layers next to
+ * the joint, from its state at the start of that stage, into a device buffer
+ * of e4c_face_slab_bytes bytes), moves the buffer to this rank and calls
+ * e4c_unpack_face.  Blocks with such faces advance with e4c_stage (e4c_integrate
+ * and e4c_gasdynamic_step return E4C_ERR_STATE). */
+int e4c_connect_remote(int h, int face);
+int e4c_face_slab_bytes(int h, int face, long long* bytes);
+int e4c_pack_face(int h, int face, int stage, void* dev_dst);
+int e4c_unpack_face(int h, int face, const void* dev_src);
+
 /* Run the time loop over all blocks for nsteps steps or until max_time:
  * dt control every cfl_count steps, dt_init at step 0, x1.5 growth cap and
  * dt_max, then the gas-dynamic step.  The loop stays on the device. */

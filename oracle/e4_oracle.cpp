@@ -817,7 +817,12 @@ void Sim::apply_bcs(Block& b) {
                 for (int i = i0; i <= i1; ++i) {
                     Cell& g1 = b.cell(i + di, j + dj, k + dk);
                     Cell& g2 = b.cell(i + 2 * di, j + 2 * dj, k + 2 * dk);
-                    if (type == E4O_BC_EXCHANGE) {
+                    if (type == E4O_BC_EXCHANGE && b.ex_block[which] < 0) {
+                        // a partner on another rank: the ghost cells hold
+                        // what e4o_unpack_face wrote before this stage
+                        // (full_face_copy.d exchange over MPI, :1134, :1255)
+                        continue;
+                    } else if (type == E4O_BC_EXCHANGE) {
                         // full_face_copy.d (orientation 0, opposite faces): the
                         // ghost layers take the partner's first two cells
                         Block& o = *blocks[b.ex_block[which]];
@@ -1065,30 +1070,51 @@ void Sim::determine_time_step_size() {
     last_cfl_max = cfl_max;
 }
 
-int Sim::gasdynamic_increment() {
-    // simcore.d:2303-2952 for euler and predictor-corrector on a fixed grid.
-    const int nstages = (cfg.update_scheme == E4O_UPDATE_PC) ? 2 : 1;
-    last_bad_cells = 0;
-    for (int stage = 1; stage <= nstages; ++stage) {
-        // every block's ghost cells first (exchange copies see no flux-loop
-        // state), then every block's fluxes
-        for (Block* b : blocks) apply_bcs(*b);
-        // simcore.d:2354-2358, turned on by the adaptive flux calculator
-        // (globalconfig.d:1942-1950)
-        if (cfg.flux_calculator == E4O_FLUX_ADAPTIVE_HANEL_AUSMDV)
-            for (Block* b : blocks) detect_shock_points(*b);
-        for (Block* b : blocks) convective_flux(*b);
-        // applyPostConvFluxAction of every block (simcore.d:2373-2377)
-        for (Block* b : blocks) simple_outflow_flux(*b);
-        for (Block* b : blocks) {
-            int rc = stage_cells(*b, stage, dt_global);
-            if (rc != 0) return rc;
-        }
+int Sim::gasdynamic_stage(int stage) {
+    // one stage of simcore.d:2303-2952 (euler / predictor-corrector, fixed
+    // grid): every block's ghost cells first (exchange copies see no
+    // flux-loop state), then every block's fluxes, then the cell updates
+    if (stage == 1) last_bad_cells = 0;
+    for (Block* b : blocks) apply_bcs(*b);
+    // simcore.d:2354-2358, turned on by the adaptive flux calculator
+    // (globalconfig.d:1942-1950)
+    if (cfg.flux_calculator == E4O_FLUX_ADAPTIVE_HANEL_AUSMDV)
+        for (Block* b : blocks) detect_shock_points(*b);
+    for (Block* b : blocks) convective_flux(*b);
+    // applyPostConvFluxAction of every block (simcore.d:2373-2377)
+    for (Block* b : blocks) simple_outflow_flux(*b);
+    for (Block* b : blocks) {
+        int rc = stage_cells(*b, stage, dt_global);
+        if (rc != 0) return rc;
     }
+    return 0;
+}
+
+void Sim::finish_gasdynamic_step() {
+    const int nstages = (cfg.update_scheme == E4O_UPDATE_PC) ? 2 : 1;
     const int end_indx = (nstages == 2) ? 2 : 1;
     for (Block* b : blocks)
         for (Cell& c : b->cells) std::swap(c.U[0], c.U[end_indx]);
     time = time + dt_global;
+}
+
+int Sim::gasdynamic_increment() {
+    const int nstages = (cfg.update_scheme == E4O_UPDATE_PC) ? 2 : 1;
+    for (int stage = 1; stage <= nstages; ++stage) {
+        int rc = gasdynamic_stage(stage);
+        if (rc != 0) return rc;
+    }
+    finish_gasdynamic_step();
+    return 0;
+}
+
+// After the gas-dynamic increment: chemistry, then the step count.
+int Sim::end_step() {
+    if (cfg.reacting) {
+        int rc = chemistry_step(dt_global);
+        if (rc != 0) { error = "chemistry step failed"; return rc; }
+    }
+    step = step + 1;
     return 0;
 }
 
@@ -1102,11 +1128,8 @@ int Sim::run(int nsteps, double max_time) {
         determine_time_step_size();
         int rc = gasdynamic_increment();
         if (rc != 0) { error = "gasdynamic step failed"; return rc; }
-        if (cfg.reacting) {
-            rc = chemistry_step(dt_global);
-            if (rc != 0) { error = "chemistry step failed"; return rc; }
-        }
-        step = step + 1;
+        rc = end_step();
+        if (rc != 0) return rc;
         if (time >= max_time) finished = true;
         if (step >= target) finished = true;
     }
@@ -1239,6 +1262,140 @@ int e4o_connect_blocks(void* sim, int a, int fa, int b, int fb, int orientation)
     };
     copy_geom(A, fa, B);
     copy_geom(B, fb, A);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Blocks whose partner lives on another rank (the reference's MPI exchange,
+// full_face_copy.d:1134-1255, with the dt and bad-cell reductions of
+// simcore.d:1399-1401, 2489 left to the caller)
+// ---------------------------------------------------------------------------
+static int face_cells(const Block& B, int which, int& i0, int& i1, int& j0, int& j1, int& k0,
+                      int& k1, int& di, int& dj, int& dk) {
+    di = dj = dk = 0;
+    switch (which) {
+        case 0: dj = 1; break;
+        case 1: di = 1; break;
+        case 2: dj = -1; break;
+        case 3: di = -1; break;
+        case 4: dk = 1; break;
+        default: dk = -1; break;
+    }
+    i0 = B.imin; i1 = B.imax; j0 = B.jmin; j1 = B.jmax; k0 = B.kmin; k1 = B.kmax;
+    if (which == 0) j0 = j1 = B.jmax;
+    if (which == 2) j0 = j1 = B.jmin;
+    if (which == 1) i0 = i1 = B.imax;
+    if (which == 3) i0 = i1 = B.imin;
+    if (which == 4) k0 = k1 = B.kmax;
+    if (which == 5) k0 = k1 = B.kmin;
+    return (i1 - i0 + 1) * (j1 - j0 + 1) * (k1 - k0 + 1);
+}
+
+static int fs_fields(const Sim& s) { return 8 + s.gm.nsp + 1; }
+
+int e4o_set_remote(void* sim, int blk, int face) {
+    Sim* s = static_cast<Sim*>(sim);
+    if (blk < 0 || blk >= int(s->blocks.size()) || face < 0 || face > 5) return E4O_ERR_ARG;
+    Block& B = *s->blocks[blk];
+    if (B.dim == 2 && face >= 4) return E4O_ERR_ARG;
+    B.bc[face] = E4O_BC_EXCHANGE;
+    B.ex_block[face] = -2;
+    return 0;
+}
+
+int e4o_face_values(void* sim, int blk, int face) {
+    Sim* s = static_cast<Sim*>(sim);
+    if (blk < 0 || blk >= int(s->blocks.size()) || face < 0 || face > 5) return E4O_ERR_ARG;
+    int i0, i1, j0, j1, k0, k1, di, dj, dk;
+    const int n = face_cells(*s->blocks[blk], face, i0, i1, j0, j1, k0, k1, di, dj, dk);
+    return 2 * n * fs_fields(*s);
+}
+
+// The flow states of the two cell layers next to a face, nearest first, as
+// the partner's ghost layers take them: [layer][face cell][field], fields
+// rho, vx, vy, vz, p, T, u, a, massf[nsp], shock flag.
+int e4o_pack_face(void* sim, int blk, int face, double* out) {
+    Sim* s = static_cast<Sim*>(sim);
+    if (blk < 0 || blk >= int(s->blocks.size()) || face < 0 || face > 5 || !out)
+        return E4O_ERR_ARG;
+    Block& B = *s->blocks[blk];
+    int i0, i1, j0, j1, k0, k1, di, dj, dk;
+    const int n = face_cells(B, face, i0, i1, j0, j1, k0, k1, di, dj, dk);
+    const int nf = fs_fields(*s), nsp = s->gm.nsp;
+    for (int g = 0; g < 2; ++g) {
+        int q = 0;
+        for (int k = k0; k <= k1; ++k)
+            for (int j = j0; j <= j1; ++j)
+                for (int i = i0; i <= i1; ++i, ++q) {
+                    const FlowState& fs = B.cell(i - g * di, j - g * dj, k - g * dk).fs;
+                    double* o = out + (size_t(g) * n + q) * nf;
+                    o[0] = fs.gas.rho; o[1] = fs.vel.x; o[2] = fs.vel.y; o[3] = fs.vel.z;
+                    o[4] = fs.gas.p; o[5] = fs.gas.T; o[6] = fs.gas.u; o[7] = fs.gas.a;
+                    for (int sp = 0; sp < nsp; ++sp) o[8 + sp] = fs.gas.massf[sp];
+                    o[8 + nsp] = double(fs.S);
+                }
+    }
+    return 0;
+}
+
+// The ghost layers of a remote face from the partner's packed layers.
+int e4o_unpack_face(void* sim, int blk, int face, const double* in) {
+    Sim* s = static_cast<Sim*>(sim);
+    if (blk < 0 || blk >= int(s->blocks.size()) || face < 0 || face > 5 || !in)
+        return E4O_ERR_ARG;
+    Block& B = *s->blocks[blk];
+    int i0, i1, j0, j1, k0, k1, di, dj, dk;
+    const int n = face_cells(B, face, i0, i1, j0, j1, k0, k1, di, dj, dk);
+    const int nf = fs_fields(*s), nsp = s->gm.nsp;
+    for (int g = 0; g < 2; ++g) {
+        int q = 0;
+        for (int k = k0; k <= k1; ++k)
+            for (int j = j0; j <= j1; ++j)
+                for (int i = i0; i <= i1; ++i, ++q) {
+                    FlowState& fs =
+                        B.cell(i + (g + 1) * di, j + (g + 1) * dj, k + (g + 1) * dk).fs;
+                    const double* v = in + (size_t(g) * n + q) * nf;
+                    fs.gas.rho = v[0]; fs.vel.x = v[1]; fs.vel.y = v[2]; fs.vel.z = v[3];
+                    fs.gas.p = v[4]; fs.gas.T = v[5]; fs.gas.u = v[6]; fs.gas.a = v[7];
+                    for (int sp = 0; sp < nsp; ++sp) fs.gas.massf[sp] = v[8 + sp];
+                    fs.S = int(v[8 + nsp]);
+                }
+    }
+    return 0;
+}
+
+// This rank's share of determine_time_step_size (simcore.d:1362-1386): the
+// minimum dt_allow and maximum CFL over its blocks, each block's rescale
+// applied; the caller reduces over ranks and takes the global decision.
+int e4o_dt_allow(void* sim, double dt_current, int check_cfl, double* dt_allow, double* cfl_max) {
+    Sim* s = static_cast<Sim*>(sim);
+    double d_all = DBL_MAX, c_all = 0.0;
+    for (Block* b : s->blocks) {
+        double d, c;
+        s->block_dt(*b, dt_current, check_cfl != 0, d, c);
+        d_all = std::min(d_all, d);
+        c_all = std::max(c_all, c);
+    }
+    *dt_allow = d_all;
+    *cfl_max = c_all;
+    return 0;
+}
+
+void e4o_set_dt_global(void* sim, double dt) { static_cast<Sim*>(sim)->dt_global = dt; }
+
+// One stage of the gas-dynamic increment over every block with dt_global;
+// the last stage also ends the step (time, chemistry, step count).
+int e4o_stage(void* sim, int stage) {
+    Sim* s = static_cast<Sim*>(sim);
+    const int nstages = (s->cfg.update_scheme == E4O_UPDATE_PC) ? 2 : 1;
+    if (stage < 1 || stage > nstages) return E4O_ERR_ARG;
+    int rc = s->gasdynamic_stage(stage);
+    if (rc != 0) { s->error = "gasdynamic step failed"; return rc; }
+    if (stage == nstages) {
+        s->finish_gasdynamic_step();
+        rc = s->end_step();
+        if (rc != 0) return rc;
+    }
     return 0;
 }
 

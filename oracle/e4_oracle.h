@@ -116,6 +116,22 @@ int e4o_get_cell_geometry(void* sim, int blk, double* out);
  * src/eilmer/simcore.d integrate_in_time.  Returns 0 or a negative error. */
 int e4o_run(void* sim, int nsteps, double max_time);
 
+/* A face whose partner lives on another rank (full_face_copy.d MPI
+ * exchange): its ghost cells keep what e4o_unpack_face writes.  Values per
+ * packed face (2 layers x face cells x fields), the packing of the two cell
+ * layers next to a face, and their unpacking into a remote face's ghosts. */
+int e4o_set_remote(void* sim, int blk, int face);
+int e4o_face_values(void* sim, int blk, int face);
+int e4o_pack_face(void* sim, int blk, int face, double* out);
+int e4o_unpack_face(void* sim, int blk, int face, const double* in);
+
+/* This rank's min dt_allow / max CFL over its blocks (simcore.d:1362-1386);
+ * dt_global set by the caller; one stage of the gas-dynamic increment (the
+ * last stage ends the step). */
+int e4o_dt_allow(void* sim, double dt_current, int check_cfl, double* dt_allow, double* cfl_max);
+void e4o_set_dt_global(void* sim, double dt);
+int e4o_stage(void* sim, int stage);
+
 double e4o_time(void* sim);
 double e4o_dt_global(void* sim);
 int e4o_step_count(void* sim);

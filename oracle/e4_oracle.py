@@ -143,6 +143,14 @@ def _declare(L):
     L.e4o_newton_test.argtypes = [ip, P(dp)]
     L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
     L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
+    L.e4o_set_remote.argtypes = [vp, ip, ip]
+    L.e4o_face_values.argtypes = [vp, ip, ip]
+    L.e4o_pack_face.argtypes = [vp, ip, ip, P(dp)]
+    L.e4o_unpack_face.argtypes = [vp, ip, ip, P(dp)]
+    L.e4o_dt_allow.argtypes = [vp, dp, ip, P(dp), P(dp)]
+    L.e4o_set_dt_global.argtypes = [vp, dp]
+    L.e4o_set_dt_global.restype = None
+    L.e4o_stage.argtypes = [vp, ip]
     return L
 
 
@@ -226,6 +234,37 @@ class OracleSim:
     def run(self, nsteps, max_time=1.0e300):
         rc = self._L.e4o_run(self._h, nsteps, max_time)
         return rc
+
+    # -- faces joined to blocks of another rank --------------------------------
+    def set_remote(self, b, face):
+        rc = self._L.e4o_set_remote(self._h, b, face)
+        if rc != 0:
+            raise RuntimeError(f"e4o_set_remote failed: {rc}")
+
+    def pack_face(self, b, face):
+        out = np.zeros(self._L.e4o_face_values(self._h, b, face))
+        rc = self._L.e4o_pack_face(self._h, b, face, _dptr(out))
+        if rc != 0:
+            raise RuntimeError(f"e4o_pack_face failed: {rc}")
+        return out
+
+    def unpack_face(self, b, face, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        rc = self._L.e4o_unpack_face(self._h, b, face, _dptr(v))
+        if rc != 0:
+            raise RuntimeError(f"e4o_unpack_face failed: {rc}")
+
+    def dt_allow(self, dt_current, check_cfl):
+        d, c = ctypes.c_double(), ctypes.c_double()
+        self._L.e4o_dt_allow(self._h, dt_current, int(check_cfl), ctypes.byref(d),
+                             ctypes.byref(c))
+        return d.value, c.value
+
+    def set_dt_global(self, dt):
+        self._L.e4o_set_dt_global(self._h, dt)
+
+    def stage(self, stage):
+        return self._L.e4o_stage(self._h, stage)
 
     @property
     def time(self):

@@ -162,7 +162,10 @@ struct Sim {
     double signal_frequency(Block& b, Cell& c, int i, int j, int k) const;
     void block_dt(Block& b, double dt_current, bool check_cfl, double& dt_allow, double& cfl_max);
     void determine_time_step_size();
+    int gasdynamic_stage(int stage);
+    void finish_gasdynamic_step();
     int gasdynamic_increment();
+    int end_step();
     int chemistry_step(double dt);
     int run(int nsteps, double max_time);
 };
