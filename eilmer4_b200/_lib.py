@@ -63,6 +63,7 @@ class E4CConfig(ctypes.Structure):
         ("shear_tolerance", ctypes.c_double),
         ("compression_tolerance", ctypes.c_double),
         ("chem_newton_iterations", ctypes.c_int),
+        ("chem_method", ctypes.c_int),
     ]
 
 

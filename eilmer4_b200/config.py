@@ -42,7 +42,13 @@ CONFIG_DEFAULTS = {
     "shear_tolerance": 0.20,                      # :585
     "compression_tolerance": -0.30,               # :600
     "chem_newton_iterations": 12,                 # whole-interval point-implicit step
+    # chemistry method: "point-implicit" (this library's update, opCall's
+    # sub-cycling as its recovery) or "rkf" (the reference's default
+    # odeStep.method, chemistry_update.d:75-80 with prep_chem.lua:51)
+    "chem_method": "point-implicit",
 }
+
+CHEM_METHOD = {"point-implicit": 0, "rkf": 1}
 
 CONTROL_DEFAULTS = {
     "dt_init": 1.0e-3,    # globalconfig.d:726
@@ -115,6 +121,9 @@ def make_config(config: dict | None = None, control: dict | None = None, *,
     cfg.shear_tolerance = float(c["shear_tolerance"])
     cfg.compression_tolerance = float(c["compression_tolerance"])
     cfg.chem_newton_iterations = int(c["chem_newton_iterations"])
+    if c["chem_method"] not in CHEM_METHOD:
+        raise UnsupportedConfig(f"chem_method {c['chem_method']!r} is not on this path")
+    cfg.chem_method = CHEM_METHOD[c["chem_method"]]
     return cfg
 
 

@@ -296,6 +296,8 @@ int e4c_init(const e4c_config* cfg) {
     if (cfg->cfl_count < 1) return fail(E4C_ERR_ARG, "cfl_count must be >= 1");
     if (cfg->chem_newton_iterations < 0 || cfg->chem_newton_iterations > 100)
         return fail(E4C_ERR_ARG, "chem_newton_iterations must be in 0..100");
+    if (cfg->chem_method != E4C_CHEM_POINT_IMPLICIT && cfg->chem_method != E4C_CHEM_RKF)
+        return fail(E4C_ERR_UNSUPPORTED, "chem_method must be point-implicit or rkf");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return fail(E4C_ERR_CUDA, "no CUDA device available");
@@ -369,6 +371,8 @@ int e4c_set_thermochem(const e4c_thermochem* tc) {
     if (set_thermochem_constants(*tc) != 0) return fail(E4C_ERR_CUDA, "copy of the mixture failed");
     if (set_chem_newton_iterations(c.cfg.chem_newton_iterations) != 0)
         return fail(E4C_ERR_CUDA, "copy of the chemistry settings failed");
+    if (set_chem_method(c.cfg.chem_method) != 0)
+        return fail(E4C_ERR_CUDA, "setting the chemistry method failed");
     c.have_thermochem = true;
     c.nreac = tc->nreac;
     for (int i = 0; i < 5; ++i) c.seed.mol.M[i] = tc->M[i];

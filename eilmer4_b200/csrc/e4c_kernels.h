@@ -56,6 +56,7 @@ void launch_check_uniform(const BlockView& b, int* flag, cudaStream_t s);
 // thermally perfect mixture / mechanism into constant memory; chemistry of one block
 int set_thermochem_constants(const e4c_thermochem& tc);
 int set_chem_newton_iterations(int n);
+int set_chem_method(int m);
 // ghost-cell geometry of an exchange boundary from the partner block
 void launch_exchange_geometry(const BlockView& b, int which, cudaStream_t s);
 // per-cell chemistry step suggestions to (to_dense = 1) or from a dense array

@@ -575,6 +575,77 @@ __device__ bool point_implicit_step(const MechD<NSP, NR>& m, const double* c0, c
     return err <= 1.0;
 }
 
+// RKFStep.opCall (chemistry_update.d:362-461): Runge-Kutta-Fehlberg with the
+// Cash-Karp coefficients on dc/dt = q - L, the fourth/fifth-order difference
+// as the error (atol = rtol = 1e-3, RMS over the species) and the step-size
+// suggestion (safety 0.9, exponent 0.2, scale limits [0.2, 10]); the same
+// operations as the oracle's rkf_step.  Returns true on a successful step.
+template <int NSP, int NR>
+__device__ bool rkf_step_d(const MechD<NSP, NR>& m, const double* y0, double h, double* yOut,
+                           double& hSuggest) {
+    const double a21 = 1. / 5., a31 = 3. / 40., a32 = 9. / 40., a41 = 3. / 10., a42 = -9. / 10.,
+                 a43 = 6. / 5., a51 = -11. / 54., a52 = 5. / 2., a53 = -70. / 27.,
+                 a54 = 35. / 27., a61 = 1631. / 55296., a62 = 175. / 512., a63 = 575. / 13824.,
+                 a64 = 44275. / 110592., a65 = 253. / 4096.;
+    const double b51 = 37. / 378., b53 = 250. / 621., b54 = 125. / 594., b56 = 512. / 1771.,
+                 b41 = 2825. / 27648., b43 = 18575. / 48384., b44 = 13525. / 55296.,
+                 b45 = 277. / 14336., b46 = 1.0 / 4.0;
+    const double tol = 1.0e-3;   // odeStep.errTol default, prep_chem.lua:51
+    double k1[NSP], k2[NSP], k3[NSP], k4[NSP], k5[NSP], k6[NSP], yt[NSP], q[NSP], L[NSP];
+    m.split_rates(y0, q, L);
+    for (int i = 0; i < NSP; ++i) k1[i] = q[i] - L[i];
+    for (int i = 0; i < NSP; ++i) yt[i] = y0[i] + h * (a21 * k1[i]);
+    m.split_rates(yt, q, L);
+    for (int i = 0; i < NSP; ++i) k2[i] = q[i] - L[i];
+    for (int i = 0; i < NSP; ++i) yt[i] = y0[i] + h * (a31 * k1[i] + a32 * k2[i]);
+    m.split_rates(yt, q, L);
+    for (int i = 0; i < NSP; ++i) k3[i] = q[i] - L[i];
+    for (int i = 0; i < NSP; ++i) yt[i] = y0[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+    m.split_rates(yt, q, L);
+    for (int i = 0; i < NSP; ++i) k4[i] = q[i] - L[i];
+    for (int i = 0; i < NSP; ++i)
+        yt[i] = y0[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+    m.split_rates(yt, q, L);
+    for (int i = 0; i < NSP; ++i) k5[i] = q[i] - L[i];
+    for (int i = 0; i < NSP; ++i)
+        yt[i] = y0[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+    m.split_rates(yt, q, L);
+    for (int i = 0; i < NSP; ++i) k6[i] = q[i] - L[i];
+    double err = 0.0;
+    for (int i = 0; i < NSP; ++i) {
+        yOut[i] = y0[i] + h * (b51 * k1[i] + b53 * k3[i] + b54 * k4[i] + b56 * k6[i]);
+        const double yErr =
+            yOut[i] - (y0[i] + h * (b41 * k1[i] + b43 * k3[i] + b44 * k4[i] + b45 * k5[i] +
+                                    b46 * k6[i]));
+        const double fa = fabs(y0[i]), fb = fabs(yOut[i]);
+        const double sk = tol + tol * ((fa < fb) ? fb : fa);
+        err += (yErr / sk) * (yErr / sk);
+    }
+    err = sqrt(err / NSP);
+    const double maxscale = 10.0, minscale = 0.2, safe = 0.9, alpha = 0.2;
+    double scale;
+    if (err <= 1.0) {
+        if (err == 0.0) {
+            scale = maxscale;
+        } else {
+            scale = safe * pm_pow(err, -alpha);
+            if (scale < minscale) scale = minscale;
+            if (scale > maxscale) scale = maxscale;
+        }
+        hSuggest = scale * h;
+        return true;
+    }
+    const double sc = safe * pm_pow(err, -alpha);
+    scale = (sc < minscale) ? minscale : sc;
+    hSuggest = scale * h;
+    return false;
+}
+
+// Chemistry method (e4c_config.chem_method): 0 the point-implicit step over
+// the whole interval with opCall's sub-cycled recovery; 1 the reference's
+// odeStep.method 'rkf' (opCall's sub-cycling with RKF steps from the start).
+static __constant__ int c_chem_method = 0;
+
 // Outcomes of point_implicit_whole.
 constexpr int PI_FAILED = 0;      // no convergence: the sub-cycled recovery takes over
 constexpr int PI_CONVERGED = 1;
@@ -679,9 +750,11 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
         if (conc0[i] < 1.0e-30) conc0[i] = 0.0;
         concOut[i] = conc0[i];
     }
+    const int method = c_chem_method;
+    if (method == 1 && probe) return CHEM_NEEDS_WORK;   // every cell sub-cycles
     MechD<NSP, NR> m(tc);
     m.rate_constants(Q.T);
-    {
+    if (method == 0) {
         int iters = 0;
         const int st =
             point_implicit_whole<NSP, NR>(m, conc0, guess, tInterval, concOut, iters, probe);
@@ -714,7 +787,10 @@ __device__ int chemistry_update_d(const e4c_thermochem& tc, TPState<NSP>& Q, dou
         int attempt = 0;
         for (; attempt < 4; ++attempt) {
             int iters = 0;
-            bool ok = point_implicit_step<NSP, NR>(m, conc0, conc0, h, concOut, dtChemSuggest,
+            const bool ok =
+                (method == 1)
+                    ? rkf_step_d<NSP, NR>(m, conc0, h, concOut, dtChemSuggest)
+                    : point_implicit_step<NSP, NR>(m, conc0, conc0, h, concOut, dtChemSuggest,
                                                    iters);
             if (cnt) cnt->newton += iters;
             bool massf_ok = true;

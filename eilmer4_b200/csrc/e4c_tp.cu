@@ -99,6 +99,10 @@ int set_chem_newton_iterations(int n) {
     return cudaMemcpyToSymbol(c_chem_newton_iterations, &n, sizeof(n)) == cudaSuccess ? 0 : -1;
 }
 
+int set_chem_method(int m) {
+    return cudaMemcpyToSymbol(c_chem_method, &m, sizeof(m)) == cudaSuccess ? 0 : -1;
+}
+
 int set_thermochem_constants(const e4c_thermochem& tc) {
     if (cudaMemcpyToSymbol(c_tc, &tc, sizeof(tc)) != cudaSuccess) return -1;
     // the shortcut with kappa = 1/4 needs a slope ratio of at least 1/2

@@ -115,7 +115,14 @@ typedef struct e4c_config {
                                        chemistry step before opCall's sub-cycling takes over
                                        (default 12; 0 sends every cell that needs Newton work
                                        to the sub-cycling) */
+    int chem_method;                /* E4C_CHEM_POINT_IMPLICIT (default) or E4C_CHEM_RKF: the
+                                       reference's odeStep.method 'rkf' (ChemistryUpdate.opCall's
+                                       sub-cycling with RKFStep, chemistry_update.d:119-307,
+                                       362-461) */
 } e4c_config;
+
+#define E4C_CHEM_POINT_IMPLICIT 0
+#define E4C_CHEM_RKF 1
 
 typedef struct e4c_run_info {
     int steps_taken;

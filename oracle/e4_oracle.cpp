@@ -1169,6 +1169,7 @@ void e4o_default_config(e4o_config* c) {
     c->shear_tolerance = 0.20;
     c->compression_tolerance = -0.30;
     c->chem_newton_iterations = 12;
+    c->chem_method = 0;
 }
 
 void* e4o_sim_new(const e4o_config* cfg) {

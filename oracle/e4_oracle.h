@@ -52,6 +52,9 @@ typedef struct e4o_config {
     double shear_tolerance;         /* adaptive flux: globalconfig.d:585 */
     double compression_tolerance;   /* shock detector: globalconfig.d:600 */
     int chem_newton_iterations;     /* whole-interval point-implicit step (default 12) */
+    int chem_method;                /* 0: point-implicit step with opCall's sub-cycled recovery;
+                                       1: the reference's odeStep.method 'rkf' (opCall with RKF
+                                       sub-steps, chemistry_update.d:119-307, 362-461) */
 } e4o_config;
 
 /* Thermally perfect mixture and reaction mechanism (plain arrays).
@@ -157,6 +160,13 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
  * single-cell entry points above (default 12; a simulation uses its own
  * configuration's value). */
 int e4o_set_chem_newton_iterations(int n);
+/* Chemistry method of the single-cell entry points (chem_method above). */
+int e4o_set_chem_method(int m);
+/* One RKF step (chemistry_update.d:362-461, tolerance 1e-3) of the
+ * mechanism's rate equations at temperature T from conc0 over h: concOut, the
+ * suggested next step; returns 0 on a successful step, 1 on a failed one. */
+int e4o_rkf_step(const e4o_thermochem* tc, double T, const double* conc0, double h,
+                 double* concOut, double* h_suggest);
 
 /* The chemistry update alone (ChemistryUpdate.opCall with the point-implicit
  * step) at constant rho and T: new mass fractions, no temperature update. */

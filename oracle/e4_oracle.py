@@ -55,6 +55,7 @@ class Config(ctypes.Structure):
         ("shear_tolerance", ctypes.c_double),
         ("compression_tolerance", ctypes.c_double),
         ("chem_newton_iterations", ctypes.c_int),
+        ("chem_method", ctypes.c_int),
     ]
 
 
@@ -143,6 +144,8 @@ def _declare(L):
     L.e4o_newton_test.argtypes = [ip, P(dp)]
     L.e4o_gpuchem_prepare.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
     L.e4o_gpuchem_finish.argtypes = [P(ThermoChem), ip] + [P(dp)] * 8
+    L.e4o_set_chem_method.argtypes = [ip]
+    L.e4o_rkf_step.argtypes = [P(ThermoChem), dp, P(dp), dp, P(dp), P(dp)]
     L.e4o_set_remote.argtypes = [vp, ip, ip]
     L.e4o_face_values.argtypes = [vp, ip, ip]
     L.e4o_pack_face.argtypes = [vp, ip, ip, P(dp)]
@@ -384,3 +387,24 @@ def newton_test(which):
 def set_chem_newton_iterations(n):
     """Newton iterations of the whole-interval step for chem_cell / chem_update."""
     lib().e4o_set_chem_newton_iterations(int(n))
+
+
+def set_chem_method(m):
+    """Chemistry method of the single-cell entry points: 0 point-implicit
+    (with opCall's sub-cycled recovery), 1 the reference's RKF (opCall with
+    RKF sub-steps)."""
+    rc = lib().e4o_set_chem_method(int(m))
+    if rc != 0:
+        raise ValueError("unknown chemistry method")
+
+
+def rkf_step(thermochem, T, conc0, h):
+    """One RKF step of the rate equations at T from conc0 over h:
+    (succeeded, concOut, suggested next step)."""
+    tc = thermochem.fill(ThermoChem())
+    c0 = np.ascontiguousarray(conc0, dtype=np.float64)
+    out = np.zeros_like(c0)
+    hs = ctypes.c_double()
+    rc = lib().e4o_rkf_step(ctypes.byref(tc), float(T), _dptr(c0), float(h), _dptr(out),
+                            ctypes.byref(hs))
+    return rc == 0, out, hs.value

@@ -517,6 +517,71 @@ static bool point_implicit_step(const Mech& m, const double* c0, double h, doubl
     return err <= 1.0;
 }
 
+// RKFStep.opCall (chemistry_update.d:362-461): Runge-Kutta-Fehlberg with the
+// Cash-Karp coefficients on dc/dt = q - L (eval_rates, reaction_mechanism.d:
+// 59-66); the fifth-order solution, the difference from the fourth-order one
+// as the error, measured with atol = rtol = tolerance as an RMS over the
+// species, and the step-size suggestion with safety 0.9, exponent 0.2 and
+// scale limits [0.2, 10].  Returns true on a successful step.
+static const double RKF_TOL = 1.0e-3;   // odeStep.errTol default, prep_chem.lua:51
+
+static bool rkf_step(const Mech& m, const double* y0, double h, double* yOut,
+                     double& hSuggest) {
+    const int n = m.tc.nsp;
+    const double a21 = 1. / 5., a31 = 3. / 40., a32 = 9. / 40., a41 = 3. / 10., a42 = -9. / 10.,
+                 a43 = 6. / 5., a51 = -11. / 54., a52 = 5. / 2., a53 = -70. / 27.,
+                 a54 = 35. / 27., a61 = 1631. / 55296., a62 = 175. / 512., a63 = 575. / 13824.,
+                 a64 = 44275. / 110592., a65 = 253. / 4096.;
+    const double b51 = 37. / 378., b53 = 250. / 621., b54 = 125. / 594., b56 = 512. / 1771.,
+                 b41 = 2825. / 27648., b43 = 18575. / 48384., b44 = 13525. / 55296.,
+                 b45 = 277. / 14336., b46 = 1.0 / 4.0;
+    double k1[E4O_MAXSP], k2[E4O_MAXSP], k3[E4O_MAXSP], k4[E4O_MAXSP], k5[E4O_MAXSP],
+        k6[E4O_MAXSP], yt[E4O_MAXSP] = {}, q[E4O_MAXSP], L[E4O_MAXSP];
+    auto eval = [&](const double* y, double* k) {
+        m.split_rates(y, q, L);
+        for (int i = 0; i < n; ++i) k[i] = q[i] - L[i];
+    };
+    eval(y0, k1);
+    for (int i = 0; i < n; ++i) yt[i] = y0[i] + h * (a21 * k1[i]);
+    eval(yt, k2);
+    for (int i = 0; i < n; ++i) yt[i] = y0[i] + h * (a31 * k1[i] + a32 * k2[i]);
+    eval(yt, k3);
+    for (int i = 0; i < n; ++i) yt[i] = y0[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+    eval(yt, k4);
+    for (int i = 0; i < n; ++i)
+        yt[i] = y0[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+    eval(yt, k5);
+    for (int i = 0; i < n; ++i)
+        yt[i] = y0[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+    eval(yt, k6);
+    double err = 0.0;
+    for (int i = 0; i < n; ++i) {
+        yOut[i] = y0[i] + h * (b51 * k1[i] + b53 * k3[i] + b54 * k4[i] + b56 * k6[i]);
+        const double yErr =
+            yOut[i] - (y0[i] + h * (b41 * k1[i] + b43 * k3[i] + b44 * k4[i] + b45 * k5[i] +
+                                    b46 * k6[i]));
+        const double sk = RKF_TOL + RKF_TOL * std::max(std::fabs(y0[i]), std::fabs(yOut[i]));
+        err += (yErr / sk) * (yErr / sk);
+    }
+    err = std::sqrt(err / n);
+    const double maxscale = 10.0, minscale = 0.2, safe = 0.9, alpha = 0.2;
+    double scale;
+    if (err <= 1.0) {
+        if (err == 0.0) {
+            scale = maxscale;
+        } else {
+            scale = safe * pm_pow(err, -alpha);
+            if (scale < minscale) scale = minscale;
+            if (scale > maxscale) scale = maxscale;
+        }
+        hSuggest = scale * h;
+        return true;
+    }
+    scale = std::max(safe * pm_pow(err, -alpha), minscale);
+    hSuggest = scale * h;
+    return false;
+}
+
 // One backward-Euler step over the whole interval h, x = c0 + h w(x), by
 // Newton iteration from the start x = c0 (at most maxit iterations, 12 unless
 // configured otherwise,
@@ -567,8 +632,10 @@ static bool point_implicit_whole(const Mech& m, const double* c0, double h, doub
 // ChemistryUpdate.opCall's sub-cycling (chemistry_update.d:119-307) takes
 // over, with error-controlled point-implicit sub-steps and the per-cell
 // dt_chem warm start.
+// With method 1 (the reference's odeStep.method 'rkf') there is no
+// whole-interval step: opCall's sub-cycling with RKF sub-steps from the start.
 static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInterval,
-                            double& dtChemSuggest, int maxit) {
+                            double& dtChemSuggest, int maxit, int method) {
     const int n = tc.nsp;
     GasState Qinit = Q;
     double conc0[E4O_MAXSP], concOut[E4O_MAXSP];
@@ -580,7 +647,7 @@ static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInter
     for (int i = 0; i < n; ++i) concOut[i] = conc0[i];
     Mech m(tc);
     m.eval_rate_constants(Q.T);
-    {
+    if (method == 0) {
         int iters;
         if (point_implicit_whole(m, conc0, tInterval, concOut, iters, maxit)) {
             double total = 0.0;
@@ -608,8 +675,9 @@ static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInter
         h = std::min(h, tInterval - t);
         int attempt = 0;
         for (; attempt < maxAttempts; ++attempt) {
-            int iters;
-            bool ok = point_implicit_step(m, conc0, h, concOut, dtChemSuggest, iters);
+            int iters = 0;
+            bool ok = (method == 1) ? rkf_step(m, conc0, h, concOut, dtChemSuggest)
+                                    : point_implicit_step(m, conc0, h, concOut, dtChemSuggest, iters);
             bool massf_ok = true;
             if (ok) {
                 double total = 0.0;
@@ -651,12 +719,12 @@ static int chemistry_update(const e4o_thermochem& tc, GasState& Q, double tInter
 
 // FVCell.thermochemical_increment (fvcell.d:1510-1621)
 static int thermochemical_increment(const e4o_thermochem& tc, double T_frozen, GasState& Q,
-                                    double dt, double& dt_chem, int maxit) {
+                                    double dt, double& dt_chem, int maxit, int method) {
     if (Q.T <= T_frozen) return 0;
-    int rc = chemistry_update(tc, Q, dt, dt_chem, maxit);
+    int rc = chemistry_update(tc, Q, dt, dt_chem, maxit, method);
     if (rc != 0) {
         dt_chem = -1.0;
-        rc = chemistry_update(tc, Q, dt, dt_chem, maxit);
+        rc = chemistry_update(tc, Q, dt, dt_chem, maxit, method);
         if (rc != 0) return rc;
     }
     TP tp(tc);
@@ -677,7 +745,7 @@ int Sim::chemistry_step(double dt) {
                     // fvcell.d:1514: frozen cells return before U.massf is touched
                     if (c.fs.gas.T <= cfg.T_frozen) continue;
                     int rc = thermochemical_increment(gm.tc, cfg.T_frozen, c.fs.gas, dt, c.dt_chem,
-                                                      cfg.chem_newton_iterations);
+                                                      cfg.chem_newton_iterations, cfg.chem_method);
                     if (rc != 0) { err = std::min(err, rc); continue; }
                     for (int s = 0; s < nsp_cons; ++s) c.U[0][5 + s] = c.fs.gas.rho * c.fs.gas.massf[s];
                 }
@@ -692,8 +760,22 @@ using namespace e4o;
 // Newton iterations of the whole-interval step for the single-cell entry
 // points (a simulation uses its configuration's value).
 static int g_chem_newton_iterations = 12;
+static int g_chem_method = 0;
 
 extern "C" {
+
+int e4o_set_chem_method(int m) {
+    if (m != 0 && m != 1) return E4O_ERR_ARG;
+    g_chem_method = m;
+    return 0;
+}
+
+int e4o_rkf_step(const e4o_thermochem* tc, double T, const double* conc0, double h,
+                 double* concOut, double* h_suggest) {
+    Mech m(*tc);
+    m.eval_rate_constants(T);
+    return rkf_step(m, conc0, h, concOut, *h_suggest) ? 0 : 1;
+}
 
 int e4o_set_chem_newton_iterations(int n) {
     g_chem_newton_iterations = n;
@@ -727,7 +809,7 @@ int e4o_chem_update(const e4o_thermochem* tc, double dt, double rho, double T, d
     GasState Q;
     Q.rho = rho; Q.T = T; Q.u = 0.0; Q.p = 0.0;
     for (int i = 0; i < tc->nsp; ++i) Q.massf[i] = massf[i];
-    int rc = chemistry_update(*tc, Q, dt, *dt_chem, g_chem_newton_iterations);
+    int rc = chemistry_update(*tc, Q, dt, *dt_chem, g_chem_newton_iterations, g_chem_method);
     if (rc != 0) return rc;
     for (int i = 0; i < tc->nsp; ++i) massf[i] = Q.massf[i];
     return 0;
@@ -738,7 +820,8 @@ int e4o_chem_cell(const e4o_thermochem* tc, double T_frozen, double dt, double r
     GasState Q;
     Q.rho = rho; Q.T = *T; Q.u = *u; Q.p = *p;
     for (int i = 0; i < tc->nsp; ++i) Q.massf[i] = massf[i];
-    int rc = thermochemical_increment(*tc, T_frozen, Q, dt, *dt_chem, g_chem_newton_iterations);
+    int rc = thermochemical_increment(*tc, T_frozen, Q, dt, *dt_chem, g_chem_newton_iterations,
+                                      g_chem_method);
     if (rc != 0) return rc;
     *T = Q.T; *u = Q.u; *p = Q.p;
     for (int i = 0; i < tc->nsp; ++i) massf[i] = Q.massf[i];

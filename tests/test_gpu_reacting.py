@@ -118,3 +118,65 @@ def test_flow_file_round_trip_through_the_gpu(oracle, e4lib, tmp_path):
         rel = np.abs(c1 - c0) / np.maximum(np.abs(c0), 1e-300)
         assert rel[:4].max() <= 1e-15 and rel[5:].max() <= 1e-15, rel.max()
         assert rel[4].max() <= 1e-9, rel[4].max()
+
+
+def test_rkf_chemistry_step_on_hot_air_bitexact(oracle, e4lib):
+    """The reference's own chemistry method (odeStep.method 'rkf':
+    ChemistryUpdate.opCall's sub-cycling with RKFStep, chemistry_update.d:
+    119-307, 362-461) on the device: every cell's mass fractions, T, u, p
+    and dt_chem equal the oracle's, whose update of the hydrogen-iodide test
+    problem gives the reference's golden value (test_oracle_kinetics_golden)."""
+    from eilmer4_b200.simcore import Simulation
+    wl = W.reacting_channel(ni=16, nj=8)
+    tc = wl.thermochem
+    b = wl.blocks[0]
+    n = b.ncell
+    rng = np.random.default_rng(8)
+    mf0 = [0.767, 0.233, 0.0, 0.0, 0.0]
+    for q in range(n):
+        T = 2500.0 + 2500.0 * rng.random()
+        p = 1.0e4 + 1.0e5 * rng.random()
+        y = np.array(mf0) + np.array([0.0, -0.05, 0.02, 0.01, 0.02]) * rng.random()
+        y = y / y.sum()
+        rho, u, a = tc.state_pT(p, T, y)
+        b.prim[:, q] = [rho, 0.0, 0.0, 0.0, p, T, u, a] + list(y)
+    dt = 1.0e-7
+    with Simulation.from_workload(wl, reacting=True, chem_method="rkf") as sim:
+        sim.chemistry_step([0], dt)
+        gp, gc = sim.download(0)
+        dchem = np.zeros(n)
+        from eilmer4_b200 import _lib
+        sim.L.e4c_block_get_dt_chem(0, _lib.dptr(dchem))
+    oracle.set_chem_method(1)
+    try:
+        for q in range(n):
+            rc, out = oracle.chem_cell(tc, 300.0, dt, b.prim[0, q], b.prim[5, q], b.prim[6, q],
+                                       b.prim[4, q], b.prim[8:, q].copy(), -1.0)
+            assert rc == 0
+            assert_same(gp[8:, q], out["massf"], f"cell {q} mass fractions")
+            assert gp[5, q] == out["T"] and gp[6, q] == out["u"] and gp[4, q] == out["p"], q
+            assert dchem[q] == out["dt_chem"], q
+    finally:
+        oracle.set_chem_method(0)
+    assert gp[12].max() > 1.0e-5   # oxygen dissociated
+
+
+def test_rkf_hot_ramp_channel_bitexact(oracle, e4lib):
+    from eilmer4_b200.simcore import Simulation
+    wl = W.reacting_channel_hot(ni=48, nj=24)
+    nsteps = 12
+    cfg = oracle.default_config(dimensions=2, flux_calculator=oracle.FLUX_AUSMDV,
+                                gas_model=oracle.GAS_THERM_PERF_5SP_AIR, reacting=1,
+                                n_threads=0, chem_method=1)
+    osim = oracle.OracleSim(cfg, wl.thermochem)
+    b = wl.blocks[0]
+    osim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
+    osim.set_flow(0, b.prim)
+    assert osim.run(nsteps) == 0
+    op, oc = osim.get_flow(0)
+    with Simulation.from_workload(wl, reacting=True, chem_method="rkf") as sim:
+        sim.run(nsteps)
+        gp, gc = sim.download(0)
+        assert sim.state()[2] == osim.step and sim.state()[0] == osim.time
+    assert_same(gc, oc, "conserved")
+    assert_same(gp, op, "primitive")

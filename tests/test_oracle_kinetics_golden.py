@@ -99,3 +99,45 @@ def test_portable_math_against_libm_on_the_hot_channel(oracle):
         if scale == 0.0:
             continue
         assert np.abs(p1[q] - p0[q]).max() <= 1e-11 * scale, q
+
+
+def test_rkf_step_order_golden(oracle):
+    """chemistry_update.d:681-698: the RKF step on the hydrogen-iodide system,
+    repeated with a fixed step to t = 60,000 s, with h = 287.175 and with
+    h * 2^(-1/5): the errors against the analytic HI concentration fall by
+    the ratio 1.96809 (to 1e-4), as a fifth-order method's do."""
+    tc = h2_i2(1.93e8, 20620.0, 5.470705805110e-07, 0.0)
+    T, c0, t_end = 700.0, 4.54, 60000.0
+    analytic = 7.1420197868416215
+
+    def estimate(dt):
+        conc = np.array([c0, c0, 0.0])
+        t = 0.0
+        while (t_end - t) > 1.0e-9:
+            dt = min(dt, t_end - t)
+            _, conc, _ = oracle.rkf_step(tc, T, conc, dt)
+            t += dt
+        return conc[2]
+
+    dt = 287.175
+    err0 = analytic - estimate(dt)
+    err1 = analytic - estimate(dt * 2.0 ** (-1.0 / 5.0))
+    assert abs(err0 / err1 - 1.96809) <= 1e-4 * 1.96809, err0 / err1
+
+
+def test_rkf_chemistry_update_golden(oracle):
+    """chemistry_update.d:720-731: the complete chemistry update (opCall's
+    sub-cycling with RKF steps, the reference's default method) over
+    60,000 s from dt_chem = 200 s gives HI = 7.14201983840 mol/m^3 (to 1e-9)."""
+    tc = h2_i2(1.93e8, 20620.0, 5.470705805110e-07, 0.0)
+    T, c0 = 700.0, 4.54
+    conc0 = np.array([c0, c0, 0.0])
+    rho = float(conc0 @ M)
+    oracle.set_chem_method(1)
+    try:
+        rc, y = oracle.chem_update(tc, 60000.0, rho, T, conc0 * M / rho, 200.0)
+    finally:
+        oracle.set_chem_method(0)
+    assert rc == 0
+    c_hi = y[2] * rho / M[2]
+    assert abs(c_hi - 7.14201983840) <= 1e-9 * 7.14201983840, c_hi
