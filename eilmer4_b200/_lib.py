@@ -22,7 +22,7 @@ E4C_ERR_CHEM = -7
 E4C_ERR_TIMEOUT = -8
 E4C_ERR_STATE = -9
 
-KCLASS = ("dt", "bc", "flux", "update", "stage", "other", "chem", "seed")
+KCLASS = ("dt", "bc", "flux", "update", "stage", "other", "chem", "seed", "chem_work")
 
 ERROR_NAMES = {
     E4C_ERR_ARG: "E4C_ERR_ARG", E4C_ERR_CUDA: "E4C_ERR_CUDA",

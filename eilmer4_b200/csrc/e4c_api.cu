@@ -177,7 +177,7 @@ void Ctx::enqueue_chemistry(const std::vector<int>& hs, const double* dt) {
                       [&] { seed_infer(b.v, dt, d_chem_work, d_chem_nwork); });
             guess = seed.d_guess;
         }
-        launch_as(*this, E4C_KCLASS_CHEM, 1, [&] {
+        launch_as(*this, E4C_KCLASS_CHEM_WORK, 1, [&] {
             launch_chem_work(b.v, d_sim, cfg.T_frozen, dt, nreac, d_chem_work, d_chem_nwork,
                              guess, d_chem_stats, stream);
         });

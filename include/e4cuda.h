@@ -368,7 +368,8 @@ long long e4c_kernel_launches(void);
 #define E4C_KCLASS_OTHER 5     /* bookkeeping kernels */
 #define E4C_KCLASS_CHEM 6      /* chemistry cell update */
 #define E4C_KCLASS_SEED 7      /* learned chemistry seed (inference) */
-#define E4C_NKCLASS 8
+#define E4C_KCLASS_CHEM_WORK 8 /* chemistry pass 2: the cells needing Newton work */
+#define E4C_NKCLASS 9
 
 /* Run nsteps time steps without graphs, timing each kernel class with CUDA
  * events on the library stream: ms[c] = total milliseconds of class c and
