@@ -61,13 +61,14 @@ BYTES_PER_CELL_UPDATE = {"fp64": 360.0, "fp32_flux": 280.0}
 # massf x5, T, p, u, a, dt_chem and rho*massf x5 (doubles)
 BYTES_PER_REACTING_CELL = 8.0 * (9 + 15)
 # DRAM bytes per launch of the fused stage kernel (dram__bytes_read.sum +
-# dram__bytes_write.sum, mean of the stage-1 and stage-2 launches) from the
-# ncu capture of the 128^3 block, scaled to 256^3 by the cell count (the
-# kernel's traffic grows with the cells it processes), keyed by (precision,
-# kernel class), for the autotuner's picks (FP64: 32x16 tile, 32-plane
-# k-chunks; FP32-flux: 16x16 tile, 16-plane k-chunks).  Algorithmic bytes per
-# launch at 256^3: 3020 MB (FP64), 2349 MB (FP32-flux).
-TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2158107648}
+# dram__bytes_write.sum, mean of the stage-1 and stage-2 launches) from ncu
+# captures, keyed by (precision, kernel class), for the autotuner's picks:
+# FP64 (32x16 tile, 32-plane k-chunks) captured on the 128^3 block and scaled
+# to 256^3 by the cell count (the kernel's traffic grows with the cells it
+# processes); FP32-flux (the 32x8 tile of the edge-warp kernel, 32-plane
+# k-chunks) captured on the 256^3 block itself.  Algorithmic bytes per launch
+# at 256^3: 3020 MB (FP64), 2349 MB (FP32-flux).
+TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2418098712}
 # FP64 arithmetic per cell-update of the fused stage kernel (both stages),
 # keyed by (precision, flux): DADD + DMUL + 2 x DFMA thread instructions per
 # cycle times cycles, from the ncu capture of the 128^3 block with the 32x16
