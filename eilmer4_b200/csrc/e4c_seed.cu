@@ -8,15 +8,15 @@
 // (Hendrycks & Gimpel 2016); output 6 values, the normalised transforms
 // asinh(dY_s / sY) (5 species) and asinh(dT / sT).  Weights are kept in FP32
 // (master copy for Adam) and run as BF16 on the tensor cores with FP32
-// accumulation.  Inference (the chemistry step and e4c_seed_predict) runs on
-// the 5th-generation tensor cores: tcgen05.mma with the accumulators in
-// tensor memory, 128 rows per CTA.  Training runs forward and backward in one
-// kernel per mini-batch of 64-row tiles on mma.sync m16n8k16, one warp per 16
-// rows, the activations of one layer passed to the next in registers (the
-// accumulator fragment of two adjacent 8-column tiles is exactly the A
-// fragment of one 16-column k-tile), with the weight gradients accumulated
-// over the tile by tensor-core products of the stored activations and output
-// gradients.
+// accumulation.  Inference (the chemistry step and e4c_seed_predict) and
+// training both run on the 5th-generation tensor cores: tcgen05.mma issued
+// by one thread, accumulators in tensor memory, operands in shared memory in
+// the canonical K-major layout, 128 rows per CTA.  Training does forward and
+// backward in one kernel per mini-batch (k_seed_train_tc): the pre-activations
+// stay in tensor memory for the backward pass, the data gradients are
+// products with the transposed weight copies, and the weight gradients
+// products of transposed copies of the output gradients and activations that
+// the threads write.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -70,81 +70,16 @@ constexpr int NBIAS = 200;                     // b1, b2, b3 (64 each), b4 (6) +
 constexpr int N_MU_IN = 0, N_SD_IN = 8, N_MU_OUT = 16, N_SD_OUT = 22, N_SY = 28, N_ST = 29;
 static_assert(E4C_SEED_NNORM == 30, "norm layout");
 
-constexpr int TILE = 64;                 // samples per CTA in training
-constexpr int SMEM_TRAIN = PACKED_N * 2 + NBIAS * 4 + (2 * 64 * S16 + 6 * 64 * S64) * 2;
-
 // ---------------------------------------------------------------------------
-// Fragment helpers (PTX ISA, mma.m16n8k16 with .bf16 inputs): g = lane/4,
-// t = lane%4; A (16x16, row) regs {A[g][2t..], A[g+8][2t..], A[g][2t+8..],
-// A[g+8][2t+8..]}; B (16x8, col) regs {B[2t..][g], B[2t+8..][g]};
-// C (16x8) {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
+// BF16 and GELU helpers
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&v);
 }
 
-__device__ __forceinline__ uint32_t pack_raw(uint16_t lo, uint16_t hi) {
-    return uint32_t(lo) | (uint32_t(hi) << 16);
-}
-
 __device__ __forceinline__ float bf16_to_f(uint16_t r) {
     return __uint_as_float(uint32_t(r) << 16);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
-                                         uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// B fragment of the weight matrix M stored [n][k] (row n contiguous in k).
-__device__ __forceinline__ void load_b(const uint16_t* M, int S, int n0, int k0, int lane,
-                                       uint32_t& b0, uint32_t& b1) {
-    const uint16_t* p = M + (n0 + (lane >> 2)) * S + k0 + 2 * (lane & 3);
-    b0 = *reinterpret_cast<const uint32_t*>(p);
-    b1 = *reinterpret_cast<const uint32_t*>(p + 8);
-}
-
-// acc[j] (16 x 8 tile j of 64 outputs) = A (16 x 16*KT) * M^T + bias.
-template <int KT>
-__device__ __forceinline__ void dense64(const uint32_t (&a)[KT][4], const uint16_t* M, int S,
-                                        const float* bias, float (&acc)[8][4], int lane) {
-    const int t = lane & 3;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const float bl = bias ? bias[8 * j + 2 * t] : 0.0f;
-        const float bh = bias ? bias[8 * j + 2 * t + 1] : 0.0f;
-        acc[j][0] = bl;
-        acc[j][1] = bh;
-        acc[j][2] = bl;
-        acc[j][3] = bh;
-#pragma unroll
-        for (int kk = 0; kk < KT; ++kk) {
-            uint32_t b0, b1;
-            load_b(M, S, 8 * j, 16 * kk, lane, b0, b1);
-            mma_bf16(acc[j], a[kk], b0, b1);
-        }
-    }
-}
-
-// Output layer: 8 columns (6 used), K = 64.
-__device__ __forceinline__ void dense_out(const uint32_t (&a)[4][4], const uint16_t* M,
-                                          const float* bias, float (&acc)[4], int lane) {
-    const int t = lane & 3;
-    acc[0] = bias[2 * t];
-    acc[1] = bias[2 * t + 1];
-    acc[2] = acc[0];
-    acc[3] = acc[1];
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-        uint32_t b0, b1;
-        load_b(M, S64, 0, 16 * kk, lane, b0, b1);
-        mma_bf16(acc, a[kk], b0, b1);
-    }
 }
 
 __device__ __forceinline__ float gelu_f(float x) {
@@ -158,70 +93,6 @@ __device__ __forceinline__ float gelu_grad_f(float x) {
     const float x2 = x * x;
     const float th = tanhf(c * (x + 0.044715f * x2 * x));
     return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * c * (1.0f + 3.0f * 0.044715f * x2);
-}
-
-// GELU in place (keeping the derivative when dg is given), then the BF16 A
-// fragments of the next layer.
-__device__ __forceinline__ void gelu_to_a(float (&z)[8][4], uint32_t (&a)[4][4],
-                                          float (*dg)[4]) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            if (dg) dg[j][e] = gelu_grad_f(z[j][e]);
-            z[j][e] = gelu_f(z[j][e]);
-        }
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-        a[kk][0] = pack_bf16(z[2 * kk][0], z[2 * kk][1]);
-        a[kk][1] = pack_bf16(z[2 * kk][2], z[2 * kk][3]);
-        a[kk][2] = pack_bf16(z[2 * kk + 1][0], z[2 * kk + 1][1]);
-        a[kk][3] = pack_bf16(z[2 * kk + 1][2], z[2 * kk + 1][3]);
-    }
-}
-
-// Backward through GELU: dZ = dH * GELU'(Z), as A fragments.
-__device__ __forceinline__ void times_to_a(const float (&dh)[8][4], const float (&dg)[8][4],
-                                           uint32_t (&a)[4][4]) {
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-        a[kk][0] = pack_bf16(dh[2 * kk][0] * dg[2 * kk][0], dh[2 * kk][1] * dg[2 * kk][1]);
-        a[kk][1] = pack_bf16(dh[2 * kk][2] * dg[2 * kk][2], dh[2 * kk][3] * dg[2 * kk][3]);
-        a[kk][2] = pack_bf16(dh[2 * kk + 1][0] * dg[2 * kk + 1][0],
-                             dh[2 * kk + 1][1] * dg[2 * kk + 1][1]);
-        a[kk][3] = pack_bf16(dh[2 * kk + 1][2] * dg[2 * kk + 1][2],
-                             dh[2 * kk + 1][3] * dg[2 * kk + 1][3]);
-    }
-}
-
-// Store a warp's 16 x 64 A fragments (BF16) as rows row0.. of a [.][S] array.
-__device__ __forceinline__ void store_a(uint16_t* H, int S, int row0, const uint32_t (&a)[4][4],
-                                        int lane) {
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-        uint32_t* r0 = reinterpret_cast<uint32_t*>(H + (row0 + g) * S + 16 * kk + 2 * t);
-        uint32_t* r8 = reinterpret_cast<uint32_t*>(H + (row0 + g + 8) * S + 16 * kk + 2 * t);
-        r0[0] = a[kk][0];
-        r8[0] = a[kk][1];
-        r0[4] = a[kk][2];
-        r8[4] = a[kk][3];
-    }
-}
-
-__device__ __forceinline__ void load_weights(uint16_t* sw, float* sb, const uint16_t* packed,
-                                             const float* params, int nelem) {
-    const uint4* src = reinterpret_cast<const uint4*>(packed);
-    uint4* dst = reinterpret_cast<uint4*>(sw);
-    for (int q = threadIdx.x; q < nelem / 8; q += blockDim.x) dst[q] = src[q];
-    for (int q = threadIdx.x; q < NBIAS; q += blockDim.x) {
-        float v = 0.0f;
-        if (q < 64) v = params[P_B1 + q];
-        else if (q < 128) v = params[P_B2 + q - 64];
-        else if (q < 192) v = params[P_B3 + q - 128];
-        else if (q < 198) v = params[P_B4 + q - 192];
-        sb[q] = v;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -255,169 +126,6 @@ __global__ void k_seed_pack(const float* __restrict__ w, uint16_t* __restrict__ 
         }
         __nv_bfloat16 b = __float2bfloat16_rn(v);
         packed[e] = *reinterpret_cast<uint16_t*>(&b);
-    }
-}
-
-// One mini-batch: rows idx[0..nbatch) of the normalised inputs X [.][8] and
-// targets Y [.][6].  Loss = sum over rows and outputs of (z - y)^2 * inv_count;
-// its gradient is added to grad (FP32, master layout) when backward is set.
-__global__ void __launch_bounds__(128) k_seed_train(const float* __restrict__ params,
-                                                    const uint16_t* __restrict__ packed,
-                                                    const float* __restrict__ X,
-                                                    const float* __restrict__ Y,
-                                                    const int* __restrict__ idx, int nbatch,
-                                                    float inv_count, int backward,
-                                                    float* __restrict__ grad,
-                                                    float* __restrict__ loss) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint16_t* sw = reinterpret_cast<uint16_t*>(smem);
-    float* sb = reinterpret_cast<float*>(smem + PACKED_N * 2);
-    uint16_t* sH0 = reinterpret_cast<uint16_t*>(smem + PACKED_N * 2 + NBIAS * 4);  // [64][24]
-    uint16_t* sH1 = sH0 + 64 * S16;   // [64][72]
-    uint16_t* sH2 = sH1 + 64 * S64;
-    uint16_t* sH3 = sH2 + 64 * S64;
-    uint16_t* sD1 = sH3 + 64 * S64;
-    uint16_t* sD2 = sD1 + 64 * S64;
-    uint16_t* sD3 = sD2 + 64 * S64;
-    uint16_t* sD4 = sD3 + 64 * S64;   // [64][24]
-    load_weights(sw, sb, packed, params, PACKED_N);
-    __syncthreads();
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int row0 = warp * 16;
-    const int ra = blockIdx.x * TILE + row0 + g, rb = ra + 8;
-    const bool va = ra < nbatch, vb = rb < nbatch;
-    const int sa = va ? idx[ra] : 0, sbi = vb ? idx[rb] : 0;
-
-    uint32_t a0[1][4];
-    a0[0][0] = pack_bf16(va ? X[sa * 8 + 2 * t] : 0.0f, va ? X[sa * 8 + 2 * t + 1] : 0.0f);
-    a0[0][1] = pack_bf16(vb ? X[sbi * 8 + 2 * t] : 0.0f, vb ? X[sbi * 8 + 2 * t + 1] : 0.0f);
-    a0[0][2] = 0u;
-    a0[0][3] = 0u;
-    *reinterpret_cast<uint32_t*>(sH0 + (row0 + g) * S16 + 2 * t) = a0[0][0];
-    *reinterpret_cast<uint32_t*>(sH0 + (row0 + g + 8) * S16 + 2 * t) = a0[0][1];
-
-    float acc[8][4];
-    float dg1[8][4], dg2[8][4], dg3[8][4];
-    uint32_t a[4][4];
-    dense64<1>(a0, sw + OFF_W1, S16, sb, acc, lane);
-    gelu_to_a(acc, a, dg1);
-    store_a(sH1, S64, row0, a, lane);
-    dense64<4>(a, sw + OFF_W2, S64, sb + 64, acc, lane);
-    gelu_to_a(acc, a, dg2);
-    store_a(sH2, S64, row0, a, lane);
-    dense64<4>(a, sw + OFF_W3, S64, sb + 128, acc, lane);
-    gelu_to_a(acc, a, dg3);
-    store_a(sH3, S64, row0, a, lane);
-    float z4[4];
-    dense_out(a, sw + OFF_W4, sb + 192, z4, lane);
-
-    // squared error on the 6 outputs and its derivative
-    float d4[4];
-    float lsum = 0.0f;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        const int col = 2 * t + (e & 1);
-        const bool row_ok = (e < 2) ? va : vb;
-        const int s = (e < 2) ? sa : sbi;
-        if (row_ok && col < 6) {
-            const float diff = z4[e] - Y[s * 6 + col];
-            lsum += diff * diff;
-            d4[e] = 2.0f * diff * inv_count;
-        } else {
-            d4[e] = 0.0f;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-    if (lane == 0) atomicAdd(loss, lsum * inv_count);
-    if (!backward) return;
-
-    uint32_t ad4[1][4];
-    ad4[0][0] = pack_bf16(d4[0], d4[1]);
-    ad4[0][1] = pack_bf16(d4[2], d4[3]);
-    ad4[0][2] = 0u;
-    ad4[0][3] = 0u;
-    {
-        uint32_t* r0 = reinterpret_cast<uint32_t*>(sD4 + (row0 + g) * S16 + 2 * t);
-        uint32_t* r8 = reinterpret_cast<uint32_t*>(sD4 + (row0 + g + 8) * S16 + 2 * t);
-        r0[0] = ad4[0][0];
-        r8[0] = ad4[0][1];
-        r0[4] = 0u;
-        r8[4] = 0u;
-    }
-    // dH3 = dZ4 W4, dZ3 = dH3 GELU'(Z3), ... down to dZ1
-    dense64<1>(ad4, sw + OFF_W4T, S16, nullptr, acc, lane);
-    times_to_a(acc, dg3, a);
-    store_a(sD3, S64, row0, a, lane);
-    dense64<4>(a, sw + OFF_W3T, S64, nullptr, acc, lane);
-    times_to_a(acc, dg2, a);
-    store_a(sD2, S64, row0, a, lane);
-    dense64<4>(a, sw + OFF_W2T, S64, nullptr, acc, lane);
-    times_to_a(acc, dg1, a);
-    store_a(sD1, S64, row0, a, lane);
-    __syncthreads();
-
-    // weight gradients over the tile: dW[out][in] = sum_s dZ[s][out] H[s][in],
-    // as (out x samples) x (samples x in) products on the tensor cores
-    for (int tile = warp; tile < 76; tile += 4) {
-        const uint16_t *D, *H;
-        int SD, SH, m0, n0, ldg, mmax;
-        float* G;
-        if (tile < 4) {
-            D = sD1; SD = S64; H = sH0; SH = S16; m0 = 16 * tile; n0 = 0;
-            G = grad + P_W1; ldg = 8; mmax = 64;
-        } else if (tile < 36) {
-            const int q = tile - 4;
-            D = sD2; SD = S64; H = sH1; SH = S64; m0 = 16 * (q >> 3); n0 = 8 * (q & 7);
-            G = grad + P_W2; ldg = 64; mmax = 64;
-        } else if (tile < 68) {
-            const int q = tile - 36;
-            D = sD3; SD = S64; H = sH2; SH = S64; m0 = 16 * (q >> 3); n0 = 8 * (q & 7);
-            G = grad + P_W3; ldg = 64; mmax = 64;
-        } else {
-            const int q = tile - 68;
-            D = sD4; SD = S16; H = sH3; SH = S64; m0 = 0; n0 = 8 * q;
-            G = grad + P_W4; ldg = 64; mmax = 6;
-        }
-        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-            const int k0 = 16 * ks;
-            uint32_t af[4];
-            af[0] = pack_raw(D[(k0 + 2 * t) * SD + m0 + g], D[(k0 + 2 * t + 1) * SD + m0 + g]);
-            af[1] = pack_raw(D[(k0 + 2 * t) * SD + m0 + g + 8], D[(k0 + 2 * t + 1) * SD + m0 + g + 8]);
-            af[2] = pack_raw(D[(k0 + 2 * t + 8) * SD + m0 + g], D[(k0 + 2 * t + 9) * SD + m0 + g]);
-            af[3] = pack_raw(D[(k0 + 2 * t + 8) * SD + m0 + g + 8],
-                             D[(k0 + 2 * t + 9) * SD + m0 + g + 8]);
-            const uint32_t b0 =
-                pack_raw(H[(k0 + 2 * t) * SH + n0 + g], H[(k0 + 2 * t + 1) * SH + n0 + g]);
-            const uint32_t b1 =
-                pack_raw(H[(k0 + 2 * t + 8) * SH + n0 + g], H[(k0 + 2 * t + 9) * SH + n0 + g]);
-            mma_bf16(c, af, b0, b1);
-        }
-        if (m0 + g < mmax) {
-            atomicAdd(G + (m0 + g) * ldg + n0 + 2 * t, c[0]);
-            atomicAdd(G + (m0 + g) * ldg + n0 + 2 * t + 1, c[1]);
-        }
-        if (m0 + g + 8 < mmax) {
-            atomicAdd(G + (m0 + g + 8) * ldg + n0 + 2 * t, c[2]);
-            atomicAdd(G + (m0 + g + 8) * ldg + n0 + 2 * t + 1, c[3]);
-        }
-    }
-    // bias gradients: column sums of dZ
-    for (int q = threadIdx.x; q < 198; q += blockDim.x) {
-        const uint16_t* D;
-        int S, col;
-        float* G;
-        if (q < 64) { D = sD1; S = S64; col = q; G = grad + P_B1; }
-        else if (q < 128) { D = sD2; S = S64; col = q - 64; G = grad + P_B2; }
-        else if (q < 192) { D = sD3; S = S64; col = q - 128; G = grad + P_B3; }
-        else { D = sD4; S = S16; col = q - 192; G = grad + P_B4; }
-        float s = 0.0f;
-        for (int r = 0; r < TILE; ++r) s += bf16_to_f(D[r * S + col]);
-        atomicAdd(G + col, s);
     }
 }
 
@@ -769,6 +477,349 @@ __global__ void __launch_bounds__(128) k_seed_infer_tc(Src src, const float* __r
                      : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Training on the 5th-generation tensor cores: one CTA per 128-row tile of a
+// mini-batch, thread t the tile's row t, warp w the tensor-memory lanes
+// 32w..32w+31.  Every product is a tcgen05.mma (kind::f16, BF16 operands,
+// FP32 accumulators in tensor memory, M = 128) issued by one thread, with
+// operands in the canonical K-major layout without swizzle:
+//   forward   Z_l = H_{l-1} W_l^T          A = H_{l-1} [128][in], B = W_l [out][in]
+//   backward  dH_{l-1} = dZ_l W_l          A = dZ_l [128][out], B = W_l^T [in][out]
+//             dW_l = dZ_l^T H_{l-1}        A = dZ_l^T [out, padded to 128][128 rows],
+//                                          B = H_{l-1}^T [in][128 rows]
+// The pre-activations Z_1..Z_3 stay in tensor memory for the GELU
+// derivatives of the backward pass; the transposed copies dZ_l^T and
+// H_{l-1}^T are written by the threads (each its own row's column), so every
+// operand is K-major.  BF16 rounding falls where the oracle's mirror puts it:
+// inputs, weights, activations and back-propagated output gradients.  The
+// weight and bias gradients of the tile are added to grad with FP32 atomics.
+// ---------------------------------------------------------------------------
+constexpr int TT_W1 = 0;          // W1: 64 rows x 16, LBO 1024
+constexpr int TT_W2 = 2048;       // W2: 64 x 64, LBO 1024
+constexpr int TT_W3 = 10240;      // W3
+constexpr int TT_W4 = 18432;      // W4: 16 rows (6 used) x 64, LBO 256
+constexpr int TT_W4T = 20480;     // W4^T: 64 rows x 16 (6 used), LBO 1024
+constexpr int TT_W3T = 22528;     // W3^T: 64 x 64
+constexpr int TT_W2T = 30720;     // W2^T
+constexpr int TT_X0 = 38912;      // inputs: 128 rows x 16, LBO 2048
+constexpr int TT_H1 = 43008;      // activations: 128 x 64, LBO 2048
+constexpr int TT_H2 = 59392;
+constexpr int TT_H3 = 75776;
+constexpr int TT_D4 = 92160;      // dZ4: 128 x 16
+constexpr int TT_DZ = 96256;      // dZ3, then dZ2: 128 x 64
+constexpr int TT_DT = 112640;     // dZ_l^T: 128 rows (out, zero beyond) x 128, LBO 2048
+constexpr int TT_HT = 145408;     // H_{l-1}^T: 64 (or 16) rows x 128, LBO 1024 (256)
+constexpr int TT_BIAS = 161792;   // NBIAS floats
+constexpr int TT_MBAR = 162592;   // mbarrier (8 B)
+constexpr int TT_TSLOT = 162600;  // tensor-memory address written by tcgen05.alloc
+constexpr int TT_FLAG = 162604;   // MMA completion seen by thread 0
+constexpr int TT_SMEM = 162608 + 1024;
+constexpr uint32_t TT_COLS = 512;
+// tensor-memory columns: pre-activations, output, data and weight gradients
+constexpr uint32_t TM_Z1 = 0, TM_Z2 = 64, TM_Z3 = 128, TM_Z4 = 192, TM_DH = 256, TM_DW = 384;
+
+// ksteps K = 16 products D (+)= A B^T of K-major operands with LBOs albo, blbo.
+__device__ __forceinline__ void umma_k(uint32_t tmem_d, uint32_t a, uint32_t albo, uint32_t b,
+                                       uint32_t blbo, int ksteps, uint32_t n) {
+    for (int k = 0; k < ksteps; ++k)
+        umma_bf16(tmem_d, umma_desc(a + 2 * k * albo, albo, 128),
+                  umma_desc(b + 2 * k * blbo, blbo, 128), umma_idesc(n), k > 0 ? 1u : 0u);
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    return static_cast<uint16_t>(pack_bf16(x, 0.0f) & 0xFFFFu);
+}
+
+__global__ void __launch_bounds__(128, 1) k_seed_train_tc(const float* __restrict__ params,
+                                                          const uint16_t* __restrict__ packed,
+                                                          const float* __restrict__ X,
+                                                          const float* __restrict__ Y,
+                                                          const int* __restrict__ idx, int nbatch,
+                                                          float inv_count, int backward,
+                                                          float* __restrict__ grad,
+                                                          float* __restrict__ loss,
+                                                          int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+    unsigned char* sm = smem_raw + pad;
+    const uint32_t sb = raw + pad;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row = blockIdx.x * 128 + tid;
+    const bool valid = row < nbatch;
+    const int src = valid ? idx[row] : 0;
+
+    // weights (forward and transposed copies) into the canonical layouts
+    const uint4* pk = reinterpret_cast<const uint4*>(packed);
+    const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+    {
+        const int r = tid >> 1, c = tid & 1;   // 64 rows x 2 chunks
+        *reinterpret_cast<uint4*>(sm + TT_W1 + tc_row_chunk(r, c, 8)) = pk[(OFF_W1 + r * S16 + 8 * c) / 8];
+        *reinterpret_cast<uint4*>(sm + TT_W4T + tc_row_chunk(r, c, 8)) = pk[(OFF_W4T + r * S16 + 8 * c) / 8];
+    }
+    for (int e = tid; e < 512; e += 128) {   // 64 rows x 8 chunks
+        const int r = e >> 3, c = e & 7;
+        *reinterpret_cast<uint4*>(sm + TT_W2 + tc_row_chunk(r, c, 8)) = pk[(OFF_W2 + r * S64 + 8 * c) / 8];
+        *reinterpret_cast<uint4*>(sm + TT_W3 + tc_row_chunk(r, c, 8)) = pk[(OFF_W3 + r * S64 + 8 * c) / 8];
+        *reinterpret_cast<uint4*>(sm + TT_W2T + tc_row_chunk(r, c, 8)) = pk[(OFF_W2T + r * S64 + 8 * c) / 8];
+        *reinterpret_cast<uint4*>(sm + TT_W3T + tc_row_chunk(r, c, 8)) = pk[(OFF_W3T + r * S64 + 8 * c) / 8];
+    }
+    {
+        const int r = tid >> 3, c = tid & 7;   // W4: 16 rows (8.. zero) x 8 chunks
+        *reinterpret_cast<uint4*>(sm + TT_W4 + tc_row_chunk(r, c, 2)) =
+            r < 8 ? pk[(OFF_W4 + r * S64 + 8 * c) / 8] : zero4;
+    }
+    float* bias = reinterpret_cast<float*>(sm + TT_BIAS);
+    for (int q = tid; q < NBIAS; q += 128) {
+        float v = 0.0f;
+        if (q < 64) v = params[P_B1 + q];
+        else if (q < 128) v = params[P_B2 + q - 64];
+        else if (q < 192) v = params[P_B3 + q - 128];
+        else if (q < 198) v = params[P_B4 + q - 192];
+        bias[q] = v;
+    }
+    // dZ^T rows beyond a layer's outputs stay zero (M padded to 128)
+    for (int e = tid; e < (TT_HT - TT_DT) / 16; e += 128)
+        reinterpret_cast<uint4*>(sm + TT_DT)[e] = zero4;
+    // this row's inputs
+    float x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = valid ? X[src * 8 + i] : 0.0f;
+    {
+        uint4 v;
+        v.x = pack_bf16(x[0], x[1]); v.y = pack_bf16(x[2], x[3]);
+        v.z = pack_bf16(x[4], x[5]); v.w = pack_bf16(x[6], x[7]);
+        *reinterpret_cast<uint4*>(sm + TT_X0 + tc_row_chunk(tid, 0, 16)) = v;
+        *reinterpret_cast<uint4*>(sm + TT_X0 + tc_row_chunk(tid, 1, 16)) = zero4;
+    }
+    const uint32_t mbar = sb + TT_MBAR;
+    volatile uint32_t* flag = reinterpret_cast<volatile uint32_t*>(sm + TT_FLAG);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(sb + TT_TSLOT), "r"(TT_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + TT_TSLOT);
+    const uint32_t tw = tmem + (uint32_t(32 * warp) << 16);
+    uint32_t phase = 0;
+    bool failed = false;
+
+    // The operands written by the threads are visible to the tensor cores
+    // (proxy fence, barrier); thread 0 issues the products and waits (bounded)
+    // for their completion; every thread learns the outcome.
+    auto sync_mma = [&](auto issue) -> bool {
+        proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            issue();
+            umma_commit(mbar);
+            *flag = mbar_wait(mbar, phase) ? 1u : 0u;
+        }
+        __syncthreads();
+        if (*flag == 0u) return false;
+        phase ^= 1u;
+        tc_fence_after();
+        return true;
+    };
+    // a hidden layer's activations from its pre-activation: GELU(Z + b) as
+    // this row of the next layer's A operand
+    auto activate = [&](uint32_t zcol, int boff, int dst) {
+        uint32_t r[64];
+        tmem_ld64(tw + zcol, r);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float h[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) h[e] = gelu_f(__uint_as_float(r[8 * c + e]) + bias[boff + 8 * c + e]);
+            uint4 v;
+            v.x = pack_bf16(h[0], h[1]); v.y = pack_bf16(h[2], h[3]);
+            v.z = pack_bf16(h[4], h[5]); v.w = pack_bf16(h[6], h[7]);
+            *reinterpret_cast<uint4*>(sm + dst + tc_row_chunk(tid, c, 16)) = v;
+        }
+    };
+    // this row's column of H^T (64 rows) from its row of H
+    auto transpose_h = [&](int srcH) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const uint4 v = *reinterpret_cast<const uint4*>(sm + srcH + tc_row_chunk(tid, c, 16));
+            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const uint16_t b = static_cast<uint16_t>((w4[e >> 1] >> (16 * (e & 1))) & 0xFFFFu);
+                *reinterpret_cast<uint16_t*>(sm + TT_HT + tc_row_chunk(8 * c + e, tid >> 3, 8) +
+                                             (tid & 7) * 2) = b;
+            }
+        }
+    };
+    // dZ = dH GELU'(Z + b) for this row: its row of the A operand (when dst
+    // >= 0) and its column of dZ^T
+    auto back_gelu = [&](uint32_t zcol, int boff, int dst) {
+        uint32_t rd[64], rz[64];
+        tmem_ld64(tw + TM_DH, rd);
+        tmem_ld64(tw + zcol, rz);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            uint16_t d[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int o = 8 * c + e;
+                const float z = __uint_as_float(rz[o]) + bias[boff + o];
+                d[e] = bf16_bits(__uint_as_float(rd[o]) * gelu_grad_f(z));
+                *reinterpret_cast<uint16_t*>(sm + TT_DT + tc_row_chunk(o, tid >> 3, 16) +
+                                             (tid & 7) * 2) = d[e];
+            }
+            if (dst >= 0) {
+                uint4 v;
+                v.x = uint32_t(d[0]) | (uint32_t(d[1]) << 16);
+                v.y = uint32_t(d[2]) | (uint32_t(d[3]) << 16);
+                v.z = uint32_t(d[4]) | (uint32_t(d[5]) << 16);
+                v.w = uint32_t(d[6]) | (uint32_t(d[7]) << 16);
+                *reinterpret_cast<uint4*>(sm + dst + tc_row_chunk(tid, c, 16)) = v;
+            }
+        }
+    };
+    // the tile's weight gradients of `rows` outputs x n inputs (warps holding
+    // those lanes) and bias gradients (column sums of dZ over the tile's rows,
+    // from dZ^T), added to grad
+    auto add_grads = [&](int rows, int n, float* gW, float* gB) {
+        if (32 * warp < rows) {
+            const int o = 32 * warp + lane;
+            if (n == 64) {
+                uint32_t r[64];
+                tmem_ld64(tw + TM_DW, r);
+                if (o < rows)
+                    for (int i = 0; i < 64; ++i) atomicAdd(gW + o * 64 + i, __uint_as_float(r[i]));
+            } else {
+                uint32_t r[16];
+                tmem_ld16(tw + TM_DW, r);
+                if (o < rows)
+                    for (int i = 0; i < 8; ++i) atomicAdd(gW + o * 8 + i, __uint_as_float(r[i]));
+            }
+        }
+        if (tid < rows) {
+            float s = 0.0f;
+            for (int c = 0; c < 16; ++c)
+                for (int e = 0; e < 8; ++e)
+                    s += bf16_to_f(*reinterpret_cast<const uint16_t*>(
+                        sm + TT_DT + tc_row_chunk(tid, c, 16) + e * 2));
+            atomicAdd(gB + tid, s);
+        }
+    };
+
+    // ---- forward ---------------------------------------------------------------
+    failed = !sync_mma([&] { umma_k(tmem + TM_Z1, sb + TT_X0, 2048, sb + TT_W1, 1024, 1, 64); });
+    if (!failed) {
+        activate(TM_Z1, 0, TT_H1);
+        failed = !sync_mma([&] { umma_k(tmem + TM_Z2, sb + TT_H1, 2048, sb + TT_W2, 1024, 4, 64); });
+    }
+    if (!failed) {
+        activate(TM_Z2, 64, TT_H2);
+        failed = !sync_mma([&] { umma_k(tmem + TM_Z3, sb + TT_H2, 2048, sb + TT_W3, 1024, 4, 64); });
+    }
+    if (!failed) {
+        activate(TM_Z3, 128, TT_H3);
+        failed = !sync_mma([&] { umma_k(tmem + TM_Z4, sb + TT_H3, 2048, sb + TT_W4, 256, 4, 16); });
+    }
+    if (!failed) {
+        // squared error on the 6 outputs and its derivative
+        uint32_t r[16];
+        tmem_ld16(tw + TM_Z4, r);
+        float lsum = 0.0f;
+        uint16_t d[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int o = 0; o < 6; ++o) {
+            if (valid) {
+                const float diff = __uint_as_float(r[o]) + bias[192 + o] - Y[src * 6 + o];
+                lsum += diff * diff;
+                d[o] = bf16_bits(2.0f * diff * inv_count);
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
+        if (lane == 0) atomicAdd(loss, lsum * inv_count);
+        if (backward) {
+            // dZ4: this row of the A operand, and its column of dZ4^T (rows 0..5)
+            uint4 v;
+            v.x = uint32_t(d[0]) | (uint32_t(d[1]) << 16);
+            v.y = uint32_t(d[2]) | (uint32_t(d[3]) << 16);
+            v.z = uint32_t(d[4]) | (uint32_t(d[5]) << 16);
+            v.w = 0u;
+            *reinterpret_cast<uint4*>(sm + TT_D4 + tc_row_chunk(tid, 0, 16)) = v;
+            *reinterpret_cast<uint4*>(sm + TT_D4 + tc_row_chunk(tid, 1, 16)) = zero4;
+#pragma unroll
+            for (int o = 0; o < 6; ++o)
+                *reinterpret_cast<uint16_t*>(sm + TT_DT + tc_row_chunk(o, tid >> 3, 16) +
+                                             (tid & 7) * 2) = d[o];
+            transpose_h(TT_H3);
+        }
+    }
+    // ---- backward --------------------------------------------------------------
+    if (!failed && backward) {
+        failed = !sync_mma([&] {
+            umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 1024, 8, 64);   // dW4
+            umma_k(tmem + TM_DH, sb + TT_D4, 2048, sb + TT_W4T, 1024, 1, 64);  // dH3
+        });
+        if (!failed) {
+            add_grads(6, 64, grad + P_W4, grad + P_B4);
+            __syncthreads();   // dZ4^T read before dZ3^T overwrites it
+            back_gelu(TM_Z3, 128, TT_DZ);
+            transpose_h(TT_H2);
+            failed = !sync_mma([&] {
+                umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 1024, 8, 64);   // dW3
+                umma_k(tmem + TM_DH, sb + TT_DZ, 2048, sb + TT_W3T, 1024, 4, 64);  // dH2
+            });
+        }
+        if (!failed) {
+            add_grads(64, 64, grad + P_W3, grad + P_B3);
+            __syncthreads();
+            back_gelu(TM_Z2, 64, TT_DZ);
+            transpose_h(TT_H1);
+            failed = !sync_mma([&] {
+                umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 1024, 8, 64);   // dW2
+                umma_k(tmem + TM_DH, sb + TT_DZ, 2048, sb + TT_W2T, 1024, 4, 64);  // dH1
+            });
+        }
+        if (!failed) {
+            add_grads(64, 64, grad + P_W2, grad + P_B2);
+            __syncthreads();
+            back_gelu(TM_Z1, 0, -1);
+            // X0^T: 16 rows (8 features, 8 zero) x 128, LBO 256
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                *reinterpret_cast<uint16_t*>(sm + TT_HT + tc_row_chunk(i, tid >> 3, 2) +
+                                             (tid & 7) * 2) = i < 8 ? bf16_bits(x[i]) : 0;
+            failed = !sync_mma([&] {
+                umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 256, 8, 16);    // dW1
+            });
+        }
+        if (!failed) add_grads(64, 16, grad + P_W1, grad + P_B1);
+    }
+    if (failed) {
+        // the tensor cores did not signal completion: report, give the products
+        // a second bounded wait, then release the tensor memory
+        if (tid == 0) {
+            if (status) atomicCAS(status, 0, E4C_ERR_TIMEOUT);
+            (void)mbar_wait(mbar, phase);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TT_COLS)
+                     : "memory");
+}
+
 // Sums over the valid samples (first feature finite) of the features, the
 // transformed targets asinh(d / s) and their squares: acc[0..13] sums,
 // acc[14..27] sums of squares, acc[28] count.
@@ -1053,8 +1104,11 @@ int e4c_seed_train(int epochs, int batch, double lr, unsigned long long rng_seed
     E4C_CUDA(cudaMemsetAsync(s.d_grad, 0, 3 * P_N * sizeof(float), c.stream));
     rc = c.seed_pack();
     if (rc != E4C_OK) { cleanup(); return rc; }
-    E4C_CUDA(cudaFuncSetAttribute(k_seed_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  SMEM_TRAIN));
+    E4C_CUDA(cudaFuncSetAttribute(k_seed_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TT_SMEM));
+    // a time-out of the tensor cores is reported here (the word after the
+    // normalisation sums, cleared with them)
+    int* d_status = reinterpret_cast<int*>(d_acc + 30);
     std::vector<int> perm(ntrain), vidx(nval);
     std::iota(perm.begin(), perm.end(), 0);
     std::iota(vidx.begin(), vidx.end(), ntrain);
@@ -1074,9 +1128,9 @@ int e4c_seed_train(int epochs, int batch, double lr, unsigned long long rng_seed
             const double frac = double(step) / double(total);
             const float lr_t = float(lr * (0.01 + 0.99 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac))));
             ++step;
-            k_seed_train<<<(nb + TILE - 1) / TILE, 128, SMEM_TRAIN, c.stream>>>(
+            k_seed_train_tc<<<(nb + 127) / 128, 128, TT_SMEM, c.stream>>>(
                 s.d_params, s.d_packed, d_X, d_Y, d_idx + off, nb, 1.0f / float(nb * 6), 1,
-                s.d_grad, s.d_loss);
+                s.d_grad, s.d_loss, d_status);
             ++s.adam_t;
             const float bc1 = float(1.0 - std::pow(0.9, double(s.adam_t)));
             const float bc2 = float(1.0 - std::pow(0.999, double(s.adam_t)));
@@ -1095,14 +1149,19 @@ int e4c_seed_train(int epochs, int batch, double lr, unsigned long long rng_seed
     E4C_CUDA(cudaMemcpyAsync(d_idx, vidx.data(), size_t(nval) * sizeof(int),
                              cudaMemcpyHostToDevice, c.stream));
     E4C_CUDA(cudaMemsetAsync(s.d_loss, 0, sizeof(float), c.stream));
-    k_seed_train<<<(nval + TILE - 1) / TILE, 128, SMEM_TRAIN, c.stream>>>(
+    k_seed_train_tc<<<(nval + 127) / 128, 128, TT_SMEM, c.stream>>>(
         s.d_params, s.d_packed, d_X, d_Y, d_idx, nval, 1.0f / float(nval * 6), 0, s.d_grad,
-        s.d_loss);
+        s.d_loss, d_status);
     float vloss = 0.0f;
+    int status = 0;
     E4C_CUDA(cudaMemcpyAsync(&vloss, s.d_loss, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     E4C_CUDA(cudaStreamSynchronize(c.stream));
     E4C_CUDA(cudaGetLastError());
     cleanup();
+    if (status != 0)
+        return fail(status, "seed training: the tensor cores did not signal completion within "
+                            "the wait limit");
     s.have_weights = true;
     c.reset_graphs();
     const double secs =
@@ -1212,7 +1271,7 @@ int e4c_seed_loss_grad(const float* x, const float* y, int n, double* loss, floa
     if (!c.seed.have_weights) return fail(E4C_ERR_STATE, "no trained or installed network");
     if (!x || !y || n <= 0 || !loss || !grad) return fail(E4C_ERR_ARG, "bad arguments");
     const size_t bytes = size_t(n) * (8 + 6) * sizeof(float) + size_t(n) * sizeof(int) +
-                         P_N * sizeof(float) + 64;
+                         P_N * sizeof(float) + 64 + 16;
     char* d = static_cast<char*>(c.dalloc(bytes));
     if (!d) return fail(E4C_ERR_CUDA, "cudaMalloc failed");
     float* dX = reinterpret_cast<float*>(d);
@@ -1225,19 +1284,26 @@ int e4c_seed_loss_grad(const float* x, const float* y, int n, double* loss, floa
     E4C_CUDA(cudaMemcpyAsync(dX, x, size_t(n) * 8 * sizeof(float), cudaMemcpyHostToDevice, c.stream));
     E4C_CUDA(cudaMemcpyAsync(dY, y, size_t(n) * 6 * sizeof(float), cudaMemcpyHostToDevice, c.stream));
     E4C_CUDA(cudaMemcpyAsync(dI, idx.data(), size_t(n) * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    int* dS = reinterpret_cast<int*>(dI + n);   // time-out status
     E4C_CUDA(cudaMemsetAsync(dG, 0, (P_N + 4) * sizeof(float), c.stream));
-    E4C_CUDA(cudaFuncSetAttribute(k_seed_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  SMEM_TRAIN));
-    k_seed_train<<<(n + TILE - 1) / TILE, 128, SMEM_TRAIN, c.stream>>>(
-        c.seed.d_params, c.seed.d_packed, dX, dY, dI, n, 1.0f / float(n * 6), 1, dG, dL);
+    E4C_CUDA(cudaMemsetAsync(dS, 0, sizeof(int), c.stream));
+    E4C_CUDA(cudaFuncSetAttribute(k_seed_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TT_SMEM));
+    k_seed_train_tc<<<(n + 127) / 128, 128, TT_SMEM, c.stream>>>(
+        c.seed.d_params, c.seed.d_packed, dX, dY, dI, n, 1.0f / float(n * 6), 1, dG, dL, dS);
     c.launches += 1;
     E4C_CUDA(cudaGetLastError());
     float l = 0.0f;
+    int status = 0;
     E4C_CUDA(cudaMemcpyAsync(grad, dG, P_N * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
     E4C_CUDA(cudaMemcpyAsync(&l, dL, sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    E4C_CUDA(cudaMemcpyAsync(&status, dS, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     E4C_CUDA(cudaStreamSynchronize(c.stream));
     *loss = l;
     c.dfree(d);
+    if (status != 0)
+        return fail(status, "seed training: the tensor cores did not signal completion within "
+                            "the wait limit");
     return E4C_OK;
 }
 
