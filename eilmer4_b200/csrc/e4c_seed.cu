@@ -482,17 +482,24 @@ __global__ void __launch_bounds__(128) k_seed_infer_tc(Src src, const float* __r
 // mini-batch, thread t the tile's row t, warp w the tensor-memory lanes
 // 32w..32w+31.  Every product is a tcgen05.mma (kind::f16, BF16 operands,
 // FP32 accumulators in tensor memory, M = 128) issued by one thread, with
-// operands in the canonical K-major layout without swizzle:
-//   forward   Z_l = H_{l-1} W_l^T          A = H_{l-1} [128][in], B = W_l [out][in]
-//   backward  dH_{l-1} = dZ_l W_l          A = dZ_l [128][out], B = W_l^T [in][out]
-//             dW_l = dZ_l^T H_{l-1}        A = dZ_l^T [out, padded to 128][128 rows],
-//                                          B = H_{l-1}^T [in][128 rows]
-// The pre-activations Z_1..Z_3 stay in tensor memory for the GELU
-// derivatives of the backward pass; the transposed copies dZ_l^T and
-// H_{l-1}^T are written by the threads (each its own row's column), so every
-// operand is K-major.  BF16 rounding falls where the oracle's mirror puts it:
-// inputs, weights, activations and back-propagated output gradients.  The
-// weight and bias gradients of the tile are added to grad with FP32 atomics.
+// operands in canonical layouts without swizzle:
+//   forward   Z_l = H_{l-1} W_l^T    A = H_{l-1} [128][in] K-major, B = W_l [out][in] K-major
+//   backward  dH_{l-1} = dZ_l W_l    A = dZ_l [128][out] K-major, B = W_l^T [in][out] K-major
+//             dW_l = dZ_l^T H_{l-1}  A = dZ_l, B = H_{l-1}, both read MN-major (the
+//                                    tile's rows are the contraction)
+//             db_l = dZ_l^T 1        A = dZ_l MN-major, B = a 16 x 128 block of ones
+// A K-major operand stored as [rows][k] with 8-row groups SBO = 128 B apart
+// and 8-element k chunks LBO apart is, read MN-major, the transposed operand
+// with K groups LBO' = 128 B apart and MN groups SBO' = the old LBO apart,
+// so the backward pass needs no transposed copies.  M = 128 for the weight
+// gradients reads 128 output rows: rows past a layer's outputs come from the
+// arrays laid out after dZ (in this CTA's shared memory) and land in
+// tensor-memory lanes nobody reads.  The pre-activations Z_1..Z_3 stay in
+// tensor memory for the GELU derivatives.  BF16 rounding falls where the
+// oracle's mirror puts it: inputs, weights, activations and back-propagated
+// output gradients.  The tile's gradients are added to grad with FP32
+// atomics.  Loops are kept rolled (tensor-memory loads 16 columns at a time)
+// so the kernel's instructions stay in the instruction cache.
 // ---------------------------------------------------------------------------
 constexpr int TT_W1 = 0;          // W1: 64 rows x 16, LBO 1024
 constexpr int TT_W2 = 2048;       // W2: 64 x 64, LBO 1024
@@ -502,21 +509,27 @@ constexpr int TT_W4T = 20480;     // W4^T: 64 rows x 16 (6 used), LBO 1024
 constexpr int TT_W3T = 22528;     // W3^T: 64 x 64
 constexpr int TT_W2T = 30720;     // W2^T
 constexpr int TT_X0 = 38912;      // inputs: 128 rows x 16, LBO 2048
-constexpr int TT_H1 = 43008;      // activations: 128 x 64, LBO 2048
-constexpr int TT_H2 = 59392;
-constexpr int TT_H3 = 75776;
-constexpr int TT_D4 = 92160;      // dZ4: 128 x 16
-constexpr int TT_DZ = 96256;      // dZ3, then dZ2: 128 x 64
-constexpr int TT_DT = 112640;     // dZ_l^T: 128 rows (out, zero beyond) x 128, LBO 2048
-constexpr int TT_HT = 145408;     // H_{l-1}^T: 64 (or 16) rows x 128, LBO 1024 (256)
-constexpr int TT_BIAS = 161792;   // NBIAS floats
-constexpr int TT_MBAR = 162592;   // mbarrier (8 B)
-constexpr int TT_TSLOT = 162600;  // tensor-memory address written by tcgen05.alloc
-constexpr int TT_FLAG = 162604;   // MMA completion seen by thread 0
-constexpr int TT_SMEM = 162608 + 1024;
+constexpr int TT_D4 = 43008;      // dZ4: 128 x 16, LBO 2048
+constexpr int TT_DZ = 47104;      // dZ3, then dZ2, dZ1: 128 x 64, LBO 2048
+constexpr int TT_H1 = 63488;      // activations: 128 x 64, LBO 2048
+constexpr int TT_H2 = 79872;
+constexpr int TT_H3 = 96256;
+constexpr int TT_ONES = 112640;   // 16 x 128 BF16 ones (K-major, LBO 256)
+constexpr int TT_BIAS = 116736;   // NBIAS floats
+constexpr int TT_MBAR = 117536;   // mbarrier (8 B)
+constexpr int TT_TSLOT = 117544;  // tensor-memory address written by tcgen05.alloc
+constexpr int TT_FLAG = 117548;   // MMA completion seen by thread 0
+constexpr int TT_SMEM = 117552 + 1024;
+// An MN-major operand of M = 128 starting at dZ4 (dZ) spans 16 groups of
+// 2048 B, to 75776 (79872): inside the arrays above.
+static_assert(TT_D4 + 16 * 2048 <= TT_ONES && TT_DZ + 16 * 2048 <= TT_ONES, "MN-major span");
+static_assert(TT_BIAS + 4 * NBIAS <= TT_MBAR, "bias");
+static_assert(TT_H2 == TT_H1 + 16384 && TT_H3 == TT_H1 + 2 * 16384 && TT_W3 == TT_W2 + 8192 &&
+                  TT_W3T == TT_W2T - 8192, "layer strides");
 constexpr uint32_t TT_COLS = 512;
-// tensor-memory columns: pre-activations, output, data and weight gradients
-constexpr uint32_t TM_Z1 = 0, TM_Z2 = 64, TM_Z3 = 128, TM_Z4 = 192, TM_DH = 256, TM_DW = 384;
+// tensor-memory columns: pre-activations, output, data, weight and bias gradients
+constexpr uint32_t TM_Z1 = 0, TM_Z4 = 192, TM_DH = 256, TM_DW = 384, TM_DB = 448;
+constexpr uint32_t IDESC_A_MN = 1u << 15, IDESC_B_MN = 1u << 16;
 
 // ksteps K = 16 products D (+)= A B^T of K-major operands with LBOs albo, blbo.
 __device__ __forceinline__ void umma_k(uint32_t tmem_d, uint32_t a, uint32_t albo, uint32_t b,
@@ -557,6 +570,7 @@ __global__ void __launch_bounds__(128, 1) k_seed_train_tc(const float* __restric
         *reinterpret_cast<uint4*>(sm + TT_W1 + tc_row_chunk(r, c, 8)) = pk[(OFF_W1 + r * S16 + 8 * c) / 8];
         *reinterpret_cast<uint4*>(sm + TT_W4T + tc_row_chunk(r, c, 8)) = pk[(OFF_W4T + r * S16 + 8 * c) / 8];
     }
+#pragma unroll 1
     for (int e = tid; e < 512; e += 128) {   // 64 rows x 8 chunks
         const int r = e >> 3, c = e & 7;
         *reinterpret_cast<uint4*>(sm + TT_W2 + tc_row_chunk(r, c, 8)) = pk[(OFF_W2 + r * S64 + 8 * c) / 8];
@@ -569,7 +583,14 @@ __global__ void __launch_bounds__(128, 1) k_seed_train_tc(const float* __restric
         *reinterpret_cast<uint4*>(sm + TT_W4 + tc_row_chunk(r, c, 2)) =
             r < 8 ? pk[(OFF_W4 + r * S64 + 8 * c) / 8] : zero4;
     }
+    {
+        const uint32_t one2 = 0x3F803F80u;     // two BF16 ones
+        const uint4 ones = make_uint4(one2, one2, one2, one2);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) reinterpret_cast<uint4*>(sm + TT_ONES)[tid + 128 * q] = ones;
+    }
     float* bias = reinterpret_cast<float*>(sm + TT_BIAS);
+#pragma unroll 1
     for (int q = tid; q < NBIAS; q += 128) {
         float v = 0.0f;
         if (q < 64) v = params[P_B1 + q];
@@ -578,14 +599,11 @@ __global__ void __launch_bounds__(128, 1) k_seed_train_tc(const float* __restric
         else if (q < 198) v = params[P_B4 + q - 192];
         bias[q] = v;
     }
-    // dZ^T rows beyond a layer's outputs stay zero (M padded to 128)
-    for (int e = tid; e < (TT_HT - TT_DT) / 16; e += 128)
-        reinterpret_cast<uint4*>(sm + TT_DT)[e] = zero4;
     // this row's inputs
-    float x[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) x[i] = valid ? X[src * 8 + i] : 0.0f;
     {
+        float x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = valid ? X[src * 8 + i] : 0.0f;
         uint4 v;
         v.x = pack_bf16(x[0], x[1]); v.y = pack_bf16(x[2], x[3]);
         v.z = pack_bf16(x[4], x[5]); v.w = pack_bf16(x[6], x[7]);
@@ -631,107 +649,38 @@ __global__ void __launch_bounds__(128, 1) k_seed_train_tc(const float* __restric
         tc_fence_after();
         return true;
     };
-    // a hidden layer's activations from its pre-activation: GELU(Z + b) as
-    // this row of the next layer's A operand
-    auto activate = [&](uint32_t zcol, int boff, int dst) {
-        uint32_t r[64];
-        tmem_ld64(tw + zcol, r);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            float h[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) h[e] = gelu_f(__uint_as_float(r[8 * c + e]) + bias[boff + 8 * c + e]);
-            uint4 v;
-            v.x = pack_bf16(h[0], h[1]); v.y = pack_bf16(h[2], h[3]);
-            v.z = pack_bf16(h[4], h[5]); v.w = pack_bf16(h[6], h[7]);
-            *reinterpret_cast<uint4*>(sm + dst + tc_row_chunk(tid, c, 16)) = v;
-        }
-    };
-    // this row's column of H^T (64 rows) from its row of H
-    auto transpose_h = [&](int srcH) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const uint4 v = *reinterpret_cast<const uint4*>(sm + srcH + tc_row_chunk(tid, c, 16));
-            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const uint16_t b = static_cast<uint16_t>((w4[e >> 1] >> (16 * (e & 1))) & 0xFFFFu);
-                *reinterpret_cast<uint16_t*>(sm + TT_HT + tc_row_chunk(8 * c + e, tid >> 3, 8) +
-                                             (tid & 7) * 2) = b;
-            }
-        }
-    };
-    // dZ = dH GELU'(Z + b) for this row: its row of the A operand (when dst
-    // >= 0) and its column of dZ^T
-    auto back_gelu = [&](uint32_t zcol, int boff, int dst) {
-        uint32_t rd[64], rz[64];
-        tmem_ld64(tw + TM_DH, rd);
-        tmem_ld64(tw + zcol, rz);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            uint16_t d[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int o = 8 * c + e;
-                const float z = __uint_as_float(rz[o]) + bias[boff + o];
-                d[e] = bf16_bits(__uint_as_float(rd[o]) * gelu_grad_f(z));
-                *reinterpret_cast<uint16_t*>(sm + TT_DT + tc_row_chunk(o, tid >> 3, 16) +
-                                             (tid & 7) * 2) = d[e];
-            }
-            if (dst >= 0) {
-                uint4 v;
-                v.x = uint32_t(d[0]) | (uint32_t(d[1]) << 16);
-                v.y = uint32_t(d[2]) | (uint32_t(d[3]) << 16);
-                v.z = uint32_t(d[4]) | (uint32_t(d[5]) << 16);
-                v.w = uint32_t(d[6]) | (uint32_t(d[7]) << 16);
-                *reinterpret_cast<uint4*>(sm + dst + tc_row_chunk(tid, c, 16)) = v;
-            }
-        }
-    };
-    // the tile's weight gradients of `rows` outputs x n inputs (warps holding
-    // those lanes) and bias gradients (column sums of dZ over the tile's rows,
-    // from dZ^T), added to grad
-    auto add_grads = [&](int rows, int n, float* gW, float* gB) {
-        if (32 * warp < rows) {
-            const int o = 32 * warp + lane;
-            if (n == 64) {
-                uint32_t r[64];
-                tmem_ld64(tw + TM_DW, r);
-                if (o < rows)
-                    for (int i = 0; i < 64; ++i) atomicAdd(gW + o * 64 + i, __uint_as_float(r[i]));
-            } else {
-                uint32_t r[16];
-                tmem_ld16(tw + TM_DW, r);
-                if (o < rows)
-                    for (int i = 0; i < 8; ++i) atomicAdd(gW + o * 8 + i, __uint_as_float(r[i]));
-            }
-        }
-        if (tid < rows) {
-            float s = 0.0f;
-            for (int c = 0; c < 16; ++c)
-                for (int e = 0; e < 8; ++e)
-                    s += bf16_to_f(*reinterpret_cast<const uint16_t*>(
-                        sm + TT_DT + tc_row_chunk(tid, c, 16) + e * 2));
-            atomicAdd(gB + tid, s);
-        }
-    };
 
-    // ---- forward ---------------------------------------------------------------
-    failed = !sync_mma([&] { umma_k(tmem + TM_Z1, sb + TT_X0, 2048, sb + TT_W1, 1024, 1, 64); });
-    if (!failed) {
-        activate(TM_Z1, 0, TT_H1);
-        failed = !sync_mma([&] { umma_k(tmem + TM_Z2, sb + TT_H1, 2048, sb + TT_W2, 1024, 4, 64); });
+    // ---- forward: Z_l in tensor memory, H_l = GELU(Z_l + b_l) as the next A
+#pragma unroll 1
+    for (int l = 0; l < 4 && !failed; ++l) {
+        const uint32_t a = l == 0 ? TT_X0 : TT_H1 + (l - 1) * 16384;
+        const uint32_t b = l == 0 ? TT_W1 : l == 3 ? TT_W4 : TT_W2 + (l - 1) * 8192;
+        const uint32_t zc = TM_Z1 + 64 * l;
+        failed = !sync_mma([&] {
+            umma_k(tmem + zc, sb + a, 2048, sb + b, l == 3 ? 256 : 1024, l == 0 ? 1 : 4,
+                   l == 3 ? 16 : 64);
+        });
+        if (failed || l == 3) break;
+        const int dst = TT_H1 + l * 16384;
+#pragma unroll 1
+        for (int c = 0; c < 8; c += 2) {
+            uint32_t r[16];
+            tmem_ld16(tw + zc + 8 * c, r);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float g[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    g[e] = gelu_f(__uint_as_float(r[8 * h + e]) + bias[64 * l + 8 * (c + h) + e]);
+                uint4 v;
+                v.x = pack_bf16(g[0], g[1]); v.y = pack_bf16(g[2], g[3]);
+                v.z = pack_bf16(g[4], g[5]); v.w = pack_bf16(g[6], g[7]);
+                *reinterpret_cast<uint4*>(sm + dst + tc_row_chunk(tid, c + h, 16)) = v;
+            }
+        }
     }
     if (!failed) {
-        activate(TM_Z2, 64, TT_H2);
-        failed = !sync_mma([&] { umma_k(tmem + TM_Z3, sb + TT_H2, 2048, sb + TT_W3, 1024, 4, 64); });
-    }
-    if (!failed) {
-        activate(TM_Z3, 128, TT_H3);
-        failed = !sync_mma([&] { umma_k(tmem + TM_Z4, sb + TT_H3, 2048, sb + TT_W4, 256, 4, 16); });
-    }
-    if (!failed) {
-        // squared error on the 6 outputs and its derivative
+        // squared error on the 6 outputs and its derivative, dZ4 as this row of A
         uint32_t r[16];
         tmem_ld16(tw + TM_Z4, r);
         float lsum = 0.0f;
@@ -747,62 +696,74 @@ __global__ void __launch_bounds__(128, 1) k_seed_train_tc(const float* __restric
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
         if (lane == 0) atomicAdd(loss, lsum * inv_count);
-        if (backward) {
-            // dZ4: this row of the A operand, and its column of dZ4^T (rows 0..5)
-            uint4 v;
-            v.x = uint32_t(d[0]) | (uint32_t(d[1]) << 16);
-            v.y = uint32_t(d[2]) | (uint32_t(d[3]) << 16);
-            v.z = uint32_t(d[4]) | (uint32_t(d[5]) << 16);
-            v.w = 0u;
-            *reinterpret_cast<uint4*>(sm + TT_D4 + tc_row_chunk(tid, 0, 16)) = v;
-            *reinterpret_cast<uint4*>(sm + TT_D4 + tc_row_chunk(tid, 1, 16)) = zero4;
-#pragma unroll
-            for (int o = 0; o < 6; ++o)
-                *reinterpret_cast<uint16_t*>(sm + TT_DT + tc_row_chunk(o, tid >> 3, 16) +
-                                             (tid & 7) * 2) = d[o];
-            transpose_h(TT_H3);
-        }
+        uint4 v;
+        v.x = uint32_t(d[0]) | (uint32_t(d[1]) << 16);
+        v.y = uint32_t(d[2]) | (uint32_t(d[3]) << 16);
+        v.z = uint32_t(d[4]) | (uint32_t(d[5]) << 16);
+        v.w = 0u;
+        *reinterpret_cast<uint4*>(sm + TT_D4 + tc_row_chunk(tid, 0, 16)) = v;
+        *reinterpret_cast<uint4*>(sm + TT_D4 + tc_row_chunk(tid, 1, 16)) = zero4;
     }
-    // ---- backward --------------------------------------------------------------
-    if (!failed && backward) {
+    // ---- backward: layer l's weight and bias gradients, then dH_{l-1}
+#pragma unroll 1
+    for (int l = 3; l >= 0 && !failed && backward; --l) {
+        const uint32_t dz = l == 3 ? TT_D4 : TT_DZ;
+        const uint32_t hp = l == 0 ? TT_X0 : TT_H1 + (l - 1) * 16384;
+        const uint32_t nin = l == 0 ? 16 : 64;
         failed = !sync_mma([&] {
-            umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 1024, 8, 64);   // dW4
-            umma_k(tmem + TM_DH, sb + TT_D4, 2048, sb + TT_W4T, 1024, 1, 64);  // dH3
+            for (int k = 0; k < 8; ++k) {   // K = the tile's 128 rows
+                const uint64_t ad = umma_desc(sb + dz + 256 * k, 128, 2048);
+                umma_bf16(tmem + TM_DW, ad, umma_desc(sb + hp + 256 * k, 128, 2048),
+                          umma_idesc(nin) | IDESC_A_MN | IDESC_B_MN, k > 0 ? 1u : 0u);
+                umma_bf16(tmem + TM_DB, ad, umma_desc(sb + TT_ONES + 512 * k, 256, 128),
+                          umma_idesc(16) | IDESC_A_MN, k > 0 ? 1u : 0u);
+            }
+            if (l > 0)
+                umma_k(tmem + TM_DH, sb + dz, 2048,
+                       sb + (l == 3 ? TT_W4T : TT_W2T - (l - 1) * 8192), 1024, l == 3 ? 1 : 4, 64);
         });
-        if (!failed) {
-            add_grads(6, 64, grad + P_W4, grad + P_B4);
-            __syncthreads();   // dZ4^T read before dZ3^T overwrites it
-            back_gelu(TM_Z3, 128, TT_DZ);
-            transpose_h(TT_H2);
-            failed = !sync_mma([&] {
-                umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 1024, 8, 64);   // dW3
-                umma_k(tmem + TM_DH, sb + TT_DZ, 2048, sb + TT_W3T, 1024, 4, 64);  // dH2
-            });
-        }
-        if (!failed) {
-            add_grads(64, 64, grad + P_W3, grad + P_B3);
-            __syncthreads();
-            back_gelu(TM_Z2, 64, TT_DZ);
-            transpose_h(TT_H1);
-            failed = !sync_mma([&] {
-                umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 1024, 8, 64);   // dW2
-                umma_k(tmem + TM_DH, sb + TT_DZ, 2048, sb + TT_W2T, 1024, 4, 64);  // dH1
-            });
-        }
-        if (!failed) {
-            add_grads(64, 64, grad + P_W2, grad + P_B2);
-            __syncthreads();
-            back_gelu(TM_Z1, 0, -1);
-            // X0^T: 16 rows (8 features, 8 zero) x 128, LBO 256
+        if (failed) break;
+        const int nout = l == 3 ? 6 : 64;
+        if (32 * warp < nout) {
+            const int o = 32 * warp + lane;
+            float* gW = grad + (l == 0 ? P_W1 : l == 1 ? P_W2 : l == 2 ? P_W3 : P_W4);
+            float* gB = grad + (l == 0 ? P_B1 : l == 1 ? P_B2 : l == 2 ? P_B3 : P_B4);
+            const int nw = l == 0 ? 8 : 64;
+            uint32_t r[16];
+            tmem_ld16(tw + TM_DB, r);
+            if (o < nout) atomicAdd(gB + o, __uint_as_float(r[0]));
+#pragma unroll 1
+            for (int c = 0; c < nw; c += 16) {
+                tmem_ld16(tw + TM_DW + c, r);
+                if (o < nout) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-                *reinterpret_cast<uint16_t*>(sm + TT_HT + tc_row_chunk(i, tid >> 3, 2) +
-                                             (tid & 7) * 2) = i < 8 ? bf16_bits(x[i]) : 0;
-            failed = !sync_mma([&] {
-                umma_k(tmem + TM_DW, sb + TT_DT, 2048, sb + TT_HT, 256, 8, 16);    // dW1
-            });
+                    for (int i = 0; i < 16; ++i)
+                        if (c + i < nw) atomicAdd(gW + o * nw + c + i, __uint_as_float(r[i]));
+                }
+            }
         }
-        if (!failed) add_grads(64, 16, grad + P_W1, grad + P_B1);
+        if (l == 0) break;
+        // dZ_{l-1} = dH_{l-1} GELU'(Z_{l-1} + b): this row of the next A
+        const uint32_t zc = TM_Z1 + 64 * (l - 1);
+#pragma unroll 1
+        for (int c = 0; c < 8; c += 2) {
+            uint32_t rd[16], rz[16];
+            tmem_ld16(tw + TM_DH + 8 * c, rd);
+            tmem_ld16(tw + zc + 8 * c, rz);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float g[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const float z = __uint_as_float(rz[8 * h + e]) + bias[64 * (l - 1) + 8 * (c + h) + e];
+                    g[e] = __uint_as_float(rd[8 * h + e]) * gelu_grad_f(z);
+                }
+                uint4 v;
+                v.x = pack_bf16(g[0], g[1]); v.y = pack_bf16(g[2], g[3]);
+                v.z = pack_bf16(g[4], g[5]); v.w = pack_bf16(g[6], g[7]);
+                *reinterpret_cast<uint4*>(sm + TT_DZ + tc_row_chunk(tid, c + h, 16)) = v;
+            }
+        }
     }
     if (failed) {
         // the tensor cores did not signal completion: report, give the products
