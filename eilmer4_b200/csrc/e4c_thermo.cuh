@@ -167,63 +167,99 @@ static __device__ E4C_COEF_FN void cea_coefficients(const e4c_thermochem& tc, in
     for (int j = 0; j < 9; ++j) a[j] = CUDART_NAN;
 }
 
+// a / b rounded to nearest, from y = RN(1/b) computed once for the divisor.
+// q = RN(a y) lies within 1.5 ulp of a/b; one correction with the FMA
+// residual makes it faithful, and the second is RN(a/b) by Markstein's
+// theorem (P. W. Markstein, IBM J. Res. Develop. 34(1), 1990: with y within
+// half an ulp of 1/b and q within one ulp of a/b, r = a - q b is exact and
+// RN(q + r y) = RN(a/b)).  For b positive, finite and normal with a/b normal
+// (the CEA curve terms); a zero keeps the sign of the quotient.  The curve
+// evaluations divide by T, T^2, 3 and 5 only, so each temperature pays for two
+// true divisions instead of about thirty.
+__device__ __forceinline__ double div_rn(double a, double b, double y) {
+    double q = a * y;
+    double r = fma(-q, b, a);
+    q = fma(r, y, q);
+    r = fma(-q, b, a);
+    q = fma(r, y, q);
+    return a == 0.0 ? a * y : q;
+}
+
+// A temperature with T^2 and the reciprocals of both, rounded to nearest.
+struct TRecip {
+    double T, T2, rT, rT2;
+    __device__ explicit TRecip(double t) : T(t), T2(t * t), rT(1.0 / t), rT2(1.0 / (t * t)) {}
+};
+
+constexpr double kThird = 1.0 / 3.0, kFifth = 1.0 / 5.0;
+
+// Cp/R and h/RT of one coefficient set at t (the operations of the
+// reference's curves, cea_thermo_curves.d; each quotient as div_rn gives it)
+__device__ __forceinline__ double cea_Cp_on_R(const double a[9], const TRecip& t) {
+    const double T = t.T;
+    double Cp_on_R = div_rn(a[0], t.T2, t.rT2) + div_rn(a[1], T, t.rT) + a[2] + a[3] * T;
+    Cp_on_R += a[4] * T * T + a[5] * T * T * T + a[6] * T * T * T * T;
+    return Cp_on_R;
+}
+__device__ __forceinline__ double cea_h_on_RT(const double a[9], const TRecip& t, double lT) {
+    const double T = t.T;
+    double h_on_RT = div_rn(-a[0], t.T2, t.rT2) + div_rn(a[1], T, t.rT) * lT + a[2] + a[3] * T / 2.0;
+    h_on_RT += div_rn(a[4] * T * T, 3.0, kThird) + a[5] * T * T * T / 4.0 +
+               div_rn(a[6] * T * T * T * T, 5.0, kFifth) + div_rn(a[7], T, t.rT);
+    return h_on_RT;
+}
+
 static __device__ E4C_CEA_FN double cea_Cp(const e4c_thermochem& tc, int isp, double R, double T) {
     const int nseg = tc.nseg[isp];
     if (T < tc.T_break[isp][0]) T = tc.T_break[isp][0];
     if (T > tc.T_break[isp][nseg]) T = tc.T_break[isp][nseg];
     double a[9];
     cea_coefficients(tc, isp, T, a);
-    double Cp_on_R = a[0] / (T * T) + a[1] / T + a[2] + a[3] * T;
-    Cp_on_R += a[4] * T * T + a[5] * T * T * T + a[6] * T * T * T * T;
-    return R * Cp_on_R;
+    return R * cea_Cp_on_R(a, TRecip(T));
 }
 
 // lT is pm_log(T), shared by the species of a mixture evaluated at one T
 static __device__ E4C_CEA_FN double cea_h_in_range(const e4c_thermochem& tc, int isp, double R,
-                                                 double T, double lT) {
+                                                 const TRecip& t, double lT) {
     double a[9];
-    cea_coefficients(tc, isp, T, a);
-    double h_on_RT = -a[0] / (T * T) + a[1] / T * lT + a[2] + a[3] * T / 2.0;
-    h_on_RT += a[4] * T * T / 3.0 + a[5] * T * T * T / 4.0 + a[6] * T * T * T * T / 5.0 + a[7] / T;
-    return R * T * h_on_RT;
+    cea_coefficients(tc, isp, t.T, a);
+    return R * t.T * cea_h_on_RT(a, t, lT);
 }
 
-static __device__ E4C_CEA_FN double cea_h(const e4c_thermochem& tc, int isp, double R, double T,
-                                        double lT) {
+static __device__ E4C_CEA_FN double cea_h(const e4c_thermochem& tc, int isp, double R,
+                                        const TRecip& t, double lT) {
     const int nseg = tc.nseg[isp];
+    const double T = t.T;
     if (T < tc.T_break[isp][0]) {
         double T_low = tc.T_break[isp][0];
-        double h_low = cea_h_in_range(tc, isp, R, T_low, pm_log(T_low));
+        double h_low = cea_h_in_range(tc, isp, R, TRecip(T_low), pm_log(T_low));
         double Cp_low = cea_Cp(tc, isp, R, T_low);
         return h_low - Cp_low * (T_low - T);
     }
     if (T > tc.T_break[isp][nseg]) {
         double T_high = tc.T_break[isp][nseg];
-        double h_high = cea_h_in_range(tc, isp, R, T_high, pm_log(T_high));
+        double h_high = cea_h_in_range(tc, isp, R, TRecip(T_high), pm_log(T_high));
         double Cp_high = cea_Cp(tc, isp, R, T_high);
         return h_high + Cp_high * (T - T_high);
     }
-    return cea_h_in_range(tc, isp, R, T, lT);
+    return cea_h_in_range(tc, isp, R, t, lT);
 }
 
 // cea_h and cea_Cp of one species at one temperature with one coefficient
 // selection (the same operations as the two functions)
-static __device__ E4C_CEA_FN void cea_h_Cp(const e4c_thermochem& tc, int isp, double R, double T,
-                                          double lT, double& h, double& Cp) {
+static __device__ E4C_CEA_FN void cea_h_Cp(const e4c_thermochem& tc, int isp, double R,
+                                          const TRecip& t, double lT, double& h, double& Cp) {
     const int nseg = tc.nseg[isp];
+    const double T = t.T;
     if (T < tc.T_break[isp][0] || T > tc.T_break[isp][nseg]) {
-        h = cea_h(tc, isp, R, T, lT);
+        h = cea_h(tc, isp, R, t, lT);
         Cp = cea_Cp(tc, isp, R, T);
         return;
     }
     double a[9];
     cea_coefficients(tc, isp, T, a);
-    double Cp_on_R = a[0] / (T * T) + a[1] / T + a[2] + a[3] * T;
-    Cp_on_R += a[4] * T * T + a[5] * T * T * T + a[6] * T * T * T * T;
-    Cp = R * Cp_on_R;
-    double h_on_RT = -a[0] / (T * T) + a[1] / T * lT + a[2] + a[3] * T / 2.0;
-    h_on_RT += a[4] * T * T / 3.0 + a[5] * T * T * T / 4.0 + a[6] * T * T * T * T / 5.0 + a[7] / T;
-    h = R * T * h_on_RT;
+    Cp = R * cea_Cp_on_R(a, t);
+    h = R * T * cea_h_on_RT(a, t, lT);
 }
 
 // ---------------------------------------------------------------------------
@@ -260,18 +296,20 @@ struct TPGas {
     __device__ double energy(const double* massf, double T) const {
         double e[NSP];
         const double lT = pm_log(T);
+        const TRecip t(T);
 #pragma unroll
-        for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], T, lT) - R[i] * T;
+        for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], t, lT) - R[i] * T;
         return mass_average(massf, e);
     }
     // energy(massf, T) and dudT(massf, T) together
     __device__ void energy_dudT(const double* massf, double T, double& u, double& du) const {
         double e[NSP], v[NSP];
         const double lT = pm_log(T);
+        const TRecip t(T);
 #pragma unroll
         for (int i = 0; i < NSP; ++i) {
             double h, cp;
-            cea_h_Cp(tc, i, R[i], T, lT, h, cp);
+            cea_h_Cp(tc, i, R[i], t, lT, h, cp);
             e[i] = h - R[i] * T;
             v[i] = cp - R[i];
         }
@@ -402,9 +440,10 @@ struct MechD {
         if (T < tc.T_lower) T = tc.T_lower;
         if (T > tc.T_upper) T = tc.T_upper;
         const double lT = pm_log(T);
+        const double rT = 1.0 / T;
         for (int r = 0; r < NR; ++r) {
-            kf[r] = tc.A_f[r] * pm_pow_l(T, lT, tc.n_f[r]) * pm_exp(-tc.C_f[r] / T);
-            kb[r] = tc.A_b[r] * pm_pow_l(T, lT, tc.n_b[r]) * pm_exp(-tc.C_b[r] / T);
+            kf[r] = tc.A_f[r] * pm_pow_l(T, lT, tc.n_f[r]) * pm_exp(div_rn(-tc.C_f[r], T, rT));
+            kb[r] = tc.A_b[r] * pm_pow_l(T, lT, tc.n_b[r]) * pm_exp(div_rn(-tc.C_b[r], T, rT));
         }
     }
     __device__ void rates(int r, const double* c, double& wf, double& wb) const {
