@@ -451,22 +451,30 @@ int e4c_connect_blocks(int ha, int fa, int hb, int fb, int orientation) {
     if (ha < 0 || ha >= nb || hb < 0 || hb >= nb || ha == hb)
         return fail(E4C_ERR_ARG, "bad block handles");
     if (fa < 0 || fa > 5 || fb < 0 || fb > 5) return fail(E4C_ERR_ARG, "bad face");
-    if (orientation != 0)
-        return fail(E4C_ERR_UNSUPPORTED, "only orientation 0 is on this path");
-    static const int opposite[6] = {SOUTH, WEST, NORTH, EAST, BOTTOM, TOP};
-    if (opposite[fa] != fb)
-        return fail(E4C_ERR_UNSUPPORTED, "only opposite faces (east-west, north-south, top-bottom) join");
     BlockHost& A = c.blocks[ha];
     BlockHost& B = c.blocks[hb];
-    if (c.cfg.dimensions == 2 && fa >= 4) return fail(E4C_ERR_ARG, "no top/bottom faces in 2-D");
+    const bool three_d = c.cfg.dimensions == 3;
+    if (!three_d && (fa >= 4 || fb >= 4)) return fail(E4C_ERR_ARG, "no top/bottom faces in 2-D");
+    if (orientation < 0 || orientation > 3 || (!three_d && orientation != 0))
+        return fail(E4C_ERR_ARG, "orientation must be 0..3 (0 in 2-D)");
     const BlockView &va = A.v, &vb = B.v;
-    const bool ew = (fa == EAST || fa == WEST), ns = (fa == NORTH || fa == SOUTH);
-    const bool same = ew ? (va.nj == vb.nj && va.nk == vb.nk)
-                     : ns ? (va.ni == vb.ni && va.nk == vb.nk) : (va.ni == vb.ni && va.nj == vb.nj);
+    // the cells of the two faces along their (p, q) indices (ffc_partner)
+    auto face_extents = [](const BlockView& v, int f, int& P, int& Q) {
+        P = (f == EAST || f == WEST) ? v.nj : v.ni;
+        Q = (f == TOP || f == BOTTOM) ? v.nj : v.nk;
+    };
+    int Pa, Qa, Pb, Qb;
+    face_extents(va, fa, Pa, Qa);
+    face_extents(vb, fb, Pb, Qb);
+    const bool same = (orientation & 1) ? (Pa == Qb && Qa == Pb) : (Pa == Pb && Qa == Qb);
     if (!same) return fail(E4C_ERR_ARG, "the joined faces differ in size");
+    static const int opposite[6] = {SOUTH, WEST, NORTH, EAST, BOTTOM, TOP};
     if (A.fused != B.fused)
         return fail(E4C_ERR_UNSUPPORTED, "a uniform (fused) block joins only another uniform block");
     if (A.fused) {
+        if (opposite[fa] != fb || orientation != 0)
+            return fail(E4C_ERR_UNSUPPORTED, "uniform (fused) blocks join opposite faces at "
+                                             "orientation 0 only (their frames are the axes)");
         const FusedDesc &x = A.f, &y = B.f;
         bool eq = x.vol == y.vol;
         for (int q = 0; q < 3; ++q) {
@@ -484,7 +492,7 @@ int e4c_connect_blocks(int ha, int fa, int hb, int fb, int orientation) {
     A.v.bc[fa] = E4C_BC_EXCHANGE;
     B.v.bc[fb] = E4C_BC_EXCHANGE;
     if (!A.fused) {
-        auto src = [](const BlockView& o) {
+        auto src = [orientation](const BlockView& o, int face) {
             ExchangeSrc e{};
             e.W = o.W;
             e.cgeom = o.cgeom;
@@ -492,13 +500,16 @@ int e4c_connect_blocks(int ha, int fa, int hb, int fb, int orientation) {
             e.npad = o.npad;
             e.nidim = o.nidim;
             e.njdim = o.njdim;
-            e.imax = o.imax;
-            e.jmax = o.jmax;
-            e.kmax = o.kmax;
+            e.ni = o.ni;
+            e.nj = o.nj;
+            e.nk = o.nk;
+            e.face = face;
+            e.orient = orientation;
+            e.kmin = o.kmin;
             return e;
         };
-        A.v.ex[fa] = src(B.v);
-        B.v.ex[fb] = src(A.v);
+        A.v.ex[fa] = src(B.v, fb);
+        B.v.ex[fb] = src(A.v, fa);
         launch_exchange_geometry(A.v, fa, c.stream);
         launch_exchange_geometry(B.v, fb, c.stream);
         c.launches += 2;

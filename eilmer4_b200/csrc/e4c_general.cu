@@ -333,16 +333,9 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
         const ExchangeSrc& o = b.ex[which];
         const size_t dst[2] = {g1, g2};
         for (int g = 0; g < 2; ++g) {
-            int si = i, sj = j, sk = k;
-            switch (which) {
-                case NORTH: sj = 2 + g; break;
-                case EAST: si = 2 + g; break;
-                case SOUTH: sj = o.jmax - g; break;
-                case WEST: si = o.imax - g; break;
-                case TOP: sk = 2 + g; break;
-                default: sk = o.kmax - g; break;
-            }
-            const size_t sc = (size_t(sk) * o.njdim + sj) * o.nidim + si;
+            int si, sj, sk;
+            ffc_partner(which, o.face, o.orient, a1, a2, g, o.ni, o.nj, o.nk, si, sj, sk);
+            const size_t sc = (size_t(sk + o.kmin) * o.njdim + sj + 2) * o.nidim + si + 2;
             for (int q = 0; q < nw; ++q) b.W[q * b.npad + dst[g]] = o.W[q * o.npad + sc];
             b.S[dst[g]] = o.S[sc];
         }
@@ -525,16 +518,9 @@ __global__ void k_exchange_geometry(BlockView b, int which) {
     }
     const ExchangeSrc& o = b.ex[which];
     for (int g = 0; g < 2; ++g) {
-        int si = i, sj = j, sk = k;
-        switch (which) {
-            case NORTH: sj = 2 + g; break;
-            case EAST: si = 2 + g; break;
-            case SOUTH: sj = o.jmax - g; break;
-            case WEST: si = o.imax - g; break;
-            case TOP: sk = 2 + g; break;
-            default: sk = o.kmax - g; break;
-        }
-        const size_t sc = (size_t(sk) * o.njdim + sj) * o.nidim + si;
+        int si, sj, sk;
+        ffc_partner(which, o.face, o.orient, a1, a2, g, o.ni, o.nj, o.nk, si, sj, sk);
+        const size_t sc = (size_t(sk + o.kmin) * o.njdim + sj + 2) * o.nidim + si + 2;
         const size_t gc = pidx(b, i + (g + 1) * di, j + (g + 1) * dj, k + (g + 1) * dk);
         for (int q = 0; q < 4; ++q) b.cgeom[q * b.npad + gc] = o.cgeom[q * o.npad + sc];
     }

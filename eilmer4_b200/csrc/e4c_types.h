@@ -20,18 +20,71 @@ enum Bnd { NORTH = 0, EAST = 1, SOUTH = 2, WEST = 3, TOP = 4, BOTTOM = 5 };
 // rho, vel.x, vel.y, vel.z, p, T, u, a (then mass fractions).
 enum PrimField { W_RHO = 0, W_VX, W_VY, W_VZ, W_P, W_T, W_U, W_A, W_NBASE };
 
-// The partner of an exchange boundary on the general path (full-face copy,
-// opposite faces, orientation 0): its padded primitive arrays and cell
-// geometry; padded indices start at 2 in every active direction.
+// The partner of an exchange boundary on the general path (full-face copy):
+// its padded primitive arrays and cell geometry, its joined face and the
+// joint's orientation, its active extents and the padded index of its first
+// active cell along k (2 in 3-D, 0 in 2-D; 2 along i and j).
 struct ExchangeSrc {
     const double* W;
     const double* cgeom;
     const int* S;
     size_t npad;
     int nidim, njdim;
-    int imax, jmax, kmax;
-    int pad_;
+    int ni, nj, nk;
+    int face, orient, kmin;
 };
+
+#ifdef __CUDACC__
+#define E4C_HD __host__ __device__
+#else
+#define E4C_HD
+#endif
+
+// The cell of the partner block that sits `depth` layers behind the joint
+// (0: the layer next to it) across from cell (p, q) of face fa, for a joint
+// of face fa with the partner's face fb at orientation r: the mapping of
+// GhostCellFullFaceCopy.set_up_cell_mapping (src/eilmer/bc/ghost_cell_effect/
+// full_face_copy.d:142-1083), written as one rule instead of its 144 cases.
+// A face's cells are indexed (p, q): north and south faces (i, k), east and
+// west (j, k), top and bottom (i, j); 2-D blocks have q = 0 and orientation 0.
+// Faces fall into two classes, {north, west, bottom} and {east, south, top};
+// from a face of the second class the orientation counts the other way
+// round (r -> 4 - r); then joints within one class and joints across the
+// classes each follow four orientation cases.  Both blocks of a joint carry
+// the same orientation (connectBlocks, src/eilmer/prep.lua), and the rule
+// maps back with it.  Returns the partner's active indices (from 0).
+E4C_HD inline void ffc_partner(int fa, int fb, int r, int p, int q, int depth, int ni, int nj,
+                               int nk, int& si, int& sj, int& sk) {
+    const bool xa = fa == NORTH || fa == WEST || fa == BOTTOM;
+    const bool xb = fb == NORTH || fb == WEST || fb == BOTTOM;
+    const int P = (fb == EAST || fb == WEST) ? nj : ni;   // extents of fb's (p, q)
+    const int Q = (fb == TOP || fb == BOTTOM) ? nj : nk;
+    if (!xa) r = (4 - r) & 3;
+    int pb, qb;
+    if (xa == xb) {
+        switch (r) {
+            case 0: pb = P - 1 - p; qb = q; break;
+            case 1: pb = q; qb = p; break;
+            case 2: pb = p; qb = Q - 1 - q; break;
+            default: pb = P - 1 - q; qb = Q - 1 - p; break;
+        }
+    } else {
+        switch (r) {
+            case 0: pb = p; qb = q; break;
+            case 1: pb = P - 1 - q; qb = p; break;
+            case 2: pb = P - 1 - p; qb = Q - 1 - q; break;
+            default: pb = q; qb = Q - 1 - p; break;
+        }
+    }
+    switch (fb) {
+        case NORTH: si = pb; sk = qb; sj = nj - 1 - depth; break;
+        case SOUTH: si = pb; sk = qb; sj = depth; break;
+        case EAST: sj = pb; sk = qb; si = ni - 1 - depth; break;
+        case WEST: sj = pb; sk = qb; si = depth; break;
+        case TOP: si = pb; sj = qb; sk = nk - 1 - depth; break;
+        default: si = pb; sj = qb; sk = depth; break;
+    }
+}
 
 // Device view of one structured block on the general-geometry path.  All
 // arrays use the reference's padded (i,j,k) index with two ghost layers,

@@ -84,7 +84,8 @@ class Simulation:
         return h
 
     def connect(self, ha, face_a, hb, face_b, orientation=0):
-        """Join two blocks' opposite faces with an exchange boundary."""
+        """Join face face_a of block ha to face face_b of block hb with an
+        exchange boundary (any face pair, orientation 0..3 in 3-D)."""
         _lib.check(self.L.e4c_connect_blocks(int(ha), int(face_a), int(hb), int(face_b),
                                              int(orientation)))
 

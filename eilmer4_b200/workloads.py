@@ -395,6 +395,79 @@ def split_block(b: BlockSpec, dimensions, parts=(2, 1, 1)):
     return blocks, conns
 
 
+# faces as (index axis, side): axis 0 = i, 1 = j, 2 = k; side 0 = low, 1 = high
+FACE_AXIS = {WEST: (0, 0), EAST: (0, 1), SOUTH: (1, 0), NORTH: (1, 1), BOTTOM: (2, 0), TOP: (2, 1)}
+AXIS_FACE = {v: f for f, v in FACE_AXIS.items()}
+
+
+def reindex_block(b: BlockSpec, axes, dimensions):
+    """The same block with its index axes turned: new axis a (i', j', k')
+    runs along old axis axes[a][0], forwards (axes[a][1] = +1) or backwards
+    (-1).  The turn must be proper (determinant +1) so cells stay
+    right-handed.  Returns (block, face_map, cell_map): face_map[old face] =
+    new face, cell_map(i, j, k) = the new indices of an old cell."""
+    nd = 3 if dimensions == 3 else 2
+    axes = [tuple(a) for a in axes][:nd]
+    if dimensions == 2:
+        axes.append((2, 1))
+    M = np.zeros((3, 3))
+    for a, (o, sgn) in enumerate(axes):
+        M[a, o] = sgn
+    if sorted(o for o, _ in axes) != [0, 1, 2] or round(np.linalg.det(M)) != 1:
+        raise ValueError("not a proper turn of the index axes")
+    n_old = (b.ni, b.nj, b.nk)
+    n_new = tuple(n_old[o] for o, _ in axes)
+
+    def turn(G, lead):
+        # G has axes (lead..., k, j, i, trailing...); numpy axis of index axis a is lead + 2 - a
+        order = list(range(lead)) + [lead + 2 - axes[a][0] for a in (2, 1, 0)]
+        order += list(range(lead + 3, G.ndim))
+        T = np.transpose(G, order)
+        for a in range(3):
+            if axes[a][1] < 0:
+                T = np.flip(T, axis=lead + 2 - a)
+        return np.ascontiguousarray(T)
+
+    nk1 = b.nk + 1 if dimensions == 3 else 1
+    V = turn(np.asarray(b.vtx).reshape(nk1, b.nj + 1, b.ni + 1, 3), 0)
+    nv = b.prim.shape[0]
+    P = turn(b.prim.reshape(nv, b.nk, b.nj, b.ni), 1)
+    face_map = {}
+    for f, (o, side) in FACE_AXIS.items():
+        a = next(q for q in range(3) if axes[q][0] == o)
+        face_map[f] = AXIS_FACE[(a, side if axes[a][1] > 0 else 1 - side)]
+    bc = [0] * 6
+    for f in range(6):
+        bc[face_map[f]] = b.bc[f]
+
+    def cell_map(i, j, k):
+        x = (i, j, k)
+        return tuple(x[o] if sgn > 0 else n_old[o] - 1 - x[o] for o, sgn in axes)
+
+    nb = BlockSpec(n_new[0], n_new[1], n_new[2], V.reshape(-1, 3).copy(), tuple(bc), b.inflow,
+                   P.reshape(nv, -1).copy())
+    return nb, face_map, cell_map
+
+
+def unturn_prim(prim, b_new: BlockSpec, axes, dimensions):
+    """The primitive array of a block made by reindex_block(…, axes, …),
+    back in the original block's cell order."""
+    nv = prim.shape[0]
+    P = prim.reshape(nv, b_new.nk, b_new.nj, b_new.ni)
+    nd = 3 if dimensions == 3 else 2
+    axes = [tuple(a) for a in axes][:nd]
+    if dimensions == 2:
+        axes.append((2, 1))
+    for a in range(3):
+        if axes[a][1] < 0:
+            P = np.flip(P, axis=1 + 2 - a)
+    # numpy axis 1 + 2 - a of P holds old axis axes[a][0]
+    inv = [0, 0, 0]
+    for a in range(3):
+        inv[2 - axes[a][0]] = 1 + 2 - a
+    return np.ascontiguousarray(np.transpose(P, [0] + inv)).reshape(nv, -1)
+
+
 def join_prims(blocks, b_shape, dimensions, parts=(2, 1, 1)):
     """Reassemble the primitive arrays of split_block's blocks (list of
     (nv, n) arrays) into the original block's (nv, ni*nj*nk) layout."""

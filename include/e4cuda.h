@@ -254,12 +254,18 @@ int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* b
 
 /* Join face face_a of block ha to face face_b of block hb
  * (GhostCellFullFaceCopy, src/eilmer/bc/ghost_cell_effect/full_face_copy.d,
- * set up by the reference's FluidBlockArray / connectBlocks in prep):
- * opposite faces (east-west, north-south, top-bottom), orientation 0, equal
- * face sizes, both blocks on the same path (both general, or both fused with
- * identical uniform geometry).  Both faces become exchange boundaries: the
- * ghost cells take the partner's cell geometry now and its flow state at the
- * start of every stage.  Call after creating the blocks, before stepping. */
+ * set up by the reference's FluidBlockArray / connectBlocks in prep): any
+ * pair of faces at orientation 0..3 in 3-D (0 in 2-D), with the reference's
+ * cell mapping for each face pair and orientation (full_face_copy.d:142-1083;
+ * both blocks carry the same orientation, as connectBlocks sets them) and
+ * matching face sizes (swapped by orientations 1 and 3).  Both blocks are on
+ * the same path: both general, or both fused with identical uniform geometry,
+ * in which case only opposite faces at orientation 0 join (a fused block's
+ * index axes are the coordinate axes).  Both faces become exchange
+ * boundaries: the ghost cells take the partner's cell geometry now (volume
+ * and the i, j, k lengths as the partner holds them, CopyDataOption.grid)
+ * and its flow state at the start of every stage.  Call after creating the
+ * blocks, before stepping. */
 int e4c_connect_blocks(int ha, int face_a, int hb, int face_b, int orientation);
 
 /* Upload a block's primitive state and encode its conserved quantities. */

@@ -784,6 +784,66 @@ void Sim::convective_flux(Block& b) {
 // ---------------------------------------------------------------------------
 // Ghost cells (src/eilmer/bc/ghost_cell_effect/*)
 // ---------------------------------------------------------------------------
+// Cells of face f of block B along its two face indices: north/south (i, k),
+// east/west (j, k), top/bottom (i, j).
+static void face_extents(const Block& B, int f, int& P, int& Q) {
+    P = (f == 1 || f == 3) ? B.nj : B.ni;
+    Q = (f == 4 || f == 5) ? B.nj : B.nk;
+}
+
+// GhostCellFullFaceCopy.set_up_cell_mapping (src/eilmer/bc/ghost_cell_effect/
+// full_face_copy.d:142-1083): the cell of partner block O (face fb, joint
+// orientation r) that fills ghost layer g (0: next to the face) of boundary
+// cell (i, j, k) on face `which` of block B, as padded indices of O.  The
+// reference's 144 cases (and the 16 of 2-D) follow one rule: faces north,
+// west, bottom form one class and east, south, top the other; seen from the
+// second class the orientation turns the other way (r -> 4 - r); a joint
+// within a class and a joint across the classes then each map the face
+// indices (p, q) to the partner's (p', q') with P', Q' its extents:
+//   within: r0 (P'-1-p, q)  r1 (q, p)      r2 (p, Q'-1-q)      r3 (P'-1-q, Q'-1-p)
+//   across: r0 (p, q)       r1 (P'-1-q, p) r2 (P'-1-p, Q'-1-q) r3 (q, Q'-1-p)
+static void map_face_cell(int which, int p, int q, int g, int fb, int r, int ni, int nj, int nk,
+                          int& ai, int& aj, int& ak) {
+    auto first_class = [](int f) { return f == 0 || f == 3 || f == 5; };
+    const bool ca = first_class(which), cb = first_class(fb);
+    if (!ca) r = (4 - r) % 4;
+    const int P = (fb == 1 || fb == 3) ? nj : ni;
+    const int Q = (fb == 4 || fb == 5) ? nj : nk;
+    // rows: r; columns: (coefficient of p, of q, constant) for p' and for q',
+    // where a constant of -1 stands for "extent - 1 -" (a reversed index)
+    static const int within[4][2][3] = {{{1, 0, -1}, {0, 1, 0}},  {{0, 1, 0}, {1, 0, 0}},
+                                        {{1, 0, 0}, {0, 1, -1}},  {{0, 1, -1}, {1, 0, -1}}};
+    static const int across[4][2][3] = {{{1, 0, 0}, {0, 1, 0}},   {{0, 1, -1}, {1, 0, 0}},
+                                        {{1, 0, -1}, {0, 1, -1}}, {{0, 1, 0}, {1, 0, -1}}};
+    const int(*m)[3] = (ca == cb) ? within[r] : across[r];
+    int out[2];
+    for (int a = 0; a < 2; ++a) {
+        const int v = m[a][0] * p + m[a][1] * q;
+        const int ext = (a == 0) ? P : Q;
+        out[a] = (m[a][2] < 0) ? ext - 1 - v : v;
+    }
+    switch (fb) {
+        case 0: ai = out[0]; ak = out[1]; aj = nj - 1 - g; break;
+        case 2: ai = out[0]; ak = out[1]; aj = g; break;
+        case 1: aj = out[0]; ak = out[1]; ai = ni - 1 - g; break;
+        case 3: aj = out[0]; ak = out[1]; ai = g; break;
+        case 4: ai = out[0]; aj = out[1]; ak = nk - 1 - g; break;
+        default: ai = out[0]; aj = out[1]; ak = g; break;
+    }
+}
+
+static void mapped_cell(const Block& B, int which, int i, int j, int k, int g, const Block& O,
+                        int fb, int r, int& si, int& sj, int& sk) {
+    // face indices of the boundary cell
+    const int p = (which == 1 || which == 3) ? j - B.jmin : i - B.imin;
+    const int q = (which == 4 || which == 5) ? j - B.jmin : k - B.kmin;
+    int ai, aj, ak;
+    map_face_cell(which, p, q, g, fb, r, O.ni, O.nj, O.nk, ai, aj, ak);
+    si = O.imin + ai;
+    sj = O.jmin + aj;
+    sk = O.kmin + ak;
+}
+
 static inline void reflect_normal_velocity(FlowState& fs, const Face& f) {
     to_local(fs.vel, f.n, f.t1, f.t2);  // ghost_cell.d:34-44
     fs.vel.x = -(fs.vel.x);
@@ -823,19 +883,13 @@ void Sim::apply_bcs(Block& b) {
                         // (full_face_copy.d exchange over MPI, :1134, :1255)
                         continue;
                     } else if (type == E4O_BC_EXCHANGE) {
-                        // full_face_copy.d (orientation 0, opposite faces): the
-                        // ghost layers take the partner's first two cells
+                        // full_face_copy.d: the ghost layers take the cells of
+                        // the partner mapped to them (set_up_cell_mapping)
                         Block& o = *blocks[b.ex_block[which]];
                         for (int g = 0; g < 2; ++g) {
-                            int si = i, sj = j, sk = k;
-                            switch (which) {
-                                case 0: sj = o.jmin + g; break;
-                                case 1: si = o.imin + g; break;
-                                case 2: sj = o.jmax - g; break;
-                                case 3: si = o.imax - g; break;
-                                case 4: sk = o.kmin + g; break;
-                                default: sk = o.kmax - g; break;
-                            }
+                            int si, sj, sk;
+                            mapped_cell(b, which, i, j, k, g, o, b.ex_face[which],
+                                        b.ex_orient[which], si, sj, sk);
                             (g == 0 ? g1 : g2).fs = o.cell(si, sj, sk).fs;
                         }
                     } else if (type == E4O_BC_INFLOW_SUPERSONIC) {
@@ -1204,23 +1258,26 @@ int e4o_add_block(void* sim, int ni, int nj, int nk, const double* vtx, const in
     return int(s->blocks.size()) - 1;
 }
 
+void e4o_ffc_map(int fa, int fb, int r, int p, int q, int depth, int ni, int nj, int nk,
+                 int* out3) {
+    e4o::map_face_cell(fa, p, q, depth, fb, r, ni, nj, nk, out3[0], out3[1], out3[2]);
+}
+
 int e4o_connect_blocks(void* sim, int a, int fa, int b, int fb, int orientation) {
     Sim* s = static_cast<Sim*>(sim);
     const int nb = int(s->blocks.size());
     if (a < 0 || a >= nb || b < 0 || b >= nb || a == b) return E4O_ERR_ARG;
-    if (fa < 0 || fa > 5 || fb < 0 || fb > 5 || orientation != 0) return E4O_ERR_ARG;
-    // opposite faces only: north-south, east-west, top-bottom
-    static const int opposite[6] = {2, 3, 0, 1, 5, 4};
-    if (opposite[fa] != fb) return E4O_ERR_ARG;
+    if (fa < 0 || fa > 5 || fb < 0 || fb > 5 || orientation < 0 || orientation > 3)
+        return E4O_ERR_ARG;
     Block& A = *s->blocks[a];
     Block& B = *s->blocks[b];
-    if (A.dim == 2 && fa >= 4) return E4O_ERR_ARG;
-    const bool ew = (fa == 1 || fa == 3), ns = (fa == 0 || fa == 2);
-    if (ew && (A.nj != B.nj || A.nk != B.nk)) return E4O_ERR_ARG;
-    if (ns && (A.ni != B.ni || A.nk != B.nk)) return E4O_ERR_ARG;
-    if (!ew && !ns && (A.ni != B.ni || A.nj != B.nj)) return E4O_ERR_ARG;
-    A.bc[fa] = E4O_BC_EXCHANGE; A.ex_block[fa] = b;
-    B.bc[fb] = E4O_BC_EXCHANGE; B.ex_block[fb] = a;
+    if (A.dim == 2 && (fa >= 4 || fb >= 4 || orientation != 0)) return E4O_ERR_ARG;
+    int Pa, Qa, Pb, Qb;
+    face_extents(A, fa, Pa, Qa);
+    face_extents(B, fb, Pb, Qb);
+    if (orientation % 2 == 0 ? (Pa != Pb || Qa != Qb) : (Pa != Qb || Qa != Pb)) return E4O_ERR_ARG;
+    A.bc[fa] = E4O_BC_EXCHANGE; A.ex_block[fa] = b; A.ex_face[fa] = fb; A.ex_orient[fa] = orientation;
+    B.bc[fb] = E4O_BC_EXCHANGE; B.ex_block[fb] = a; B.ex_face[fb] = fa; B.ex_orient[fb] = orientation;
     // exchange_geometry (full_face_copy.d:963-1083, CopyDataOption.grid):
     // ghost cells take the partner cells' volume and lengths
     auto copy_geom = [](Block& D, int which, Block& O) {
@@ -1244,15 +1301,9 @@ int e4o_connect_blocks(void* sim, int a, int fa, int b, int fb, int orientation)
             for (int j = j0; j <= j1; ++j)
                 for (int i = i0; i <= i1; ++i)
                     for (int g = 0; g < 2; ++g) {
-                        int si = i, sj = j, sk = k;
-                        switch (which) {
-                            case 0: sj = O.jmin + g; break;
-                            case 1: si = O.imin + g; break;
-                            case 2: sj = O.jmax - g; break;
-                            case 3: si = O.imax - g; break;
-                            case 4: sk = O.kmin + g; break;
-                            default: sk = O.kmax - g; break;
-                        }
+                        int si, sj, sk;
+                        mapped_cell(D, which, i, j, k, g, O, D.ex_face[which], D.ex_orient[which],
+                                    si, sj, sk);
                         Cell& gc = D.cell(i + (g + 1) * di, j + (g + 1) * dj, k + (g + 1) * dk);
                         const Cell& sc = O.cell(si, sj, sk);
                         gc.vol = sc.vol;

@@ -101,6 +101,11 @@ int e4o_add_block(void* sim, int ni, int nj, int nk, const double* vtx,
  * Both faces become exchange boundaries; the ghost cells take the partner's
  * cell geometry now and its flow state at every stage. */
 int e4o_connect_blocks(void* sim, int a, int fa, int b, int fb, int orientation);
+/* The active (from 0) indices of the partner cell that fills ghost layer
+ * `depth` behind cell (p, q) of face fa, for a joint with the partner's face
+ * fb at orientation r (full_face_copy.d:142-1083); partner extents ni, nj, nk. */
+void e4o_ffc_map(int fa, int fb, int r, int p, int q, int depth, int ni, int nj, int nk,
+                 int* out3);
 
 /* Set the interior flow state from a primitive SoA array and encode the
  * conserved quantities (src/eilmer/fvcell.d encode_conserved). */

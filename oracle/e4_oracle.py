@@ -123,6 +123,8 @@ def _declare(L):
     L.e4o_add_block.restype = ip
     L.e4o_set_flow.argtypes = [vp, ip, P(dp)]
     L.e4o_connect_blocks.argtypes = [vp, ip, ip, ip, ip, ip]
+    L.e4o_ffc_map.argtypes = [ip, ip, ip, ip, ip, ip, ip, ip, ip, P(ip)]
+    L.e4o_ffc_map.restype = None
     L.e4o_get_flow.argtypes = [vp, ip, P(dp), P(dp)]
     L.e4o_get_cell_geometry.argtypes = [vp, ip, P(dp)]
     L.e4o_run.argtypes = [vp, ip, dp]
@@ -168,6 +170,14 @@ def default_config(**kw) -> Config:
     for k, v in kw.items():
         setattr(c, k, v)
     return c
+
+
+def ffc_map(fa, fb, r, p, q, depth, ni, nj, nk):
+    """The partner cell (active indices) filling ghost layer `depth` behind
+    cell (p, q) of face fa, for a joint with face fb at orientation r."""
+    out = (ctypes.c_int * 3)()
+    lib().e4o_ffc_map(fa, fb, r, p, q, depth, ni, nj, nk, out)
+    return tuple(out)
 
 
 class OracleSim:

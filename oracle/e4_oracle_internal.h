@@ -66,6 +66,8 @@ struct Block {
     std::vector<Vec3> vtx;
     int bc[6] = {0, 0, 0, 0, 0, 0};
     int ex_block[6] = {-1, -1, -1, -1, -1, -1};   // partner block of an exchange boundary
+    int ex_face[6] = {-1, -1, -1, -1, -1, -1};    // the partner's joined face
+    int ex_orient[6] = {0, 0, 0, 0, 0, 0};         // orientation of the joint
     FlowState inflow;
     bool axis_frames = true;
 

@@ -49,9 +49,9 @@ def test_connect_rejects_bad_pairs(oracle):
     for b in blocks:
         sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
     with pytest.raises(RuntimeError):
-        sim.connect(0, W.EAST, 1, W.NORTH)      # not opposite faces
+        sim.connect(0, W.EAST, 1, W.NORTH)      # faces of 8 and 10 cells
     with pytest.raises(RuntimeError):
-        sim.connect(0, W.EAST, 1, W.WEST, 1)    # orientation other than 0
+        sim.connect(0, W.EAST, 1, W.WEST, 1)    # 2-D joints have orientation 0
 
 
 def gpu_run(wl, blocks, conns, nsteps, precision="fp64", **cfg):
