@@ -129,6 +129,8 @@ void Ctx::enqueue_stage(const std::vector<int>& hs, int stage, int final_stage) 
     for (int h : hs) {
         const BlockHost& b = blocks[h];
         if (!b.fused) launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc(b.v, d_sim, stream); });
+        if (b.linear_bc)
+            launch_as(*this, E4C_KCLASS_BC, 1, [&] { launch_bc_linear(b.v, d_sim, gas, stream); });
     }
     // simcore.d:2354-2358: shock points after every block's ghost cells
     if (cfg.flux_calculator == E4C_FLUX_ADAPTIVE_HANEL_AUSMDV) {
@@ -429,7 +431,7 @@ int e4c_block_create(int ni, int nj, int nk, const double* vtx_xyz, const int* b
     if (ni < 2 || nj < 2 || (dim == 3 && nk < 2))
         return fail(E4C_ERR_ARG, "a block needs at least 2 cells in each active direction");
     for (int q = 0; q < 6; ++q)
-        if (bc_type[q] < 0 || bc_type[q] > E4C_BC_OUTFLOW_SIMPLE_FLUX || bc_type[q] == E4C_BC_EXCHANGE)
+        if (bc_type[q] < 0 || bc_type[q] > E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR || bc_type[q] == E4C_BC_EXCHANGE)
             return fail(E4C_ERR_UNSUPPORTED, "unknown boundary type");
     BlockHost b;
     int rc = c.build_block(ni, nj, nk, vtx_xyz, bc_type, inflow_prim, b);
@@ -534,6 +536,7 @@ int e4c_block_upload(int h, const double* prim) {
         if (rc != E4C_OK) return rc;
     } else {
         launch_upload(b.v, c.d_staging, c.stream);
+        if (b.linear_bc) launch_ghost_defaults(b.v, c.gas, c.stream);
     }
     E4C_CUDA(cudaGetLastError());
     E4C_CUDA(cudaStreamSynchronize(c.stream));
@@ -649,6 +652,7 @@ int e4c_block_upload_async(int h, const double* prim) {
         if (rc != E4C_OK) return rc;
     } else {
         launch_upload(b.v, c.d_stage_in, c.stream);
+        if (b.linear_bc) launch_ghost_defaults(b.v, c.gas, c.stream);
     }
     c.launches += 1;
     E4C_CUDA(cudaGetLastError());

@@ -108,10 +108,12 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     const bool uniform = (flags[0] == 0);
     out.simple_flux = false;
     for (int q = 0; q < 6; ++q) out.simple_flux = out.simple_flux || bc[q] == E4C_BC_OUTFLOW_SIMPLE_FLUX;
+    out.linear_bc = false;
+    for (int q = 0; q < 6; ++q) out.linear_bc = out.linear_bc || bc[q] == E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR;
     // the fused kernel carries the ausmdv and hllc fluxes (no shock flags)
     // and the ghost-cell boundaries (no flux computed in a boundary)
     out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC && v.nsp == 1 &&
-                cfg.flux_calculator <= E4C_FLUX_HLLC && !out.simple_flux;
+                cfg.flux_calculator <= E4C_FLUX_HLLC && !out.simple_flux && !out.linear_bc;
     if (cfg.precision == E4C_PREC_FP32_FLUX && !out.fused)
         return fail(E4C_ERR_UNSUPPORTED,
                     "the FP32-flux form needs a 3-D block with uniform geometry and the "
@@ -361,6 +363,7 @@ int Ctx::upload_cons(BlockHost& b, const double* dev_cons) {
                     "temperature iteration needs a starting temperature)");
     if (b.fused) return fused_upload_cons(b, dev_cons);
     launch_upload_cons(b.v, dev_cons, d_sim, gas, stream);
+    if (b.linear_bc) launch_ghost_defaults(b.v, gas, stream);
     return E4C_OK;
 }
 

@@ -259,6 +259,139 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
     }
 }
 
+// ---------------------------------------------------------------------------
+// OutFlowBC_SimpleExtrapolate{xOrder=1}: ExtrapolateCopy with x_order 1
+// (src/eilmer/bc/ghost_cell_effect/extrapolate_copy.d:206-258 for the east
+// face, the same steps for every face).  Each ghost layer is extrapolated
+// linearly from the two cells before it (the second layer from the first
+// ghost and the boundary cell): rho, u and the mass fractions (scaled), then
+// T and p by update_thermo_from_rhou (from the ghost's own T for a mixture),
+// then the velocity.  The sound speed and the shock flag stay as they were:
+// the ghost cell's initial FlowState (k_ghost_defaults).  A failed thermo
+// update or mass-fraction scaling (the reference throws) stops the run with
+// E4C_ERR_THERMO.
+// ---------------------------------------------------------------------------
+template <int NSP, int GAS>
+__global__ void k_bc_linear(BlockView b, SimDev* sim, GasConsts gas) {
+    if (sim->status != 0 || sim->finished) return;
+    const int which = blockIdx.y;
+    if (b.dim == 2 && which >= 4) return;
+    if (b.bc[which] != E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR) return;
+    int n1, n2;
+    if (which == NORTH || which == SOUTH) { n1 = b.ni; n2 = b.nk; }
+    else if (which == EAST || which == WEST) { n1 = b.nj; n2 = b.nk; }
+    else { n1 = b.ni; n2 = b.nj; }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n1 * n2) return;
+    const int a1 = t % n1, a2 = t / n1;
+    int i, j, k, di = 0, dj = 0, dk = 0;
+    switch (which) {
+        case NORTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmax; dj = 1; break;
+        case SOUTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmin; dj = -1; break;
+        case EAST: j = b.jmin + a1; k = b.kmin + a2; i = b.imax; di = 1; break;
+        case WEST: j = b.jmin + a1; k = b.kmin + a2; i = b.imin; di = -1; break;
+        case TOP: i = b.imin + a1; j = b.jmin + a2; k = b.kmax; dk = 1; break;
+        default: i = b.imin + a1; j = b.jmin + a2; k = b.kmin; dk = -1; break;
+    }
+    size_t c1 = pidx(b, i, j, k), c2 = pidx(b, i - di, j - dj, k - dk);
+    const size_t dst[2] = {pidx(b, i + di, j + dj, k + dk), pidx(b, i + 2 * di, j + 2 * dj, k + 2 * dk)};
+    double* W = b.W;
+    const size_t np = b.npad;
+    for (int g = 0; g < 2; ++g) {
+        const size_t d = dst[g];
+        const double rho = 2.0 * W[W_RHO * np + c1] - W[W_RHO * np + c2];
+        const double u = 2.0 * W[W_U * np + c1] - W[W_U * np + c2];
+        bool ok = true;
+        double p, T;
+        if (GAS == 0) {
+            ok = ideal_rhou<double>(gas, rho, u, p, T);
+            W[W_U * np + d] = u;
+        } else {
+            TPState<NSP> Q;
+            Q.rho = rho; Q.u = u; Q.T = W[W_T * np + d]; Q.p = W[W_P * np + d]; Q.a = W[W_A * np + d];
+#pragma unroll
+            for (int q = 0; q < NSP; ++q)
+                Q.massf[q] = 2.0 * W[(W_NBASE + q) * np + c1] - W[(W_NBASE + q) * np + c2];
+            if (NSP > 1) ok = scale_mass_fractions<double, NSP>(Q.massf);
+            if (ok) {
+                TPGas<NSP> gm(c_tc);
+                ok = gm.rhou(Q);
+            }
+            p = Q.p; T = Q.T;
+            W[W_U * np + d] = Q.u;
+#pragma unroll
+            for (int q = 0; q < NSP; ++q) W[(W_NBASE + q) * np + d] = Q.massf[q];
+        }
+        if (!ok) {
+            set_status(sim, E4C_ERR_THERMO);
+            return;
+        }
+        W[W_RHO * np + d] = rho;
+        W[W_P * np + d] = p;
+        W[W_T * np + d] = T;
+        W[W_VX * np + d] = 2.0 * W[W_VX * np + c1] - W[W_VX * np + c2];
+        W[W_VY * np + d] = 2.0 * W[W_VY * np + c1] - W[W_VY * np + c2];
+        W[W_VZ * np + d] = 2.0 * W[W_VZ * np + c1] - W[W_VZ * np + c2];
+        c2 = c1;
+        c1 = d;
+    }
+}
+
+// Both ghost layers of the block's x_order 1 boundaries as a cell's initial
+// FlowState (fvcell.d:168-170 with flowstate.d:46-60 and gas_state.d:64-88):
+// 100 kPa, 300 K, at rest, mass fractions (1, 0, ...), rho and u from
+// update_thermo_from_pT, a from update_sound_speed, shock flag clear.
+template <int NSP, int GAS>
+__global__ void k_ghost_defaults(BlockView b, GasConsts gas) {
+    const int which = blockIdx.y;
+    if (b.dim == 2 && which >= 4) return;
+    if (b.bc[which] != E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR) return;
+    int n1, n2;
+    if (which == NORTH || which == SOUTH) { n1 = b.ni; n2 = b.nk; }
+    else if (which == EAST || which == WEST) { n1 = b.nj; n2 = b.nk; }
+    else { n1 = b.ni; n2 = b.nj; }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n1 * n2) return;
+    const int a1 = t % n1, a2 = t / n1;
+    int i, j, k, di = 0, dj = 0, dk = 0;
+    switch (which) {
+        case NORTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmax; dj = 1; break;
+        case SOUTH: i = b.imin + a1; k = b.kmin + a2; j = b.jmin; dj = -1; break;
+        case EAST: j = b.jmin + a1; k = b.kmin + a2; i = b.imax; di = 1; break;
+        case WEST: j = b.jmin + a1; k = b.kmin + a2; i = b.imin; di = -1; break;
+        case TOP: i = b.imin + a1; j = b.jmin + a2; k = b.kmax; dk = 1; break;
+        default: i = b.imin + a1; j = b.jmin + a2; k = b.kmin; dk = -1; break;
+    }
+    const double p = 100.0e3, T = 300.0;
+    double rho, u, a, massf[NSP > 1 ? NSP : 1];
+    massf[0] = 1.0;
+    for (int q = 1; q < NSP; ++q) massf[q] = 0.0;
+    if (GAS == 0) {
+        rho = p / (T * gas.Rgas);   // ideal_gas.d:89-97
+        u = gas.Cv * T;
+        a = ideal_sound_speed<double>(gas, T);
+    } else {
+        TPGas<NSP> gm(c_tc);
+        rho = p / (gm.Rmix(massf) * T);   // perf_gas_mix_eos.d:55-62
+        u = gm.energy(massf, T);
+        a = gm.sound_speed(massf, T);
+    }
+    for (int g = 1; g <= 2; ++g) {
+        const size_t d = pidx(b, i + g * di, j + g * dj, k + g * dk);
+        b.W[W_RHO * b.npad + d] = rho;
+        b.W[W_VX * b.npad + d] = 0.0;
+        b.W[W_VY * b.npad + d] = 0.0;
+        b.W[W_VZ * b.npad + d] = 0.0;
+        b.W[W_P * b.npad + d] = p;
+        b.W[W_T * b.npad + d] = T;
+        b.W[W_U * b.npad + d] = u;
+        b.W[W_A * b.npad + d] = a;
+        if (NSP > 1)
+            for (int q = 0; q < NSP; ++q) b.W[(W_NBASE + q) * b.npad + d] = massf[q];
+        b.S[d] = 0;
+    }
+}
+
 // 8-byte asynchronous global -> shared copies of one thread (cp.async; the
 // thread waits for its own copies only).
 __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {

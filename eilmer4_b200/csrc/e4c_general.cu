@@ -329,6 +329,7 @@ __global__ void k_bc(BlockView b, const SimDev* sim) {
     const size_t g2 = pidx(b, i + 2 * di, j + 2 * dj, k + 2 * dk);
     const int nw = W_NBASE + (NSP > 1 ? NSP : 0);
     const int type = b.bc[which];
+    if (type == E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR) return;   // k_bc_linear
     if (type == 3) {  // full-face copy: the partner's first two cells
         const ExchangeSrc& o = b.ex[which];
         const size_t dst[2] = {g1, g2};
@@ -708,6 +709,26 @@ void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s) {
     dim3 grid((m + 127) / 128, b.dim == 3 ? 6 : 4);
     if (b.nsp == 5) k_bc<5><<<grid, 128, 0, s>>>(b, sim);
     else k_bc<1><<<grid, 128, 0, s>>>(b, sim);
+}
+
+void launch_bc_linear(const BlockView& b, SimDev* sim, const GasConsts& gas, cudaStream_t s) {
+    if (b.nsp == 5) {
+        launch_bc_linear_tp(b, sim, gas, s);
+        return;
+    }
+    const int m = boundary_extent(b);
+    dim3 grid((m + 127) / 128, b.dim == 3 ? 6 : 4);
+    k_bc_linear<1, 0><<<grid, 128, 0, s>>>(b, sim, gas);
+}
+
+void launch_ghost_defaults(const BlockView& b, const GasConsts& gas, cudaStream_t s) {
+    if (b.nsp == 5) {
+        launch_ghost_defaults_tp(b, gas, s);
+        return;
+    }
+    const int m = boundary_extent(b);
+    dim3 grid((m + 127) / 128, b.dim == 3 ? 6 : 4);
+    k_ghost_defaults<1, 0><<<grid, 128, 0, s>>>(b, gas);
 }
 
 void launch_bc_flux(const BlockView& b, const SimDev* sim, const FluxOpts& o, cudaStream_t s) {

@@ -28,6 +28,7 @@ struct BlockHost {
     size_t nprim_vars = 8;
     bool fused = false;
     bool simple_flux = false;   // has an OutFlowBC_SimpleFlux boundary
+    bool linear_bc = false;     // has an x_order 1 extrapolation boundary
     FusedDesc f{};          // fused path: storage and uniform geometry
     int ex_block[6] = {-1, -1, -1, -1, -1, -1};   // partner handle of an exchange boundary
     int remote[6] = {-1, -1, -1, -1, -1, -1};     // shadow of a partner on another rank

@@ -28,6 +28,12 @@ void launch_download(const BlockView& b, double* prim, double* cons, cudaStream_
 void launch_upload_cons(const BlockView& b, const double* cons, SimDev* sim, const GasConsts& gas,
                         cudaStream_t s);
 void launch_bc(const BlockView& b, const SimDev* sim, cudaStream_t s);
+// x_order 1 extrapolation boundaries of a general block, after launch_bc
+void launch_bc_linear(const BlockView& b, SimDev* sim, const GasConsts& gas, cudaStream_t s);
+void launch_bc_linear_tp(const BlockView& b, SimDev* sim, const GasConsts& gas, cudaStream_t s);
+// the ghost cells of its x_order 1 boundaries as a cell's initial FlowState
+void launch_ghost_defaults(const BlockView& b, const GasConsts& gas, cudaStream_t s);
+void launch_ghost_defaults_tp(const BlockView& b, const GasConsts& gas, cudaStream_t s);
 // shock points (detect_shock_points with the PJ detector)
 void launch_shock(const BlockView& b, const SimDev* sim, double tol, cudaStream_t s);
 // velocities of the interior cells after their i (and j) face round trips

@@ -193,6 +193,21 @@ void launch_flux_tp(const BlockView& b, const SimDev* sim, const FluxOpts& o, in
     else k_flux<5, 0, 1><<<g, T, 0, s>>>(b, sim, o, dir);
 }
 
+static int boundary_cells(const BlockView& b) {
+    const int m1 = b.ni * b.nk, m2 = b.nj * b.nk, m3 = b.ni * b.nj;
+    return m1 > m2 ? (m1 > m3 ? m1 : m3) : (m2 > m3 ? m2 : m3);
+}
+
+void launch_bc_linear_tp(const BlockView& b, SimDev* sim, const GasConsts& gas, cudaStream_t s) {
+    dim3 grid((boundary_cells(b) + 127) / 128, b.dim == 3 ? 6 : 4);
+    k_bc_linear<5, 1><<<grid, 128, 0, s>>>(b, sim, gas);
+}
+
+void launch_ghost_defaults_tp(const BlockView& b, const GasConsts& gas, cudaStream_t s) {
+    dim3 grid((boundary_cells(b) + 127) / 128, b.dim == 3 ? 6 : 4);
+    k_ghost_defaults<5, 1><<<grid, 128, 0, s>>>(b, gas);
+}
+
 void launch_update_tp(const BlockView& b, SimDev* sim, const GasConsts& gas, int stage,
                       int final_stage, int g, int T, cudaStream_t s) {
     k_update<5, 1><<<g, T, 0, s>>>(b, sim, gas, stage, final_stage);

@@ -35,6 +35,7 @@ BC_SLIP_WALL = 0
 BC_INFLOW_SUPERSONIC = 1
 BC_OUTFLOW_EXTRAPOLATE = 2
 BC_OUTFLOW_SIMPLE_FLUX = 4   # OutFlowBC_SimpleFlux (bc.lua:1124-1146)
+BC_OUTFLOW_EXTRAPOLATE_LINEAR = 5   # OutFlowBC_SimpleExtrapolate{xOrder=1}
 
 DEFAULT_SEED = 20261203
 

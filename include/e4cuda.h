@@ -68,6 +68,14 @@ extern "C" {
 /* OutFlowBC_SimpleFlux (bc.lua:1124-1146): extrapolated ghost cells and the
  * boundary-face flux from the interior cell (boundary_flux_effect.d:367-546) */
 #define E4C_BC_OUTFLOW_SIMPLE_FLUX 4
+/* OutFlowBC_SimpleExtrapolate{xOrder=1} (bc.lua:1108-1120): ExtrapolateCopy
+ * with x_order 1 (extrapolate_copy.d:206-258 and alike for each face), each
+ * ghost layer extrapolated linearly from the two cells before it in rho, u,
+ * mass fractions and velocity, T and p from update_thermo_from_rhou, the
+ * sound speed and shock flag left as they were (from a ghost cell's initial
+ * FlowState: 100 kPa, 300 K, at rest, the first species, set at upload, as
+ * fvcell.d:168-170 constructs every cell).  General path only. */
+#define E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR 5
 
 /* flux_calculator (src/eilmer/fvcore.d:184-228, plus the new "hllc"). */
 #define E4C_FLUX_AUSMDV 0

@@ -850,7 +850,7 @@ static inline void reflect_normal_velocity(FlowState& fs, const Face& f) {
     to_global(fs.vel, f.n, f.t1, f.t2);
 }
 
-void Sim::apply_bcs(Block& b) {
+int Sim::apply_bcs(Block& b) {
     // Boundaries in the order north, east, south, west, top, bottom.
     const int nb = (b.dim == 3) ? 6 : 4;
     for (int which = 0; which < nb; ++which) {
@@ -892,6 +892,35 @@ void Sim::apply_bcs(Block& b) {
                                         b.ex_orient[which], si, sj, sk);
                             (g == 0 ? g1 : g2).fs = o.cell(si, sj, sk).fs;
                         }
+                    } else if (type == E4O_BC_OUTFLOW_EXTRAPOLATE_LINEAR) {
+                        // extrapolate_copy.d:206-258 (east; alike for every
+                        // face), x_order 1: each ghost layer from the two
+                        // cells before it, rho, u and mass fractions, then
+                        // update_thermo_from_rhou, then the velocity; the
+                        // sound speed and shock flag are not touched
+                        const Cell* c1 = &b.cell(i, j, k);
+                        const Cell* c2 = &b.cell(i - di, j - dj, k - dk);
+                        Cell* dst[2] = {&g1, &g2};
+                        for (int g = 0; g < 2; ++g) {
+                            GasState& d = dst[g]->fs.gas;
+                            const GasState &q1 = c1->fs.gas, &q2 = c2->fs.gas;
+                            d.rho = 2.0 * q1.rho - q2.rho;
+                            d.u = 2.0 * q1.u - q2.u;
+                            if (gm.nsp > 1) {
+                                for (int sp = 0; sp < gm.nsp; ++sp)
+                                    d.massf[sp] = 2.0 * q1.massf[sp] - q2.massf[sp];
+                                if (!scale_mass_fractions(d.massf)) return E4O_ERR_THERMO;
+                            } else {
+                                d.massf[0] = 1.0;
+                            }
+                            if (!gm.update_thermo_from_rhou(d)) return E4O_ERR_THERMO;
+                            Vec3& v = dst[g]->fs.vel;
+                            v.x = 2.0 * c1->fs.vel.x - c2->fs.vel.x;
+                            v.y = 2.0 * c1->fs.vel.y - c2->fs.vel.y;
+                            v.z = 2.0 * c1->fs.vel.z - c2->fs.vel.z;
+                            c2 = c1;
+                            c1 = dst[g];
+                        }
                     } else if (type == E4O_BC_INFLOW_SUPERSONIC) {
                         g1.fs = b.inflow;  // flow_state_copy.d:66+
                         g2.fs = b.inflow;
@@ -920,6 +949,45 @@ void Sim::apply_bcs(Block& b) {
                         reflect_normal_velocity(g2.fs, *f);
                     }
                 }
+    }
+    return 0;
+}
+
+// The ghost cells of a block's x_order 1 boundaries as a cell's initial
+// FlowState (fvcell.d:168-170, flowstate.d:115-131): 100 kPa, 300 K, at rest,
+// mass fractions (1, 0, ...), from update_thermo_from_pT and update_sound_speed.
+void Sim::reset_linear_ghosts(Block& b) {
+    FlowState fs;
+    fs.gas.p = 100.0e3;
+    fs.gas.T = 300.0;
+    for (int sp = 0; sp < NSPMAX; ++sp) fs.gas.massf[sp] = (sp == 0) ? 1.0 : 0.0;
+    gm.update_thermo_from_pT(fs.gas);
+    gm.update_sound_speed(fs.gas);
+    fs.vel = {0.0, 0.0, 0.0};
+    fs.S = 0;
+    const int nb = (b.dim == 3) ? 6 : 4;
+    for (int which = 0; which < nb; ++which) {
+        if (b.bc[which] != E4O_BC_OUTFLOW_EXTRAPOLATE_LINEAR) continue;
+        int di = 0, dj = 0, dk = 0;
+        switch (which) {
+            case 0: dj = 1; break;
+            case 1: di = 1; break;
+            case 2: dj = -1; break;
+            case 3: di = -1; break;
+            case 4: dk = 1; break;
+            default: dk = -1; break;
+        }
+        int i0 = b.imin, i1 = b.imax, j0 = b.jmin, j1 = b.jmax, k0 = b.kmin, k1 = b.kmax;
+        if (which == 0) j0 = j1 = b.jmax;
+        if (which == 2) j0 = j1 = b.jmin;
+        if (which == 1) i0 = i1 = b.imax;
+        if (which == 3) i0 = i1 = b.imin;
+        if (which == 4) k0 = k1 = b.kmax;
+        if (which == 5) k0 = k1 = b.kmin;
+        for (int k = k0; k <= k1; ++k)
+            for (int j = j0; j <= j1; ++j)
+                for (int i = i0; i <= i1; ++i)
+                    for (int g = 1; g <= 2; ++g) b.cell(i + g * di, j + g * dj, k + g * dk).fs = fs;
     }
 }
 
@@ -1129,7 +1197,10 @@ int Sim::gasdynamic_stage(int stage) {
     // grid): every block's ghost cells first (exchange copies see no
     // flux-loop state), then every block's fluxes, then the cell updates
     if (stage == 1) last_bad_cells = 0;
-    for (Block* b : blocks) apply_bcs(*b);
+    for (Block* b : blocks) {
+        int rc = apply_bcs(*b);
+        if (rc != 0) return rc;
+    }
     // simcore.d:2354-2358, turned on by the adaptive flux calculator
     // (globalconfig.d:1942-1950)
     if (cfg.flux_calculator == E4O_FLUX_ADAPTIVE_HANEL_AUSMDV)
@@ -1465,6 +1536,7 @@ int e4o_set_flow(void* sim, int blk, const double* prim) {
                 s->encode_conserved(c, 0);
                 c.dt_chem = -1.0;
             }
+    s->reset_linear_ghosts(b);
     return 0;
 }
 

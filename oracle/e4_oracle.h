@@ -25,7 +25,8 @@ extern "C" {
 #endif
 
 enum { E4O_BC_SLIP_WALL = 0, E4O_BC_INFLOW_SUPERSONIC = 1, E4O_BC_OUTFLOW_EXTRAPOLATE = 2,
-       E4O_BC_EXCHANGE = 3, E4O_BC_OUTFLOW_SIMPLE_FLUX = 4 };
+       E4O_BC_EXCHANGE = 3, E4O_BC_OUTFLOW_SIMPLE_FLUX = 4,
+       E4O_BC_OUTFLOW_EXTRAPOLATE_LINEAR = 5 /* OutFlowBC_SimpleExtrapolate{xOrder=1} */ };
 enum { E4O_FLUX_AUSMDV = 0, E4O_FLUX_HLLC = 1, E4O_FLUX_HANEL = 2, E4O_FLUX_ADAPTIVE_HANEL_AUSMDV = 3 };
 enum { E4O_UPDATE_EULER = 0, E4O_UPDATE_PC = 1 };
 enum { E4O_GAS_IDEAL = 0, E4O_GAS_THERM_PERF_5SP_AIR = 1 };

@@ -155,7 +155,8 @@ struct Sim {
     void face_flux(Block& b, Face& f, Cell& cL1, Cell& cL0, Cell& cR0, Cell& cR1, int dir) const;
     void convective_flux(Block& b);
     void simple_outflow_flux(Block& b);
-    void apply_bcs(Block& b);
+    int apply_bcs(Block& b);
+    void reset_linear_ghosts(Block& b);
     void encode_conserved(Cell& c, int ftl) const;
     int decode_conserved(Cell& c, int ftl) const;
     void time_derivatives(Block& b, Cell& c, int i, int j, int k, int ftl) const;
