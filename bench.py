@@ -759,6 +759,11 @@ def run_ours(args, rank, world, local_rank):
         res, _ = euler_case(args, "fp64", local_rank, dist, world, headline=False,
                             flux=other_flux)
         extra[f"{other_flux}_fp64"] = res
+        # the reference's default flux (adaptive Hanel/AUSMDV with the shock
+        # detector, fluxcalc.d:824-838) on the fused path
+        res, _ = euler_case(args, "fp64", local_rank, dist, world, headline=False,
+                            flux="adaptive_hanel_ausmdv")
+        extra["adaptive_hanel_ausmdv_fp64"] = res
         extra["batched"] = batched_case(args, local_rank)
         extra["curvilinear"] = curvilinear_case(args, local_rank)
         extra["reacting"], _ = reacting_case(args, local_rank)

@@ -112,8 +112,12 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
     for (int q = 0; q < 6; ++q) out.linear_bc = out.linear_bc || bc[q] == E4C_BC_OUTFLOW_EXTRAPOLATE_LINEAR;
     // the fused kernel carries the ausmdv and hllc fluxes (no shock flags)
     // and the ghost-cell boundaries (no flux computed in a boundary)
+    // (the Hanel and adaptive fluxes on the FP64 form only)
+    const bool fused_flux = cfg.flux_calculator <= E4C_FLUX_HLLC ||
+                            (cfg.precision != E4C_PREC_FP32_FLUX &&
+                             cfg.flux_calculator <= E4C_FLUX_ADAPTIVE_HANEL_AUSMDV);
     out.fused = uniform && dim == 3 && cfg.gasdynamic_update_scheme == E4C_UPDATE_PC && v.nsp == 1 &&
-                cfg.flux_calculator <= E4C_FLUX_HLLC && !out.simple_flux && !out.linear_bc;
+                fused_flux && !out.simple_flux && !out.linear_bc;
     if (cfg.precision == E4C_PREC_FP32_FLUX && !out.fused)
         return fail(E4C_ERR_UNSUPPORTED,
                     "the FP32-flux form needs a 3-D block with uniform geometry and the "
@@ -167,9 +171,11 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
         dfree(geom);
         const size_t nc = out.ncell;
         const size_t rsz = (cfg.precision == E4C_PREC_FP32_FLUX) ? sizeof(float) : sizeof(double);
-        char* s = static_cast<char*>(dalloc(2 * 5 * nc * rsz + (1 + 10) * nc * sizeof(double) + 256));
+        // (+ two bytes per cell: the adaptive flux's shock flags, both stages)
+        const size_t nbytes = 2 * 5 * nc * rsz + (1 + 10) * nc * sizeof(double) + 256 + 2 * nc;
+        char* s = static_cast<char*>(dalloc(nbytes));
         if (!s) return fail(E4C_ERR_CUDA, "cudaMalloc of fused block storage failed");
-        E4C_CUDA(cudaMemsetAsync(s, 0, 2 * 5 * nc * rsz + (1 + 10) * nc * sizeof(double) + 256, stream));
+        E4C_CUDA(cudaMemsetAsync(s, 0, nbytes, stream));
         double* dp = reinterpret_cast<double*>(s);
         f.U0 = dp; dp += 5 * nc;
         f.dUdt0 = dp; dp += 5 * nc;
@@ -177,7 +183,9 @@ int Ctx::build_block(int ni, int nj, int nk, const double* vtx, const int* bc,
         f.use_a0 = reinterpret_cast<int*>(dp); dp += 32;
         char* rp = reinterpret_cast<char*>(dp);
         f.WA = rp; rp += 5 * nc * rsz;
-        f.WB = rp;
+        f.WB = rp; rp += 5 * nc * rsz;
+        f.S[0] = reinterpret_cast<unsigned char*>(rp);
+        f.S[1] = f.S[0] + nc;
         v.W = v.U0 = v.dUdt0 = v.Fi = v.Fj = v.Fk = nullptr;
         v.cgeom = v.fgi = v.fgj = v.fgk = nullptr;
         max_cells_fused = std::max(max_cells_fused, int(nc));

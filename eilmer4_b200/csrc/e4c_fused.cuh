@@ -196,7 +196,7 @@ template <typename R, int FLUX, int DIR>
 __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R, 1> sR0,
                                           Prim<R, 1> sR1, const L2R2<R>& w, const FluxOpts& o,
                                           R* F, const R* vaL = nullptr, const R* vaR = nullptr,
-                                          int vs = 0) {
+                                          int vs = 0, int shock = 0) {
     Prim<R, 1> Lf = sL0, Rt = sR0;
     if (o.order2) {
         if (o.local_frame) {
@@ -245,11 +245,92 @@ __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R
         axis_to_local<DIR>(Lf.vel);
         axis_to_local<DIR>(Rt.vel);
     }
-    if (FLUX == 1) hllc<R, 1, 0>(Lf, Rt, F);
-    else ausmdv<R, 1, 0>(Lf, Rt, F);
+    if (FLUX == 1) {
+        hllc<R, 1, 0>(Lf, Rt, F);
+    } else if (FLUX == 2) {
+        hanel<R, 1, 0>(Lf, Rt, F);
+    } else if (FLUX == 3) {
+        // adaptive_hanel_ausmdv (fluxcalc.d:824-838): Hanel where either
+        // cell is a shock point and the shear is small, AUSMDV elsewhere
+        const R sound_speed = R(0.5) * (Lf.a + Rt.a);
+        const R shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
+        const R shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
+        const bool shear_is_small = fmax(shear_y, shear_z) <= R(o.shear_tol);
+        if (shock && shear_is_small) hanel<R, 1, 0>(Lf, Rt, F);
+        else ausmdv<R, 1, 0>(Lf, Rt, F);
+    } else {
+        ausmdv<R, 1, 0>(Lf, Rt, F);
+    }
     V3<R> m{F[1], F[2], F[3]};
     axis_to_global<DIR>(m);
     F[1] = m.x; F[2] = m.y; F[3] = m.z;
+}
+
+// detect_shock_points (fluidblock.d:415-431) with PJ_ShockDetector
+// (shockdetectors.d:20-59) for the cell at offset off of plane p0 (pm and pp
+// the planes below and above): a face flags compression when
+// (uR - uL) / min(aL, aR) < tol, u the velocity along the face normal (an
+// axis here, so the component itself: v.n = v.x*1 + v.y*0 + v.z*0 differs
+// from it at most in the sign of a zero, which the test cannot see); the
+// cell is a shock point if any of its six faces does.
+template <typename R, int PI>
+__device__ __forceinline__ int cell_shock(const R* pm, const R* p0, const R* pp, int off, int FS,
+                                          double tol) {
+    auto face = [tol](double uL, double uR, double aL, double aR) {
+        const double a_min = (aL < aR) ? aL : aR;
+        return ((uR - uL) / a_min) < tol ? 1 : 0;
+    };
+    const R a = p0[5 * FS + off];
+    int S = 0;
+    S |= face(p0[FS + off - 1], p0[FS + off], p0[5 * FS + off - 1], a);
+    S |= face(p0[FS + off], p0[FS + off + 1], a, p0[5 * FS + off + 1]);
+    S |= face(p0[2 * FS + off - PI], p0[2 * FS + off], p0[5 * FS + off - PI], a);
+    S |= face(p0[2 * FS + off], p0[2 * FS + off + PI], a, p0[5 * FS + off + PI]);
+    S |= face(pm[3 * FS + off], p0[3 * FS + off], pm[5 * FS + off], a);
+    S |= face(p0[3 * FS + off], pp[3 * FS + off], a, pp[5 * FS + off]);
+    return S;
+}
+
+// The flag of the first ghost cell beyond one face of block d at (gi, gj,
+// gk) (exactly one index outside): what the boundary condition copied at the
+// start of the stage, i.e. the previous stage's flag of the cell the ghost
+// copies (the mirror or first interior cell for walls and outflow, the
+// partner's cell across a joint), 0 for an inflow.
+__device__ __forceinline__ int ghost_shock(const FusedDesc* __restrict__ descs, const FusedDesc& d,
+                                           int stage, int gi, int gj, int gk) {
+    const int prev = (stage == 1) ? 1 : 0;
+    int which;
+    if (gi < 0) which = WEST;
+    else if (gi >= d.ni) which = EAST;
+    else if (gj < 0) which = SOUTH;
+    else if (gj >= d.nj) which = NORTH;
+    else if (gk < 0) which = BOTTOM;
+    else which = TOP;
+    const int type = d.bc[which];
+    if (type == 1) return 0;
+    if (type == 3) {
+        const FusedDesc& o = descs[d.ex[which]];
+        if (!o.S[prev]) return 0;
+        int si = gi, sj = gj, sk = gk;
+        switch (which) {
+            case WEST: si = o.ni - 1; break;
+            case EAST: si = 0; break;
+            case SOUTH: sj = o.nj - 1; break;
+            case NORTH: sj = 0; break;
+            case BOTTOM: sk = o.nk - 1; break;
+            default: sk = 0; break;
+        }
+        return o.S[prev][(size_t(sk) * o.nj + sj) * o.ni + si];
+    }
+    switch (which) {
+        case WEST: gi = 0; break;
+        case EAST: gi = d.ni - 1; break;
+        case SOUTH: gj = 0; break;
+        case NORTH: gj = d.nj - 1; break;
+        case BOTTOM: gk = 0; break;
+        default: gk = d.nk - 1; break;
+    }
+    return d.S[prev][(size_t(gk) * d.nj + gj) * d.ni + gi];
 }
 
 template <typename R>
@@ -358,6 +439,13 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
     const int ti = threadIdx.x % TI, tj = threadIdx.x / TI;
     const double dt = sim->dt_global;
     int bad = 0;
+    // adaptive flux: shock flags of two planes (the tile and its one-cell
+    // ring, pitch TI + 2), this thread's cell's in registers
+    constexpr bool ADAPT = (FLUX == 3);
+    constexpr int SP = TI + 2;
+    constexpr int RING = 2 * (TI + TJ);
+    static_assert(RING <= TI * TJ, "the ring's flags take one thread each");
+    __shared__ unsigned char s_S[2][ADAPT ? SP * (TJ + 2) : 1];
 
     for (;;) {
         __syncthreads();  // s_item of the previous item has been read by all
@@ -390,6 +478,42 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
         for (int kk = k0 - 2; kk <= k0 + 1; ++kk)
             load_plane<R, TI, TJ>(descs, stage, d, Win, use_a0, gas, planes + ((kk + 8) & 3) * S::PLANE, i0, j0, kk);
         __syncthreads();
+        // the shock flag of tile position (li, lj) (-1..TI, -1..TJ) in plane
+        // kk, from planes kk-1..kk+1; the first ghost cell beyond a face
+        // takes its boundary's copy
+        auto flag_at = [&](int li, int lj, int kk) -> int {
+            const int gi = i0 + li, gj = j0 + lj;
+            const int out = int(gi < 0 || gi >= d.ni) + int(gj < 0 || gj >= d.nj) +
+                            int(kk < 0 || kk >= d.nk);
+            if (out == 1) return ghost_shock(descs, d, stage, gi, gj, kk);
+            if (out > 1) return 0;
+            return cell_shock<R, PI>(planes + ((kk - 1 + 8) & 3) * S::PLANE,
+                                     planes + ((kk + 8) & 3) * S::PLANE,
+                                     planes + ((kk + 1 + 8) & 3) * S::PLANE,
+                                     (lj + 2) * PI + (li + 2), FS, o.compression_tol);
+        };
+        // flags of plane kk into slot kk & 1: each thread its own position,
+        // the first threads the ring; returns this thread's own flag
+        auto flag_plane = [&](int kk) -> int {
+            int own = 0;
+            if (cell_thread) {
+                own = flag_at(ti, tj, kk);
+                s_S[kk & 1][(tj + 1) * SP + ti + 1] = (unsigned char)own;
+            }
+            if (threadIdx.x < RING) {
+                int li, lj;
+                const int r = threadIdx.x;
+                if (r < 2 * TJ) { li = (r & 1) ? TI : -1; lj = r >> 1; }
+                else { li = (r - 2 * TJ) >> 1; lj = ((r - 2 * TJ) & 1) ? TJ : -1; }
+                s_S[kk & 1][(lj + 1) * SP + li + 1] = (unsigned char)flag_at(li, lj, kk);
+            }
+            return own;
+        };
+        int s_cur = 0, s_below = 0;
+        if (ADAPT) {
+            if (active) s_below = flag_at(ti, tj, k0 - 1);
+            s_cur = flag_plane(k0);
+        }
         R Fbot[5];
         const int coff = (tj + 2) * PI + (ti + 2);
         if (active) {
@@ -398,7 +522,8 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
             get_cell(planes + ((k0 - 1 + 8) & 3) * S::PLANE, coff, FS, gas, c1);
             get_cell(planes + ((k0 + 8) & 3) * S::PLANE, coff, FS, gas, c2);
             get_cell(planes + ((k0 + 1 + 8) & 3) * S::PLANE, coff, FS, gas, c3);
-            face_flux<R, FLUX, 2>(c0, c1, c2, c3, w[2], o, Fbot);
+            face_flux<R, FLUX, 2>(c0, c1, c2, c3, w[2], o, Fbot, nullptr, nullptr, 0,
+                                  s_below | s_cur);
         }
         __syncthreads();  // plane k0-2 is overwritten by the first load below
         for (int k = k0; k < k1; ++k) {
@@ -436,6 +561,12 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
             // was loaded two iterations ago: the values need no barrier of
             // their own, and the loads overlap their divisions)
             __syncthreads();
+            // shock flags of plane k+1 (slot (k+1) & 1, last read by the
+            // previous plane's faces); the ring's are read after the next
+            // plane's barrier, this thread's own at once
+            int s_next = 0;
+            if (ADAPT) s_next = flag_plane(k + 1);
+            const unsigned char* sk_ = s_S[k & 1];
             // i-faces, (TI+1) x TJ (face fi is the west face of cell i0+fi), then
             // j-faces, TI x (TJ+1) (face fj is the south face of cell j0+fj), as
             // one list over all the CTA's threads
@@ -453,11 +584,12 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                     get_cell(pk, off + 2, FS, gas, a2);
                     get_cell(pk, off + 3, FS, gas, a3);
                     R F[5];
+                    const int sh = ADAPT ? (sk_[(fj + 1) * SP + fi] | sk_[(fj + 1) * SP + fi + 1]) : 0;
                     if (share_va) {
                         const R* v = VAi + fj * (TI + 2) + fi;
-                        face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F, v, v + 1, S::NVI);
+                        face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F, v, v + 1, S::NVI, sh);
                     } else {
-                        face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F);
+                        face_flux<R, FLUX, 0>(a0, a1, a2, a3, w[0], o, F, nullptr, nullptr, 0, sh);
                     }
 #pragma unroll
                     for (int v = 0; v < 5; ++v) Fi[(v * TJ + fj) * (TI + 1) + fi] = F[v];
@@ -472,11 +604,12 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                     get_cell(pk, off + 2 * PI, FS, gas, a2);
                     get_cell(pk, off + 3 * PI, FS, gas, a3);
                     R F[5];
+                    const int sh = ADAPT ? (sk_[fj * SP + fi + 1] | sk_[(fj + 1) * SP + fi + 1]) : 0;
                     if (share_va) {
                         const R* v = VAj + fj * TI + fi;
-                        face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F, v, v + TI, S::NVJ);
+                        face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F, v, v + TI, S::NVJ, sh);
                     } else {
-                        face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F);
+                        face_flux<R, FLUX, 1>(a0, a1, a2, a3, w[1], o, F, nullptr, nullptr, 0, sh);
                     }
 #pragma unroll
                     for (int v = 0; v < 5; ++v) Fj[(v * (TJ + 1) + fj) * TI + fi] = F[v];
@@ -490,7 +623,8 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                 get_cell(pk, coff, FS, gas, c1);
                 get_cell(planes + ((k + 1 + 8) & 3) * S::PLANE, coff, FS, gas, c2);
                 get_cell(planes + ((k + 2 + 8) & 3) * S::PLANE, coff, FS, gas, c3);
-                face_flux<R, FLUX, 2>(c0, c1, c2, c3, w[2], o, Ftop);
+                face_flux<R, FLUX, 2>(c0, c1, c2, c3, w[2], o, Ftop, nullptr, nullptr, 0,
+                                      s_cur | s_next);
             }
             __syncthreads();
             if (active) {
@@ -564,7 +698,9 @@ k_fused_stage(const FusedDesc* __restrict__ descs, int nblocks, long long nitems
                 if (!ok) ++bad;
 #pragma unroll
                 for (int v = 0; v < 5; ++v) Fbot[v] = Ftop[v];
+                if (ADAPT) d.S[stage == 1 ? 0 : 1][c] = (unsigned char)s_cur;
             }
+            s_cur = s_next;
             // no barrier here: the update reads only Fi/Fj (rewritten after the
             // next plane's load barrier) and its own registers; the next load
             // overwrites plane k-1, last read by this plane's k-faces

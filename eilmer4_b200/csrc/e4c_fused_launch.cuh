@@ -96,9 +96,14 @@ int fused_stage(const FusedLaunch& L, SimDev* sim, const GasConsts& gas, const F
 #undef E4C_WS_CASE
     }
 #endif
+// Hanel and the adaptive Hanel/AUSMDV flux: the FP64 form only
 #define E4C_CASE(TI_, TJ_)                                                        \
     if (L.ti == TI_ && L.tj == TJ_) {                                            \
         if (o.flux == 1) return launch_one<1, TI_, TJ_>(L, sim, gas, o, stage, s); \
+        if constexpr (sizeof(RT) == 8) {                                         \
+            if (o.flux == 2) return launch_one<2, TI_, TJ_>(L, sim, gas, o, stage, s); \
+            if (o.flux == 3) return launch_one<3, TI_, TJ_>(L, sim, gas, o, stage, s); \
+        }                                                                        \
         return launch_one<0, TI_, TJ_>(L, sim, gas, o, stage, s);                  \
     }
     E4C_TILES(E4C_CASE)
@@ -117,6 +122,10 @@ int fused_occupancy(int flux, int ti, int tj) {
 #endif
 #define E4C_CASE(TI_, TJ_)                                          \
     if (ti == TI_ && tj == TJ_) {                                  \
+        if constexpr (sizeof(RT) == 8) {                           \
+            if (flux == 2) return occupancy_one<2, TI_, TJ_>();    \
+            if (flux == 3) return occupancy_one<3, TI_, TJ_>();    \
+        }                                                          \
         return flux == 1 ? occupancy_one<1, TI_, TJ_>() : occupancy_one<0, TI_, TJ_>(); \
     }
     E4C_TILES(E4C_CASE)

@@ -86,6 +86,9 @@ int e4c_connect_remote(int h, int face) {
     if (!b.fused)
         return fail(E4C_ERR_UNSUPPORTED, "faces joined to another rank are on the fused "
                                          "(uniform 3-D block) path only");
+    if (c.cfg.flux_calculator == E4C_FLUX_ADAPTIVE_HANEL_AUSMDV)
+        return fail(E4C_ERR_UNSUPPORTED, "the exchanged layers carry no shock flags: "
+                                         "joints to another rank take the non-adaptive fluxes");
     if (b.remote[face] >= 0 || b.ex_block[face] >= 0)
         return fail(E4C_ERR_ARG, "the face is joined already");
     RemoteFace r;
@@ -108,6 +111,7 @@ int e4c_connect_remote(int h, int face) {
     d.A0 = reinterpret_cast<const double*>(p + 5 * n * rsz);
     d.use_a0 = reinterpret_cast<int*>(p + 5 * n * rsz + n * sizeof(double));
     d.U0 = nullptr;
+    d.S[0] = d.S[1] = nullptr;
     d.dUdt0 = nullptr;
     d.acc = nullptr;
     for (int w = 0; w < 6; ++w) { d.bc[w] = E4C_BC_WALL_WITH_SLIP; d.ex[w] = -1; }

@@ -162,6 +162,10 @@ struct FusedDesc {
     double fn[3][3], ft1[3][3], ft2[3][3];
     double inflow[6];           // rho, vx, vy, vz, u, a
     int ex[6];                  // descriptor index of the partner of an exchange boundary
+    // shock flags of the adaptive flux (ncell each): stage 1 writes S[0] and
+    // takes the ghost cells' flags from S[1] (the previous stage's), stage 2
+    // the other way round
+    unsigned char* S[2];
 };
 
 // Molar masses of the five species, for the chemistry seed's guesses.
