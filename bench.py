@@ -7,7 +7,8 @@ CFL 0.5.  A bench "step" is one full time step (both predictor-corrector
 stages, ghost cells, decode and the dt control every 10 steps) over the block.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32_flux]
-                  [--impl ours|reference] [--n 256] [--flux hllc|ausmdv] [--headline-only]
+                  [--impl ours|reference] [--n 256] [--flux hllc|ausmdv|hanel|adaptive_hanel_ausmdv]
+                  [--headline-only]
 
 Prints one JSON line (rank 0).  The headline (value, roofline, e2e, clocks,
 gpu_launches) is the --precision form of the 256^3 block.  On one GPU the
@@ -76,6 +77,12 @@ TRAFFIC = {("fp64", "stage"): 2758515712, ("fp32_flux", "stage"): 2418098712}
 # shape).  Compiled without FMA contraction, the kernel's ceiling is half the
 # FP64 peak (64 DFMA per SM per cycle, 2 FLOP each).
 FP64_FLOP_PER_CELL_UPDATE = {("fp64", "hllc"): 2430.0}
+
+
+def oracle_flux(O, flux):
+    """The oracle's code of a flux calculator name."""
+    return {"ausmdv": O.FLUX_AUSMDV, "hllc": O.FLUX_HLLC, "hanel": O.FLUX_HANEL,
+            "adaptive_hanel_ausmdv": O.FLUX_ADAPTIVE_HANEL_AUSMDV}[flux]
 
 
 def peaks():
@@ -147,8 +154,7 @@ def cpu_oracle_rate(n, steps, flux, threads=0, seed=None):
     from oracle import e4_oracle as O
     O.build()
     b = W.inflow_3d_block(n, n, n, seed if seed is not None else W.DEFAULT_SEED)
-    cfg = O.default_config(dimensions=3, flux_calculator=O.FLUX_HLLC if flux == "hllc"
-                           else O.FLUX_AUSMDV, n_threads=threads)
+    cfg = O.default_config(dimensions=3, flux_calculator=oracle_flux(O, flux), n_threads=threads)
     sim = O.OracleSim(cfg)
     sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
     sim.set_flow(0, b.prim)
@@ -278,8 +284,7 @@ def run_reference(args, rank, world):
     O.build()
     n = args.ref_sample or args.n
     b = W.inflow_3d_block(n, n, n, W.DEFAULT_SEED)
-    cfg = O.default_config(dimensions=3, flux_calculator=O.FLUX_HLLC if args.flux == "hllc"
-                           else O.FLUX_AUSMDV, n_threads=0)
+    cfg = O.default_config(dimensions=3, flux_calculator=oracle_flux(O, args.flux), n_threads=0)
     sim = O.OracleSim(cfg)
     sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
     sim.set_flow(0, b.prim)
@@ -511,8 +516,7 @@ def cpu_oracle_curvilinear(n, steps, flux):
     O.build()
     wl = W.skewed_box_3d(ni=n, nj=n, nk=n, flux=flux)
     b = wl.blocks[0]
-    cfg = O.default_config(dimensions=3, flux_calculator=O.FLUX_HLLC if flux == "hllc"
-                           else O.FLUX_AUSMDV, n_threads=0)
+    cfg = O.default_config(dimensions=3, flux_calculator=oracle_flux(O, flux), n_threads=0)
     sim = O.OracleSim(cfg)
     sim.add_block(b.ni, b.nj, b.nk, b.vtx, b.bc, b.inflow)
     sim.set_flow(0, b.prim)
@@ -745,6 +749,9 @@ def run_ours(args, rank, world, local_rank):
         return
     head, rho_head = euler_case(args, args.precision, local_rank, dist, world, headline=True)
     extra = {}
+    if not args.headline_only and world == 1 and args.flux not in ("hllc", "ausmdv"):
+        raise SystemExit("the full line (FP32-flux form included) runs with --flux hllc or "
+                         "ausmdv; add --headline-only for the other fluxes")
     if not args.headline_only and world == 1:
         other = "fp32_flux" if args.precision == "fp64" else "fp64"
         res, rho_other = euler_case(args, other, local_rank, dist, world, headline=False)
@@ -811,7 +818,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_flux"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--flux", default="hllc", choices=["hllc", "ausmdv"])
+    ap.add_argument("--flux", default="hllc", choices=["hllc", "ausmdv", "hanel", "adaptive_hanel_ausmdv"])
     ap.add_argument("--profile-steps", type=int, default=4)
     # CPU baseline samples: about 10 s of oracle work each on a 16-core host
     ap.add_argument("--cpu-sample", type=int, default=128)

@@ -240,11 +240,15 @@ __global__ void k_flux(BlockView b, const SimDev* sim, FluxOpts o, int dir_arg) 
         } else if (FLUX == 3) {
             // adaptive_hanel_ausmdv (fluxcalc.d:824-838); the states carry the
             // shock flags of the cells they were reconstructed from
-            const double sound_speed = 0.5 * (Lf.a + Rt.a);
-            const double shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
-            const double shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
-            const bool shear_is_small = fmax(shear_y, shear_z) <= o.shear_tol;
-            if ((b.S[cL0] == 1 || b.S[cR0] == 1) && shear_is_small)
+            // (the shear matters only at shock points)
+            bool use_hanel = false;
+            if (b.S[cL0] == 1 || b.S[cR0] == 1) {
+                const double sound_speed = 0.5 * (Lf.a + Rt.a);
+                const double shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
+                const double shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
+                use_hanel = fmax(shear_y, shear_z) <= o.shear_tol;
+            }
+            if (use_hanel)
                 hanel<double, NSP, NSPC>(Lf, Rt, F);
             else
                 ausmdv<double, NSP, NSPC>(Lf, Rt, F);
@@ -602,11 +606,15 @@ __global__ void __launch_bounds__(kRowThreads) k_flux_rows(BlockView b, const Si
             } else if (FLUX == 2) {
                 hanel<double, NSP, NSPC>(Lf, Rt, F);
             } else if (FLUX == 3) {
-                const double sound_speed = 0.5 * (Lf.a + Rt.a);
-                const double shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
-                const double shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
-                const bool shear_is_small = fmax(shear_y, shear_z) <= o.shear_tol;
-                if ((b.S[f - stride] == 1 || b.S[f] == 1) && shear_is_small)
+                // (the shear matters only at shock points)
+                bool use_hanel = false;
+                if (b.S[f - stride] == 1 || b.S[f] == 1) {
+                    const double sound_speed = 0.5 * (Lf.a + Rt.a);
+                    const double shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
+                    const double shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
+                    use_hanel = fmax(shear_y, shear_z) <= o.shear_tol;
+                }
+                if (use_hanel)
                     hanel<double, NSP, NSPC>(Lf, Rt, F);
                 else
                     ausmdv<double, NSP, NSPC>(Lf, Rt, F);

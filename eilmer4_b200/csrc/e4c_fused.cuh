@@ -252,11 +252,15 @@ __device__ __forceinline__ void face_flux(Prim<R, 1> sL1, Prim<R, 1> sL0, Prim<R
     } else if (FLUX == 3) {
         // adaptive_hanel_ausmdv (fluxcalc.d:824-838): Hanel where either
         // cell is a shock point and the shear is small, AUSMDV elsewhere
-        const R sound_speed = R(0.5) * (Lf.a + Rt.a);
-        const R shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
-        const R shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
-        const bool shear_is_small = fmax(shear_y, shear_z) <= R(o.shear_tol);
-        if (shock && shear_is_small) hanel<R, 1, 0>(Lf, Rt, F);
+        // (the shear matters only at shock points)
+        bool use_hanel = false;
+        if (shock) {
+            const R sound_speed = R(0.5) * (Lf.a + Rt.a);
+            const R shear_y = fabs(Lf.vel.y - Rt.vel.y) / sound_speed;
+            const R shear_z = fabs(Lf.vel.z - Rt.vel.z) / sound_speed;
+            use_hanel = fmax(shear_y, shear_z) <= R(o.shear_tol);
+        }
+        if (use_hanel) hanel<R, 1, 0>(Lf, Rt, F);
         else ausmdv<R, 1, 0>(Lf, Rt, F);
     } else {
         ausmdv<R, 1, 0>(Lf, Rt, F);
