@@ -282,7 +282,7 @@ __device__ __forceinline__ int cell_shock(const R* pm, const R* p0, const R* pp,
                                           double tol) {
     auto face = [tol](double uL, double uR, double aL, double aR) {
         const double a_min = (aL < aR) ? aL : aR;
-        return ((uR - uL) / a_min) < tol ? 1 : 0;
+        return quotient_below(uR - uL, a_min, tol) ? 1 : 0;
     };
     const R a = p0[5 * FS + off];
     int S = 0;

@@ -472,7 +472,7 @@ __device__ __forceinline__ int face_shock(const BlockView& b, const double* fg, 
                       b.W[W_VZ * b.npad + cr] * nz;
     const double aL = b.W[W_A * b.npad + cl], aR = b.W[W_A * b.npad + cr];
     const double a_min = (aL < aR) ? aL : aR;
-    return ((uR - uL) / a_min) < tol ? 1 : 0;
+    return quotient_below(uR - uL, a_min, tol) ? 1 : 0;
 }
 
 __global__ void k_shock(BlockView b, const SimDev* sim, double tol) {

@@ -7,6 +7,7 @@
 // instantiated with float serve the FP32 reconstruction/flux form.
 #pragma once
 
+#include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -57,6 +58,23 @@ struct Prim {
     V3<R> vel;
     R massf[NSP];
 };
+
+// RN(d / a) < tol for a shock detector's compression test, the quotient
+// formed only where the outcome is not already certain: with a > 0 and
+// P = RN(tol a) in the normal range, d < P - |P| 2^-49 puts d / a below tol by
+// more than 2^-50 |tol| (so its rounded value is below tol as well), and
+// d > P + |P| 2^-49 puts it above tol; in the band between, and for values
+// outside the normal range, the division decides.  The outcome is the
+// division's in every case.
+__device__ __forceinline__ bool quotient_below(double d, double a, double tol) {
+    const double P = tol * a;
+    const double band = fabs(P) * 0x1p-49;
+    if (a > 0.0 && tol != 0.0 && fabs(P) >= 0x1p-1000 && fabs(P) <= DBL_MAX && fabs(d) <= DBL_MAX) {
+        if (d < P - band) return true;
+        if (d > P + band) return false;
+    }
+    return (d / a) < tol;
+}
 
 // clip_to_limits, src/eilmer/limiters.d:31-38
 template <typename R>
