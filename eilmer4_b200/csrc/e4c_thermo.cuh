@@ -278,6 +278,65 @@ struct TPState {
 // set_thermochem_constants)
 static __constant__ double c_bracket_kappa = 0.0;
 
+// Per-species values passed by value (no address taken, so they stay in
+// registers across the call).
+template <int NSP>
+struct SpVals {
+    double v[NSP];
+};
+struct EnergySlope {
+    double u, du;
+};
+
+// The mixture's energy e = sum Y_i (h_i - R_i T) and -sum Y_i (Cp_i - R_i)
+// at T, every species in one call (one call boundary per temperature instead
+// of one per species): the operations of TPGas::energy_dudT's loop over
+// cea_h_Cp, in the same order.
+template <int NSP>
+static __device__ E4C_CEA_FN EnergySlope mix_energy_slope(const e4c_thermochem& tc, SpVals<NSP> R,
+                                                          SpVals<NSP> massf, double T) {
+    const double lT = pm_log(T);
+    const TRecip t(T);
+    double e[NSP], v[NSP];
+#pragma unroll
+    for (int i = 0; i < NSP; ++i) {
+        double h, cp;
+        const int nseg = tc.nseg[i];
+        if (T < tc.T_break[i][0] || T > tc.T_break[i][nseg]) {
+            h = cea_h(tc, i, R.v[i], t, lT);
+            cp = cea_Cp(tc, i, R.v[i], T);
+        } else {
+            double a[9];
+            cea_coefficients(tc, i, T, a);
+            cp = R.v[i] * cea_Cp_on_R(a, t);
+            h = R.v[i] * T * cea_h_on_RT(a, t, lT);
+        }
+        e[i] = h - R.v[i] * T;
+        v[i] = cp - R.v[i];
+    }
+    double su = 0.0, sv = 0.0;
+#pragma unroll
+    for (int i = 0; i < NSP; ++i) su += massf.v[i] * e[i];
+#pragma unroll
+    for (int i = 0; i < NSP; ++i) sv += massf.v[i] * v[i];
+    return EnergySlope{su, -1.0 * sv};
+}
+
+// The mixture's energy at T alone (TPGas::energy's loop over cea_h).
+template <int NSP>
+static __device__ E4C_CEA_FN double mix_energy(const e4c_thermochem& tc, SpVals<NSP> R,
+                                               SpVals<NSP> massf, double T) {
+    const double lT = pm_log(T);
+    const TRecip t(T);
+    double e[NSP];
+#pragma unroll
+    for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R.v[i], t, lT) - R.v[i] * T;
+    double su = 0.0;
+#pragma unroll
+    for (int i = 0; i < NSP; ++i) su += massf.v[i] * e[i];
+    return su;
+}
+
 template <int NSP>
 struct TPGas {
     const e4c_thermochem& tc;
@@ -293,28 +352,26 @@ struct TPGas {
         return result;
     }
     __device__ double Rmix(const double* massf) const { return mass_average(massf, R); }
-    __device__ double energy(const double* massf, double T) const {
-        double e[NSP];
-        const double lT = pm_log(T);
-        const TRecip t(T);
+    __device__ SpVals<NSP> Rvals() const {
+        SpVals<NSP> r;
 #pragma unroll
-        for (int i = 0; i < NSP; ++i) e[i] = cea_h(tc, i, R[i], t, lT) - R[i] * T;
-        return mass_average(massf, e);
+        for (int i = 0; i < NSP; ++i) r.v[i] = R[i];
+        return r;
+    }
+    __device__ static SpVals<NSP> vals(const double* x) {
+        SpVals<NSP> r;
+#pragma unroll
+        for (int i = 0; i < NSP; ++i) r.v[i] = x[i];
+        return r;
+    }
+    __device__ double energy(const double* massf, double T) const {
+        return mix_energy<NSP>(tc, Rvals(), vals(massf), T);
     }
     // energy(massf, T) and dudT(massf, T) together
     __device__ void energy_dudT(const double* massf, double T, double& u, double& du) const {
-        double e[NSP], v[NSP];
-        const double lT = pm_log(T);
-        const TRecip t(T);
-#pragma unroll
-        for (int i = 0; i < NSP; ++i) {
-            double h, cp;
-            cea_h_Cp(tc, i, R[i], t, lT, h, cp);
-            e[i] = h - R[i] * T;
-            v[i] = cp - R[i];
-        }
-        u = mass_average(massf, e);
-        du = -1.0 * mass_average(massf, v);
+        const EnergySlope r = mix_energy_slope<NSP>(tc, Rvals(), vals(massf), T);
+        u = r.u;
+        du = r.du;
     }
     __device__ double dudT(const double* massf, double T) const {
         double v[NSP];
