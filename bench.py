@@ -783,6 +783,12 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{args.cpu_sample}^3 block of the same workload, {args.cpu_steps} steps "
                          f"({secs:.1f} s), CPU FP64 restatement, OpenMP"}
+        # and one thread (the restatement's scalar rate)
+        n1 = args.cpu_single_sample
+        rate1, _, secs1 = cpu_oracle_rate(n1, args.cpu_single_steps, args.flux, threads=1)
+        cpu["single_thread"] = {"value": rate1, "unit": UNIT, "cores": 1,
+                                "sample": f"{n1}^3 block, {args.cpu_single_steps} steps "
+                                          f"({secs1:.1f} s), one thread"}
 
     if rank == 0:
         line = {
@@ -823,6 +829,8 @@ def main():
     # CPU baseline samples: about 10 s of oracle work each on a 16-core host
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--cpu-single-sample", type=int, default=64)
+    ap.add_argument("--cpu-single-steps", type=int, default=10)
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="--impl reference: edge of the timed block (default: --n, the "
                          "bench's own block)")
