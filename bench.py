@@ -16,6 +16,10 @@ same line also carries, each timed the same way on its own simulation:
   "fp32_flux" (or "plain_fp64"): the other precision form of the 256^3 block,
       its speed-up over FP64 and its max relative density difference from the
       FP64 run after the same steps;
+  "ausmdv_fp64" (or "hllc_fp64"): the same block with the other of the two
+      fluxes in the FP64 form (AUSMDV is the reference's own, its parity pinned);
+  "adaptive_hanel_ausmdv_fp64": the same block with the reference's default
+      flux (shock detector and per-face Hanel/AUSMDV choice) in the FP64 form;
   "batched": 64 uneven blocks (edges log-uniform in [16, 96]) in one
       persistent launch per stage inside a CUDA graph, autotuned tiles;
   "curvilinear": a 128^3 curvilinear block (the unit box with every vertex
